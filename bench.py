@@ -1,0 +1,407 @@
+"""Benchmark of the engine's headline workload: path-steps per second of the fused local-vol Phoenix kernel.
+
+Workload (default `lv_phoenix`): Dupire local vol of the SSVI power-law surface (theta_t = 0.04 t, rho -0.6, eta 1,
+gamma 0.5) tabulated on 200 log-strikes x 40 expiries; a 3-year Phoenix autocall (quarterly, autocall 100 %, coupon
+2 % at 70 % with memory, daily knock-in at 60 % into a put at 100 %); 756 daily steps; 2^20 paths; FP32 path
+evolution with FP64 sums. `--workload heston_qe` runs the Heston QE ladder (2^16 paths x 252 steps, FP64).
+
+One step = one launch of the fused kernel over the whole batch (plus the one-block kernel that adds the block totals),
+inputs resident on the device; between steps a 512 MB buffer is written to flush L2. `value` is path-steps/s of the
+device-timed steps (CUDA events on the launching stream), max over ranks. `e2e` is the same metric through the public
+call with host inputs (`optlab_b200.engine.mc_price`: upload, kernel, read-back). Ranks (torchrun) each take their own
+range of pairs (first_pair = rank x pairs): weak scaling, with one FP64 all-reduce of the sums per step.
+
+`--impl reference` times the reference's CPU implementation of the same workload instead: its path engine
+(optlab::api::paths, compiled from the reference's sources into oracle/_ref) writing the 12 quarterly columns and the
+daily knock-in window, then the Phoenix payoff evaluated on those columns, on all host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "option-pricing-lab_b200"))
+
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}
+
+# Executed warp instructions per path-step of the dominant kernel, measured by ncu (smsp__inst_executed.sum of one
+# launch divided by its path-steps) and recorded under profiles/. The issue roofline below multiplies it by the live
+# path-step rate. A launch's instruction count does not depend on timing, so a profiled launch gives it exactly.
+INST_PER_PATH_STEP = {"lv_phoenix": None, "heston_qe": None}
+
+
+def load_peaks():
+    if PEAKS_FILE.exists():
+        d = json.loads(PEAKS_FILE.read_text())
+        return d, "measured"
+    return FALLBACK_PEAKS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, device: int):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def build_workload(name: str, n_paths: int | None):
+    from optlab_b200 import workloads
+
+    if name == "lv_phoenix":
+        return workloads.lv_phoenix(n_paths=n_paths or 2**20, seed=7), "fp32", {
+            "workload": "lv_phoenix",
+            "model": "Dupire local vol, SSVI power law (rho -0.6, eta 1, gamma 0.5, theta 0.04 t), 200 x 40 table",
+            "product": "3y Phoenix, quarterly autocall 100%, coupon 2% at 70% with memory, daily KI 60%",
+            "n_paths": n_paths or 2**20,
+            "n_steps": 756,
+            "precision": "fp32 paths, fp64 sums",
+        }
+    if name == "heston_qe":
+        return workloads.heston_qe_ladder(n_paths=n_paths or 2**16, seed=1), "fp64", {
+            "workload": "heston_qe",
+            "model": "Heston QE-M (S0 100, v0 .04, kappa 1.5, theta .04, xi .5, rho -.7, r .02, q .01)",
+            "product": "11 calls K 80..120 + daily up-and-out call K 100 B 130",
+            "n_paths": n_paths or 2**16,
+            "n_steps": 252,
+            "precision": "fp64",
+        }
+    raise SystemExit(f"unknown workload {name}")
+
+
+def input_bytes(held) -> int:
+    return int(sum(a.nbytes for a in held.keep if isinstance(a, np.ndarray)))
+
+
+# ---------------------------------------------------------------------------------------------------- CPU baseline
+
+
+def cpu_reference_sample(name: str, n_paths: int, threads: int):
+    """Time the reference's CPU implementation of the workload on n_paths paths: (seconds, kind, cores, detail)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import Oracle, Reference, reference_available
+
+    from optlab_b200 import workloads
+    from optlab_b200.requests import paths_request
+
+    held, _, _ = build_workload(name, n_paths)
+    s = held.struct
+    kind = "reference" if reference_available() else "port"
+    if name == "heston_qe":
+        if kind == "reference":
+            R = Reference()
+            lt = np.ones(12, np.int32)
+            ks = np.append(np.arange(80.0, 121.0, 4.0), 100.0)
+            up = np.zeros(12, np.int32)
+            up[-1] = 1
+            lv = np.zeros(12)
+            lv[-1] = 130.0
+            t = time.perf_counter()
+            R.qe_ladder(100.0, 0.02, 0.01, 1.0, 252, workloads.HESTON_CFG0, n_paths // 2, 1, lt, ks, up, lv,
+                        threads=threads)
+            return time.perf_counter() - t, kind, threads, "reference QE-M step on the reference Philox stream"
+        t = time.perf_counter()
+        Oracle().mc_price(held, threads)
+        return time.perf_counter() - t, kind, threads, "oracle port (C, double)"
+    # local-vol Phoenix: the reference's path engine writes the quarterly columns and the daily window, then the
+    # payoff is evaluated on the columns (the reference's structured engine does this in NumPy).
+    ph = workloads.Phoenix()
+    obs_step, _ = ph.schedule(252)
+    n_steps = s.n_steps
+    all_obs = np.arange(0, n_steps + 1, dtype=np.int32)  # every step end (and t = 0) for the daily window
+    col_of = np.full(len(all_obs), -1, np.int32)
+    col_of[obs_step] = np.arange(len(obs_step), dtype=np.int32)
+    m = workloads.FlatMarket(100.0, 0.02, 0.01)
+    dt = np.ctypeslib.as_array(s.dt, shape=(n_steps,)).copy()
+    t_end = np.concatenate([[0.0], np.cumsum(dt)])
+    g = workloads.lv_grid()
+    t0 = t_end[:-1]
+    rq = paths_request(
+        dt=dt, t0=t0, obs_step=all_obs, root=[[1.0]], kind=[1], cvar=[0.0], heston=[0.0, 1, 1, 0, 0], same=1,
+        fwd=m.F(t_end)[None, :], n_pairs=n_paths // 2, seed=7, step_row=g.row_of(t0), lo=g.lo, inv_dx=g.inv_dx,
+        table=g.rows, n_x=g.n_x, col_of=col_of, n_keep=len(obs_step), win_lo=[0], win_hi=[n_steps],
+    )
+    t = time.perf_counter()
+    if kind == "reference":
+        Reference().paths(rq, threads)
+    else:
+        Oracle().paths(rq, threads)
+    out = next(a for a in rq.keep if isinstance(a, np.ndarray) and a.ndim == 3)[0]
+    phoenix_payoff(out[: len(obs_step)].T / 100.0, out[len(obs_step)] / 100.0, ph, m)
+    return time.perf_counter() - t, kind, threads, "reference path engine (columns + daily window) + payoff on columns"
+
+
+def phoenix_payoff(perf, low, ph, market):
+    """Pair-averaged Phoenix value from observation performances (paths x obs) and the window lows (paths)."""
+    n, n_obs = perf.shape
+    _, obs_t = ph.schedule(252)
+    D = market.D(obs_t)
+    pv, missed, alive = np.zeros(n), np.zeros(n), np.ones(n, bool)
+    for j in range(n_obs):
+        p = perf[:, j]
+        hit = alive & (p >= ph.coupon_barrier)
+        pv += np.where(hit, D[j] * ph.coupon * (1 + missed), 0.0)
+        missed = np.where(hit, 0.0, np.where(alive, missed + 1, missed))
+        if j < n_obs - 1:
+            call = alive & (p >= ph.trigger)
+            pv += np.where(call, D[j], 0.0)
+            alive &= ~call
+        else:
+            ki = low < ph.ki_barrier
+            pv += np.where(alive, D[j] * np.where(ki, 1 - np.maximum(ph.put_strike - p, 0), 1.0), 0.0)
+    h = n // 2
+    y = 0.5 * (pv[:h] + pv[h:])
+    return float(y.mean()), float(y.std(ddof=1) / np.sqrt(h))
+
+
+# ---------------------------------------------------------------------------------------------------- main
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe"])
+    ap.add_argument("--paths", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from optlab_b200 import engine
+    from optlab_b200.workloads import path_steps
+
+    held, prec, config = build_workload(args.workload, args.paths)
+    n_pairs = held.struct.n_pairs
+    first = rank * n_pairs
+    units = path_steps(held)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    plan = engine.McPlan(held, prec)
+    sums = torch.zeros(2, dtype=torch.float64, device="cuda")
+
+    def step():
+        plan.run(n_pairs, first, held.struct.seed, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    warm = plan.result()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        t_wall = time.perf_counter()
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+            if dist:  # the exchange step: per-rank sums into the job's price (a few doubles)
+                dist.all_reduce(sums)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    if dist:
+        dist.barrier()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    res = plan.result()
+    per_step = ms_max / args.steps
+    value = units * world * args.steps / (ms_max / 1e3)
+
+    # end to end through the public call: host arrays in, prices out
+    e2e_ms = []
+    for _ in range(max(3, min(args.steps, 10))):
+        t = time.perf_counter()
+        r_e2e = engine.mc_price(held, prec)
+        e2e_ms.append((time.perf_counter() - t) * 1e3)
+    e2e_value = units / (statistics.median(e2e_ms) / 1e3)
+
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peaks, peak_kind = load_peaks()
+    props = torch.cuda.get_device_properties(local)
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    issue_peak = props.multi_processor_count * 4 * sm_max * 1e6 / 1e9  # G warp-instructions/s
+    ipu = INST_PER_PATH_STEP.get(args.workload)
+    roofline = {
+        "bound": "issue",
+        "achieved": (ipu * value / world / 1e9) if ipu else None,
+        "peak": issue_peak,
+        "unit": "Gwarp-inst/s",
+        "frac": (ipu * value / world / 1e9 / issue_peak) if ipu else None,
+        "traffic": None,
+        "note": "FP32/SFU issue-bound kernel (no HBM or tensor-core bound applies); peak = SMs x 4 schedulers x "
+        f"max SM clock ({sm_max:.0f} MHz, {peak_kind}); achieved = ncu instructions per path-step x live rate",
+    }
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        n_s = 2**18
+        threads = os.cpu_count() or 1
+        secs, kind, cores, detail = cpu_reference_sample(args.workload, n_s, threads)
+        n_units = n_s * config["n_steps"]
+        cpu = {"value": n_units / secs, "unit": "path-steps/s", "cores": cores, "kind": kind,
+               "sample": f"{n_s} paths x {config['n_steps']} steps of the same workload ({detail})"}
+    clk = clocks.summary()
+    line = {
+        "metric": "path-steps/s",
+        "value": value,
+        "unit": "path-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if prec == "fp32" else "f64",
+        "data": "synthetic (seeded SSVI surface and Heston parameters; no market data)",
+        "config": dict(config, l2="flushed between steps (512 MB write)", parallelism=f"pairs sharded over {world}"),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {
+            "value": e2e_value,
+            "unit": "path-steps/s",
+            "h2d_bytes_per_step": input_bytes(held),
+            "d2h_bytes_per_step": 2 * 32 * 8,
+            "ms_per_call": statistics.median(e2e_ms),
+        },
+        "gpu_launches": 2 * args.steps,
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "wall_s": t_wall,
+        "result": {"price": list(res.price[: res.n_out]), "se": list(res.se[: res.n_out]),
+                   "e2e_price": r_e2e.price[0], "warmup_price": warm.price[0]},
+    }
+    print(json.dumps(line))
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n_s = 2**18
+    for _ in range(args.warmup):
+        cpu_reference_sample(args.workload, n_s, threads)
+    secs = []
+    for _ in range(args.steps):
+        s, kind, cores, detail = cpu_reference_sample(args.workload, n_s, threads)
+        secs.append(s)
+    _, _, config = build_workload(args.workload, None)
+    n_units = n_s * config["n_steps"]
+    tot = sum(secs)
+    value = n_units * args.steps / tot
+    line = {
+        "impl": "reference",
+        "metric": "path-steps/s",
+        "value": value,
+        "unit": "path-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": tot / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": config,
+        "cpu_baseline": {"value": value, "unit": "path-steps/s", "cores": cores, "kind": kind,
+                         "sample": f"{n_s} paths x {config['n_steps']} steps per step ({detail})"},
+        "e2e": {"value": value, "unit": "path-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,240 @@
+/* optlab_b200: a Monte Carlo path engine for NVIDIA B200 (sm_100a), reached through a C ABI.
+ *
+ * Every entry point returns an int status (OB_OK = 0) and never exits, aborts or traps: the engine runs inside the
+ * caller's process. On an error, ob_last_error() gives a message for the calling thread. The status splits the
+ * reference's exceptions: OB_EINVAL where it throws std::invalid_argument (a bad request), OB_ENODEV and OB_ECUDA
+ * where it throws std::runtime_error (no device, a CUDA failure), OB_ETIMEOUT where a bounded device wait gave up.
+ *
+ * Reference interfaces replaced (paths relative to the reference project, RC = packages/native/cuda):
+ *   optlab::api::paths     RC/include/optlab_cuda/requests.hpp:105-106, request layout :36-63   -> ob_paths
+ *   optlab::api::leverage  RC/include/optlab_cuda/requests.hpp:107-108, request layout :76-93   -> ob_leverage
+ *   optlab::api::price     RC/include/optlab_cuda/requests.hpp:103-104, layouts :12-29         -> ob_price
+ *   optlab::api::{gpu_count,has_cuda,cpu_threads,device_info}  requests.hpp:97-101            -> ob_gpu_count, ...
+ * The request structs below keep the reference's field order and types, so a binding written for the reference's
+ * structs binds these unchanged. The fused, adjoint and batched entry points (ob_mc_*, ob_adjoint_*, ob_batch_*) have
+ * no counterpart in the reference ABI: they replace the host NumPy evaluation and bump-and-revalue loops that sit on
+ * top of optlab::api::paths (packages/structured/src/optlab/structured/engine.py:143-153,260-330 and
+ * packages/risk/src/optlab/risk/engine.py:382-425).
+ *
+ * Precision argument: OB_FP32 evolves the paths in float (sums in double), OB_FP64 in double throughout.
+ * Threading: one caller thread at a time per process (an internal mutex serialises calls), as the reference's
+ * "not thread-safe on the GPU" (requests.hpp:103).
+ */
+#ifndef OPTLAB_B200_H
+#define OPTLAB_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OB_OK 0
+#define OB_EINVAL 1
+#define OB_ENODEV 2
+#define OB_ECUDA 3
+#define OB_ETIMEOUT 4
+#define OB_ENOMEM 5
+
+#define OB_FP32 0
+#define OB_FP64 1
+
+#define OB_MAX_NAMES 8
+#define OB_MAX_WINDOWS 2
+#define OB_MAX_OUT 32
+
+/* ---------------------------------------------------------------------------------------------- requests (mirrors) */
+
+/* Same layout as optlab_request (RC/include/optlab_cuda/requests.hpp:12-23). model: 0 Black-Scholes, 1 Heston (QE);
+   product: 0 European, 1 Asian, 2 down-and-out barrier; legs: 0 none, 1 call, 2 put, 3 forward. */
+typedef struct {
+    int model, product;
+    int legs[3];
+    double strikes[3];
+    double H;
+    int n_steps;
+    double S0, r, q, T;
+    double sigma;
+    double v0, kappa, theta, xi, rho;
+    long long n_paths;
+    unsigned long long seed;
+} ob_request;
+
+/* Same layout as optlab_result (requests.hpp:25-29). */
+typedef struct {
+    double price[4], se[4];
+    long long n_paths;
+    double kernel_ms, total_ms;
+} ob_result;
+
+/* Same layout as optlab_paths_request (requests.hpp:36-63): host pointers, double, row major. out holds
+   n_names x n_cols columns of 2 n_pairs rows, column (a, c) at out + (a * n_cols + c) * 2 n_pairs. */
+typedef struct {
+    int n_names, n_steps, n_obs, n_x, n_rows;
+    long long n_pairs, first_pair;
+    unsigned long long seed;
+    const double* dt;
+    const double* t0;
+    const int* obs_step;
+    const double* root;
+    const int* kind;
+    const double* cvar;
+    const double* heston;
+    int same;
+    const int* step_row;
+    const double* row_lo;
+    const double* row_inv_dx;
+    const double* table;
+    const double* fwd;
+    int mixer;
+    double mix[8];
+    const double* low_root;
+    int n_cols, n_keep;
+    const int* col_of;
+    int n_windows;
+    const int* win_lo;
+    const int* win_hi;
+    double* out;
+    double kernel_ms, total_ms;
+} ob_paths_request;
+
+/* Same layout as optlab_device (requests.hpp:66-71). */
+typedef struct {
+    char name[256];
+    int major, minor, sm_count, clock_mhz;
+    long long total_mem, free_mem;
+    int integrated, kernel_timeout;
+} ob_device;
+
+/* Same layout as optlab_leverage_request (requests.hpp:76-93). */
+typedef struct {
+    int n_steps;
+    const double* dt;
+    const double* t0;
+    long long n_pairs;
+    unsigned long long seed;
+    double v0, kappa, theta, xi, rho;
+    int n_x, n_bins, n_fine;
+    double atm_vol, bandwidth_scale, l_min, l_max, q_lo, q_hi;
+    int local_linear, positive_part;
+    int n_lv;
+    const double* lv_lo;
+    const double* lv_inv_dx;
+    const double* lv_rows;
+    double* x_grids;
+    double* values;
+    double total_ms;
+} ob_leverage_request;
+
+/* ---------------------------------------------------------------------------------------------- fused pricing */
+
+#define OB_MODEL_PATHS 0     /* the log-Euler step of paths.hpp, per name kind (constant, table, Heston, SLV) */
+#define OB_MODEL_HESTON_QE 1 /* Andersen QE-M for one Heston name (schemes.hpp:154-187), uniform steps */
+
+#define OB_PRODUCT_LADDER 0   /* payoffs at maturity, each with an optional barrier monitored at every step end */
+#define OB_PRODUCT_AUTOCALL 1 /* Phoenix / worst-of autocall with coupon memory and a knock-in put */
+
+#define OB_BARRIER_NONE 0
+#define OB_BARRIER_UP_OUT 1
+#define OB_BARRIER_DOWN_OUT 2
+#define OB_BARRIER_UP_IN 3
+#define OB_BARRIER_DOWN_IN 4
+
+/* A simulation plus a product, priced in one launch: path, payoff and the FP64 sums of the pair averages.
+   The model part reads as ob_paths_request; the spot of name a at grid point i is spot[a] * exp(log_fwd[a, i] + x)
+   under OB_MODEL_PATHS and spot[0] * exp(y) under OB_MODEL_HESTON_QE (y = ln S / S0, drift (r - q) dt).
+   Ladder: output k = leg k's discounted payoff at maturity; then E[S_T] of name 0 (undiscounted).
+   Autocall: output 0 = price (notional 1); 1 = probability of an early redemption; 2 = probability of a knock-in;
+   3 = the expected number of coupons paid. */
+typedef struct {
+    int model;
+    int n_names, n_steps;
+    long long n_pairs, first_pair;
+    unsigned long long seed;
+    const double* dt;          /* n_steps */
+    const double* t0;          /* n_steps */
+    const double* root;        /* n_names x n_names */
+    const int* kind;           /* n_names: 0 constant, 1 table, 2 Heston (Euler), 3 SLV */
+    const double* cvar;        /* n_names */
+    const double* heston;      /* n_names x 5: v0, kappa, theta, xi, rho */
+    int same;                  /* variance residuals correlated like the spots */
+    int n_x, n_rows;
+    const int* step_row;       /* n_names x n_steps */
+    const double* row_lo;      /* n_rows */
+    const double* row_inv_dx;  /* n_rows */
+    const double* table;       /* n_rows x n_x */
+    const double* spot;        /* n_names */
+    const double* log_fwd;     /* n_names x (n_steps + 1): ln(F(t_i) / S0), t_0 = 0 */
+    double r, q;               /* OB_MODEL_HESTON_QE: flat rates */
+    int product;
+    /* ladder */
+    int n_legs;                /* <= OB_MAX_OUT - 1 */
+    const int* leg_type;       /* 1 call, 2 put, 3 forward */
+    const double* leg_strike;
+    const int* leg_barrier;    /* OB_BARRIER_* */
+    const double* leg_level;   /* barrier level (spot units) */
+    double discount;           /* D(T) */
+    /* autocall */
+    int n_obs;
+    const int* obs_step;       /* n_obs, increasing, in 1..n_steps: observation j after step obs_step[j] */
+    const double* obs_discount;/* n_obs: discount factor of the payment of observation j */
+    const double* trigger;     /* n_obs: autocall level of perf (<= 0: no call on that date; never on the last) */
+    double coupon_barrier, coupon, ki_barrier, put_strike;
+    int memory;                /* coupons missed are paid at the next coupon */
+    int ki_daily;              /* 1: knock-in on the lowest close of every step end; 0: at maturity only */
+} ob_mc_request;
+
+typedef struct {
+    int n_out;
+    double price[OB_MAX_OUT], se[OB_MAX_OUT];
+    long long n_paths;
+    double kernel_ms, total_ms;
+} ob_mc_result;
+
+typedef struct ob_mc_plan ob_mc_plan;
+
+/* ---------------------------------------------------------------------------------------------- entry points */
+
+const char* ob_last_error(void);
+int ob_version(void);
+/* requests.hpp:97: CUDA devices, 0 without device or driver (never an error). */
+int ob_gpu_count(void);
+/* requests.hpp:98: 1, this library always has its CUDA backend. */
+int ob_has_cuda(void);
+/* requests.hpp:99: hardware threads of the host. */
+int ob_cpu_threads(void);
+/* requests.hpp:101: properties of a device; OB_ENODEV without it. */
+int ob_device_info(int device, ob_device* out);
+
+/* The engine's random numbers for RNG parity: for pairs first_pair .. first_pair + n_pairs - 1 of key seed, blocks
+   first_block .. first_block + n_blocks - 1 of the stream tagged `tag` (0 or 0x80000000, paths.hpp:207-233),
+   the Philox4x32-10 outputs (4 u32 per block) and their Box-Muller normals in double and float. Host outputs of
+   n_pairs x n_blocks x 4 values, pair-major; any output may be NULL. */
+int ob_philox_normals(unsigned long long seed, long long first_pair, long long n_pairs, unsigned tag,
+                      unsigned long long first_block, int n_blocks, unsigned* u32, double* z64, float* z32);
+
+/* Drop-in for optlab::api::paths(rq, 1, 0) (requests.hpp:105-106): fills rq->out and the timings. */
+int ob_paths(ob_paths_request* rq, int precision);
+
+/* Drop-in for optlab::api::leverage(rq, 1, 0) (requests.hpp:107-108): fills x_grids, values and total_ms.
+   The whole calibration runs on the device; the host reads the two output tables once. */
+int ob_leverage(ob_leverage_request* rq, int precision);
+
+/* Drop-in for optlab::api::price(rq, 1, 0) (requests.hpp:103-104): the fixed products of the reference's study,
+   with the engine's Philox normals (pair p reads stream 0 of pair p) instead of cuRAND. */
+int ob_price(const ob_request* rq, ob_result* res, int precision);
+
+/* Fused pricing, end to end: host request in, result out (copies and allocations included). */
+int ob_mc_price(const ob_mc_request* rq, int precision, ob_mc_result* res);
+
+/* The same in three steps, for callers that keep the inputs resident on the device: create validates the request
+   and uploads it; run launches n_pairs pairs from first_pair on `stream` (a cudaStream_t, NULL: the legacy stream)
+   without waiting; result waits for the stream and reads the sums of every run since the last result. */
+int ob_mc_plan_create(const ob_mc_request* rq, int precision, ob_mc_plan** plan);
+int ob_mc_run(ob_mc_plan* plan, long long n_pairs, long long first_pair, unsigned long long seed, void* stream);
+int ob_mc_result_get(ob_mc_plan* plan, ob_mc_result* res);
+int ob_mc_plan_destroy(ob_mc_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPTLAB_B200_H */

@@ -1,0 +1,207 @@
+// Shared device code of the engine: status handling, the counter-based normals, and small math helpers.
+//
+// Normals follow the reference's definition (RC = packages/native/cuda of Luca-CS/option-pricing-lab):
+//   Philox4x32-10 on counter {pair_lo, pair_hi, block_lo, block_hi | tag}, key {seed_lo, seed_hi}
+//     (RC/include/optlab_cuda/philox.hpp:22-44, RC/include/optlab_cuda/paths.hpp:207-233);
+//   u = (i + 1/2) 2^-32 (philox.hpp:45-49); Box-Muller r = sqrt(-2 ln u), (cos, sin)(2 pi v) by sincospi
+//     (philox.hpp:51-66).
+// The integer stream is bit-exact with the reference; the normals differ from its CPU's only by libm rounding.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/optlab_b200.h"
+
+namespace ob {
+
+// ------------------------------------------------------------------------------------------------ status
+
+void set_error(const char* fmt, ...);
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Error(OB_ECUDA, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+inline void invalid(const char* msg) { throw Error(OB_EINVAL, msg); }
+
+// Runs f, turning exceptions into a status and the thread's last error. Serialised by one process-wide mutex.
+std::mutex& api_mutex();
+template <typename F>
+int guarded(F&& f) {
+    std::lock_guard<std::mutex> lock(api_mutex());
+    try {
+        f();
+        return OB_OK;
+    } catch (const Error& e) {
+        set_error("%s", e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_error("out of host memory");
+        return OB_ENOMEM;
+    } catch (const std::exception& e) {
+        set_error("%s", e.what());
+        return OB_ECUDA;
+    }
+}
+
+// Device 0 must exist; returns its SM count.
+int require_device();
+
+// ------------------------------------------------------------------------------------------------ device memory
+
+// Owns device allocations for one call or one plan.
+struct DeviceArena {
+    void* ptrs[64] = {};
+    int n = 0;
+    ~DeviceArena() { release(); }
+    void release() {
+        for (int i = 0; i < n; ++i) cudaFree(ptrs[i]);
+        n = 0;
+    }
+    void* raw(size_t bytes) {
+        if (n == 64) throw Error(OB_ENOMEM, "too many device buffers");
+        void* d = nullptr;
+        const cudaError_t e = cudaMalloc(&d, bytes ? bytes : 16);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw Error(OB_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        ptrs[n++] = d;
+        return d;
+    }
+    template <typename T>
+    T* alloc(size_t count) {
+        return static_cast<T*>(raw(count * sizeof(T)));
+    }
+    // Host array of count elements (converted to T) to a new device buffer; null or empty gives null.
+    template <typename T, typename S>
+    T* put(const S* host, size_t count, cudaStream_t st = nullptr) {
+        if (!host || !count) return nullptr;
+        T* d = alloc<T>(count);
+        T* tmp = static_cast<T*>(std::malloc(count * sizeof(T)));
+        if (!tmp) throw std::bad_alloc();
+        for (size_t i = 0; i < count; ++i) tmp[i] = static_cast<T>(host[i]);
+        const cudaError_t e = cudaMemcpyAsync(d, tmp, count * sizeof(T), cudaMemcpyHostToDevice, st);
+        const cudaError_t e2 = cudaStreamSynchronize(st);
+        std::free(tmp);
+        check_cuda(e, "cudaMemcpyAsync (inputs)");
+        check_cuda(e2, "cudaStreamSynchronize (inputs)");
+        return d;
+    }
+};
+
+// ------------------------------------------------------------------------------------------------ normals
+
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t& x, uint32_t& y, uint32_t& z, uint32_t& w,
+                                                       uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+        const uint32_t hi0 = __umulhi(0xD2511F53u, x), lo0 = 0xD2511F53u * x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, z), lo1 = 0xCD9E8D57u * z;
+#else
+        const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * x, p1 = static_cast<uint64_t>(0xCD9E8D57u) * z;
+        const uint32_t hi0 = static_cast<uint32_t>(p0 >> 32), lo0 = static_cast<uint32_t>(p0);
+        const uint32_t hi1 = static_cast<uint32_t>(p1 >> 32), lo1 = static_cast<uint32_t>(p1);
+#endif
+        const uint32_t nx = hi1 ^ y ^ k0, nz = hi0 ^ w ^ k1;
+        x = nx, y = lo1, z = nz, w = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ R to_unit(uint32_t i);
+template <>
+__device__ __forceinline__ float to_unit<float>(uint32_t i) {
+    return static_cast<float>(i) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
+}
+template <>
+__device__ __forceinline__ double to_unit<double>(uint32_t i) {
+    return static_cast<double>(i) * 2.3283064365386963e-10 + 1.1641532182693481e-10;
+}
+
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, float& z1) {
+    const float r = sqrtf(-2.0f * logf(to_unit<float>(a)));
+    float s, c;
+    sincospif(2.0f * to_unit<float>(b), &s, &c);
+    z0 = r * c, z1 = r * s;
+}
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double& z0, double& z1) {
+    const double r = sqrt(-2.0 * log(to_unit<double>(a)));
+    double s, c;
+    sincospi(2.0 * to_unit<double>(b), &s, &c);
+    z0 = r * c, z1 = r * s;
+}
+
+// The four normals of block `block` of one pair's stream.
+template <typename R>
+__device__ __forceinline__ void normals4(uint64_t pair, uint64_t block, uint32_t tag, uint32_t k0, uint32_t k1,
+                                         R& z0, R& z1, R& z2, R& z3) {
+    uint32_t x = static_cast<uint32_t>(pair), y = static_cast<uint32_t>(pair >> 32);
+    uint32_t z = static_cast<uint32_t>(block), w = static_cast<uint32_t>(block >> 32) | tag;
+    philox4x32_10(x, y, z, w, k0, k1);
+    box_muller(x, y, z0, z1);
+    box_muller(z, w, z2, z3);
+}
+
+// Normals of one pair along one stream, read in order (block b gives normals 4b .. 4b+3). The buffer stays in
+// registers: the slot is picked by selects, never by a dynamic index.
+template <typename R>
+struct NormalStream {
+    uint64_t pair;
+    uint64_t block;
+    uint32_t k0, k1, tag;
+    int used;
+    R b0, b1, b2, b3;
+
+    __device__ __forceinline__ void init(uint64_t p, uint32_t key0, uint32_t key1, uint32_t t) {
+        pair = p, block = 0, k0 = key0, k1 = key1, tag = t, used = 4;
+        b0 = b1 = b2 = b3 = R(0);
+    }
+    __device__ __forceinline__ R next() {
+        if (used == 4) {
+            normals4<R>(pair, block, tag, k0, k1, b0, b1, b2, b3);
+            ++block, used = 0;
+        }
+        const R z = used == 0 ? b0 : used == 1 ? b1 : used == 2 ? b2 : b3;
+        ++used;
+        return z;
+    }
+};
+
+// ------------------------------------------------------------------------------------------------ math helpers
+
+__device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float m_exp(float x) { return expf(x); }
+__device__ __forceinline__ double m_exp(double x) { return exp(x); }
+__device__ __forceinline__ float m_log(float x) { return logf(x); }
+__device__ __forceinline__ double m_log(double x) { return log(x); }
+__device__ __forceinline__ float m_ncdf(float x) { return normcdff(x); }
+__device__ __forceinline__ double m_ncdf(double x) { return normcdf(x); }
+template <typename R>
+__device__ __forceinline__ R m_max(R a, R b) { return a > b ? a : b; }
+template <typename R>
+__device__ __forceinline__ R m_min(R a, R b) { return a < b ? a : b; }
+
+// Warp sum of a double.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    return v;
+}
+
+}  // namespace ob

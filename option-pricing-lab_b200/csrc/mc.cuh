@@ -1,0 +1,70 @@
+// Fused pricing plan: a checked ob_mc_request packed for the device, launched any number of times.
+#pragma once
+
+#include "model.cuh"
+
+namespace ob {
+
+// Byte offsets of each array inside the packed blob (16-byte aligned).
+struct McOffsets {
+    int dt, root, kind, cvar, hes, step_row, lo, inv_dx, lf, obs_of_step, ln_trig, obs_disc, leg_type, leg_strike,
+        leg_barrier, ln_level, table;
+};
+
+template <typename R>
+struct McArgs {
+    McOffsets off;
+    const unsigned char* blob;  // device copy of the blob, staged into shared memory by each block
+    int smem_blob;              // bytes of the blob copied to shared memory (table included when it fits)
+    int table_in_smem;
+    const R* table_global;      // the table, when it stays in global memory
+    int n_names, n_steps, n_x, same, has_var, has_slv;
+    int n_out, n_legs, n_obs;
+    QeConsts<R> qe;
+    R spot0;
+    double discount;
+    // autocall
+    int has_coupon, memory, ki_daily;
+    R ln_cb, ln_ki;
+    double coupon, put_strike;
+};
+
+void check_mc_request(const ob_mc_request& rq);
+
+struct McPlan {
+    DeviceArena arena;
+    int precision = OB_FP32;
+    int n_out = 0, sms = 0, blocks_per_sm = 1, max_blocks = 0;
+    int block = 256, grid_waves = 1;
+    size_t smem_bytes = 0;
+    const void* kernel = nullptr;
+    McArgs<float> args_f{};
+    McArgs<double> args_d{};
+    double* d_partial = nullptr;
+    double* d_sums = nullptr;
+    long long pairs_run = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool timing = false;
+    cudaStream_t last_stream = nullptr;
+
+    template <typename R>
+    McArgs<R>& args();
+    template <typename R>
+    void build(const ob_mc_request& rq);
+    void create(const ob_mc_request& rq, int precision);
+    int grid_for(long long n_pairs) const;
+    void run(long long n_pairs, long long first_pair, unsigned long long seed, cudaStream_t st);
+    void result(ob_mc_result& res);
+    ~McPlan();
+};
+
+template <>
+inline McArgs<float>& McPlan::args<float>() {
+    return args_f;
+}
+template <>
+inline McArgs<double>& McPlan::args<double>() {
+    return args_d;
+}
+
+}  // namespace ob
