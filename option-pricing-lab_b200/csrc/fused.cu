@@ -1,0 +1,406 @@
+// The specialised fused kernel (fused.cuh): path, payoff and FP64 sums for baskets whose names share one kind.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "mc.cuh"
+
+namespace ob {
+
+namespace {
+
+constexpr int gcd4(int c) { return c % 4 == 0 ? 4 : c % 2 == 0 ? 2 : 1; }
+
+// Product bookkeeping of one leg, kept small: the ladder's extremes or the autocall's state.
+template <typename R>
+struct Leg {
+    R hi, lo;       // ladder: extremes of ln perf; autocall: lo is the lowest ln perf
+    double pv;      // autocall: discounted cash flows
+    float coupons;  // autocall: coupons paid
+    int flags;      // autocall: missed coupons (bits 0-15), alive (16), called (17), knocked (18)
+};
+
+constexpr int kAlive = 1 << 16, kCalled = 1 << 17, kKnocked = 1 << 18;
+
+template <typename R, int PRODUCT>
+__device__ __forceinline__ void leg_init(Leg<R>& l) {
+    l.hi = R(-1e30), l.lo = PRODUCT == OB_PRODUCT_LADDER ? R(1e30) : R(0);
+    l.pv = 0.0, l.coupons = 0.0f, l.flags = kAlive;
+}
+
+// Observation j of one leg (autocall): coupon with memory, then the call, or the redemption on the last date
+// (packages/structured/src/optlab/structured/compiler.py:114-127,141-161,271-280).
+template <typename R>
+__device__ __forceinline__ void leg_observe(const FusedArgs<R>& a, const R* ln_trig, const double* disc, Leg<R>& l,
+                                            R lp, int j) {
+    if (!(l.flags & kAlive)) return;
+    const double D = disc[j];
+    if (a.has_coupon) {
+        if (lp >= a.ln_cb) {
+            const int k = a.memory ? 1 + (l.flags & 0xFFFF) : 1;
+            l.pv += D * a.coupon * k, l.coupons += static_cast<float>(k), l.flags &= ~0xFFFF;
+        } else {
+            l.flags += 1;
+        }
+    }
+    if (j < a.n_obs - 1) {
+        if (lp >= ln_trig[j]) l.pv += D, l.flags = (l.flags & ~kAlive) | kCalled;
+    } else {
+        const bool ki = a.ki_daily ? l.lo < a.ln_ki : lp < a.ln_ki;
+        const double perf = static_cast<double>(m_exp(lp));
+        const double put = a.put_strike - perf > 0.0 ? a.put_strike - perf : 0.0;
+        l.pv += D * (ki ? 1.0 - put : 1.0);
+        l.flags = (l.flags & ~kAlive) | (ki ? kKnocked : 0);
+    }
+}
+
+template <typename R, int PRODUCT>
+__device__ __forceinline__ double leg_output(const FusedArgs<R>& a, const int* leg_type, const R* leg_strike,
+                                             const int* leg_barrier, const R* ln_level, const Leg<R>& l, R lp_T,
+                                             int k) {
+    if (PRODUCT == OB_PRODUCT_AUTOCALL) {
+        return k == 0 ? l.pv : k == 1 ? ((l.flags & kCalled) ? 1.0 : 0.0)
+                                      : k == 2 ? ((l.flags & kKnocked) ? 1.0 : 0.0) : static_cast<double>(l.coupons);
+    }
+    const R U = a.spot0 * m_exp(lp_T);
+    if (k == a.n_legs) return static_cast<double>(U);
+    const int type = leg_type[k];
+    const R K = leg_strike[k];
+    R pay = type == 1 ? m_max(U - K, R(0)) : type == 2 ? m_max(K - U, R(0)) : type == 3 ? U - K : R(0);
+    const int bt = leg_barrier[k];
+    const R H = ln_level[k];
+    const bool up = l.hi >= H, down = l.lo <= H;
+    if ((bt == OB_BARRIER_UP_OUT && up) || (bt == OB_BARRIER_DOWN_OUT && down) || (bt == OB_BARRIER_UP_IN && !up) ||
+        (bt == OB_BARRIER_DOWN_IN && !down))
+        pay = R(0);
+    return a.discount * static_cast<double>(pay);
+}
+
+template <typename R>
+constexpr int min_blocks() {
+    return sizeof(R) == 4 ? 2 : 1;
+}
+
+// KIND: 1 local vol (table), 2 Heston (Euler), 3 SLV (table x Heston, residuals on the aux stream), 4 Heston QE-M.
+template <typename R, int N, int KIND, int PRODUCT>
+__global__ void __launch_bounds__(512, min_blocks<R>())
+    fused_kernel(FusedArgs<R> a, long long n_pairs, long long first_pair, uint32_t k0, uint32_t k1,
+                 double* __restrict__ partial) {
+    constexpr bool QE = KIND == 4;
+    constexpr bool VAR = KIND == 2 || KIND == 3;
+    constexpr bool TABLE = KIND == 1 || KIND == 3;
+    constexpr int C = QE ? 2 : (KIND == 2 ? 2 * N : N);  // normals per step, stream 0
+    constexpr int CA = KIND == 3 ? N : 0;                // normals per step, aux stream
+    constexpr int G = 4 / gcd4(C);                       // steps per batch of whole Philox blocks
+    constexpr int NB = C * G / 4, NBA = CA * G / 4;
+
+    extern __shared__ __align__(16) unsigned char sm[];
+    {
+        const int4* src = reinterpret_cast<const int4*>(a.blob);
+        int4* dst = reinterpret_cast<int4*>(sm);
+        for (int t = threadIdx.x; t < a.smem_blob / 16; t += blockDim.x) dst[t] = src[t];
+    }
+    const int n_warps = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n_acc = 2 * a.n_out;
+    double* wacc = reinterpret_cast<double*>(sm + a.smem_blob);
+    for (int t = threadIdx.x; t < n_warps * n_acc; t += blockDim.x) wacc[t] = 0.0;
+    __syncthreads();
+    const R* s_dt = reinterpret_cast<const R*>(sm + a.off.step_dt);
+    const int* s_obs = reinterpret_cast<const int*>(sm + a.off.step_obs);
+    const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
+    const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
+    const R* s_hes = reinterpret_cast<const R*>(sm + a.off.hes);
+    const Pair2<R>* s_tab = reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
+    const R* s_trig = reinterpret_cast<const R*>(sm + a.off.ln_trig);
+    const double* s_disc = reinterpret_cast<const double*>(sm + a.off.obs_disc);
+    const int S = a.n_steps;
+
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n_pairs;
+         base += stride) {
+        const bool active = base + lane < n_pairs;
+        const uint64_t pair = static_cast<uint64_t>(first_pair + (active ? base + lane : n_pairs - 1));
+        R x0[N], x1[N], v0[N], v1[N];
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            x0[n] = x1[n] = R(0);
+            v0[n] = v1[n] = QE ? a.qe.v0 : (VAR ? s_hes[8 * n] : R(0));
+        }
+        Leg<R> l0, l1;
+        leg_init<R, PRODUCT>(l0), leg_init<R, PRODUCT>(l1);
+        R lp0 = R(0), lp1 = R(0);
+        for (int i0 = 1, batch = 0; i0 <= S; i0 += G, ++batch) {
+            R z[C * G];
+            R za[CA > 0 ? CA * G : 1];
+#pragma unroll
+            for (int k = 0; k < NB; ++k)
+                normals4<R>(pair, static_cast<uint64_t>(batch) * NB + k, 0u, k0, k1, z[4 * k], z[4 * k + 1],
+                            z[4 * k + 2], z[4 * k + 3]);
+#pragma unroll
+            for (int k = 0; k < NBA; ++k)
+                normals4<R>(pair, static_cast<uint64_t>(batch) * NBA + k, kAuxStream, k0, k1, za[4 * k],
+                            za[4 * k + 1], za[4 * k + 2], za[4 * k + 3]);
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int i = i0 + g;
+                if (G > 1 && i > S) break;
+                if (QE) {
+                    const R zv = z[2 * g], zx = z[2 * g + 1];
+                    qe_step(a.qe, x0[0], v0[0], zv, zx);
+                    qe_step(a.qe, x1[0], v1[0], -zv, -zx);
+                    lp0 = x0[0], lp1 = x1[0];
+                } else {
+                    const R dt = s_dt[i - 1];
+                    const R* zs = &z[g * C];
+                    R zc[N], wc[N];
+#pragma unroll
+                    for (int n = 0; n < N; ++n) {
+                        R acc = R(0);
+#pragma unroll
+                        for (int b = 0; b < N; ++b) acc += s_root[n * N + b] * zs[b];
+                        zc[n] = acc;
+                    }
+                    if (VAR) {
+                        const R* zr = KIND == 3 ? &za[g * CA] : &z[g * C + N];
+#pragma unroll
+                        for (int n = 0; n < N; ++n) {
+                            if (a.same) {
+                                R acc = R(0);
+#pragma unroll
+                                for (int b = 0; b < N; ++b) acc += s_root[n * N + b] * zr[b];
+                                wc[n] = acc;
+                            } else {
+                                wc[n] = zr[n];
+                            }
+                        }
+                    }
+                    R w0 = R(1e30), w1 = R(1e30);
+#pragma unroll
+                    for (int n = 0; n < N; ++n) {
+                        const NameStep<R> ns = s_ns[(i - 1) * N + n];
+                        R var0, var1, vp0 = R(0), vp1 = R(0);
+                        if (VAR) vp0 = m_max(v0[n], R(0)), vp1 = m_max(v1[n], R(0));
+                        if (TABLE) {
+                            R u0 = (x0[n] - ns.lo) * ns.inv_dx, u1 = (x1[n] - ns.lo) * ns.inv_dx;
+                            u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
+                            const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
+                            const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
+                            const Pair2<R> y0 = s_tab[ns.row + j0], y1 = s_tab[ns.row + j1];
+                            const R t0 = y0.a * (R(1) - f0) + y0.b * f0, t1 = y1.a * (R(1) - f1) + y1.b * f1;
+                            var0 = KIND == 1 ? t0 : t0 * vp0, var1 = KIND == 1 ? t1 : t1 * vp1;
+                        } else {
+                            var0 = vp0, var1 = vp1;
+                        }
+                        if (VAR) {
+                            const R* h = s_hes + 8 * n;  // v0, kappa, theta, xi, rho, sqrt(1 - rho^2)
+                            const R zv = h[4] * zc[n] + h[5] * wc[n];
+                            v0[n] += h[1] * (h[2] - vp0) * dt + h[3] * m_sqrt(vp0 * dt) * zv;
+                            v1[n] += h[1] * (h[2] - vp1) * dt + h[3] * m_sqrt(vp1 * dt) * (-zv);
+                        }
+                        x0[n] += R(-0.5) * var0 * dt + m_sqrt(var0 * dt) * zc[n];
+                        x1[n] += R(-0.5) * var1 * dt + m_sqrt(var1 * dt) * (-zc[n]);
+                        w0 = m_min(w0, x0[n] + ns.lf), w1 = m_min(w1, x1[n] + ns.lf);
+                    }
+                    lp0 = w0, lp1 = w1;
+                }
+                if (PRODUCT == OB_PRODUCT_LADDER) {
+                    l0.hi = m_max(l0.hi, lp0), l0.lo = m_min(l0.lo, lp0);
+                    l1.hi = m_max(l1.hi, lp1), l1.lo = m_min(l1.lo, lp1);
+                } else {
+                    l0.lo = m_min(l0.lo, lp0), l1.lo = m_min(l1.lo, lp1);
+                    const int j = s_obs[i];
+                    if (j >= 0) {
+                        leg_observe(a, s_trig, s_disc, l0, lp0, j);
+                        leg_observe(a, s_trig, s_disc, l1, lp1, j);
+                    }
+                }
+            }
+        }
+        const int* leg_type = reinterpret_cast<const int*>(sm + a.off.leg_type);
+        const R* leg_strike = reinterpret_cast<const R*>(sm + a.off.leg_strike);
+        const int* leg_barrier = reinterpret_cast<const int*>(sm + a.off.leg_barrier);
+        const R* ln_level = reinterpret_cast<const R*>(sm + a.off.ln_level);
+        for (int k = 0; k < a.n_out; ++k) {
+            const double y =
+                active ? 0.5 * (leg_output<R, PRODUCT>(a, leg_type, leg_strike, leg_barrier, ln_level, l0, lp0, k) +
+                                leg_output<R, PRODUCT>(a, leg_type, leg_strike, leg_barrier, ln_level, l1, lp1, k))
+                       : 0.0;
+            const double s1 = warp_sum(y), s2 = warp_sum(y * y);
+            if (lane == 0) wacc[warp * n_acc + k] += s1, wacc[warp * n_acc + a.n_out + k] += s2;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n_acc; t += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < n_warps; ++w) s += wacc[w * n_acc + t];
+        partial[static_cast<long long>(blockIdx.x) * n_acc + t] = s;
+    }
+}
+
+template <typename R>
+using FusedFn = void (*)(FusedArgs<R>, long long, long long, uint32_t, uint32_t, double*);
+
+template <typename R, int KIND, int PRODUCT>
+FusedFn<R> pick_n(int n) {
+    if (n == 1) return fused_kernel<R, 1, KIND, PRODUCT>;
+    if (n == 2) return fused_kernel<R, 2, KIND, PRODUCT>;
+    if (n == 3) return fused_kernel<R, 3, KIND, PRODUCT>;
+    if constexpr (KIND == 1) {
+        if (n == 4) return fused_kernel<R, 4, 1, PRODUCT>;
+        if (n == 5) return fused_kernel<R, 5, 1, PRODUCT>;
+    }
+    return nullptr;
+}
+
+template <typename R, int PRODUCT>
+FusedFn<R> pick_fused(int kind, int n) {
+    switch (kind) {
+        case 1: return pick_n<R, 1, PRODUCT>(n);
+        case 2: return pick_n<R, 2, PRODUCT>(n);
+        case 3: return pick_n<R, 3, PRODUCT>(n);
+        case 4: return n == 1 ? fused_kernel<R, 1, 4, PRODUCT> : nullptr;
+        default: return nullptr;
+    }
+}
+
+struct Blob {
+    std::vector<unsigned char> bytes;
+    template <typename T>
+    int put(const T* src, size_t count) {
+        const size_t at = (bytes.size() + 15) & ~static_cast<size_t>(15);
+        const size_t n = count * sizeof(T);
+        bytes.resize(at + ((n + 15) & ~static_cast<size_t>(15)), 0);
+        if (src && n) std::memcpy(bytes.data() + at, src, n);
+        return static_cast<int>(at);
+    }
+    template <typename T>
+    int put(const std::vector<T>& v) {
+        return put(v.data(), v.size());
+    }
+};
+
+}  // namespace
+
+// Packs the request for the specialised kernel; false when it does not apply (mixed kinds, a basket size without an
+// instantiation, or inputs that would not fit the shared-memory budget), and the generic kernel then runs.
+template <typename R>
+bool fused_build(McPlan& plan, const ob_mc_request& rq) {
+    const int n = rq.n_names, S = rq.n_steps;
+    int kind = -1;
+    if (rq.model == OB_MODEL_HESTON_QE) {
+        kind = 4;
+    } else {
+        kind = rq.kind[0];
+        for (int a = 1; a < n; ++a)
+            if (rq.kind[a] != kind) return false;
+        if (kind == 0) return false;
+    }
+    FusedFn<R> fn = rq.product == OB_PRODUCT_LADDER ? pick_fused<R, OB_PRODUCT_LADDER>(kind, n)
+                                                    : pick_fused<R, OB_PRODUCT_AUTOCALL>(kind, n);
+    if (!fn) return false;
+    FusedArgs<R> a{};
+    a.n_steps = S, a.n_x = rq.n_x, a.same = rq.same;
+    a.n_obs = rq.product == OB_PRODUCT_AUTOCALL ? rq.n_obs : 0;
+    a.n_legs = rq.product == OB_PRODUCT_LADDER ? rq.n_legs : 0;
+    a.n_out = rq.product == OB_PRODUCT_LADDER ? rq.n_legs + 1 : 4;
+    a.top = static_cast<R>(rq.n_x - 1) - static_cast<R>(1e-4);
+    a.spot0 = static_cast<R>(rq.spot[0]);
+    Blob blob;
+    std::vector<R> dt(S);
+    for (int i = 0; i < S; ++i) dt[i] = static_cast<R>(rq.dt[i]);
+    a.off.step_dt = blob.put(dt);
+    std::vector<int> obs_of(S + 1, -1);
+    if (rq.product == OB_PRODUCT_AUTOCALL)
+        for (int j = 0; j < rq.n_obs; ++j) obs_of[rq.obs_step[j]] = j;
+    a.off.step_obs = blob.put(obs_of);
+    const bool table = kind == 1 || kind == 3;
+    if (kind == 4) {
+        a.qe = make_qe_consts<R>(rq.heston, rq.r, rq.q, rq.dt[0]);
+    } else {
+        std::vector<NameStep<R>> ns(static_cast<size_t>(S) * n);
+        for (int i = 1; i <= S; ++i)
+            for (int k = 0; k < n; ++k) {
+                NameStep<R>& r = ns[static_cast<size_t>(i - 1) * n + k];
+                std::memset(&r, 0, sizeof r);
+                r.lf = static_cast<R>(rq.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
+                if (table) {
+                    const int row = rq.step_row[static_cast<size_t>(k) * S + (i - 1)];
+                    r.lo = static_cast<R>(rq.row_lo[row]);
+                    r.inv_dx = static_cast<R>(rq.row_inv_dx[row]);
+                    r.row = row * (rq.n_x - 1);
+                }
+            }
+        a.off.name_step = blob.put(ns);
+        std::vector<R> root(static_cast<size_t>(n) * n);
+        for (size_t k = 0; k < root.size(); ++k) root[k] = static_cast<R>(rq.root[k]);
+        a.off.root = blob.put(root);
+        std::vector<R> hes(8 * static_cast<size_t>(n), R(0));
+        for (int k = 0; k < n; ++k) {
+            for (int f = 0; f < 5; ++f) hes[8 * k + f] = static_cast<R>(rq.heston[5 * k + f]);
+            const R rho = hes[8 * k + 4];
+            hes[8 * k + 5] = static_cast<R>(std::sqrt(R(1) - rho * rho));
+        }
+        a.off.hes = blob.put(hes);
+        if (table) {
+            std::vector<Pair2<R>> tab(static_cast<size_t>(rq.n_rows) * (rq.n_x - 1));
+            for (int r = 0; r < rq.n_rows; ++r)
+                for (int k = 0; k + 1 < rq.n_x; ++k) {
+                    const double* row = rq.table + static_cast<size_t>(r) * rq.n_x;
+                    tab[static_cast<size_t>(r) * (rq.n_x - 1) + k] = {static_cast<R>(row[k]), static_cast<R>(row[k + 1])};
+                }
+            a.off.table2 = blob.put(tab);
+        }
+    }
+    if (rq.product == OB_PRODUCT_LADDER) {
+        std::vector<int> type(rq.n_legs), bar(rq.n_legs);
+        std::vector<R> strike(rq.n_legs), lvl(rq.n_legs);
+        for (int k = 0; k < rq.n_legs; ++k) {
+            type[k] = rq.leg_type[k];
+            strike[k] = static_cast<R>(rq.leg_strike[k]);
+            bar[k] = rq.leg_barrier ? rq.leg_barrier[k] : 0;
+            lvl[k] = bar[k] ? static_cast<R>(std::log(rq.leg_level[k] / rq.spot[0])) : R(0);
+        }
+        a.off.leg_type = blob.put(type), a.off.leg_strike = blob.put(strike);
+        a.off.leg_barrier = blob.put(bar), a.off.ln_level = blob.put(lvl);
+        a.discount = rq.discount;
+    } else {
+        std::vector<R> trig(rq.n_obs);
+        for (int j = 0; j < rq.n_obs; ++j)
+            trig[j] = rq.trigger[j] > 0 ? static_cast<R>(std::log(rq.trigger[j])) : R(1e30);
+        a.off.ln_trig = blob.put(trig);
+        a.off.obs_disc = blob.put(rq.obs_discount, rq.n_obs);
+        a.has_coupon = rq.coupon > 0.0 || rq.coupon_barrier > 0.0;
+        a.ln_cb = rq.coupon_barrier > 0 ? static_cast<R>(std::log(rq.coupon_barrier)) : R(-1e30);
+        a.ln_ki = rq.ki_barrier > 0 ? static_cast<R>(std::log(rq.ki_barrier)) : R(-1e30);
+        a.coupon = rq.coupon, a.put_strike = rq.put_strike, a.memory = rq.memory, a.ki_daily = rq.ki_daily;
+    }
+    a.smem_blob = static_cast<int>((blob.bytes.size() + 15) & ~static_cast<size_t>(15));
+    const int block = 512;
+    const size_t acc_bytes = static_cast<size_t>(block / 32) * 2 * a.n_out * sizeof(double);
+    const size_t smem = a.smem_blob + acc_bytes;
+    const size_t budget = sizeof(R) == 4 ? (110u << 10) : (220u << 10);  // two blocks a SM in float, one in double
+    if (smem > budget) return false;
+    unsigned char* d = plan.arena.alloc<unsigned char>(std::max<size_t>(16, blob.bytes.size()));
+    check_cuda(cudaMemcpy(d, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice), "copy blob");
+    a.blob = d;
+    const void* k = reinterpret_cast<const void*>(fn);
+    check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+               "cudaFuncSetAttribute");
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem), "occupancy");
+    if (per_sm < 1) return false;
+    plan.fused = true;
+    plan.kernel = k;
+    plan.block = block;
+    plan.smem_bytes = smem;
+    plan.blocks_per_sm = per_sm;
+    plan.n_out = a.n_out;
+    plan.fused_args<R>() = a;
+    return true;
+}
+
+template bool fused_build<float>(McPlan&, const ob_mc_request&);
+template bool fused_build<double>(McPlan&, const ob_mc_request&);
+
+}  // namespace ob

@@ -1,0 +1,54 @@
+// The specialised fused kernel: every name of one kind (local vol, Heston by Euler, SLV, or one Heston name by QE),
+// N names known at compile time, everything a step reads staged in shared memory.
+//
+// Per step and name one 16-byte record {lo, inv_dx, log-forward at the step end, table row} (32 bytes in double)
+// is read as a warp-wide broadcast; the local-variance table is stored as (y_i, y_i+1) pairs so that an
+// interpolation is one 8-byte shared load. Normals are drawn in batches of G steps whose count is a multiple of four,
+// so each Philox block fills registers by constant indices; the correlated normal root z is computed once per pair
+// and step and used with both signs (the reference's two legs read the same z with opposite signs,
+// RC/include/optlab_cuda/paths.hpp:301-329). The arithmetic of each leg is the reference's, operation for operation.
+#pragma once
+
+#include "model.cuh"
+
+namespace ob {
+
+template <typename R>
+struct alignas(16) NameStep;
+template <>
+struct alignas(16) NameStep<float> {
+    float lo, inv_dx, lf;
+    int row;  // first (y_i, y_i+1) pair of the step's table row
+};
+template <>
+struct alignas(16) NameStep<double> {
+    double lo, inv_dx, lf;
+    int row, pad;
+};
+
+template <typename R>
+struct alignas(8) Pair2 {
+    R a, b;
+};
+
+// Byte offsets inside the staged blob.
+struct FusedOffsets {
+    int step_dt, step_obs, name_step, root, hes, table2, ln_trig, obs_disc, leg_type, leg_strike, leg_barrier, ln_level;
+};
+
+template <typename R>
+struct FusedArgs {
+    FusedOffsets off;
+    const unsigned char* blob;
+    int smem_blob;
+    int n_steps, n_obs, n_out, n_legs, n_x, same;
+    R top;  // n_x - 1 - 1e-4, the clamp of the table interpolation
+    QeConsts<R> qe;
+    R spot0;
+    double discount;
+    int has_coupon, memory, ki_daily;
+    R ln_cb, ln_ki;
+    double coupon, put_strike;
+};
+
+}  // namespace ob

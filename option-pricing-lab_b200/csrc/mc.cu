@@ -17,6 +17,7 @@
 // so a result is bit-reproducible for a given launch shape.
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <vector>
 
@@ -319,6 +320,7 @@ void check_mc_request(const ob_mc_request& rq) {
 
 template <typename R>
 void McPlan::build(const ob_mc_request& rq) {
+    if (!force_generic && fused_build<R>(*this, rq)) return;
     const int n = rq.n_names, S = rq.n_steps;
     McArgs<R>& a = args<R>();
     a = McArgs<R>{};
@@ -405,6 +407,8 @@ template void McPlan::build<double>(const ob_mc_request&);
 
 void McPlan::create(const ob_mc_request& rq, int prec) {
     check_mc_request(rq);
+    const char* generic = std::getenv("OPTLAB_B200_GENERIC");  // 1: the generic kernel even where fused.cu applies
+    force_generic = generic && generic[0] == '1';
     sms = require_device();
     precision = prec;
     if (prec == OB_FP32) build<float>(rq);
@@ -433,12 +437,19 @@ void McPlan::run(long long n_pairs, long long first_pair, unsigned long long see
     const int grid = grid_for(n_pairs);
     const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
     if (!timing) check_cuda(cudaEventRecord(e0, st), "cudaEventRecord"), timing = true;
-    if (precision == OB_FP32)
-        reinterpret_cast<KernelFn<float>>(const_cast<void*>(kernel))<<<grid, block, smem_bytes, st>>>(
-            args_f, n_pairs, first_pair, k0, k1, d_partial);
+    using FusedF = void (*)(FusedArgs<float>, long long, long long, uint32_t, uint32_t, double*);
+    using FusedD = void (*)(FusedArgs<double>, long long, long long, uint32_t, uint32_t, double*);
+    void* fn = const_cast<void*>(kernel);
+    if (fused && precision == OB_FP32)
+        reinterpret_cast<FusedF>(fn)<<<grid, block, smem_bytes, st>>>(fa_f, n_pairs, first_pair, k0, k1, d_partial);
+    else if (fused)
+        reinterpret_cast<FusedD>(fn)<<<grid, block, smem_bytes, st>>>(fa_d, n_pairs, first_pair, k0, k1, d_partial);
+    else if (precision == OB_FP32)
+        reinterpret_cast<KernelFn<float>>(fn)<<<grid, block, smem_bytes, st>>>(args_f, n_pairs, first_pair, k0, k1,
+                                                                              d_partial);
     else
-        reinterpret_cast<KernelFn<double>>(const_cast<void*>(kernel))<<<grid, block, smem_bytes, st>>>(
-            args_d, n_pairs, first_pair, k0, k1, d_partial);
+        reinterpret_cast<KernelFn<double>>(fn)<<<grid, block, smem_bytes, st>>>(args_d, n_pairs, first_pair, k0, k1,
+                                                                               d_partial);
     check_cuda(cudaGetLastError(), "mc_kernel launch");
     mc_finalize<<<1, 64, 0, st>>>(d_partial, grid, 2 * n_out, d_sums);
     check_cuda(cudaGetLastError(), "mc_finalize launch");

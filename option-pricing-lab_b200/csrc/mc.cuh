@@ -1,7 +1,7 @@
 // Fused pricing plan: a checked ob_mc_request packed for the device, launched any number of times.
 #pragma once
 
-#include "model.cuh"
+#include "fused.cuh"
 
 namespace ob {
 
@@ -36,6 +36,7 @@ struct McPlan {
     int precision = OB_FP32;
     int n_out = 0, sms = 0, blocks_per_sm = 1, max_blocks = 0;
     int block = 256, grid_waves = 1;
+    bool force_generic = false;  // tests: run the generic kernel even where the specialised one applies
     size_t smem_bytes = 0;
     const void* kernel = nullptr;
     McArgs<float> args_f{};
@@ -46,6 +47,12 @@ struct McPlan {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     bool timing = false;
     cudaStream_t last_stream = nullptr;
+    bool fused = false;  // the specialised kernel of fused.cu runs this plan
+    FusedArgs<float> fa_f{};
+    FusedArgs<double> fa_d{};
+
+    template <typename R>
+    FusedArgs<R>& fused_args();
 
     template <typename R>
     McArgs<R>& args();
@@ -57,6 +64,18 @@ struct McPlan {
     void result(ob_mc_result& res);
     ~McPlan();
 };
+
+template <>
+inline FusedArgs<float>& McPlan::fused_args<float>() {
+    return fa_f;
+}
+template <>
+inline FusedArgs<double>& McPlan::fused_args<double>() {
+    return fa_d;
+}
+
+template <typename R>
+bool fused_build(McPlan& plan, const ob_mc_request& rq);
 
 template <>
 inline McArgs<float>& McPlan::args<float>() {

@@ -1,7 +1,369 @@
-"""optlab_b200: a B200 (sm_100a) Monte Carlo path engine behind the reference's engine-by-name interface."""
+"""optlab_b200: a Monte Carlo path engine for NVIDIA B200 (sm_100a), as a drop-in for the reference's `optlab.native`.
+
+This module is the `Engine` of the reference's registry (packages/core/src/optlab/core/engines.py:32-63): the same
+names and arguments as packages/native/src/optlab/native/__init__.py (`available`, `gpu_available`, `cpu_threads`,
+`unsupported`, `plan`, `run`, `simulate`, `calibrate_leverage`, `MAX_WINDOWS`), declared under the entry point group
+`optlab.engines` as `native` (option-pricing-lab_b200/pyproject.toml), or installed into a running registry with
+`register()`. It runs on the GPU only: backend "gpu" and "auto" use the device, and "cpu" raises EngineError (there is
+no CPU fallback). Paths evolve in float by default (`precision="fp32"`, the reference GPU's arithmetic) or in double
+(`precision="fp64"`).
+
+Model objects are read by class name and attribute, so the reference's own (optlab.core.models, optlab.structured)
+and this package's restatements (optlab_b200.models) both work.
+"""
 
 from __future__ import annotations
 
-from ._abi import EngineError, load
+import os
+from collections import OrderedDict
+from dataclasses import asdict, dataclass
+from typing import Any
 
-__all__ = ["EngineError", "load"]
+import numpy as np
+
+from . import _abi, engine
+from ._abi import EngineError
+from .models import Leverage, SLVModel, aligned_factors, time_grid
+from .surfaces import local_var_rows
+
+__all__ = [
+    "MAX_NAMES",
+    "MAX_WINDOWS",
+    "N_X",
+    "Device",
+    "EngineError",
+    "Plan",
+    "available",
+    "calibrate_leverage",
+    "cpu_threads",
+    "devices",
+    "gpu_available",
+    "plan",
+    "register",
+    "run",
+    "seed64",
+    "simulate",
+    "summary",
+    "unsupported",
+]
+
+_KIND = {"const": 0, "table": 1, "heston": 2, "slv": 3}
+N_X = 801
+MAX_NAMES = 8
+MAX_WINDOWS = 2
+
+
+def available() -> bool:
+    """The engine library is built and loads."""
+    try:
+        _abi.load()
+        return True
+    except (EngineError, OSError):
+        return False
+
+
+def gpu_available() -> bool:
+    return available() and engine.gpu_count() > 0
+
+
+def cpu_threads() -> int:
+    return int(_abi.load().ob_cpu_threads()) if available() else (os.cpu_count() or 1)
+
+
+@dataclass(frozen=True)
+class Device:
+    name: str
+    compute_capability: str
+    sm_count: int
+    clock_mhz: int
+    memory_gb: float
+    free_gb: float
+    integrated: bool
+    watchdog: bool
+
+
+def devices() -> list[Device]:
+    if not gpu_available():
+        return []
+    out = []
+    for i in range(engine.gpu_count()):
+        d = engine.device_info(i)
+        if d is not None:
+            out.append(
+                Device(d["name"], f"{d['major']}.{d['minor']}", d["sm_count"], d["clock_mhz"], d["total_mem"] / 2**30,
+                       d["free_mem"] / 2**30, bool(d["integrated"]), bool(d["kernel_timeout"]))
+            )
+    return out
+
+
+def seed64(seed) -> int:
+    """A 64-bit Philox key from an int, a SeedSequence or None (packages/core/src/optlab/core/engines.py:131-137)."""
+    if isinstance(seed, np.random.SeedSequence):
+        return int(seed.generate_state(1, np.uint64)[0])
+    if seed is None:
+        return int(np.random.SeedSequence().generate_state(1, np.uint64)[0])
+    return int(seed) & (2**64 - 1)
+
+
+# ------------------------------------------------------------------------------------------------ models to tables
+
+_TABLES: OrderedDict = OrderedDict()
+
+
+def _cached(key, obj, build):
+    hit = _TABLES.get(key)
+    if hit is not None and hit[0] is obj:
+        _TABLES.move_to_end(key)
+        return hit[1]
+    rows = build()
+    _TABLES[key] = (obj, rows)
+    while len(_TABLES) > 16:
+        _TABLES.popitem(last=False)
+    return rows
+
+
+def _local_var_rows(surface, t0: np.ndarray, n_x: int, sd_range=(-8.0, 6.0)):
+    return _cached((id(surface), "lv", n_x, t0.tobytes(), tuple(sd_range)), surface,
+                   lambda: local_var_rows(surface, t0, n_x, sd_range))
+
+
+def _leverage_rows(leverage, t0: np.ndarray, n_x: int):
+    """(lo, inv_dx, squared leverage rows, row of each step): packages/native/src/optlab/native/__init__.py:147-167."""
+
+    def build():
+        times = np.asarray(leverage.times, dtype=float)
+        if hasattr(leverage, "rows"):
+            src = [(x0, x0 + (len(y) - 1) / inv, np.linspace(x0, x0 + (len(y) - 1) / inv, len(y)), y)
+                   for x0, inv, y in leverage.rows]
+        else:
+            src = [(xs[0], xs[-1], xs, vs) for xs, vs in zip(leverage.x_grids, leverage.values)]
+        lo, inv, rows = np.empty(len(src)), np.empty(len(src)), np.empty((len(src), n_x))
+        for r, (a, b, xs, vs) in enumerate(src):
+            grid = np.linspace(a, b, n_x)
+            lo[r], inv[r] = a, (n_x - 1) / (b - a)
+            rows[r] = np.interp(grid, xs, vs) ** 2
+        step = np.clip(np.searchsorted(times, t0 + 1e-12, side="right") - 1, 0, len(times) - 1).astype(np.int32)
+        return lo, inv, rows, step
+
+    return _cached((id(leverage), "lev", n_x, t0.tobytes()), leverage, build)
+
+
+def _name(model) -> str:
+    return type(model).__name__
+
+
+def _heston_tuple(model):
+    h = model.heston
+    return (h.v0, h.kappa, h.theta, h.xi, h.rho)
+
+
+def _describe(model, t0: np.ndarray, n_x: int):
+    """(kind, constant variance, Heston parameters, table rows or None, step rows or None) of one name
+    (packages/native/src/optlab/native/__init__.py:170-187)."""
+    name = _name(model)
+    if name == "BlackScholesModel":
+        return _KIND["const"], model.vol**2, (0.0, 1.0, 1.0, 0.0, 0.0), None, None
+    if name in ("LocalVolModel", "TabulatedLocalVol"):
+        sd = getattr(model, "sd_range", (-8.0, 6.0))
+        lo, inv, rows = _local_var_rows(model.surface, t0, n_x, sd)
+        return _KIND["table"], 0.0, (0.0, 1.0, 1.0, 0.0, 0.0), (lo, inv, rows), np.arange(len(t0), dtype=np.int32)
+    if name == "SLVModel":
+        lo, inv, rows, step = _leverage_rows(model.leverage, t0, n_x)
+        return _KIND["slv"], 0.0, _heston_tuple(model), (lo, inv, rows), step
+    if name == "HestonModel":
+        return _KIND["heston"], 0.0, _heston_tuple(model), None, None
+    raise NotImplementedError(f"{name} is not in the path engine")
+
+
+_KNOWN = ("BlackScholesModel", "LocalVolModel", "TabulatedLocalVol", "SLVModel", "HestonModel")
+
+
+def _is_basket(model) -> bool:
+    return _name(model) == "Basket"
+
+
+def unsupported(model) -> str | None:
+    """Why the engine cannot simulate this model or basket, or None (native/__init__.py:190-212)."""
+    if _is_basket(model):
+        if len(model.names) > MAX_NAMES:
+            return f"more than {MAX_NAMES} names"
+        bad = [n for n, m in model.models.items() if _name(m) not in _KNOWN]
+        if bad:
+            return f"{', '.join(_name(model.models[n]) for n in bad)} not in the path engine"
+        if model.mixer is not None and _name(model.mixer) != "LocalCorrelation":
+            return f"{_name(model.mixer)} is not in the path engine (local correlation only)"
+        return None
+    if _name(model) not in _KNOWN:
+        return f"{_name(model)} is not in the path engine"
+    if _name(model) == "SLVModel":
+        lev = model.leverage
+        if not hasattr(lev, "rows") and not (hasattr(lev, "x_grids") and hasattr(lev, "values")):
+            return "this leverage is not in the path engine"
+    return None
+
+
+@dataclass
+class Plan:
+    """Everything of a simulation but the pairs (native/__init__.py:215-240)."""
+
+    names: tuple
+    kind: np.ndarray
+    cvar: np.ndarray
+    heston: np.ndarray
+    root: np.ndarray
+    same: int
+    dt: np.ndarray
+    t0: np.ndarray
+    obs_step: np.ndarray
+    fwd: np.ndarray
+    step_row: np.ndarray | None
+    lo: np.ndarray | None
+    inv_dx: np.ndarray | None
+    table: np.ndarray | None
+    mixer: int
+    mix: tuple
+    low_root: np.ndarray | None
+    n_x: int
+
+    @property
+    def n_obs(self) -> int:
+        return len(self.obs_step)
+
+
+def plan(model, market, times, dt_max=1 / 252, dt_min=1 / 2000, n_x: int = N_X) -> Plan:
+    """A model or basket as the engine's arrays (native/__init__.py:243-302)."""
+    why = unsupported(model)
+    if why:
+        raise NotImplementedError(why)
+    times = np.asarray(times, dtype=float)
+    if _is_basket(model):
+        names, models = tuple(model.names), [model.models[n] for n in model.names]
+        markets = [model.markets[n] for n in model.names]
+        root, same = np.asarray(model.root, dtype=float), int(model.vol_corr == "same")
+    else:
+        names, models, markets, root, same = ("_",), [model], [market], np.eye(1), 1
+    if all(_name(m) == "BlackScholesModel" for m in models):
+        dt_max, dt_min = np.inf, None
+    grid = time_grid(times, dt_max, dt_min)
+    obs = np.searchsorted(grid, times).astype(np.int32)
+    dt, t0 = np.diff(grid), grid[:-1].copy()
+    k = len(models)
+    kind, cvar, hes = np.empty(k, np.int32), np.empty(k), np.empty((k, 5))
+    lo, inv, tab, rows_of = [], [], [], np.zeros((k, len(dt)), np.int32)
+    offset = 0
+    for a, m in enumerate(models):
+        kind[a], cvar[a], hes[a], rows, step = _describe(m, t0, n_x)
+        if rows is not None:
+            lo.append(rows[0]), inv.append(rows[1]), tab.append(rows[2])
+            rows_of[a] = step + offset
+            offset += len(rows[0])
+    fwd = np.stack([np.asarray(mk.F(times), dtype=float) for mk in markets]) if len(times) else np.zeros((k, 0))
+    mixer, mix, low = 0, (0.0,) * 8, None
+    if _is_basket(model) and model.mixer is not None:
+        mx = model.mixer
+        low, sign, turn = aligned_factors(model.corr, model.root, mx.w0)
+        mixer, mix = 1, (mx.w0, mx.level, mx.down, mx.up, mx.sigma, sign, np.cos(turn), np.sin(turn))
+        low = np.ascontiguousarray(low, dtype=float)
+    return Plan(
+        names, kind, cvar, np.ascontiguousarray(hes), np.ascontiguousarray(root), same, dt, t0, obs,
+        np.ascontiguousarray(fwd), rows_of if tab else None, np.concatenate(lo) if lo else None,
+        np.concatenate(inv) if inv else None, np.ascontiguousarray(np.concatenate(tab)) if tab else None, mixer,
+        tuple(float(x) for x in mix), low, n_x,
+    )
+
+
+def _backend(backend: str) -> str:
+    if backend == "auto":
+        backend = "gpu"
+    if backend not in ("cpu", "gpu"):
+        raise ValueError(f"backend must be cpu, gpu or auto, not {backend!r}")
+    if backend == "cpu":
+        raise EngineError("optlab_b200 runs on the GPU only (there is no CPU backend): use backend='gpu'")
+    return backend
+
+
+def run(p: Plan, n_pairs: int, seed: int, first_pair: int = 0, backend: str = "gpu", threads: int = 0, keep=None,
+        windows=(), precision: str = "fp32"):
+    """(spots, extremes, timing): spots[a] is a (2 n_pairs, len(keep)) Fortran-order view of name a at the kept
+    observations, pair i at row i and its antithetic at row n_pairs + i; extremes[a][w] = (lowest, highest) over
+    window w; timing = {kernel_ms, total_ms, backend} (native/__init__.py:317-374)."""
+    from .requests import paths_request
+
+    del threads  # the reference's CPU thread count: no meaning on the device
+    backend = _backend(backend)
+    k = len(p.names)
+    keep = np.arange(p.n_obs) if keep is None else np.asarray(keep, dtype=int)
+    if len(windows) > MAX_WINDOWS:
+        raise ValueError(f"at most {MAX_WINDOWS} windows")
+    col_of = np.full(p.n_obs, -1, np.int32)
+    col_of[keep] = np.arange(len(keep), dtype=np.int32)
+    n_cols = len(keep) + 2 * len(windows)
+    out = np.empty((k, n_cols, 2 * n_pairs))
+    held = paths_request(
+        dt=p.dt, t0=p.t0, obs_step=p.obs_step, root=p.root, kind=p.kind, cvar=p.cvar, heston=p.heston, same=p.same,
+        fwd=p.fwd, n_pairs=n_pairs, seed=seed, first_pair=first_pair, step_row=p.step_row, lo=p.lo, inv_dx=p.inv_dx,
+        table=p.table, n_x=p.n_x, mixer=p.mixer, mix=p.mix, low_root=p.low_root, col_of=col_of, n_keep=len(keep),
+        win_lo=[w[0] for w in windows], win_hi=[w[1] for w in windows], out=out,
+    )
+    kernel_ms, total_ms = engine.paths(held, precision)
+    m = len(keep)
+    spots = [out[a, :m].T for a in range(k)]
+    extremes = [[(out[a, m + 2 * w], out[a, m + 2 * w + 1]) for w in range(len(windows))] for a in range(k)]
+    return spots, extremes, {"kernel_ms": kernel_ms, "total_ms": total_ms, "backend": backend}
+
+
+def simulate(model, market, times, n_paths: int, seed=None, dt_max=1 / 252, dt_min=1 / 2000, backend: str = "auto",
+             first_pair: int = 0, threads: int = 0, precision: str = "fp32"):
+    """`models.simulate` (a {name: array} dict for a Basket) on the engine (native/__init__.py:407-426)."""
+    p = plan(model, market, times, dt_max, dt_min)
+    spots, _, _ = run(p, n_paths // 2, seed64(seed), first_pair, backend, threads, precision=precision)
+    if _is_basket(model):
+        return dict(zip(p.names, spots))
+    return spots[0]
+
+
+def calibrate_leverage(params, surface, market, T_max: float, mix: float = 1.0, n_particles: int = 100_000,
+                       dt_max=1 / 100, dt_min=1 / 2000, n_x=81, bandwidth_scale=1.0, rng=None, l_bounds=(0.05, 8.0),
+                       regression="nadaraya_watson", positive_part=False, backend: str = "auto", threads: int = 0,
+                       precision: str = "fp32", n_bins: int = 400, n_fine: int = 8192):
+    """The SLV leverage by the particle method on the device (native/__init__.py:429-496): an SLVModel."""
+    from .leverage import leverage_request
+
+    del market, threads
+    _backend(backend)
+    if regression not in ("nadaraya_watson", "local_linear"):
+        raise ValueError(f"unknown regression {regression!r}, expected nadaraya_watson or local_linear")
+    grid = time_grid([T_max], dt_max, dt_min)
+    dt, t0 = np.diff(grid), grid[:-1].copy()
+    lv_lo, lv_inv, lv_rows = _local_var_rows(surface, t0, N_X)
+    T1 = min(1.0, float(surface.maturities[-1]))
+    atm_vol = float(np.sqrt(surface.theta(T1) / T1))
+    h = (params.v0, params.kappa, params.theta, mix * params.xi, params.rho)
+    held = leverage_request(
+        dt=dt, t0=t0, n_pairs=n_particles // 2, seed=seed64(rng), heston=h, n_x=n_x, lv_lo=lv_lo, lv_inv_dx=lv_inv,
+        lv_rows=lv_rows, atm_vol=atm_vol, n_bins=n_bins, n_fine=n_fine, bandwidth_scale=bandwidth_scale,
+        l_bounds=l_bounds, local_linear=int(regression == "local_linear"), positive_part=int(positive_part),
+    )
+    engine.leverage(held, precision)
+    return SLVModel(params, Leverage(t0, held.x_grids, held.values), mix)
+
+
+def summary() -> dict[str, Any]:
+    return {
+        "engine": "optlab_b200",
+        "compiled": available(),
+        "cuda_build": available(),
+        "devices": [asdict(d) for d in devices()],
+        "cpu_threads": cpu_threads(),
+        "resolved": "gpu" if gpu_available() else "none",
+    }
+
+
+def register() -> None:
+    """Make this module the compiled engine of a running reference registry (optlab.core.engines), as its entry point
+    would once installed."""
+    import sys
+
+    from optlab.core import engines as registry
+
+    registry._compiled[:] = [sys.modules[__name__]]

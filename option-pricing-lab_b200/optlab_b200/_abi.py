@@ -26,7 +26,13 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
-class EngineError(RuntimeError):
+try:  # where the reference's registry is importable, its callers catch its EngineError: be that class
+    from optlab.core.engines import EngineError as _RegistryError
+except ImportError:  # standalone
+    _RegistryError = RuntimeError
+
+
+class EngineError(_RegistryError):
     """The engine failed, or cannot run what was asked of it (optlab.core.engines.EngineError's role)."""
 
 
