@@ -222,6 +222,14 @@ int ob_leverage(ob_leverage_request* rq, int precision);
    with the engine's Philox normals (pair p reads stream 0 of pair p) instead of cuRAND. */
 int ob_price(const ob_request* rq, ob_result* res, int precision);
 
+/* ob_price without any device allocation, for callers that own all device memory through another allocator or
+   must not call cudaMalloc/cudaFree while pricing. No counterpart in the reference: it has no allocation-free path.
+   Its scratch (the per-block and final sums) is a fixed array in the library, about 256 KiB on every device that
+   loads it, kept until exit; launches needing more than 4096 blocks are refused (OB_EINVAL). The first call on a
+   device looks up that array's address and should come before any stream capture. Calls share the array: calls
+   that overlap on the GPU race and must not be made. */
+int ob_price_noalloc(const ob_request* rq, ob_result* res, int precision);
+
 /* Fused pricing, end to end: host request in, result out (copies and allocations included). */
 int ob_mc_price(const ob_mc_request* rq, int precision, ob_mc_result* res);
 

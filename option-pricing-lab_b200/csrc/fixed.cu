@@ -176,3 +176,92 @@ extern "C" int ob_price(const ob_request* rq, ob_result* res, int precision) {
         else ob::run_fixed<double>(*rq, *res);
     });
 }
+
+// ------------------------------------------------------------------------------------------------ no allocation
+//
+// ob_price_noalloc: ob_price for callers that must not allocate device memory while they price. Some risk services
+// hand all device memory to one allocator at start-up (a framework's caching pool, a fixed budget per desk) and
+// cannot have a library take more behind its back; others run quote loops where cudaMalloc and cudaFree are not
+// allowed, because they take the driver's allocation lock and cudaFree waits for the whole device. This entry point
+// runs the same kernel as ob_price, with its per-block partial sums and final sums in a fixed array that is part of
+// the library image: g_noalloc_scratch, 4096 blocks x 8 sums + 8 totals (about 256 KiB), held on every device that
+// loads the library until the process exits. A launch needing more blocks than that is refused.
+//
+// Set-up: the first call on a device, with that device current, asks the driver for the array's device address
+// (cudaGetSymbolAddress); make that first call before any stream capture. Every call uses the same array, and each
+// call overwrites in full the slots it reads (every block writes its partial sums, the last kernel writes the
+// totals), so nothing carries over from one call to the next; calls that overlap on the GPU (two host threads, or
+// work queued on other streams) would race for the array and must not be made.
+namespace ob {
+namespace {
+
+constexpr int kNoAllocMaxBlocks = 4096;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks * 8 + 8];
+double* g_noalloc_address[64] = {};  // per device: the array's device address, as the driver gives it
+
+double* noalloc_scratch() {
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) invalid("device index beyond 63");
+    if (!g_noalloc_address[dev]) {
+        void* p = nullptr;
+        check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+        g_noalloc_address[dev] = static_cast<double*>(p);
+    }
+    return g_noalloc_address[dev];
+}
+
+template <typename R>
+void run_fixed_noalloc(const ob_request& rq, ob_result& res) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const int sms = require_device();
+    FixedDev f{};
+    f.model = rq.model, f.product = rq.product, f.n_steps = rq.n_steps;
+    for (int k = 0; k < 3; ++k) f.leg[k] = rq.legs[k], f.K[k] = rq.strikes[k];
+    const double dt = rq.T / rq.n_steps;
+    f.S0 = rq.S0, f.D = std::exp(-rq.r * rq.T);
+    f.bs_drift = (rq.r - rq.q - 0.5 * rq.sigma * rq.sigma) * dt;
+    f.bs_vol = rq.sigma * std::sqrt(dt);
+    f.ln_h = rq.product == 2 ? std::log(rq.H / rq.S0) : 0.0;
+    f.inv_n = 1.0 / rq.n_steps;
+    const double h[5] = {rq.v0, rq.kappa, rq.theta, rq.xi, rq.rho};
+    QeConsts<R> qe{};
+    if (rq.model == 1) qe = make_qe_consts<R>(h, rq.r, rq.q, dt);
+    const long long n_units = rq.n_paths / 2;
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fixed_kernel<R>, 256, 0), "occupancy");
+    const long long grid = std::max<long long>(
+        1, std::min<long long>((n_units + 255) / 256, static_cast<long long>(sms) * std::max(1, per_sm)));
+    if (grid > kNoAllocMaxBlocks) invalid("the launch needs more blocks than the no-allocation scratch holds (4096)");
+    double* partial = noalloc_scratch();
+    double* sums = partial + static_cast<size_t>(kNoAllocMaxBlocks) * 8;
+    fixed_kernel<R><<<static_cast<unsigned>(grid), 256>>>(f, qe, n_units, static_cast<uint32_t>(rq.seed),
+                                                          static_cast<uint32_t>(rq.seed >> 32), partial);
+    check_cuda(cudaGetLastError(), "fixed_kernel launch");
+    fixed_finalize<<<1, 32>>>(partial, static_cast<int>(grid), sums);
+    check_cuda(cudaGetLastError(), "fixed_finalize launch");
+    double hs[8];
+    check_cuda(cudaMemcpy(hs, sums, sizeof hs, cudaMemcpyDeviceToHost), "fixed_kernel");
+    std::memset(&res, 0, sizeof res);
+    const double n = static_cast<double>(n_units);
+    for (int k = 0; k < 4; ++k) {
+        const double mean = hs[k] / n, var = hs[4 + k] / n - mean * mean;
+        res.price[k] = mean, res.se[k] = n_units > 1 ? std::sqrt(std::fmax(var, 0.0) / (n - 1.0)) : 0.0;
+    }
+    res.n_paths = rq.n_paths;
+    res.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    res.kernel_ms = res.total_ms;  // no events: creating them is an allocation this entry point avoids
+}
+
+}  // namespace
+}  // namespace ob
+
+extern "C" int ob_price_noalloc(const ob_request* rq, ob_result* res, int precision) {
+    return ob::guarded([&] {
+        if (!rq || !res) ob::invalid("null argument");
+        if (precision != OB_FP32 && precision != OB_FP64) ob::invalid("precision must be OB_FP32 or OB_FP64");
+        ob::check_request(*rq);
+        if (precision == OB_FP32) ob::run_fixed_noalloc<float>(*rq, *res);
+        else ob::run_fixed_noalloc<double>(*rq, *res);
+    });
+}

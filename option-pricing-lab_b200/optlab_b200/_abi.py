@@ -235,6 +235,7 @@ SIGNATURES = {
     "ob_paths": (C.c_int, [C.POINTER(ObPathsRequest), C.c_int]),
     "ob_leverage": (C.c_int, [C.POINTER(ObLeverageRequest), C.c_int]),
     "ob_price": (C.c_int, [C.POINTER(ObRequest), C.POINTER(ObResult), C.c_int]),
+    "ob_price_noalloc": (C.c_int, [C.POINTER(ObRequest), C.POINTER(ObResult), C.c_int]),
     "ob_mc_price": (C.c_int, [C.POINTER(ObMcRequest), C.c_int, C.POINTER(ObMcResult)]),
     "ob_mc_plan_create": (C.c_int, [C.POINTER(ObMcRequest), C.c_int, C.POINTER(C.c_void_p)]),
     "ob_mc_run": (C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_ulonglong, C.c_void_p]),
