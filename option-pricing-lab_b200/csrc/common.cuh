@@ -107,14 +107,10 @@ __host__ __device__ __forceinline__ void philox4x32_10(uint32_t& x, uint32_t& y,
                                                        uint32_t k0, uint32_t k1) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-#ifdef __CUDA_ARCH__
-        const uint32_t hi0 = __umulhi(0xD2511F53u, x), lo0 = 0xD2511F53u * x;
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, z), lo1 = 0xCD9E8D57u * z;
-#else
+        // one 32 x 32 -> 64-bit product gives both halves (a single wide multiply on the device)
         const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * x, p1 = static_cast<uint64_t>(0xCD9E8D57u) * z;
         const uint32_t hi0 = static_cast<uint32_t>(p0 >> 32), lo0 = static_cast<uint32_t>(p0);
         const uint32_t hi1 = static_cast<uint32_t>(p1 >> 32), lo1 = static_cast<uint32_t>(p1);
-#endif
         const uint32_t nx = hi1 ^ y ^ k0, nz = hi0 ^ w ^ k1;
         x = nx, y = lo1, z = nz, w = lo0;
         k0 += 0x9E3779B9u;

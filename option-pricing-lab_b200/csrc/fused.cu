@@ -106,8 +106,7 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
     double* wacc = reinterpret_cast<double*>(sm + a.smem_blob);
     for (int t = threadIdx.x; t < n_warps * n_acc; t += blockDim.x) wacc[t] = 0.0;
     __syncthreads();
-    const R* s_dt = reinterpret_cast<const R*>(sm + a.off.step_dt);
-    const int* s_obs = reinterpret_cast<const int*>(sm + a.off.step_obs);
+    const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
     const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
     const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
     const R* s_hes = reinterpret_cast<const R*>(sm + a.off.hes);
@@ -151,7 +150,7 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                     qe_step(a.qe, x1[0], v1[0], -zv, -zx);
                     lp0 = x0[0], lp1 = x1[0];
                 } else {
-                    const R dt = s_dt[i - 1];
+                    const StepRec<R> st = s_step[i - 1];
                     const R* zs = &z[g * C];
                     R zc[N], wc[N];
 #pragma unroll
@@ -187,7 +186,7 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                             const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
                             const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
                             const Pair2<R> y0 = s_tab[ns.row + j0], y1 = s_tab[ns.row + j1];
-                            const R t0 = y0.a * (R(1) - f0) + y0.b * f0, t1 = y1.a * (R(1) - f1) + y1.b * f1;
+                            const R t0 = y0.a + f0 * y0.b, t1 = y1.a + f1 * y1.b;
                             var0 = KIND == 1 ? t0 : t0 * vp0, var1 = KIND == 1 ? t1 : t1 * vp1;
                         } else {
                             var0 = vp0, var1 = vp1;
@@ -195,11 +194,11 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                         if (VAR) {
                             const R* h = s_hes + 8 * n;  // v0, kappa, theta, xi, rho, sqrt(1 - rho^2)
                             const R zv = h[4] * zc[n] + h[5] * wc[n];
-                            v0[n] += h[1] * (h[2] - vp0) * dt + h[3] * m_sqrt(vp0 * dt) * zv;
-                            v1[n] += h[1] * (h[2] - vp1) * dt + h[3] * m_sqrt(vp1 * dt) * (-zv);
+                            v0[n] += h[1] * (h[2] - vp0) * st.dt + h[3] * (m_sqrt(vp0) * st.sdt) * zv;
+                            v1[n] += h[1] * (h[2] - vp1) * st.dt + h[3] * (m_sqrt(vp1) * st.sdt) * (-zv);
                         }
-                        x0[n] += R(-0.5) * var0 * dt + m_sqrt(var0 * dt) * zc[n];
-                        x1[n] += R(-0.5) * var1 * dt + m_sqrt(var1 * dt) * (-zc[n]);
+                        x0[n] += var0 * st.hdt + (m_sqrt(var0) * st.sdt) * zc[n];
+                        x1[n] += var1 * st.hdt + (m_sqrt(var1) * st.sdt) * (-zc[n]);
                         w0 = m_min(w0, x0[n] + ns.lf), w1 = m_min(w1, x1[n] + ns.lf);
                     }
                     lp0 = w0, lp1 = w1;
@@ -209,7 +208,7 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                     l1.hi = m_max(l1.hi, lp1), l1.lo = m_min(l1.lo, lp1);
                 } else {
                     l0.lo = m_min(l0.lo, lp0), l1.lo = m_min(l1.lo, lp1);
-                    const int j = s_obs[i];
+                    const int j = s_step[i - 1].obs;
                     if (j >= 0) {
                         leg_observe(a, s_trig, s_disc, l0, lp0, j);
                         leg_observe(a, s_trig, s_disc, l1, lp1, j);
@@ -307,13 +306,17 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
     a.top = static_cast<R>(rq.n_x - 1) - static_cast<R>(1e-4);
     a.spot0 = static_cast<R>(rq.spot[0]);
     Blob blob;
-    std::vector<R> dt(S);
-    for (int i = 0; i < S; ++i) dt[i] = static_cast<R>(rq.dt[i]);
-    a.off.step_dt = blob.put(dt);
-    std::vector<int> obs_of(S + 1, -1);
+    std::vector<StepRec<R>> steps(S);
+    for (int i = 0; i < S; ++i) {
+        std::memset(&steps[i], 0, sizeof steps[i]);
+        steps[i].dt = static_cast<R>(rq.dt[i]);
+        steps[i].hdt = static_cast<R>(-0.5 * rq.dt[i]);
+        steps[i].sdt = static_cast<R>(std::sqrt(rq.dt[i]));
+        steps[i].obs = -1;
+    }
     if (rq.product == OB_PRODUCT_AUTOCALL)
-        for (int j = 0; j < rq.n_obs; ++j) obs_of[rq.obs_step[j]] = j;
-    a.off.step_obs = blob.put(obs_of);
+        for (int j = 0; j < rq.n_obs; ++j) steps[rq.obs_step[j] - 1].obs = j;
+    a.off.step = blob.put(steps);
     const bool table = kind == 1 || kind == 3;
     if (kind == 4) {
         a.qe = make_qe_consts<R>(rq.heston, rq.r, rq.q, rq.dt[0]);
@@ -347,7 +350,8 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
             for (int r = 0; r < rq.n_rows; ++r)
                 for (int k = 0; k + 1 < rq.n_x; ++k) {
                     const double* row = rq.table + static_cast<size_t>(r) * rq.n_x;
-                    tab[static_cast<size_t>(r) * (rq.n_x - 1) + k] = {static_cast<R>(row[k]), static_cast<R>(row[k + 1])};
+                    tab[static_cast<size_t>(r) * (rq.n_x - 1) + k] = {static_cast<R>(row[k]),
+                                                                       static_cast<R>(row[k + 1] - row[k])};
                 }
             a.off.table2 = blob.put(tab);
         }

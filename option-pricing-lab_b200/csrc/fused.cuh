@@ -6,7 +6,9 @@
 // interpolation is one 8-byte shared load. Normals are drawn in batches of G steps whose count is a multiple of four,
 // so each Philox block fills registers by constant indices; the correlated normal root z is computed once per pair
 // and step and used with both signs (the reference's two legs read the same z with opposite signs,
-// RC/include/optlab_cuda/paths.hpp:301-329). The arithmetic of each leg is the reference's, operation for operation.
+// RC/include/optlab_cuda/paths.hpp:301-329). Each leg's step is the reference's arithmetic up to reassociation:
+// x += var (-dt / 2) + sqrt(var) sqrt(dt) z with -dt / 2 and sqrt(dt) precomputed per step, and the table read as
+// y + w dy.
 #pragma once
 
 #include "model.cuh"
@@ -26,14 +28,23 @@ struct alignas(16) NameStep<double> {
     int row, pad;
 };
 
+// One table interval: the value at its left point and the increment to the right one, so that an interpolation is
+// one multiply-add (y + w dy, the reference's y_i (1 - w) + y_i+1 w up to rounding).
 template <typename R>
-struct alignas(8) Pair2 {
+struct alignas(2 * sizeof(R)) Pair2 {
     R a, b;
+};
+
+// Per step: -dt / 2, sqrt(dt), dt, and the index of the observation taken at the step's end (-1: none).
+template <typename R>
+struct alignas(16) StepRec {
+    R hdt, sdt, dt;
+    int obs;
 };
 
 // Byte offsets inside the staged blob.
 struct FusedOffsets {
-    int step_dt, step_obs, name_step, root, hes, table2, ln_trig, obs_disc, leg_type, leg_strike, leg_barrier, ln_level;
+    int step, name_step, root, hes, table2, ln_trig, obs_disc, leg_type, leg_strike, leg_barrier, ln_level;
 };
 
 template <typename R>

@@ -217,13 +217,16 @@ __global__ void __launch_bounds__(256) mc_kernel(McArgs<R> a, long long n_pairs,
     }
 }
 
-// Adds the blocks' totals in block order to the plan's running sums.
+// Adds the blocks' totals to the plan's running sums: one warp per sum, lane l adding blocks l, l + 32, ... and the
+// lanes combined by a fixed shuffle tree, so the order (and the result) depends only on the grid.
 __global__ void mc_finalize(const double* __restrict__ partial, int n_blocks, int n_acc, double* sums) {
-    const int t = threadIdx.x;
-    if (t >= n_acc) return;
-    double s = 0.0;
-    for (int b = 0; b < n_blocks; ++b) s += partial[static_cast<long long>(b) * n_acc + t];
-    sums[t] += s;
+    const int lane = threadIdx.x & 31;
+    for (int t = threadIdx.x >> 5; t < n_acc; t += blockDim.x >> 5) {
+        double s = 0.0;
+        for (int b = lane; b < n_blocks; b += 32) s += partial[static_cast<long long>(b) * n_acc + t];
+        s = warp_sum(s);
+        if (lane == 0) sums[t] += s;
+    }
 }
 
 template <typename R>
@@ -426,32 +429,63 @@ McPlan::~McPlan() {
     if (e1) cudaEventDestroy(e1);
 }
 
-int McPlan::grid_for(long long n_pairs) const {
-    const long long need = (n_pairs + block - 1) / block;
-    const long long full = static_cast<long long>(sms) * blocks_per_sm * grid_waves;
+// Block size and grid of a run. Among the plan's block and its halves down to 64 threads, the shape that keeps the
+// most warps resident on the most SMs: a small batch (2^15 pairs of the QE ladder) then spreads over every SM in
+// small blocks, while a large one keeps 512-thread blocks. The grid fills each SM once with resident blocks and the
+// pairs are handed out grid-stride.
+int McPlan::occupancy_at(int blk) {
+    if (blk == block) return blocks_per_sm;
+    for (int k = 0; k < 4; ++k)
+        if (occ_block[k] == blk) return occ_blocks[k];
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, blk, smem_bytes), "occupancy");
+    per_sm = std::max(1, per_sm);
+    for (int k = 0; k < 4; ++k)
+        if (!occ_block[k]) {
+            occ_block[k] = blk, occ_blocks[k] = per_sm;
+            break;
+        }
+    return per_sm;
+}
+
+int McPlan::launch_shape(long long n_pairs, int& blk) {
+    double best = -1.0;
+    int best_blk = block;
+    for (int b = block; b >= 64; b /= 2) {
+        const long long need = (n_pairs + b - 1) / b;
+        const long long resident = static_cast<long long>(sms) * occupancy_at(b);
+        const long long blocks = std::min(need, resident);
+        const double busy = std::min(1.0, static_cast<double>(blocks) / sms);  // share of SMs with work
+        const double score = static_cast<double>(blocks) * (b / 32) * busy;
+        if (score > best * 1.0001) best = score, best_blk = b;
+    }
+    blk = best_blk;
+    const long long need = (n_pairs + blk - 1) / blk;
+    const long long full = static_cast<long long>(sms) * occupancy_at(blk) * grid_waves;
     return static_cast<int>(std::max<long long>(1, std::min<long long>({need, full, max_blocks})));
 }
 
 void McPlan::run(long long n_pairs, long long first_pair, unsigned long long seed, cudaStream_t st) {
     if (n_pairs < 1 || first_pair < 0) invalid("n_pairs must be >= 1 and first_pair >= 0");
-    const int grid = grid_for(n_pairs);
+    int blk = block;
+    const int grid = launch_shape(n_pairs, blk);
     const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
     if (!timing) check_cuda(cudaEventRecord(e0, st), "cudaEventRecord"), timing = true;
     using FusedF = void (*)(FusedArgs<float>, long long, long long, uint32_t, uint32_t, double*);
     using FusedD = void (*)(FusedArgs<double>, long long, long long, uint32_t, uint32_t, double*);
     void* fn = const_cast<void*>(kernel);
     if (fused && precision == OB_FP32)
-        reinterpret_cast<FusedF>(fn)<<<grid, block, smem_bytes, st>>>(fa_f, n_pairs, first_pair, k0, k1, d_partial);
+        reinterpret_cast<FusedF>(fn)<<<grid, blk, smem_bytes, st>>>(fa_f, n_pairs, first_pair, k0, k1, d_partial);
     else if (fused)
-        reinterpret_cast<FusedD>(fn)<<<grid, block, smem_bytes, st>>>(fa_d, n_pairs, first_pair, k0, k1, d_partial);
+        reinterpret_cast<FusedD>(fn)<<<grid, blk, smem_bytes, st>>>(fa_d, n_pairs, first_pair, k0, k1, d_partial);
     else if (precision == OB_FP32)
-        reinterpret_cast<KernelFn<float>>(fn)<<<grid, block, smem_bytes, st>>>(args_f, n_pairs, first_pair, k0, k1,
+        reinterpret_cast<KernelFn<float>>(fn)<<<grid, blk, smem_bytes, st>>>(args_f, n_pairs, first_pair, k0, k1,
                                                                               d_partial);
     else
-        reinterpret_cast<KernelFn<double>>(fn)<<<grid, block, smem_bytes, st>>>(args_d, n_pairs, first_pair, k0, k1,
+        reinterpret_cast<KernelFn<double>>(fn)<<<grid, blk, smem_bytes, st>>>(args_d, n_pairs, first_pair, k0, k1,
                                                                                d_partial);
     check_cuda(cudaGetLastError(), "mc_kernel launch");
-    mc_finalize<<<1, 64, 0, st>>>(d_partial, grid, 2 * n_out, d_sums);
+    mc_finalize<<<1, 1024, 0, st>>>(d_partial, grid, 2 * n_out, d_sums);
     check_cuda(cudaGetLastError(), "mc_finalize launch");
     check_cuda(cudaEventRecord(e1, st), "cudaEventRecord");
     pairs_run += n_pairs;

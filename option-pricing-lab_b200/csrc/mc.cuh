@@ -59,7 +59,9 @@ struct McPlan {
     template <typename R>
     void build(const ob_mc_request& rq);
     void create(const ob_mc_request& rq, int precision);
-    int grid_for(long long n_pairs) const;
+    int launch_shape(long long n_pairs, int& blk);
+    int occupancy_at(int blk);
+    int occ_block[4] = {}, occ_blocks[4] = {};  // resident blocks a SM at other block sizes, as queried
     void run(long long n_pairs, long long first_pair, unsigned long long seed, cudaStream_t st);
     void result(ob_mc_result& res);
     ~McPlan();

@@ -182,8 +182,19 @@ def _is_basket(model) -> bool:
     return _name(model) == "Basket"
 
 
+NO_DEVICE = "no CUDA device (optlab_b200 runs on the GPU only)"
+
+
 def unsupported(model) -> str | None:
-    """Why the engine cannot simulate this model or basket, or None (native/__init__.py:190-212)."""
+    """Why the engine cannot simulate this model or basket, or None (native/__init__.py:190-212). Without a device
+    the answer is NO_DEVICE, so that the registry's "auto" falls back to NumPy and "gpu" or "cpu" raise, as the
+    reference's registry does for an engine it cannot use (packages/core/src/optlab/core/engines.py:96-120)."""
+    if not gpu_available():
+        return NO_DEVICE
+    return _model_unsupported(model)
+
+
+def _model_unsupported(model) -> str | None:
     if _is_basket(model):
         if len(model.names) > MAX_NAMES:
             return f"more than {MAX_NAMES} names"
@@ -232,7 +243,7 @@ class Plan:
 
 def plan(model, market, times, dt_max=1 / 252, dt_min=1 / 2000, n_x: int = N_X) -> Plan:
     """A model or basket as the engine's arrays (native/__init__.py:243-302)."""
-    why = unsupported(model)
+    why = _model_unsupported(model)
     if why:
         raise NotImplementedError(why)
     times = np.asarray(times, dtype=float)
