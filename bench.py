@@ -226,7 +226,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe"])
+    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint"])
     ap.add_argument("--paths", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -239,6 +239,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload == "adjoint":
+        return run_adjoint(args, world, rank)
 
     import torch
 
@@ -362,6 +364,80 @@ def main():
         "wall_s": t_wall,
         "result": {"price": list(res.price[: res.n_out]), "se": list(res.se[: res.n_out]),
                    "e2e_price": r_e2e.price[0], "warmup_price": warm.price[0]},
+    }
+    print(json.dumps(line))
+
+
+def run_adjoint(args, world, rank):
+    """cfg3: the Greeks ladder of the 3-name worst-of (2^19 paths x 1008 steps) by the FP32 adjoint, against FP64
+    bump-and-revalue on the same GPU (central differences: 1 + 2 x (3 + 450) revaluations, each timed as the FP64
+    smoothed revaluation of the same request; a bounded number is timed and the ladder's time is their mean times
+    907). Also the FP32 adjoint against the FP64 adjoint on the same paths (the 4 SE / 1e-4 criterion)."""
+    import torch
+
+    from optlab_b200 import workloads
+    from optlab_b200.adjoint import AdjointPlan, VegaNodes, autocall_greeks
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    w = workloads.worst_of(n_paths=args.paths or 2**19)
+    nodes = VegaNodes(w.row_name, w.row_T, w.row_lo, w.row_inv_dx, w.n_x, w.node_T, w.node_k)
+    n_greeks = w.held.struct.n_names * (1 + len(w.node_T) * len(w.node_k))
+    s = w.held.struct
+    units = 2 * s.n_pairs * s.n_steps * s.n_names
+    plan = AdjointPlan(w.held, 0.005, "fp32")
+    for _ in range(args.warmup):
+        autocall_greeks(w.held, nodes, 0.005, plan=plan)
+    torch.cuda.synchronize()
+    times, fwd, bwd = [], [], []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            g32 = autocall_greeks(w.held, nodes, 0.005, plan=plan)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t)
+            fwd.append(g32["forward_ms"]), bwd.append(g32["backward_ms"])
+    plan.close()
+    t_adj = statistics.median(times)
+    # FP64 references: the adjoint in double (agreement) and the smoothed revaluation (bump-and-revalue cost)
+    p64 = AdjointPlan(w.held, 0.005, "fp64")
+    g64 = autocall_greeks(w.held, nodes, 0.005, plan=p64)
+    reval = []
+    for _ in range(max(3, min(args.steps, 6))):
+        r = p64.run(grad=False)
+        reval.append(r.forward_ms / 1e3)
+    p64.close()
+    t_rev = statistics.median(reval)
+    n_reval = 1 + 2 * n_greeks
+    vscale = np.abs(g64["vega"]).max()
+    dv = np.abs(g32["vega"] - g64["vega"])
+    line = {
+        "metric": "Greeks/s (delta per name + vega per node, FP32 adjoint)",
+        "value": n_greeks / t_adj,
+        "unit": "Greeks/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_adj * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded SSVI surfaces)",
+        "config": {"workload": "adjoint_worst_of", "n_paths": 2 * s.n_pairs, "n_steps": s.n_steps, "names": s.n_names,
+                   "nodes_per_name": [len(w.node_T), len(w.node_k)], "smoothing": 0.005},
+        "adjoint": {"forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
+                    "path_steps_per_s": 2 * units / (t_adj), "price": g32["price"], "price_se": g32["price_se"]},
+        "bump_and_revalue_fp64": {"revaluation_ms": t_rev * 1e3, "revaluations": n_reval,
+                                   "ladder_s": n_reval * t_rev, "greeks_per_s": n_greeks / (n_reval * t_rev),
+                                   "timed_revaluations": len(reval)},
+        "speedup_vs_fp64_bump": (n_reval * t_rev) / t_adj,
+        "fp32_vs_fp64": {"max_vega_diff_over_se": float(np.max(dv / np.maximum(g64["vega_se"], 1e-30))),
+                         "max_vega_diff_rel_to_largest": float(dv.max() / vscale),
+                         "max_delta_diff_over_se": float(np.max(np.abs(g32["delta"] - g64["delta"]) /
+                                                                np.maximum(g64["delta_se"], 1e-30))),
+                         "price_diff_over_se": abs(g32["price"] - g64["price"]) / g64["price_se"]},
+        "clocks": {k: v for k, v in clocks.summary().items() if k != "samples"},
+        "gpu_launches": 2 * args.steps,
     }
     print(json.dumps(line))
 

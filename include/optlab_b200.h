@@ -191,6 +191,28 @@ typedef struct {
 
 typedef struct ob_mc_plan ob_mc_plan;
 
+/* ---------------------------------------------------------------------------------------------- adjoint Greeks */
+
+#define OB_ADJ_BATCHES 32 /* batches of pairs of the gradient (standard errors by batch means) */
+
+/* An autocall under the path engine's local vol (every name kind 1, 1 to 4 names, pairs 0 .. n_pairs - 1) with its
+   digitals smoothed as ramps of relative width `smoothing` (the reference's risk engine uses 0.005 for Greeks,
+   packages/risk/src/optlab/risk/greeks.py:430; 0 gives the exact payoff). */
+typedef struct {
+    ob_mc_request base;
+    double smoothing;
+} ob_adjoint_request;
+
+typedef struct {
+    double price, price_se;                              /* smoothed price, notional 1 */
+    double delta[OB_MAX_NAMES], delta_se[OB_MAX_NAMES];  /* dV/dS_a, local vol moving with the spot (log-moneyness) */
+    long long n_paths;
+    int n_batches;
+    double forward_ms, backward_ms;
+} ob_adjoint_result;
+
+typedef struct ob_adjoint_plan ob_adjoint_plan;
+
 /* ---------------------------------------------------------------------------------------------- entry points */
 
 const char* ob_last_error(void);
@@ -240,6 +262,18 @@ int ob_mc_plan_create(const ob_mc_request* rq, int precision, ob_mc_plan** plan)
 int ob_mc_run(ob_mc_plan* plan, long long n_pairs, long long first_pair, unsigned long long seed, void* stream);
 int ob_mc_result_get(ob_mc_plan* plan, ob_mc_result* res);
 int ob_mc_plan_destroy(ob_mc_plan* plan);
+
+/* Adjoint (pathwise) Greeks: no counterpart in the reference ABI; it replaces the bump-and-revalue loop of
+   packages/risk/src/optlab/risk/engine.py:382-425 and greeks.py:199-244 for local-vol autocalls. create uploads the
+   request; run makes one forward pass on `stream` (d_table: a device n_rows x n_x double table of local variance
+   replacing the current one, NULL keeps it) and, with d_grad non-null, the backward pass, filling d_grad (device,
+   OB_ADJ_BATCHES x n_rows x n_x doubles) with each batch's sum over its pairs of d(pair value)/d(table entry);
+   result waits, returns price and deltas with standard errors, and the pairs of each batch (batch_pairs may be
+   NULL). Without d_grad, run is the smoothed revaluation of a bump-and-revalue. */
+int ob_adjoint_plan_create(const ob_adjoint_request* rq, int precision, ob_adjoint_plan** plan);
+int ob_adjoint_run(ob_adjoint_plan* plan, const double* d_table, double* d_grad, void* stream);
+int ob_adjoint_result_get(ob_adjoint_plan* plan, ob_adjoint_result* res, long long* batch_pairs);
+int ob_adjoint_plan_destroy(ob_adjoint_plan* plan);
 
 #ifdef __cplusplus
 }

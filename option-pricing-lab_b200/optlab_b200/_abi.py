@@ -210,6 +210,26 @@ class ObMcResult(C.Structure):
     ]
 
 
+OB_ADJ_BATCHES = 32
+
+
+class ObAdjointRequest(C.Structure):
+    _fields_ = [("base", ObMcRequest), ("smoothing", C.c_double)]
+
+
+class ObAdjointResult(C.Structure):
+    _fields_ = [
+        ("price", C.c_double),
+        ("price_se", C.c_double),
+        ("delta", C.c_double * OB_MAX_NAMES),
+        ("delta_se", C.c_double * OB_MAX_NAMES),
+        ("n_paths", C.c_longlong),
+        ("n_batches", C.c_int),
+        ("forward_ms", C.c_double),
+        ("backward_ms", C.c_double),
+    ]
+
+
 # Every symbol include/optlab_b200.h declares, with its ctypes signature (restype, argtypes).
 SIGNATURES = {
     "ob_last_error": (C.c_char_p, []),
@@ -241,6 +261,10 @@ SIGNATURES = {
     "ob_mc_run": (C.c_int, [C.c_void_p, C.c_longlong, C.c_longlong, C.c_ulonglong, C.c_void_p]),
     "ob_mc_result_get": (C.c_int, [C.c_void_p, C.POINTER(ObMcResult)]),
     "ob_mc_plan_destroy": (C.c_int, [C.c_void_p]),
+    "ob_adjoint_plan_create": (C.c_int, [C.POINTER(ObAdjointRequest), C.c_int, C.POINTER(C.c_void_p)]),
+    "ob_adjoint_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ob_adjoint_result_get": (C.c_int, [C.c_void_p, C.POINTER(ObAdjointResult), C.POINTER(C.c_longlong)]),
+    "ob_adjoint_plan_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _lib: list = []

@@ -7,6 +7,10 @@
   on 200 log-strikes x 40 expiries (T_j = 3 j / 40); a 3-year single-name Phoenix, quarterly observations,
   autocall at 100 %, coupon 2 % at 70 % with memory, knock-in at 60 % on daily closes into a put struck at 100 %;
   756 daily steps, 2^20 paths; flat market r .02, q .01.
+- `worst_of`: three names, each its own SSVI power-law surface (theta_t = c t with c = 0.03, 0.045, 0.06; rho = -0.7,
+  -0.55, -0.4; eta 1, gamma 0.5) tabulated on 40 expiries x 200 log-strikes over four years, pairwise correlation 0.6;
+  a worst-of Phoenix, quarterly over four years (16 observations), 1008 daily steps, 2^19 paths. Its Greeks: delta per
+  name and vega per node of each local-vol surface on 10 expiries x 15 log-strikes.
 """
 
 from __future__ import annotations
@@ -16,6 +20,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._abi import BARRIER, OB_MODEL_HESTON_QE, OB_MODEL_PATHS, OB_PRODUCT_AUTOCALL, OB_PRODUCT_LADDER
+from .models import correlation_root
 from .requests import Held, mc_request
 from .surfaces import SSVI, LocalVarGrid
 
@@ -153,3 +158,63 @@ def path_steps(held: Held) -> int:
     """Path-steps of one run of a fused request: 2 n_pairs paths x n_steps steps x n_names names."""
     s = held.struct
     return 2 * s.n_pairs * s.n_steps * s.n_names
+
+
+@dataclass
+class WorstOf:
+    """The worst-of request with what its node vegas need: each table row's name, expiry and log-strike grid."""
+
+    held: Held
+    row_name: np.ndarray
+    row_T: np.ndarray
+    row_lo: np.ndarray
+    row_inv_dx: np.ndarray
+    n_x: int
+    node_T: np.ndarray
+    node_k: np.ndarray
+    spots: np.ndarray
+
+
+def worst_of(n_paths: int = 2**19, seed: int = 11, years: float = 4.0, steps_per_year: int = 252, n_names: int = 3,
+             c=(0.03, 0.045, 0.06), rho=(-0.7, -0.55, -0.4), corr: float = 0.6, n_exp: int = 40, n_x: int = 200,
+             n_node_T: int = 10, n_node_k: int = 15, phoenix: Phoenix | None = None) -> WorstOf:
+    ph = phoenix or Phoenix(years=years)
+    m = FlatMarket(100.0, 0.02, 0.01)
+    n_steps = int(round(years * steps_per_year))
+    dt, t0 = uniform_grid(years, n_steps)
+    t_end = np.concatenate([[0.0], t0 + dt])
+    T = years * np.arange(1, n_exp + 1) / n_exp
+    grids = [lv_grid(SSVI.power_law(rho[a], 1.0, 0.5, T, c[a] * T), horizon=years, n_exp=n_exp, n_x=n_x)
+             for a in range(n_names)]
+    step_row = np.stack([g.row_of(t0) + a * n_exp for a, g in enumerate(grids)])
+    C = np.full((n_names, n_names), corr) + (1.0 - corr) * np.eye(n_names)
+    spots = np.full(n_names, m.spot)
+    held = mc_request(
+        model=OB_MODEL_PATHS,
+        dt=dt,
+        t0=t0,
+        spot=spots,
+        n_pairs=n_paths // 2,
+        seed=seed,
+        root=correlation_root(C),
+        kind=np.ones(n_names, np.int32),
+        cvar=np.zeros(n_names),
+        log_fwd=np.tile(m.log_fwd(t_end), (n_names, 1)),
+        step_row=step_row,
+        lo=np.concatenate([g.lo for g in grids]),
+        inv_dx=np.concatenate([g.inv_dx for g in grids]),
+        table=np.vstack([g.rows for g in grids]),
+        n_x=n_x,
+        **autocall_fields(ph, m, steps_per_year),
+    )
+    return WorstOf(
+        held,
+        np.repeat(np.arange(n_names), n_exp),
+        np.tile(T, n_names),
+        np.concatenate([g.lo for g in grids]),
+        np.concatenate([g.inv_dx for g in grids]),
+        n_x,
+        years * np.arange(1, n_node_T + 1) / n_node_T,
+        np.linspace(-1.0, 0.5, n_node_k),
+        spots,
+    )

@@ -893,3 +893,108 @@ int or_leverage(ob_leverage_request* s) {
     free(x), free(v), free(fine), free(acc), free(x_eval), free(cond), free(lev), free(centres);
     return OB_OK;
 }
+
+/* ------------------------------------------------------------------------------------------- smoothed autocall
+ * The autocall above with its digitals smoothed as the reference's script evaluator does for Greeks
+ * (packages/structured/src/optlab/structured/script/evaluator.py:93-107, 185-220): a >= b becomes
+ * clip((a - b) / (eps |b|) + 1/2, 0, 1), a < b clip((b - a) / (eps |b|) + 1/2, 0, 1); inside an `if` a payment is
+ * weighted by the mask times the alive mass, an assignment becomes m e + (1 - m) old, and `terminate` multiplies the
+ * alive mass by 1 - m. Price only, on the path engine's local vol (or any kind), for the adjoint's checks. */
+
+static double ramp_ge(double a, double b, double eps) {
+    if (eps <= 0.0) return a >= b ? 1.0 : 0.0;
+    const double t = (a - b) / (eps * fabs(b)) + 0.5;
+    return t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+}
+static double ramp_lt(double a, double b, double eps) {
+    if (eps <= 0.0) return a < b ? 1.0 : 0.0;
+    const double t = (b - a) / (eps * fabs(b)) + 0.5;
+    return t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+}
+
+static double smooth_leg(const ob_mc_request* rq, double eps, const double* perf, double low) {
+    double pv = 0.0, alive = 1.0, missed = 0.0;
+    const int has_coupon = rq->coupon > 0.0 || rq->coupon_barrier > 0.0;
+    for (int j = 0; j < rq->n_obs; ++j) {
+        const double p = perf[j], D = rq->obs_discount[j];
+        if (has_coupon) {
+            const double c = ramp_ge(p, rq->coupon_barrier, eps);
+            const double mult = rq->memory ? 1.0 + missed : 1.0;
+            pv += D * rq->coupon * mult * c * alive;
+            missed = rq->memory ? (1.0 - c) * (missed + 1.0) : 0.0;
+        }
+        if (j < rq->n_obs - 1) {
+            const double q = rq->trigger[j] > 0.0 ? ramp_ge(p, rq->trigger[j], eps) : 0.0;
+            pv += D * q * alive;
+            alive *= 1.0 - q;
+        } else {
+            const double k = ramp_lt(rq->ki_daily ? low : p, rq->ki_barrier, eps);
+            const double put = rq->put_strike - p > 0.0 ? rq->put_strike - p : 0.0;
+            pv += D * alive * (1.0 - k * put);
+        }
+    }
+    return pv;
+}
+
+typedef struct {
+    const ob_mc_request* rq;
+    Model m;
+    double eps;
+} SmoothCtx;
+
+static void smooth_block(const void* vctx, long long blk, void* vpartial) {
+    const SmoothCtx* c = (const SmoothCtx*)vctx;
+    const ob_mc_request* rq = c->rq;
+    double* part = (double*)vpartial;
+    part[0] = part[1] = 0.0;
+    const long long p0 = blk * OR_BLOCK, p1 = p0 + OR_BLOCK < rq->n_pairs ? p0 + OR_BLOCK : rq->n_pairs;
+    double* perf = (double*)malloc((size_t)2 * rq->n_obs * sizeof(double));
+    if (!perf) return;
+    for (long long p = p0; p < p1; ++p) {
+        PairState s;
+        pair_init(&c->m, &s, (uint64_t)(rq->first_pair + p));
+        double low[2] = {1.0, 1.0};
+        int j = 0;
+        for (int i = 1; i <= rq->n_steps; ++i) {
+            pair_step(&c->m, &s, i);
+            for (int leg = 0; leg < 2; ++leg) {
+                double w = INFINITY;
+                for (int a = 0; a < rq->n_names; ++a) {
+                    const double q = exp(rq->log_fwd[a * (rq->n_steps + 1) + i] + s.x[leg][a]);
+                    w = q < w ? q : w;
+                }
+                low[leg] = w < low[leg] ? w : low[leg];
+                if (j < rq->n_obs && rq->obs_step[j] == i) perf[leg * rq->n_obs + j] = w;
+            }
+            if (j < rq->n_obs && rq->obs_step[j] == i) ++j;
+        }
+        const double y = 0.5 * (smooth_leg(rq, c->eps, perf, low[0]) + smooth_leg(rq, c->eps, perf + rq->n_obs, low[1]));
+        part[0] += y, part[1] += y * y;
+    }
+    free(perf);
+}
+
+int or_autocall_smooth(const ob_mc_request* rq, double eps, int n_threads, ob_mc_result* res) {
+    const int st = check_mc(rq);
+    if (st) return st;
+    if (rq->product != OB_PRODUCT_AUTOCALL || rq->model != OB_MODEL_PATHS) return fail("a path-engine autocall only");
+    SmoothCtx c;
+    memset(&c, 0, sizeof c);
+    c.rq = rq, c.eps = eps;
+    c.m.n_names = rq->n_names, c.m.n_steps = rq->n_steps, c.m.n_x = rq->n_x, c.m.seed = rq->seed;
+    c.m.dt = rq->dt, c.m.t0 = rq->t0, c.m.root = rq->root, c.m.cvar = rq->cvar, c.m.hes = rq->heston;
+    c.m.lo = rq->row_lo, c.m.inv_dx = rq->row_inv_dx, c.m.table = rq->table, c.m.kind = rq->kind;
+    c.m.step_row = rq->step_row, c.m.same = rq->same;
+    const long long n_blocks = (rq->n_pairs + OR_BLOCK - 1) / OR_BLOCK;
+    double* parts = (double*)calloc((size_t)n_blocks * 2, sizeof(double));
+    if (!parts) return fail("out of memory");
+    run_blocks(smooth_block, &c, n_blocks, parts, 2 * sizeof(double), n_threads);
+    double s = 0.0, s2 = 0.0;
+    for (long long b = 0; b < n_blocks; ++b) s += parts[2 * b], s2 += parts[2 * b + 1];
+    free(parts);
+    memset(res, 0, sizeof *res);
+    const double n = (double)rq->n_pairs, mean = s / n;
+    res->n_out = 1, res->n_paths = 2 * rq->n_pairs;
+    res->price[0] = mean, res->se[0] = sqrt(fmax(s2 / n - mean * mean, 0.0) / (n - 1.0));
+    return OB_OK;
+}

@@ -53,6 +53,7 @@ class Oracle:
         lib.or_mc_price.argtypes = [C.POINTER(ObMcRequest), C.c_int, C.POINTER(ObMcResult)]
         lib.or_price.argtypes = [C.POINTER(ObRequest), C.c_int, C.POINTER(ObResult)]
         lib.or_leverage.argtypes = [C.POINTER(ObLeverageRequest)]
+        lib.or_autocall_smooth.argtypes = [C.POINTER(ObMcRequest), C.c_double, C.c_int, C.POINTER(ObMcResult)]
         lib.or_philox_normals.argtypes = [
             C.c_ulonglong,
             C.c_longlong,
@@ -77,6 +78,12 @@ class Oracle:
         res = ObMcResult()
         self._check(self.lib.or_mc_price(held.ref(), int(threads) or _cores(), C.byref(res)))
         return res
+
+    def autocall_smooth(self, held, eps: float, threads: int = 0):
+        """(price, SE) of the smoothed autocall (the reference evaluator's ramps of relative width eps)."""
+        res = ObMcResult()
+        self._check(self.lib.or_autocall_smooth(held.ref(), float(eps), int(threads) or _cores(), C.byref(res)))
+        return res.price[0], res.se[0]
 
     def price(self, rq: ObRequest, threads: int = 0) -> ObResult:
         res = ObResult()

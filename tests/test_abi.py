@@ -56,6 +56,8 @@ PAIRS = {
     "ob_leverage_request": _abi.ObLeverageRequest,
     "ob_mc_request": _abi.ObMcRequest,
     "ob_mc_result": _abi.ObMcResult,
+    "ob_adjoint_request": _abi.ObAdjointRequest,
+    "ob_adjoint_result": _abi.ObAdjointResult,
 }
 
 
