@@ -226,7 +226,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint"])
+    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint", "batch"])
+    ap.add_argument("--trades", type=int, default=512, help="batch workload: trades in the book")
     ap.add_argument("--paths", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -241,6 +242,8 @@ def main():
         return run_reference(args, world, rank)
     if args.workload == "adjoint":
         return run_adjoint(args, world, rank)
+    if args.workload == "batch":
+        return run_batch(args, world, rank)
 
     import torch
 
@@ -440,6 +443,111 @@ def run_adjoint(args, world, rank):
         "gpu_launches": 2 * args.steps,
     }
     print(json.dumps(line))
+
+
+def run_batch(args, world, rank):
+    """cfg4: the seeded book (512 trades, 60 scenarios) revalued by one replay of the captured graph, FP32 paths with
+    FP64 sums; against the same simulations as one launch per trade simulation. Units: name-path-steps simulated
+    (2 paths per pair x steps x names, over the base and the vol-scenario simulations; spot moves ride on the base
+    simulation). One rank: the book is one job (more GPUs would split its trades)."""
+    import torch
+
+    from optlab_b200.batch import Batch, sample_book
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    book = sample_book(n_trades=args.trades)
+    units = book.path_steps()
+    t0 = time.perf_counter()
+    b = Batch(book, "fp32")
+    t_create = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b.tune()
+    t_tune = time.perf_counter() - t0
+    b.capture()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        flush.zero_()
+        b.launch(stream)
+        b.result()
+    ms = []
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            b.launch(stream)
+            ms.append(b.result()[2])
+    price, se, _ = b.result()
+    per_trade = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush.zero_()
+        b.run_per_trade(stream)
+        per_trade.append(b.result()[2])
+    b.close()
+    # end to end: the public calls from host arrays (upload, one direct run, read back the values)
+    e2e = []
+    for _ in range(max(1, min(args.steps, 2))):
+        t = time.perf_counter()
+        with Batch(book, "fp32") as g:
+            g.launch()
+            g.result()
+        e2e.append(time.perf_counter() - t)
+    h2d = sum(getattr(book, k).nbytes for k in ("table", "row_lo", "row_inv_dx", "root", "leg_type", "leg_strike",
+                                                  "leg_barrier", "leg_level", "obs_step", "obs_trigger",
+                                                  "obs_discount", "spot_shift", "vol_shift", "vol_tilt"))
+    h2d += book.n_trades * ctypes_sizeof_trade()
+    n_sims = book.simulations()
+    t_step = statistics.median(ms) / 1e3
+    t_pt = statistics.median(per_trade) / 1e3
+    cpu = None
+    if not args.no_cpu_baseline:
+        n_s = 2**18
+        secs, kind, cores, detail = cpu_reference_sample("lv_phoenix", n_s, os.cpu_count() or 1)
+        cpu = {"value": n_s * 756 / secs, "unit": "path-steps/s", "cores": cores, "kind": kind,
+               "sample": f"{n_s} paths x 756 steps of the local-vol Phoenix, the book's dominant kind of simulation "
+               f"({detail})"}
+    clk = clocks.summary()
+    line = {
+        "metric": "path-steps/s",
+        "value": units / t_step,
+        "unit": "path-steps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_step * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded book, SSVI surfaces and Heston parameters)",
+        "config": {"workload": "batch_revaluation", "trades": book.n_trades, "scenarios": book.n_scenarios - 1,
+                   "simulations": n_sims, "revaluations": book.revaluations(), "path_steps": units,
+                   "l2": "flushed between steps (512 MB write); the book's paths are far larger than L2"},
+        "revaluations_per_s": book.revaluations() / t_step,
+        "per_trade_launches": {"ms_per_step": t_pt * 1e3, "path_steps_per_s": units / t_pt,
+                               "speedup_of_graph": t_pt / t_step, "launches": n_sims},
+        "autotune": {"seconds": t_tune, "create_seconds": t_create},
+        "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": "Gwarp-inst/s", "frac": None,
+                     "traffic": None, "note": "see the lv_phoenix line: the same FP32/SFU issue-bound stepping"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": units / statistics.median(e2e), "unit": "path-steps/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": n_sims * 32 * 2 * 8, "seconds_per_call": statistics.median(e2e)},
+        "gpu_launches": args.steps * (1 + len({(t.model, t.n_names, t.product) for t in book.trades})),
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "result": {"mean_base_price": float(price[:, 0].mean()), "median_se": float(np.median(se[:, 0]))},
+    }
+    print(json.dumps(line))
+
+
+def ctypes_sizeof_trade() -> int:
+    import ctypes
+
+    from optlab_b200._abi import ObBatchTrade
+
+    return ctypes.sizeof(ObBatchTrade)
 
 
 def run_reference(args, world, rank):

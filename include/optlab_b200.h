@@ -213,6 +213,57 @@ typedef struct {
 
 typedef struct ob_adjoint_plan ob_adjoint_plan;
 
+/* ---------------------------------------------------------------------------------------------- batched risk */
+
+/* One trade of a revaluation batch. Local-vol trades (model OB_MODEL_PATHS) have 1 to 5 names, each a block of
+   n_exp table rows of the batch's pool starting at table_row0 + a n_exp; Heston trades (OB_MODEL_HESTON_QE) one name.
+   Ladder legs and autocall schedules are read from the pools at leg0 / obs0; strikes, barrier levels, triggers and
+   the knock-in are fractions of the initial spot, applied to the worst performance of the names. */
+typedef struct {
+    int model, product, n_names, n_steps;
+    long long n_pairs;
+    unsigned long long seed;
+    int table_row0, root0;
+    double heston[5];
+    double r, q;
+    int n_legs, leg0;
+    int n_obs, obs0;
+    double coupon_barrier, coupon, ki_barrier, put_strike;
+    int memory, ki_daily;
+    double discount;
+} ob_batch_trade;
+
+/* The batch: trades, pools and scenarios. Every trade steps by dt; a local-vol table row j of a trade is the
+   expiry horizon (j + 1) / n_exp, read by steps starting before it (the first expiry after a step's start). The
+   scenarios of each trade: the base, then n_spot relative spot moves (evaluated on the base simulation: the local vol
+   is in log-moneyness, so a spot move scales the paths), then n_vol moves of local volatility sigma(k) + shift +
+   tilt k (floored at 1 %), each a simulation on the same random numbers (Heston trades do not move under them, as
+   the reference's Heston model ignores the surface). */
+typedef struct {
+    int n_trades;
+    const ob_batch_trade* trades;
+    double dt, horizon;
+    int n_exp, n_x;
+    const double* table;       /* pool rows x n_x: local variance */
+    const double* row_lo;      /* pool rows */
+    const double* row_inv_dx;  /* pool rows */
+    const double* root;        /* pool of correlation roots */
+    const int* leg_type;
+    const double* leg_strike;
+    const int* leg_barrier;
+    const double* leg_level;
+    const int* obs_step;
+    const double* obs_trigger;
+    const double* obs_discount;
+    int n_spot;
+    const double* spot_shift;
+    int n_vol;
+    const double* vol_shift;
+    const double* vol_tilt;
+} ob_batch_request;
+
+typedef struct ob_batch ob_batch;
+
 /* ---------------------------------------------------------------------------------------------- entry points */
 
 const char* ob_last_error(void);
@@ -274,6 +325,21 @@ int ob_adjoint_plan_create(const ob_adjoint_request* rq, int precision, ob_adjoi
 int ob_adjoint_run(ob_adjoint_plan* plan, const double* d_table, double* d_grad, void* stream);
 int ob_adjoint_result_get(ob_adjoint_plan* plan, ob_adjoint_result* res, long long* batch_pairs);
 int ob_adjoint_plan_destroy(ob_adjoint_plan* plan);
+
+/* Batched risk revaluation: no counterpart in the reference ABI; it replaces the per-shock simulations of
+   packages/risk/src/optlab/risk/engine.py:382-425,563-644 for a book of trades. create checks and uploads the batch;
+   tune times candidate tiles (pairs per work item) and block sizes on a sample of each trade class's work and keeps
+   the fastest (budget_ms bounds its time; 0: the defaults); capture records one run (every class's persistent kernel
+   on its own stream, then the reduction) as a CUDA graph; launch replays it on `stream` (or runs the kernels directly
+   without a capture); run_per_trade runs the same work as one launch per trade simulation, the comparison; result
+   waits and writes price and se (n_trades x (1 + n_spot + n_vol), row-major) and the last run's device time. */
+int ob_batch_create(const ob_batch_request* rq, int precision, ob_batch** batch);
+int ob_batch_tune(ob_batch* batch, int budget_ms);
+int ob_batch_capture(ob_batch* batch, void* stream);
+int ob_batch_launch(ob_batch* batch, void* stream);
+int ob_batch_run_per_trade(ob_batch* batch, void* stream);
+int ob_batch_result(ob_batch* batch, double* price, double* se, double* device_ms);
+int ob_batch_destroy(ob_batch* batch);
 
 #ifdef __cplusplus
 }

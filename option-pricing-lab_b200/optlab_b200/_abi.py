@@ -230,6 +230,60 @@ class ObAdjointResult(C.Structure):
     ]
 
 
+class ObBatchTrade(C.Structure):
+    _fields_ = [
+        ("model", C.c_int),
+        ("product", C.c_int),
+        ("n_names", C.c_int),
+        ("n_steps", C.c_int),
+        ("n_pairs", C.c_longlong),
+        ("seed", C.c_ulonglong),
+        ("table_row0", C.c_int),
+        ("root0", C.c_int),
+        ("heston", C.c_double * 5),
+        ("r", C.c_double),
+        ("q", C.c_double),
+        ("n_legs", C.c_int),
+        ("leg0", C.c_int),
+        ("n_obs", C.c_int),
+        ("obs0", C.c_int),
+        ("coupon_barrier", C.c_double),
+        ("coupon", C.c_double),
+        ("ki_barrier", C.c_double),
+        ("put_strike", C.c_double),
+        ("memory", C.c_int),
+        ("ki_daily", C.c_int),
+        ("discount", C.c_double),
+    ]
+
+
+class ObBatchRequest(C.Structure):
+    _fields_ = [
+        ("n_trades", C.c_int),
+        ("trades", C.POINTER(ObBatchTrade)),
+        ("dt", C.c_double),
+        ("horizon", C.c_double),
+        ("n_exp", C.c_int),
+        ("n_x", C.c_int),
+        ("table", _dp),
+        ("row_lo", _dp),
+        ("row_inv_dx", _dp),
+        ("root", _dp),
+        ("leg_type", _ip),
+        ("leg_strike", _dp),
+        ("leg_barrier", _ip),
+        ("leg_level", _dp),
+        ("obs_step", _ip),
+        ("obs_trigger", _dp),
+        ("obs_discount", _dp),
+        ("n_spot", C.c_int),
+        ("spot_shift", _dp),
+        ("n_vol", C.c_int),
+        ("vol_shift", _dp),
+        ("vol_tilt", _dp),
+    ]
+
+
 # Every symbol include/optlab_b200.h declares, with its ctypes signature (restype, argtypes).
 SIGNATURES = {
     "ob_last_error": (C.c_char_p, []),
@@ -265,6 +319,13 @@ SIGNATURES = {
     "ob_adjoint_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ob_adjoint_result_get": (C.c_int, [C.c_void_p, C.POINTER(ObAdjointResult), C.POINTER(C.c_longlong)]),
     "ob_adjoint_plan_destroy": (C.c_int, [C.c_void_p]),
+    "ob_batch_create": (C.c_int, [C.POINTER(ObBatchRequest), C.c_int, C.POINTER(C.c_void_p)]),
+    "ob_batch_tune": (C.c_int, [C.c_void_p, C.c_int]),
+    "ob_batch_capture": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ob_batch_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ob_batch_run_per_trade": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ob_batch_result": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "ob_batch_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _lib: list = []

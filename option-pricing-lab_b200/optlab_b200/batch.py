@@ -1,0 +1,298 @@
+"""Batched risk revaluation: a seeded book of uneven trades, each revalued under spot, parallel-vol and skew scenarios,
+in one replay of a CUDA graph of persistent kernels (csrc/batch.cu through ob_batch_*).
+
+The reference revalues a book group by group and scenario by scenario (packages/risk/src/optlab/risk/engine.py:382-425:
+every shock that moves the model is its own simulation on the group's seed; :563-644: shocks that move only the spot
+share the base simulation as factors on its paths). `Batch` keeps that split: per trade one base simulation carries
+the base and every spot move, and each vol or skew move is one more simulation on the same random numbers; all of
+them are work items of the same launch.
+
+`sample_book` draws the benchmark's book: 512 trades of 1 to 5 names, 1 to 5 years of daily steps, 2^14 to 2^18 paths,
+European, barrier or autocall payoffs (worst-of with several names), under Heston QE or local vol of per-name SSVI
+surfaces, with 60 scenarios: 20 spot moves of +-1..20 %, 20 parallel moves of local vol of +-1..10 points, 20 skew
+tilts of +-1..10 points per unit of log-moneyness.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from ._abi import (
+    BARRIER,
+    OB_MODEL_HESTON_QE,
+    OB_MODEL_PATHS,
+    OB_PRODUCT_AUTOCALL,
+    OB_PRODUCT_LADDER,
+    ObBatchRequest,
+    ObBatchTrade,
+    check,
+    load,
+)
+from .engine import precision_code
+from .models import correlation_root
+from .surfaces import SSVI, LocalVarGrid
+
+_STEPS = np.array([0.01, 0.02, 0.03, 0.04, 0.05, 0.075, 0.10, 0.125, 0.15, 0.20])
+SPOT_MOVES = np.concatenate([-_STEPS[::-1], _STEPS])
+VOL_SHIFTS = np.concatenate([-np.arange(10, 0, -1), np.arange(1, 11)]) / 100.0
+SKEW_TILTS = VOL_SHIFTS.copy()
+MAX_OBS = 64
+MAX_SPOT = 31
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+@dataclass
+class Book:
+    """Trades, their pools and the scenarios, held for the C ABI (the arrays stay alive with the book)."""
+
+    trades: list
+    labels: list
+    dt: float
+    horizon: float
+    n_exp: int
+    n_x: int
+    table: np.ndarray
+    row_lo: np.ndarray
+    row_inv_dx: np.ndarray
+    root: np.ndarray
+    leg_type: np.ndarray
+    leg_strike: np.ndarray
+    leg_barrier: np.ndarray
+    leg_level: np.ndarray
+    obs_step: np.ndarray
+    obs_trigger: np.ndarray
+    obs_discount: np.ndarray
+    spot_shift: np.ndarray
+    vol_shift: np.ndarray
+    vol_tilt: np.ndarray
+    struct: ObBatchRequest = field(init=False)
+
+    def __post_init__(self):
+        for k in ("table", "row_lo", "row_inv_dx", "root", "leg_strike", "leg_level", "obs_trigger", "obs_discount",
+                  "spot_shift", "vol_shift", "vol_tilt"):
+            setattr(self, k, _arr(getattr(self, k), np.float64).ravel())
+        for k in ("leg_type", "leg_barrier", "obs_step"):
+            setattr(self, k, _arr(getattr(self, k), np.int32).ravel())
+        self._trades = (ObBatchTrade * len(self.trades))(*self.trades)
+        s = ObBatchRequest()
+        s.n_trades = len(self.trades)
+        s.trades = self._trades
+        s.dt, s.horizon, s.n_exp, s.n_x = self.dt, self.horizon, self.n_exp, self.n_x
+        for k in ("table", "row_lo", "row_inv_dx", "root", "leg_strike", "leg_level", "obs_trigger", "obs_discount",
+                  "spot_shift", "vol_shift", "vol_tilt"):
+            a = getattr(self, k)
+            setattr(s, k, a.ctypes.data_as(_dp) if a.size else None)
+        for k in ("leg_type", "leg_barrier", "obs_step"):
+            a = getattr(self, k)
+            setattr(s, k, a.ctypes.data_as(_ip) if a.size else None)
+        s.n_spot, s.n_vol = len(self.spot_shift), len(self.vol_shift)
+        self.struct = s
+
+    @property
+    def n_trades(self) -> int:
+        return len(self.trades)
+
+    @property
+    def n_spot(self) -> int:
+        return len(self.spot_shift)
+
+    @property
+    def n_vol(self) -> int:
+        return len(self.vol_shift)
+
+    @property
+    def n_scenarios(self) -> int:
+        return 1 + self.n_spot + self.n_vol
+
+    def simulations(self) -> int:
+        """Simulations of one revaluation: per trade the base, and under local vol one per vol scenario."""
+        return sum(1 + (self.n_vol if t.model == OB_MODEL_PATHS else 0) for t in self.trades)
+
+    def path_steps(self) -> int:
+        """Name-path-steps of one revaluation: 2 paths per pair x steps x names over every simulation."""
+        return sum(2 * t.n_pairs * t.n_steps * t.n_names * (1 + (self.n_vol if t.model == OB_MODEL_PATHS else 0))
+                   for t in self.trades)
+
+    def revaluations(self) -> int:
+        """(trade, scenario) values of one revaluation."""
+        return self.n_trades * self.n_scenarios
+
+
+def _surfaces(rng, n_names, horizon, n_exp, n_x):
+    """Per-name SSVI power-law surfaces (theta_t = c t, c in 0.03..0.06, rho in -0.7..-0.4, eta 1, gamma 0.5)
+    tabulated as local variance on n_exp expiries x n_x log-strikes over the horizon."""
+    T = horizon * np.arange(1, n_exp + 1) / n_exp
+    grids = []
+    for _ in range(n_names):
+        c, rho = rng.uniform(0.03, 0.06), rng.uniform(-0.7, -0.4)
+        grids.append(LocalVarGrid.from_surface(SSVI.power_law(rho, 1.0, 0.5, T, c * T), T, n_x))
+    return grids
+
+
+def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), years=(1, 5), steps_per_year: int = 252,
+                max_names: int = 5, heston_share: float = 0.25, n_surfaces: int = 16, n_exp: int = 40, n_x: int = 200,
+                spot_moves=SPOT_MOVES, vol_shifts=VOL_SHIFTS, skew_tilts=SKEW_TILTS) -> Book:
+    """A seeded book of uneven trades. Each trade: Heston QE (one name, heston_share of the book) or local vol of
+    1..max_names consecutive names of a pool of per-name surfaces; maturity a whole number of years in `years`, one
+    step a day; 2^k paths with k uniform in paths_log2; a European ladder (1 to 3 calls or puts), a barrier option
+    (up-and-out or up-and-in call, down-and-in or down-and-out put), or a Phoenix autocall (quarterly or monthly),
+    each on the worst performance of its names. Scenarios: the spot moves, then the parallel vol shifts, then the
+    skew tilts (a vol scenario is a (shift, tilt) pair: (s, 0) or (0, t))."""
+    rng = np.random.default_rng(seed)
+    horizon = float(years[1])
+    dt = 1.0 / steps_per_year
+    grids = _surfaces(rng, n_surfaces, horizon, n_exp, n_x)
+    table = np.vstack([g.rows for g in grids])
+    row_lo = np.concatenate([g.lo for g in grids])
+    row_inv = np.concatenate([g.inv_dx for g in grids])
+    root, legs, obs = [], [], []
+    trades, labels = [], []
+    r = 0.02
+    for _ in range(n_trades):
+        heston = rng.random() < heston_share
+        n = 1 if heston else int(rng.integers(1, max_names + 1))
+        T = int(rng.integers(years[0], years[1] + 1))
+        k = int(rng.integers(paths_log2[0], paths_log2[1] + 1))
+        product = ("european", "barrier", "autocall")[int(rng.integers(0, 3))]
+        t = ObBatchTrade()
+        t.model = OB_MODEL_HESTON_QE if heston else OB_MODEL_PATHS
+        t.n_names, t.n_steps, t.n_pairs = n, T * steps_per_year, 2 ** (k - 1)
+        t.seed = int(rng.integers(1, 2**62))
+        t.r, t.q = r, float(rng.uniform(0.0, 0.02))
+        if heston:
+            t.heston[:] = [rng.uniform(0.02, 0.06), rng.uniform(1.0, 3.0), rng.uniform(0.02, 0.06),
+                           rng.uniform(0.3, 0.7), rng.uniform(-0.8, -0.4)]
+        else:
+            first = int(rng.integers(0, n_surfaces - n + 1))
+            t.table_row0 = first * n_exp
+            rho = rng.uniform(0.3, 0.8)
+            corr = np.full((n, n), rho) + (1.0 - rho) * np.eye(n)
+            t.root0 = sum(len(x) for x in root)
+            root.append(np.asarray(correlation_root(corr), dtype=float).ravel())
+            t.heston[:] = [0.04, 1.0, 0.04, 0.5, 0.0]
+        if product in ("european", "barrier"):
+            t.product = OB_PRODUCT_LADDER
+            t.discount = float(np.exp(-r * T))
+            if product == "european":
+                m = int(rng.integers(1, 4))
+                rows = [(int(rng.integers(1, 3)), rng.uniform(0.8, 1.2), 0, 0.0) for _ in range(m)]
+            else:
+                kind = int(rng.integers(0, 4))
+                K = rng.uniform(0.9, 1.1)
+                if kind == 0:
+                    rows = [(1, K, BARRIER["up-out"], rng.uniform(1.2, 1.5))]
+                elif kind == 1:
+                    rows = [(1, K, BARRIER["up-in"], rng.uniform(1.2, 1.5))]
+                elif kind == 2:
+                    rows = [(2, K, BARRIER["down-in"], rng.uniform(0.6, 0.8))]
+                else:
+                    rows = [(2, K, BARRIER["down-out"], rng.uniform(0.6, 0.8))]
+            t.n_legs, t.leg0 = len(rows), sum(len(x) for x in legs)
+            legs.append(rows)
+        else:
+            t.product = OB_PRODUCT_AUTOCALL
+            per_year = 4 if rng.random() < 0.6 else 12
+            n_obs = T * per_year
+            steps = (np.arange(1, n_obs + 1) * steps_per_year) // per_year
+            times = np.arange(1, n_obs + 1) / per_year
+            trig = np.full(n_obs, 1.0)
+            trig[-1] = 0.0
+            t.n_obs, t.obs0 = n_obs, sum(len(x) for x in obs)
+            obs.append(list(zip(steps, trig, np.exp(-r * times))))
+            t.coupon_barrier = rng.uniform(0.6, 0.8)
+            t.coupon = rng.uniform(0.02, 0.10) / per_year
+            t.ki_barrier, t.put_strike = rng.uniform(0.5, 0.7), 1.0
+            t.memory, t.ki_daily = int(rng.random() < 0.5), int(rng.random() < 0.7)
+        trades.append(t)
+        labels.append(f"{'heston' if heston else 'lv'}-{n}-{product}-{T}y-2^{k}")
+    legs_flat = [x for rows in legs for x in rows] or [(0, 0.0, 0, 0.0)]
+    obs_flat = [x for rows in obs for x in rows] or [(1, 0.0, 1.0)]
+    vs = np.concatenate([np.asarray(vol_shifts, float), np.zeros(len(skew_tilts))])
+    vt = np.concatenate([np.zeros(len(vol_shifts)), np.asarray(skew_tilts, float)])
+    return Book(
+        trades=trades,
+        labels=labels,
+        dt=dt,
+        horizon=horizon,
+        n_exp=n_exp,
+        n_x=n_x,
+        table=table,
+        row_lo=row_lo,
+        row_inv_dx=row_inv,
+        root=np.concatenate(root) if root else np.ones(1),
+        leg_type=[x[0] for x in legs_flat],
+        leg_strike=[x[1] for x in legs_flat],
+        leg_barrier=[x[2] for x in legs_flat],
+        leg_level=[x[3] for x in legs_flat],
+        obs_step=[x[0] for x in obs_flat],
+        obs_trigger=[x[1] for x in obs_flat],
+        obs_discount=[x[2] for x in obs_flat],
+        spot_shift=np.asarray(spot_moves, float),
+        vol_shift=vs,
+        vol_tilt=vt,
+    )
+
+
+class Batch:
+    """A book uploaded for revaluation: tune picks tiles and block sizes per trade class, capture records the whole
+    revaluation as one CUDA graph, launch replays it (or runs it directly before a capture); run_per_trade runs the
+    same simulations as one launch each, the comparison."""
+
+    def __init__(self, book: Book, precision="fp32"):
+        self.book = book
+        self._p = C.c_void_p()
+        check(load().ob_batch_create(C.byref(book.struct), precision_code(precision), C.byref(self._p)))
+
+    def tune(self, budget_ms: int = 0) -> None:
+        check(load().ob_batch_tune(self._p, int(budget_ms)))
+
+    def capture(self, stream=None) -> None:
+        check(load().ob_batch_capture(self._p, _stream(stream)))
+
+    def launch(self, stream=None) -> None:
+        check(load().ob_batch_launch(self._p, _stream(stream)))
+
+    def run_per_trade(self, stream=None) -> None:
+        check(load().ob_batch_run_per_trade(self._p, _stream(stream)))
+
+    def result(self):
+        """(price, se) as (n_trades, 1 + n_spot + n_vol) arrays, and the last run's device time in ms."""
+        b = self.book
+        price = np.empty((b.n_trades, b.n_scenarios))
+        se = np.empty_like(price)
+        ms = C.c_double()
+        check(load().ob_batch_result(self._p, price.ctypes.data_as(_dp), se.ctypes.data_as(_dp), C.byref(ms)))
+        return price, se, ms.value
+
+    def close(self) -> None:
+        if self._p:
+            load().ob_batch_destroy(self._p)
+            self._p = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 (interpreter shutdown)
+            pass
+
+
+def _stream(stream):
+    if stream is None:
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream) if torch.cuda.is_available() else None
+    return C.c_void_p(stream.cuda_stream)

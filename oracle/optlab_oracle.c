@@ -449,6 +449,8 @@ typedef struct {
     Model m;
     QeConsts qe;
     int n_out;
+    double ln_shift; /* a relative spot move ln(1 + move) on every performance, the start's included (0: none) */
+    int sum_legs;    /* ladder: output 0 is the sum of the legs (the value of a trade made of them) */
 } McCtx;
 
 typedef struct {
@@ -480,10 +482,10 @@ static void book_init(LegBook* b) {
 /* Performance of the basket (worst of S_a / S0_a) at grid point i of one leg. */
 static double worst_perf(const McCtx* c, const PairState* s, const double* y_qe, int leg, int i) {
     const ob_mc_request* rq = c->rq;
-    if (rq->model == OB_MODEL_HESTON_QE) return exp(y_qe[leg]);
+    if (rq->model == OB_MODEL_HESTON_QE) return exp(y_qe[leg] + c->ln_shift);
     double w = INFINITY;
     for (int a = 0; a < rq->n_names; ++a) {
-        const double p = exp(rq->log_fwd[a * (rq->n_steps + 1) + i] + s->x[leg][a]);
+        const double p = exp(rq->log_fwd[a * (rq->n_steps + 1) + i] + s->x[leg][a] + c->ln_shift);
         w = p < w ? p : w;
     }
     return w;
@@ -554,6 +556,7 @@ static void mc_block(const void* vctx, long long blk, void* vpartial) {
         double y[2] = {0.0, 0.0}, v[2];
         LegBook book[2];
         book_init(&book[0]), book_init(&book[1]);
+        book[0].low_perf = book[1].low_perf = exp(c->ln_shift);
         if (rq->model == OB_MODEL_HESTON_QE) {
             stream_init(&s.rng, pair, rq->seed, 0u);
             v[0] = v[1] = c->qe.v0;
@@ -574,6 +577,11 @@ static void mc_block(const void* vctx, long long blk, void* vpartial) {
         double o0[OB_MAX_OUT], o1[OB_MAX_OUT];
         book_outputs(c, &book[0], worst_perf(c, &s, y, 0, rq->n_steps), o0);
         book_outputs(c, &book[1], worst_perf(c, &s, y, 1, rq->n_steps), o1);
+        if (c->sum_legs && rq->product == OB_PRODUCT_LADDER) {
+            double t0 = 0.0, t1 = 0.0;
+            for (int k = 0; k < rq->n_legs; ++k) t0 += o0[k], t1 += o1[k];
+            o0[0] = t0, o1[0] = t1;
+        }
         for (int k = 0; k < c->n_out; ++k) {
             const double a = 0.5 * (o0[k] + o1[k]);
             part->s[k] += a, part->s[OB_MAX_OUT + k] += a * a;
@@ -618,12 +626,15 @@ static int check_mc(const ob_mc_request* rq) {
     return OB_OK;
 }
 
-int or_mc_price(const ob_mc_request* rq, int n_threads, ob_mc_result* res) {
+static int mc_price_shifted(const ob_mc_request* rq, double ln_shift, int sum_legs, int n_threads,
+                            ob_mc_result* res) {
     const int st = check_mc(rq);
     if (st) return st;
     McCtx c;
     memset(&c, 0, sizeof c);
     c.rq = rq;
+    c.ln_shift = ln_shift;
+    c.sum_legs = sum_legs;
     c.n_out = rq->product == OB_PRODUCT_LADDER ? rq->n_legs + 1 : 4;
     if (rq->model == OB_MODEL_HESTON_QE) {
         c.qe = qe_consts(rq->heston, rq->r, rq->q, rq->dt[0]);
@@ -651,6 +662,96 @@ int or_mc_price(const ob_mc_request* rq, int n_threads, ob_mc_result* res) {
         res->se[k] = rq->n_pairs > 1 ? sqrt(fmax(var, 0.0) / (n - 1.0)) : 0.0;
     }
     return OB_OK;
+}
+
+int or_mc_price(const ob_mc_request* rq, int n_threads, ob_mc_result* res) {
+    return mc_price_shifted(rq, 0.0, 0, n_threads, res);
+}
+
+/* ------------------------------------------------------------------------------------------- batched revaluation
+ * One trade of an ob_batch_request under each of its scenarios, every scenario its own simulation on the trade's
+ * seed: the trade as an ob_mc_request (spot 1, so that strikes and levels are fractions of the initial spot), a spot
+ * move as a shift ln(1 + move) of every performance (the reference's path factors, packages/risk/src/optlab/risk/
+ * engine.py:585-590), a vol move as the local-variance rows rebuilt as (max(sigma + shift + tilt k, 0.01))^2 at each
+ * node k, the Heston model unmoved by it (its parameters do not depend on the surface,
+ * packages/structured/src/optlab/structured/context.py:163-164). price and se: 1 + n_spot + n_vol values. */
+int or_batch_trade(const ob_batch_request* b, int trade, int n_threads, double* price, double* se) {
+    if (!b || trade < 0 || trade >= b->n_trades || !price || !se) return fail("bad batch trade");
+    const ob_batch_trade* t = &b->trades[trade];
+    const int S = t->n_steps, N = t->n_names, E = b->n_exp, X = b->n_x;
+    const int lv = t->model == OB_MODEL_PATHS;
+    double* dt = (double*)malloc(sizeof(double) * S);
+    double* t0 = (double*)malloc(sizeof(double) * S);
+    double* lf = (double*)malloc(sizeof(double) * N * (S + 1));
+    int* step_row = (int*)malloc(sizeof(int) * N * S);
+    double* table = (double*)malloc(sizeof(double) * (lv ? N * E * X : 1));
+    double* lo = (double*)malloc(sizeof(double) * N * E);
+    double* inv = (double*)malloc(sizeof(double) * N * E);
+    double spot[OB_MAX_NAMES], cvar[OB_MAX_NAMES], hes[5 * OB_MAX_NAMES];
+    int kind[OB_MAX_NAMES];
+    if (!dt || !t0 || !lf || !step_row || !table || !lo || !inv) return fail("out of memory");
+    for (int i = 0; i < S; ++i) {
+        dt[i] = b->dt, t0[i] = i * b->dt;
+        int j = 0;
+        while (j < E - 1 && b->horizon * (j + 1) / E <= t0[i] + 1e-12) ++j;
+        for (int a = 0; a < N; ++a) step_row[a * S + i] = a * E + j;
+    }
+    for (int a = 0; a < N; ++a) {
+        spot[a] = 1.0, cvar[a] = 0.0, kind[a] = 1;
+        for (int k = 0; k < 5; ++k) hes[5 * a + k] = t->heston[k];
+        for (int i = 0; i <= S; ++i) lf[a * (S + 1) + i] = (t->r - t->q) * (i * b->dt);
+        if (lv)
+            for (int e = 0; e < E; ++e) lo[a * E + e] = b->row_lo[t->table_row0 + a * E + e],
+                                        inv[a * E + e] = b->row_inv_dx[t->table_row0 + a * E + e];
+    }
+    ob_mc_request rq;
+    memset(&rq, 0, sizeof rq);
+    rq.model = t->model, rq.n_names = N, rq.n_steps = S, rq.n_pairs = t->n_pairs, rq.seed = t->seed;
+    rq.dt = dt, rq.t0 = t0, rq.spot = spot, rq.heston = hes, rq.r = t->r, rq.q = t->q;
+    if (lv) {
+        rq.root = b->root + t->root0, rq.kind = kind, rq.cvar = cvar, rq.same = 0, rq.log_fwd = lf;
+        rq.n_x = X, rq.n_rows = N * E, rq.step_row = step_row, rq.row_lo = lo, rq.row_inv_dx = inv, rq.table = table;
+    }
+    rq.product = t->product;
+    if (t->product == OB_PRODUCT_LADDER) {
+        rq.n_legs = t->n_legs, rq.leg_type = b->leg_type + t->leg0, rq.leg_strike = b->leg_strike + t->leg0;
+        rq.leg_barrier = b->leg_barrier + t->leg0, rq.leg_level = b->leg_level + t->leg0;
+        rq.discount = t->discount;
+    } else {
+        rq.n_obs = t->n_obs, rq.obs_step = b->obs_step + t->obs0, rq.obs_discount = b->obs_discount + t->obs0;
+        rq.trigger = b->obs_trigger + t->obs0, rq.coupon_barrier = t->coupon_barrier, rq.coupon = t->coupon;
+        rq.ki_barrier = t->ki_barrier, rq.put_strike = t->put_strike, rq.memory = t->memory;
+        rq.ki_daily = t->ki_daily;
+    }
+    int st = OB_OK;
+    const int n_sc = 1 + b->n_spot + b->n_vol;
+    for (int sc = 0; sc < n_sc && st == OB_OK; ++sc) {
+        const int vol = sc > b->n_spot ? sc - 1 - b->n_spot : -1;
+        if (vol >= 0 && !lv) { /* the Heston model ignores the surface */
+            price[sc] = price[0], se[sc] = se[0];
+            continue;
+        }
+        if (lv)
+            for (int r = 0; r < N * E; ++r) {
+                const double* src = b->table + (size_t)(t->table_row0 + r) * X;
+                const double dx = 1.0 / inv[r];
+                for (int k = 0; k < X; ++k) {
+                    double v = src[k];
+                    if (vol >= 0) {
+                        double sg = sqrt(v) + b->vol_shift[vol] + b->vol_tilt[vol] * (lo[r] + k * dx);
+                        sg = sg > 0.01 ? sg : 0.01;
+                        v = sg * sg;
+                    }
+                    table[(size_t)r * X + k] = v;
+                }
+            }
+        const double shift = sc >= 1 && sc <= b->n_spot ? log1p(b->spot_shift[sc - 1]) : 0.0;
+        ob_mc_result res;
+        st = mc_price_shifted(&rq, shift, 1, n_threads, &res);
+        if (st == OB_OK) price[sc] = res.price[0], se[sc] = res.se[0];
+    }
+    free(dt), free(t0), free(lf), free(step_row), free(table), free(lo), free(inv);
+    return st;
 }
 
 /* ------------------------------------------------------------------------------------------- fixed products

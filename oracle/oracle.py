@@ -22,6 +22,7 @@ if str(_PKG) not in sys.path:
     sys.path.insert(0, str(_PKG))
 
 from optlab_b200._abi import (  # noqa: E402
+    ObBatchRequest,
     ObLeverageRequest,
     ObMcRequest,
     ObMcResult,
@@ -65,6 +66,7 @@ class Oracle:
             _dp,
         ]
         lib.or_philox.argtypes = [C.POINTER(C.c_uint), C.c_uint, C.c_uint, C.POINTER(C.c_uint)]
+        lib.or_batch_trade.argtypes = [C.POINTER(ObBatchRequest), C.c_int, C.c_int, _dp, _dp]
         self.lib = lib
 
     def _check(self, st: int) -> None:
@@ -84,6 +86,15 @@ class Oracle:
         res = ObMcResult()
         self._check(self.lib.or_autocall_smooth(held.ref(), float(eps), int(threads) or _cores(), C.byref(res)))
         return res.price[0], res.se[0]
+
+    def batch_trade(self, book, trade: int, threads: int = 0):
+        """(price, se) of one trade of a batch under each of its scenarios (base, spot moves, vol moves), each
+        scenario its own simulation on the trade's seed."""
+        n = 1 + book.n_spot + book.n_vol
+        price, se = np.empty(n), np.empty(n)
+        self._check(self.lib.or_batch_trade(C.byref(book.struct), int(trade), int(threads) or _cores(),
+                                            price.ctypes.data_as(_dp), se.ctypes.data_as(_dp)))
+        return price, se
 
     def price(self, rq: ObRequest, threads: int = 0) -> ObResult:
         res = ObResult()

@@ -58,6 +58,8 @@ PAIRS = {
     "ob_mc_result": _abi.ObMcResult,
     "ob_adjoint_request": _abi.ObAdjointRequest,
     "ob_adjoint_result": _abi.ObAdjointResult,
+    "ob_batch_trade": _abi.ObBatchTrade,
+    "ob_batch_request": _abi.ObBatchRequest,
 }
 
 
