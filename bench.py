@@ -466,6 +466,7 @@ def run_batch(args, world, rank):
     t0 = time.perf_counter()
     b.tune()
     t_tune = time.perf_counter() - t0
+    shapes = b.classes()
     b.capture()
     stream = torch.cuda.current_stream()
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -529,7 +530,7 @@ def run_batch(args, world, rank):
         "revaluations_per_s": book.revaluations() / t_step,
         "per_trade_launches": {"ms_per_step": t_pt * 1e3, "path_steps_per_s": units / t_pt,
                                "speedup_of_graph": t_pt / t_step, "launches": n_sims},
-        "autotune": {"seconds": t_tune, "create_seconds": t_create},
+        "autotune": {"seconds": t_tune, "create_seconds": t_create, "classes": shapes},
         "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": "Gwarp-inst/s", "frac": None,
                      "traffic": None, "note": "see the lv_phoenix line: the same FP32/SFU issue-bound stepping"},
         "cpu_baseline": cpu,

@@ -339,6 +339,9 @@ int ob_batch_capture(ob_batch* batch, void* stream);
 int ob_batch_launch(ob_batch* batch, void* stream);
 int ob_batch_run_per_trade(ob_batch* batch, void* stream);
 int ob_batch_result(ob_batch* batch, double* price, double* se, double* device_ms);
+/* The trade classes (one persistent kernel each) and their current shapes: *n_classes, and for the first
+   max_classes of them 6 ints each in info: model, names, product, trades, tile (pairs per work item), block. */
+int ob_batch_classes(const ob_batch* batch, int max_classes, int* n_classes, int* info);
 int ob_batch_destroy(ob_batch* batch);
 
 #ifdef __cplusplus

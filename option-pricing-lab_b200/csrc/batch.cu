@@ -374,13 +374,13 @@ struct Batch {
     template <typename R>
     void build(const ob_batch_request& rq);
     void simulations();
-    void layout(BLayout& L, const std::vector<int>& tiles, int only_class = -1);
+    void layout(BLayout& L, const std::vector<int>& tiles, int only_class = -1, int max_sims = 0);
     template <typename R>
     void launch_class(const BLayout& L, int ci, cudaStream_t st, const int4* items, int n_items, int* counter,
                       int grid, int block);
     void run_all(cudaStream_t st);
     void reduce(const BLayout& L, cudaStream_t st);
-    double time_class(int ci, int tile, int block);
+    double time_class(int ci, int tile, int block, int max_sims);
     std::vector<int> tiles() const {
         std::vector<int> t;
         for (const auto& c : classes) t.push_back(c.tile);
@@ -579,21 +579,39 @@ void Batch::simulations() {
 }
 
 // Slots and items for per-class tiles. Items of a class go largest trade first, so that the persistent blocks end
-// together. With only_class, the items of that class alone (the autotuner's measure).
-void Batch::layout(BLayout& L, const std::vector<int>& tiles, int only_class) {
+// together. With only_class, the items of that class alone, and with max_sims > 0 of at most that many of its
+// simulations, evenly spread over its largest-first order (the autotuner's sample).
+void Batch::layout(BLayout& L, const std::vector<int>& tiles, int only_class, int max_sims) {
     L.arena.release();
     L.pt_items.clear(), L.pt_first.clear(), L.pt_count.clear(), L.pt_class.clear();
     L.tile_of_class = tiles;
     L.sim_tiles.assign(n_sims, 0), L.sim_slot.assign(n_sims, 0);
     L.n_slots = 0;
+    std::vector<char> keep(n_sims, 1);
+    if (only_class >= 0 && max_sims > 0) {
+        std::vector<int> sims;
+        std::vector<int> order = classes[only_class].trades;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return static_cast<double>(trades[a].n_steps) * trades[a].n_pairs >
+                   static_cast<double>(trades[b].n_steps) * trades[b].n_pairs;
+        });
+        for (int t : order)
+            for (int s = 0; s < (trades[t].model == OB_MODEL_PATHS ? 1 + n_vol : 1); ++s)
+                sims.push_back(sim_of_trade[t] + s);
+        if (static_cast<int>(sims.size()) > max_sims) {
+            std::fill(keep.begin(), keep.end(), 0);
+            for (int k = 0; k < max_sims; ++k)
+                keep[sims[static_cast<size_t>(static_cast<double>(k) * sims.size() / max_sims)]] = 1;
+        }
+    }
     for (int i = 0; i < n_trades; ++i) {
         const int tile = tiles[class_of_trade[i]];
         const int tl = static_cast<int>((trades[i].n_pairs + tile - 1) / tile);
         const int n_sim = trades[i].model == OB_MODEL_PATHS ? 1 + n_vol : 1;
         for (int s = 0; s < n_sim; ++s) {
             const int sim = sim_of_trade[i] + s;
-            L.sim_slot[sim] = L.n_slots, L.sim_tiles[sim] = tl;
-            if (only_class < 0 || class_of_trade[i] == only_class) L.n_slots += tl;
+            L.sim_slot[sim] = L.n_slots, L.sim_tiles[sim] = keep[sim] ? tl : 0;
+            if (only_class < 0 || class_of_trade[i] == only_class) L.n_slots += L.sim_tiles[sim];
         }
     }
     L.d_sim_slot = L.arena.put<int>(L.sim_slot.data(), L.sim_slot.size());
@@ -667,12 +685,13 @@ void Batch::run_all(cudaStream_t st) {
     last_layout = &main;
 }
 
-// Time of one class's whole work at a given tile and block (the autotuner's measure), in ms.
-double Batch::time_class(int ci, int tile, int block) {
+// Time of a sample of one class's work (at most max_sims of its simulations) at a given tile and block, in ms: the
+// autotuner's measure.
+double Batch::time_class(int ci, int tile, int block, int max_sims) {
     BLayout L;
     std::vector<int> t = tiles();
     t[ci] = tile;
-    layout(L, t, ci);
+    layout(L, t, ci, max_sims);
     BClass& c = classes[ci];
     cudaEvent_t a, b;
     check_cuda(cudaEventCreate(&a), "cudaEventCreate");
@@ -725,25 +744,28 @@ int ob_batch_create(const ob_batch_request* rq, int precision, ob_batch** batch)
     });
 }
 
-// The autotuner: for each class, every (tile, block) candidate is timed on the class's whole work (its real mix of
-// trades, largest first) and the fastest kept; past budget_ms the untried candidates are skipped.
+// The autotuner: for each class, every (tile, block) candidate is timed on the same sample of the class's work (up to
+// kTuneSims of its simulations, spread over its sizes: enough pairs to fill the GPU several times over) after one
+// untimed launch, and the fastest kept; past budget_ms the untried candidates are skipped.
 int ob_batch_tune(ob_batch* batch, int budget_ms) {
     return ob::guarded([&] {
         if (!batch) ob::invalid("null batch");
         ob::Batch& b = batch->impl;
         if (b.exec) ob::invalid("tune before capture");
+        constexpr int kTuneSims = 32;
         const auto t0 = std::chrono::steady_clock::now();
-        const int tiles[] = {1024, 4096, 16384};
+        const int tiles[] = {512, 1024, 2048, 4096, 8192, 16384};
         const int blocks[] = {128, 256};
         for (size_t ci = 0; ci < b.classes.size(); ++ci) {
             double best = 1e300;
             int bt = b.classes[ci].tile, bb = b.classes[ci].block;
+            b.time_class(static_cast<int>(ci), bt, bb, kTuneSims);  // warm: module load, caches
             for (int tile : tiles)
                 for (int block : blocks) {
                     const double el =
                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
                     if (budget_ms > 0 && el > budget_ms) continue;
-                    const double ms = b.time_class(static_cast<int>(ci), tile, block);
+                    const double ms = b.time_class(static_cast<int>(ci), tile, block, kTuneSims);
                     if (ms < best) best = ms, bt = tile, bb = block;
                 }
             b.classes[ci].tile = bt, b.classes[ci].block = bb;
@@ -867,6 +889,20 @@ int ob_batch_result(ob_batch* batch, double* price, double* se, double* device_m
             float ms = 0.0f;
             ob::check_cuda(cudaEventElapsedTime(&ms, b.e0, b.e1), "cudaEventElapsedTime");
             *device_ms = ms;
+        }
+    });
+}
+
+int ob_batch_classes(const ob_batch* batch, int max_classes, int* n_classes, int* info) {
+    return ob::guarded([&] {
+        if (!batch || !n_classes) ob::invalid("null argument");
+        const ob::Batch& b = batch->impl;
+        *n_classes = static_cast<int>(b.classes.size());
+        for (int k = 0; k < std::min(max_classes, *n_classes) && info; ++k) {
+            const ob::BClass& c = b.classes[k];
+            int* o = info + 6 * k;
+            o[0] = c.qe ? OB_MODEL_HESTON_QE : OB_MODEL_PATHS, o[1] = c.n, o[2] = c.product;
+            o[3] = static_cast<int>(c.trades.size()), o[4] = c.tile, o[5] = c.block;
         }
     });
 }

@@ -325,6 +325,7 @@ SIGNATURES = {
     "ob_batch_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ob_batch_run_per_trade": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ob_batch_result": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "ob_batch_classes": (C.c_int, [C.c_void_p, C.c_int, _ip, _ip]),
     "ob_batch_destroy": (C.c_int, [C.c_void_p]),
 }
 

@@ -274,6 +274,15 @@ class Batch:
         check(load().ob_batch_result(self._p, price.ctypes.data_as(_dp), se.ctypes.data_as(_dp), C.byref(ms)))
         return price, se, ms.value
 
+    def classes(self) -> list[dict]:
+        """The trade classes (one persistent kernel each) with their trades and current tile and block."""
+        n = C.c_int()
+        check(load().ob_batch_classes(self._p, 0, C.byref(n), None))
+        info = np.zeros(6 * max(n.value, 1), np.int32)
+        check(load().ob_batch_classes(self._p, n.value, C.byref(n), info.ctypes.data_as(_ip)))
+        keys = ("model", "names", "product", "trades", "tile", "block")
+        return [dict(zip(keys, map(int, info[6 * k:6 * k + 6]))) for k in range(n.value)]
+
     def close(self) -> None:
         if self._p:
             load().ob_batch_destroy(self._p)
