@@ -9,7 +9,9 @@ One step = one launch of the fused kernel over the whole batch (plus the one-blo
 inputs resident on the device; between steps a 512 MB buffer is written to flush L2. `value` is path-steps/s of the
 device-timed steps (CUDA events on the launching stream), max over ranks. `e2e` is the same metric through the public
 call with host inputs (`optlab_b200.engine.mc_price`: upload, kernel, read-back). Ranks (torchrun) each take their own
-range of pairs (first_pair = rank x pairs): weak scaling, with one FP64 all-reduce of the sums per step.
+range of pairs (first_pair = rank x pairs): weak scaling, no collective in the timed steps, and one FP64 all-reduce
+of the sums after them (optlab_b200.shard). `--workload adjoint` times the Greeks of the worst-of autocall (FP32
+adjoint against FP64 bump-and-revalue); `--workload batch` the batched revaluation of a 512-trade book.
 
 `--impl reference` times the reference's CPU implementation of the same workload instead: its path engine
 (optlab::api::paths, compiled from the reference's sources into oracle/_ref) writing the 12 quarterly columns and the
@@ -226,7 +228,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint", "batch"])
+    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage"])
     ap.add_argument("--trades", type=int, default=512, help="batch workload: trades in the book")
     ap.add_argument("--paths", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -244,6 +246,8 @@ def main():
         return run_adjoint(args, world, rank)
     if args.workload == "batch":
         return run_batch(args, world, rank)
+    if args.workload == "leverage":
+        return run_leverage(args, world, rank)
 
     import torch
 
@@ -266,7 +270,6 @@ def main():
     stream = torch.cuda.current_stream()
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     plan = engine.McPlan(held, prec)
-    sums = torch.zeros(2, dtype=torch.float64, device="cuda")
 
     def step():
         plan.run(n_pairs, first, held.struct.seed, stream.cuda_stream)
@@ -287,8 +290,6 @@ def main():
             starts[k].record(stream)
             step()
             ends[k].record(stream)
-            if dist:  # the exchange step: per-rank sums into the job's price (a few doubles)
-                dist.all_reduce(sums)
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
     if dist:
@@ -299,6 +300,12 @@ def main():
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
     res = plan.result()
+    price, se = list(res.price[: res.n_out]), list(res.se[: res.n_out])
+    if dist:  # the one exchange: every rank's FP64 sums into the job's price and SE
+        from optlab_b200.shard import allreduce_result
+
+        p, e = allreduce_result(price, se, n_pairs * args.steps, device="cuda")
+        price, se = list(p), list(e)
     per_step = ms_max / args.steps
     value = units * world * args.steps / (ms_max / 1e3)
 
@@ -365,7 +372,7 @@ def main():
         "gpu_launches": 2 * args.steps,
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "wall_s": t_wall,
-        "result": {"price": list(res.price[: res.n_out]), "se": list(res.se[: res.n_out]),
+        "result": {"price": price, "se": se,
                    "e2e_price": r_e2e.price[0], "warmup_price": warm.price[0]},
     }
     print(json.dumps(line))
@@ -539,6 +546,83 @@ def run_batch(args, world, rank):
         "gpu_launches": args.steps * (1 + len({(t.model, t.n_names, t.product) for t in book.trades})),
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "result": {"mean_base_price": float(price[:, 0].mean()), "median_se": float(np.median(se[:, 0]))},
+    }
+    print(json.dumps(line))
+
+
+def run_leverage(args, world, rank):
+    """cfg2: the SLV leverage calibration by particles (2^18 particles x 504 steps, 128-point regression grid, 400
+    bins), FP32 particles with FP64 bins and regression, through ob_leverage (upload of the 504 x 801 local-variance
+    rows, 504 dependent steps of bin / regress / step kernels, read-back of the two 504 x 128 tables). Units:
+    particle-steps. `value` is timed by CUDA events around the call on its stream (the upload of 3.2 MB is inside
+    it); `e2e` by the host clock around the same call."""
+    import torch
+
+    from optlab_b200 import engine, workloads
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    n_particles = args.paths or 2**18
+    held = workloads.slv_leverage(n_particles=n_particles)
+    s = held.struct
+    units = 2 * s.n_pairs * s.n_steps
+    for _ in range(args.warmup):
+        engine.leverage(held, "fp32")
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    wall = []
+    with ClockSampler(local) as clocks:
+        for a, b in ev:
+            t = time.perf_counter()
+            a.record()
+            engine.leverage(held, "fp32")
+            b.record()
+            torch.cuda.synchronize()
+            wall.append(time.perf_counter() - t)
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        from oracle import Reference, reference_available
+
+        if reference_available():
+            n_s = 2**16
+            small = workloads.slv_leverage(n_particles=n_s)
+            threads = os.cpu_count() or 1
+            t = time.perf_counter()
+            Reference().leverage(small, threads=threads)
+            secs = time.perf_counter() - t
+            cpu = {"value": n_s * s.n_steps / secs, "unit": "path-steps/s", "cores": threads, "kind": "reference",
+                   "sample": f"{n_s} particles x {s.n_steps} steps of the same calibration (optlab::api::leverage, "
+                   f"CPU backend, compiled from the reference's sources)"}
+    clk = clocks.summary()
+    line = {
+        "metric": "path-steps/s",
+        "value": units / (ms / 1e3),
+        "unit": "path-steps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "us_per_time_step": ms * 1e3 / s.n_steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (SSVI surface, Heston parameters)",
+        "config": {"workload": "slv_leverage", "particles": 2 * s.n_pairs, "n_steps": s.n_steps, "n_x": s.n_x,
+                   "n_bins": s.n_bins, "n_fine": s.n_fine, "lv_row_points": s.n_lv,
+                   "l2": "particles (2 MB) stay in L2 by design: the calibration is latency-bound"},
+        "roofline": {"bound": "latency", "achieved": None, "peak": None, "unit": "us per time step", "frac": None,
+                     "traffic": None, "note": "504 dependent steps of 5 small launches each"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": units / statistics.median(wall), "unit": "path-steps/s",
+                "h2d_bytes_per_step": s.n_steps * (s.n_lv + 4) * 8, "d2h_bytes_per_step": 2 * s.n_steps * s.n_x * 8},
+        "gpu_launches": args.steps * (1 + 5 * s.n_steps),
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "result": {"leverage_at_atm_last_step": float(held.values[-1, s.n_x // 2])},
     }
     print(json.dumps(line))
 

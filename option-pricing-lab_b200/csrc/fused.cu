@@ -237,6 +237,90 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
     }
 }
 
+// Heston QE-M with the two legs of an antithetic pair on neighbouring lanes (lane 2k: +z, lane 2k+1: -z): twice the
+// threads of fused_kernel for the same pairs, for the small path counts of QE books (2^15 pairs are 7 warps an SM at
+// one pair a thread; the FP64 step is a long dependent chain and needs the warps to hide its latency). Philox block b
+// of a pair holds (zv, zx) of steps 2b + 1 and 2b + 2; the two lanes draw alternate blocks (lane 2k block 2m, lane
+// 2k + 1 block 2m + 1) and swap them, so each lane draws half the normals and steps one leg. The pair's value is
+// the average of the lanes' payoffs, added once (by the even lane).
+template <typename R, int PRODUCT>
+__global__ void __launch_bounds__(512, min_blocks<R>())
+    qe_pair_kernel(FusedArgs<R> a, long long n_pairs, long long first_pair, uint32_t k0, uint32_t k1,
+                   double* __restrict__ partial) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    {
+        const int4* src = reinterpret_cast<const int4*>(a.blob);
+        int4* dst = reinterpret_cast<int4*>(sm);
+        for (int t = threadIdx.x; t < a.smem_blob / 16; t += blockDim.x) dst[t] = src[t];
+    }
+    const int n_warps = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n_acc = 2 * a.n_out;
+    double* wacc = reinterpret_cast<double*>(sm + a.smem_blob);
+    for (int t = threadIdx.x; t < n_warps * n_acc; t += blockDim.x) wacc[t] = 0.0;
+    __syncthreads();
+    const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
+    const R* s_trig = reinterpret_cast<const R*>(sm + a.off.ln_trig);
+    const double* s_disc = reinterpret_cast<const double*>(sm + a.off.obs_disc);
+    const int* leg_type = reinterpret_cast<const int*>(sm + a.off.leg_type);
+    const R* leg_strike = reinterpret_cast<const R*>(sm + a.off.leg_strike);
+    const int* leg_barrier = reinterpret_cast<const int*>(sm + a.off.leg_barrier);
+    const R* ln_level = reinterpret_cast<const R*>(sm + a.off.ln_level);
+    const int S = a.n_steps;
+    const int odd = lane & 1;
+    const R sgn = odd ? R(-1) : R(1);
+    constexpr unsigned kFull = 0xffffffffu;
+
+    const long long stride = (static_cast<long long>(gridDim.x) * blockDim.x) >> 1;
+    for (long long base = (static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31)) >> 1;
+         base < n_pairs; base += stride) {
+        const long long p = base + (lane >> 1);
+        const bool active = p < n_pairs;
+        const uint64_t pair = static_cast<uint64_t>(first_pair + (active ? p : n_pairs - 1));
+        R x = R(0), v = a.qe.v0, lp = R(0);
+        Leg<R> l;
+        leg_init<R, PRODUCT>(l);
+        for (int i0 = 1, m = 0; i0 <= S; i0 += 4, ++m) {
+            R z[4], e[8];
+            normals4<R>(pair, static_cast<uint64_t>(2 * m + odd), 0u, k0, k1, z[0], z[1], z[2], z[3]);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const R o = __shfl_xor_sync(kFull, z[k], 1);
+                e[k] = odd ? o : z[k];      // block 2m: steps i0, i0 + 1
+                e[4 + k] = odd ? z[k] : o;  // block 2m + 1: steps i0 + 2, i0 + 3
+            }
+            // one copy of the (long, FP64) step in the loop body: the four steps rotate the normals through e[0..1]
+#pragma unroll 1
+            for (int g = 0; g < 4; ++g) {
+                const int i = i0 + g;
+                if (i > S) break;
+                qe_step(a.qe, x, v, sgn * e[0], sgn * e[1]);
+                e[0] = e[2], e[1] = e[3], e[2] = e[4], e[3] = e[5], e[4] = e[6], e[5] = e[7];
+                lp = x;
+                if (PRODUCT == OB_PRODUCT_LADDER) {
+                    l.hi = m_max(l.hi, lp), l.lo = m_min(l.lo, lp);
+                } else {
+                    l.lo = m_min(l.lo, lp);
+                    const int j = s_step[i - 1].obs;
+                    if (j >= 0) leg_observe(a, s_trig, s_disc, l, lp, j);
+                }
+            }
+        }
+        for (int k = 0; k < a.n_out; ++k) {
+            const double mine = leg_output<R, PRODUCT>(a, leg_type, leg_strike, leg_barrier, ln_level, l, lp, k);
+            const double other = __shfl_xor_sync(kFull, mine, 1);
+            const double y = active && !odd ? 0.5 * (mine + other) : 0.0;
+            const double s1 = warp_sum(y), s2 = warp_sum(y * y);
+            if (lane == 0) wacc[warp * n_acc + k] += s1, wacc[warp * n_acc + a.n_out + k] += s2;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n_acc; t += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < n_warps; ++w) s += wacc[w * n_acc + t];
+        partial[static_cast<long long>(blockIdx.x) * n_acc + t] = s;
+    }
+}
+
 template <typename R>
 using FusedFn = void (*)(FusedArgs<R>, long long, long long, uint32_t, uint32_t, double*);
 
@@ -258,7 +342,7 @@ FusedFn<R> pick_fused(int kind, int n) {
         case 1: return pick_n<R, 1, PRODUCT>(n);
         case 2: return pick_n<R, 2, PRODUCT>(n);
         case 3: return pick_n<R, 3, PRODUCT>(n);
-        case 4: return n == 1 ? fused_kernel<R, 1, 4, PRODUCT> : nullptr;
+        case 4: return n == 1 ? qe_pair_kernel<R, PRODUCT> : nullptr;
         default: return nullptr;
     }
 }
@@ -395,6 +479,7 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem), "occupancy");
     if (per_sm < 1) return false;
     plan.fused = true;
+    plan.threads_per_pair = kind == 4 ? 2 : 1;
     plan.kernel = k;
     plan.block = block;
     plan.smem_bytes = smem;

@@ -435,12 +435,12 @@ McPlan::~McPlan() {
 // pairs are handed out grid-stride.
 int McPlan::occupancy_at(int blk) {
     if (blk == block) return blocks_per_sm;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < 16; ++k)
         if (occ_block[k] == blk) return occ_blocks[k];
     int per_sm = 0;
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, blk, smem_bytes), "occupancy");
     per_sm = std::max(1, per_sm);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < 16; ++k)
         if (!occ_block[k]) {
             occ_block[k] = blk, occ_blocks[k] = per_sm;
             break;
@@ -448,19 +448,28 @@ int McPlan::occupancy_at(int blk) {
     return per_sm;
 }
 
+// Block size and grid of a launch. A warp works through its pairs in chunks of 32 lanes, every chunk the whole path,
+// so the run lasts ceil(chunks / resident warps) rounds: the block size is chosen (multiples of 32 up to the plan's
+// block) to keep that ceiling close to the exact quotient, with enough warps on each SM to keep its schedulers
+// issuing (kIssueWarps; fewer count as proportionally slower).
 int McPlan::launch_shape(long long n_pairs, int& blk) {
+    constexpr double kIssueWarps = 24.0;
+    const long long units = n_pairs * threads_per_pair;
+    const long long chunks = (units + 31) / 32;
     double best = -1.0;
     int best_blk = block;
-    for (int b = block; b >= 64; b /= 2) {
-        const long long need = (n_pairs + b - 1) / b;
-        const long long resident = static_cast<long long>(sms) * occupancy_at(b);
-        const long long blocks = std::min(need, resident);
-        const double busy = std::min(1.0, static_cast<double>(blocks) / sms);  // share of SMs with work
-        const double score = static_cast<double>(blocks) * (b / 32) * busy;
+    for (int b = block; b >= 64; b -= 32) {
+        const long long need = (units + b - 1) / b;
+        const long long grid = std::min<long long>(need, static_cast<long long>(sms) * occupancy_at(b));
+        const long long warps = grid * (b / 32);
+        const long long rounds = (chunks + warps - 1) / warps;
+        const double fill = static_cast<double>(chunks) / static_cast<double>(rounds * warps);
+        const double per_sm = static_cast<double>(warps) / sms;
+        const double score = fill * std::min(1.0, per_sm / kIssueWarps) * std::min(1.0, static_cast<double>(grid) / sms);
         if (score > best * 1.0001) best = score, best_blk = b;
     }
     blk = best_blk;
-    const long long need = (n_pairs + blk - 1) / blk;
+    const long long need = (units + blk - 1) / blk;
     const long long full = static_cast<long long>(sms) * occupancy_at(blk) * grid_waves;
     return static_cast<int>(std::max<long long>(1, std::min<long long>({need, full, max_blocks})));
 }

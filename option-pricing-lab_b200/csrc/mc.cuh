@@ -36,6 +36,7 @@ struct McPlan {
     int precision = OB_FP32;
     int n_out = 0, sms = 0, blocks_per_sm = 1, max_blocks = 0;
     int block = 256, grid_waves = 1;
+    int threads_per_pair = 1;  // 2: the QE kernel runs the two legs of a pair on two lanes
     bool force_generic = false;  // tests: run the generic kernel even where the specialised one applies
     size_t smem_bytes = 0;
     const void* kernel = nullptr;
@@ -61,7 +62,7 @@ struct McPlan {
     void create(const ob_mc_request& rq, int precision);
     int launch_shape(long long n_pairs, int& blk);
     int occupancy_at(int blk);
-    int occ_block[4] = {}, occ_blocks[4] = {};  // resident blocks a SM at other block sizes, as queried
+    int occ_block[16] = {}, occ_blocks[16] = {};  // resident blocks a SM at other block sizes, as queried
     void run(long long n_pairs, long long first_pair, unsigned long long seed, cudaStream_t st);
     void result(ob_mc_result& res);
     ~McPlan();

@@ -191,7 +191,10 @@ inline QeConsts<R> make_qe_consts(const double* h, double r, double q, double dt
     return c;
 }
 
-// One QE-M step of (y, v) with independent normals zv (variance) and zx (log-spot), schemes.hpp:154-186.
+// One QE-M step of (y, v) with independent normals zv (variance) and zx (log-spot), schemes.hpp:154-186. The
+// arithmetic is the reference's, rearranged to fewer divisions and square roots (exact algebra, not approximations):
+// sqrt(inv) sqrt(inv - 1) as one root of their product (inv = 2 / psi >= 4/3 there), the finiteness test A < 1 / (2 a)
+// as 1 - 2 A a > 0 (a > 0), and 1 / beta = m (psi + 1) / 2 in the exponential branch.
 template <typename R>
 __device__ __forceinline__ void qe_step(const QeConsts<R>& c, R& y, R& v, R zv, R zx) {
     const R m = c.theta + (v - c.theta) * c.E;
@@ -200,18 +203,20 @@ __device__ __forceinline__ void qe_step(const QeConsts<R>& c, R& y, R& v, R zv, 
     bool finite;
     if (psi <= R(1.5)) {
         const R inv = R(2) / psi;
-        const R b2 = inv - R(1) + m_sqrt(inv) * m_sqrt(m_max(inv - R(1), R(0)));
+        const R b2 = inv - R(1) + m_sqrt(inv * m_max(inv - R(1), R(0)));
         const R a = m / (R(1) + b2), b = m_sqrt(b2);
         vn = a * (b + zv) * (b + zv);
         arg = R(1) - R(2) * c.A * a;
-        finite = c.A < R(1) / (R(2) * a);
+        finite = arg > R(0);
         lin = -c.A * b2 * a / arg;
         w = R(0.5);
     } else {
-        const R p = (psi - R(1)) / (psi + R(1)), beta = (R(1) - p) / m;
+        const R h = R(1) / (psi + R(1));
+        const R p = (psi - R(1)) * h, q = R(2) * h;  // q = 1 - p
+        const R beta = q / m;
         const R one_minus_u = m_ncdf(-zv);
-        vn = one_minus_u >= R(1) - p ? R(0) : m_log((R(1) - p) / one_minus_u) / beta;
-        arg = p + beta * (R(1) - p) / (beta - c.A);
+        vn = one_minus_u >= q ? R(0) : m_log(q / one_minus_u) * (R(0.5) * m * (psi + R(1)));
+        arg = p + beta * q / (beta - c.A);
         finite = c.A < beta;
         lin = R(0);
         w = R(-1);

@@ -133,7 +133,7 @@ class VegaNodes:
     node_k: np.ndarray
 
     def __post_init__(self):
-        dev = torch.device("cuda", torch.cuda.current_device())
+        dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else torch.device("cpu")
         k = self.row_lo[:, None] + np.arange(self.n_x)[None, :] / self.row_inv_dx[:, None]
         self.phi = torch.tensor(hats(self.row_T, self.node_T), dtype=torch.float64, device=dev)  # (rows, E)
         psi = hats(k.ravel(), self.node_k).reshape(k.shape[0], self.n_x, -1)
@@ -157,6 +157,12 @@ class VegaNodes:
         h = 2.0 * torch.sqrt(base_var) * table_grad
         return torch.einsum("rn,re,rjk,rj->nek", self.onehot, self.phi, self.psi, h)
 
+    def contract_batches(self, table_grads: torch.Tensor, base_var: torch.Tensor) -> torch.Tensor:
+        """contract of a stack of table gradients (B, rows, n_x): (B, names, E, K)."""
+        h = 2.0 * torch.sqrt(base_var)[None] * table_grads
+        per_row = torch.einsum("rjk,brj->brk", self.psi, h)
+        return torch.einsum("rn,re,brk->bnek", self.onehot, self.phi, per_row)
+
 
 def autocall_greeks(held, nodes: VegaNodes, smoothing: float = 0.005, precision="fp32", plan: AdjointPlan | None = None):
     """Price, deltas and node vegas (each with its standard error) of a local-vol autocall, by one forward and one
@@ -172,10 +178,9 @@ def autocall_greeks(held, nodes: VegaNodes, smoothing: float = 0.005, precision=
         price = AutocallPrice.apply(nodes.table(base, bumps), plan)
         (vega,) = torch.autograd.grad(price, bumps)
         res = plan.last
-        # batch means: each batch's vegas from its own gradient
+        # batch means: each batch's vegas from its own gradient, all batches in one contraction
         pairs = plan.batch_pairs
-        vb = torch.stack([nodes.contract(plan.batch_grad[b] / max(float(pairs[b]), 1.0), base)
-                          for b in range(plan.batch_grad.shape[0])])
+        vb = nodes.contract_batches(plan.batch_grad / pairs.clamp(min=1.0)[:, None, None], base)
         w = pairs / pairs.sum()
         mean = (w[:, None, None, None] * vb).sum(0)
         var = (w[:, None, None, None] * (vb - mean) ** 2).sum(0) * (len(pairs) / (len(pairs) - 1)) / len(pairs)

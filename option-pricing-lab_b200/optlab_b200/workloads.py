@@ -7,6 +7,9 @@
   on 200 log-strikes x 40 expiries (T_j = 3 j / 40); a 3-year single-name Phoenix, quarterly observations,
   autocall at 100 %, coupon 2 % at 70 % with memory, knock-in at 60 % on daily closes into a put struck at 100 %;
   756 daily steps, 2^20 paths; flat market r .02, q .01.
+- `slv_leverage`: the SLV leverage by particles, Heston of `heston_qe_ladder` (xi unscaled, mix 1) on the surface of
+  `lv_phoenix`; 2^18 particles, 504 uniform steps over two years; regression on 128 points, 400 bins, 8192 fine bins,
+  Nadaraya-Watson with the reference's bandwidth; the local variance on rows of 801 points per step.
 - `worst_of`: three names, each its own SSVI power-law surface (theta_t = c t with c = 0.03, 0.045, 0.06; rho = -0.7,
   -0.55, -0.4; eta 1, gamma 0.5) tabulated on 40 expiries x 200 log-strikes over four years, pairwise correlation 0.6;
   a worst-of Phoenix, quarterly over four years (16 observations), 1008 daily steps, 2^19 paths. Its Greeks: delta per
@@ -151,6 +154,21 @@ def lv_phoenix(n_paths: int = 2**20, seed: int = 7, steps_per_year: int = 252, p
         table=g.rows,
         n_x=g.n_x,
         **autocall_fields(ph, m, steps_per_year),
+    )
+
+
+def slv_leverage(n_particles: int = 2**18, seed: int = 5, n_steps: int = 504, T: float = 2.0, n_x: int = 128,
+                 n_lv: int = 801, local_linear: int = 0):
+    from .leverage import leverage_request
+    from .surfaces import local_var_rows
+
+    surface = lv_surface(horizon=3.0)
+    dt, t0 = uniform_grid(T, n_steps)
+    lo, inv, rows = local_var_rows(surface, t0, n_lv)
+    atm_vol = float(np.sqrt(surface.theta(1.0) / 1.0))
+    return leverage_request(
+        dt=dt, t0=t0, n_pairs=n_particles // 2, seed=seed, heston=HESTON_CFG0, n_x=n_x, lv_lo=lo, lv_inv_dx=inv,
+        lv_rows=rows, atm_vol=atm_vol, local_linear=local_linear, positive_part=local_linear,
     )
 
 
