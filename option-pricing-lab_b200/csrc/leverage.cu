@@ -3,16 +3,21 @@
 // the particle device of RC/src/leverage.cpp:156-214 / RC/src/leverage_gpu.cu:40-106.
 //
 // Per step i, everything stays on the device (the reference crosses PCIe three times a step):
-//   lev_bin        particles -> fine histogram (u32) and the regression's binned sums (count, v, x, x^2, x v) in FP64,
-//                  accumulated per block in shared memory, then added to the step's totals
+//   lev_bin        one block an SM: its particles into a private fine histogram (u32) and regression bins (u32
+//                  count, the v sums in 64-bit fixed point, the local-linear moments in FP64) in shared memory, then
+//                  stored whole as the block's partial (no global atomics)
+//   lev_merge      one thread per histogram or bin entry: the blocks' partials added in block order (so the step's
+//                  counts and sums do not depend on the schedule)
 //   lev_regress    one block per grid point g: the quantiles of the fine histogram bound the grid (the reference's
-//                  sequential search, restated as a parallel first-match), the Gaussian-kernel regression E[v | x_g]
+//                  first-match search, by a block-wide scan of the counts), the Gaussian-kernel regression E[v | x_g]
 //                  (Nadaraya-Watson or local linear) over the bins in FP64, and L_g = clip(sqrt(sigma_loc^2 / E), lmin,
 //                  lmax) with the local variance interpolated on its uniform row; the row and the grid go straight
 //                  into the output tables
 //   lev_step       one thread per antithetic pair: the SLV Euler step with the leverage row staged in shared memory,
 //                  normals from Philox counter (pair, step + 1, 0, 0), the new range of x by block then global min/max
-// Particles are float (OB_FP32) or double (OB_FP64); bins, regression and the leverage ratio are FP64 in both.
+//                  (two range slots alternate by step, each cleared by the step before its writer)
+// Particles are float (OB_FP32) or double (OB_FP64); bins, regression and the leverage ratio are FP64 in both (a v
+// enters its block's sum rounded to 2^-37).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -40,7 +45,11 @@ struct LevDev {
     const double* lv_rows;
     unsigned* fine;            // n_fine
     double* acc;               // 5 n_bins + 1 (the last: sum of v)
-    long long* range;          // ordered min and max of x (double keys)
+    long long* range;          // 2 slots of the ordered min and max of x (double keys), alternating by step
+    int n_part;                // blocks of lev_bin, each with its partial below
+    unsigned* part_u32;        // n_part x (n_fine + n_bins): fine histogram, counts
+    long long* part_i64;       // n_part x (n_bins + 1): v sums (fixed point), the total v sum
+    double* part_f64;          // n_part x 3 n_bins: x, x^2, x v sums (local linear only)
     double* x_eval;            // n_x, the current grid
     double* lev;               // n_x, the current leverage row
     double* x_grids;           // n_steps x n_x
@@ -56,84 +65,123 @@ __device__ __forceinline__ double unordered(long long i) {
     return __longlong_as_double(i >= 0 ? i : i ^ 0x7FFFFFFFFFFFFFFFLL);
 }
 
-__global__ void lev_reset(LevDev d) {
-    for (int k = threadIdx.x; k < d.n_fine; k += blockDim.x) d.fine[k] = 0u;
-    for (int k = threadIdx.x; k < 5 * d.n_bins + 1; k += blockDim.x) d.acc[k] = 0.0;
+// The v sums of a block are 64-bit fixed point with 2^36 units per unit of v (exact whatever the order of the
+// atomics: |v| may reach 2^27 / particles of a block, far above any variance); the merge adds the blocks' sums in
+// FP64 in block order.
+constexpr double kFix = 68719476736.0;
+
+__device__ __forceinline__ long long warp_sum_i64(long long v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+__device__ __forceinline__ void range_clear(long long* r) {
+    r[0] = 0x7FFFFFFFFFFFFFFFLL;
+    r[1] = static_cast<long long>(0x8000000000000000ULL);
 }
 
 template <typename R>
 __global__ void lev_init(R* x, R* v, long long n, R v0, long long* range) {
     const long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (j < n) x[j] = R(0), v[j] = v0;
-    if (j == 0) range[0] = ordered(0.0), range[1] = ordered(0.0);
+    if (j == 0) range[0] = ordered(0.0), range[1] = ordered(0.0), range_clear(range + 2);
 }
 
-// Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU.
+// Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU. Slot: the range
+// of the particles' x written by the previous step.
 template <typename R>
-__global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x, const R* __restrict__ v) {
+__global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x, const R* __restrict__ v, int slot) {
     extern __shared__ __align__(16) unsigned char sm[];
-    double* sacc = reinterpret_cast<double*>(sm);                     // 5 nb + 1
-    unsigned* sfine = reinterpret_cast<unsigned*>(sacc + 5 * d.n_bins + 1);  // n_fine
-    const int nb = d.n_bins, nf = d.n_fine;
-    for (int k = threadIdx.x; k < 5 * nb + 1; k += blockDim.x) sacc[k] = 0.0;
-    for (int k = threadIdx.x; k < nf; k += blockDim.x) sfine[k] = 0u;
+    const int nb = d.n_bins, nf = d.n_fine, ll = d.local_linear;
+    unsigned long long* s_sv = reinterpret_cast<unsigned long long*>(sm);  // nb, then the total
+    double* s_ll = reinterpret_cast<double*>(s_sv + nb + 1);               // 3 nb when local linear
+    unsigned* s_fine = reinterpret_cast<unsigned*>(s_ll + (ll ? 3 * nb : 0));
+    unsigned* s_cnt = s_fine + nf;
+    for (int k = threadIdx.x; k < nb + 1; k += blockDim.x) s_sv[k] = 0ull;
+    if (ll)
+        for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) s_ll[k] = 0.0;
+    for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) s_fine[k] = 0u;
     __syncthreads();
-    const R lo = static_cast<R>(unordered(d.range[0])), hi = static_cast<R>(unordered(d.range[1]));
+    const long long* rg = d.range + 2 * slot;
+    const R lo = static_cast<R>(unordered(rg[0])), hi = static_cast<R>(unordered(rg[1]));
     const R wf = (hi - lo) / static_cast<R>(nf), we = (hi + static_cast<R>(1e-12) - lo) / static_cast<R>(nb);
     const long long n = 2 * d.n_pairs;
+    long long tot = 0;
     for (long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
          j += static_cast<long long>(gridDim.x) * blockDim.x) {
         const R xj = x[j], vj = d.positive_part ? m_max(v[j], R(0)) : v[j];
         const int f = wf > R(0) ? static_cast<int>((xj - lo) / wf) : 0;
-        atomicAdd(&sfine[min(max(f, 0), nf - 1)], 1u);
+        atomicAdd(&s_fine[min(max(f, 0), nf - 1)], 1u);
         const int k = min(max(static_cast<int>((xj - lo) / we), 0), nb - 1);
         const double xd = static_cast<double>(xj), vd = static_cast<double>(vj);
-        atomicAdd(&sacc[k], 1.0);
-        atomicAdd(&sacc[nb + k], vd);
-        atomicAdd(&sacc[2 * nb + k], xd);
-        atomicAdd(&sacc[3 * nb + k], xd * xd);
-        atomicAdd(&sacc[4 * nb + k], xd * vd);
-        atomicAdd(&sacc[5 * nb], vd);
+        const long long q = __double2ll_rn(vd * kFix);
+        atomicAdd(&s_cnt[k], 1u);
+        atomicAdd(&s_sv[k], static_cast<unsigned long long>(q));
+        if (ll) {
+            atomicAdd(&s_ll[k], xd);
+            atomicAdd(&s_ll[nb + k], xd * xd);
+            atomicAdd(&s_ll[2 * nb + k], xd * vd);
+        }
+        tot += q;
     }
+    tot = warp_sum_i64(tot);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_sv[nb], static_cast<unsigned long long>(tot));
     __syncthreads();
-    for (int k = threadIdx.x; k < 5 * nb + 1; k += blockDim.x)
-        if (sacc[k] != 0.0) atomicAdd(&d.acc[k], sacc[k]);
-    for (int k = threadIdx.x; k < nf; k += blockDim.x)
-        if (sfine[k]) atomicAdd(&d.fine[k], sfine[k]);
+    unsigned* pu = d.part_u32 + static_cast<long long>(blockIdx.x) * (nf + nb);
+    long long* pi = d.part_i64 + static_cast<long long>(blockIdx.x) * (nb + 1);
+    for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) pu[k] = s_fine[k];
+    for (int k = threadIdx.x; k < nb + 1; k += blockDim.x) pi[k] = static_cast<long long>(s_sv[k]);
+    if (ll) {
+        double* pf = d.part_f64 + static_cast<long long>(blockIdx.x) * 3 * nb;
+        for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) pf[k] = s_ll[k];
+    }
 }
 
-// First fine bin k with count > 0 and (counts before k) + count >= target (RC/src/leverage.cpp:26-38), found by a
-// block of 256 threads over contiguous chunks; returns lo + (k + (target - before) / count) width, or hi.
-__device__ double block_quantile(const unsigned* fine, int nf, double lo, double hi, double q, double total,
-                                 double* s_chunk, double* s_cum, int* s_best) {
-    const int t = threadIdx.x, nt = blockDim.x, per = (nf + nt - 1) / nt;
-    const int a = min(t * per, nf), b = min(a + per, nf);
-    double mine = 0.0;
-    for (int k = a; k < b; ++k) mine += static_cast<double>(fine[k]);
-    s_chunk[t] = mine;
-    if (t == 0) *s_best = nf;
-    __syncthreads();
-    double before = 0.0;
-    for (int u = 0; u < t; ++u) before += s_chunk[u];  // exact: integer counts below 2^53
-    const double target = q * total;
-    double cum = before;
-    int found = nf;
-    for (int k = a; k < b; ++k) {
-        const double c = static_cast<double>(fine[k]), next = cum + c;
-        if (next >= target && fine[k] > 0) {
-            found = k;
-            break;
-        }
-        cum = next;
+// The step's histogram and bins: entry e of the fine histogram, counts, v sums (and total), local-linear sums, each
+// the sum of the n_part partials in block order.
+__global__ void __launch_bounds__(256) lev_merge(LevDev d) {
+    const int nb = d.n_bins, nf = d.n_fine, P = d.n_part;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n_u = nf + nb, n_i = nb + 1, n_f = d.local_linear ? 3 * nb : 0;
+    if (e < n_u) {
+        unsigned long long s = 0;
+        for (int b = 0; b < P; ++b) s += d.part_u32[static_cast<long long>(b) * n_u + e];
+        if (e < nf) d.fine[e] = static_cast<unsigned>(s);
+        else d.acc[e - nf] = static_cast<double>(s);
+    } else if (e < n_u + n_i) {
+        const int k = e - n_u;
+        double s = 0.0;
+        for (int b = 0; b < P; ++b) s += static_cast<double>(d.part_i64[static_cast<long long>(b) * n_i + k]) / kFix;
+        d.acc[k < nb ? nb + k : 5 * nb] = s;
+    } else if (e < n_u + n_i + n_f) {
+        const int k = e - n_u - n_i;
+        double s = 0.0;
+        for (int b = 0; b < P; ++b) s += d.part_f64[static_cast<long long>(b) * n_f + k];
+        d.acc[2 * nb + k] = s;
     }
-    if (found < nf) atomicMin(s_best, found), s_cum[t] = cum;
+}
+
+// Exclusive prefix of x over the block and the block's total (any block size that is a multiple of 32, up to 1024).
+__device__ unsigned long long block_scan(unsigned long long x, unsigned long long* s_warp, unsigned long long& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned long long inc = x;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += y;
+    }
+    if (lane == 31) s_warp[warp] = inc;
     __syncthreads();
-    const int kb = *s_best;
-    const double cb = kb < nf ? s_cum[kb / per] : 0.0;  // counts before kb, from the thread that owns kb's chunk
+    unsigned long long before = 0, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+        const unsigned long long c = s_warp[w];
+        before += w < warp ? c : 0ull;
+        tot += c;
+    }
     __syncthreads();
-    if (kb >= nf) return hi;
-    const double width = (hi - lo) / static_cast<double>(nf);
-    return lo + (static_cast<double>(kb) + (target - cb) / static_cast<double>(fine[kb])) * width;
+    total = tot;
+    return before + inc - x;
 }
 
 __device__ __forceinline__ double interp_uniform(double x, double a, double b, const double* y, int n) {
@@ -146,66 +194,91 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 }
 
 // Grid, regression and leverage of step i; block g computes grid point g. Step 0 uses the reference's initial grid
-// and E[v | x] = v0.
+// and E[v | x] = v0. The quantiles (RC/src/leverage.cpp:26-38): the first fine bin k with a count and (counts before
+// k) + count >= q total, at lo + (k + (q total - before) / count) width; each thread owns a run of bins, and a block
+// scan of the runs' counts gives every thread the counts before its run.
 __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_particles) {
-    __shared__ double s_chunk[256];
-    __shared__ double s_cum[256];
-    __shared__ double s_red[5][256];
-    __shared__ int s_best;
-    __shared__ double s_q[2];
-    const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, t = threadIdx.x;
+    __shared__ unsigned long long s_warp[32];
+    __shared__ double s_cum[2][256];
+    __shared__ int s_best[2];
+    __shared__ double s_red[5][32];
+    const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
     const double t0 = d.t0[i], h = d.dt[i];
     double x0, cond;
     if (i == 0) {
         x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
         cond = d.v0;
     } else {
-        const double lo = unordered(d.range[0]), hi = unordered(d.range[1]);
-        double total = 0.0;
-        {
-            // total count, the same in every thread (sum over chunks in order)
-            const int per = (d.n_fine + blockDim.x - 1) / blockDim.x;
-            const int a = min(t * per, d.n_fine), b = min(a + per, d.n_fine);
-            double mine = 0.0;
-            for (int k = a; k < b; ++k) mine += static_cast<double>(d.fine[k]);
-            s_chunk[t] = mine;
-            __syncthreads();
-            for (int u = 0; u < static_cast<int>(blockDim.x); ++u) total += s_chunk[u];
-            __syncthreads();
+        const long long* rg = d.range + 2 * (i & 1);
+        const double lo = unordered(rg[0]), hi = unordered(rg[1]);
+        const int per = (nf + blockDim.x - 1) / blockDim.x;
+        const int a = min(t * per, nf), b = min(a + per, nf);
+        unsigned long long mine = 0;
+        for (int k = a; k < b; ++k) mine += d.fine[k];
+        if (t < 2) s_best[t] = nf;
+        unsigned long long total_u;
+        const unsigned long long before = block_scan(mine, s_warp, total_u);
+        const double total = static_cast<double>(total_u);
+        const double q2[2] = {d.q_lo, d.q_hi};
+#pragma unroll
+        for (int qi = 0; qi < 2; ++qi) {
+            const double target = q2[qi] * total;
+            double cum = static_cast<double>(before);
+            for (int k = a; k < b; ++k) {
+                const unsigned c = d.fine[k];
+                const double next = cum + static_cast<double>(c);
+                if (next >= target && c > 0) {
+                    atomicMin(&s_best[qi], k);
+                    s_cum[qi][t] = cum;
+                    break;
+                }
+                cum = next;
+            }
         }
-        const double qa = block_quantile(d.fine, d.n_fine, lo, hi, d.q_lo, total, s_chunk, s_cum, &s_best);
-        const double qb = block_quantile(d.fine, d.n_fine, lo, hi, d.q_hi, total, s_chunk, s_cum, &s_best);
-        if (t == 0) s_q[0] = qa, s_q[1] = qb;
         __syncthreads();
-        const double a = s_q[0], b = s_q[1];
-        x0 = a + (b - a) * g / (nx - 1);
+        const double width = (hi - lo) / static_cast<double>(nf);
+        double qv[2];
+#pragma unroll
+        for (int qi = 0; qi < 2; ++qi) {
+            const int kb = s_best[qi];
+            qv[qi] = kb >= nf ? hi
+                              : lo + (static_cast<double>(kb) + (q2[qi] * total - s_cum[qi][kb / per]) /
+                                                                    static_cast<double>(d.fine[kb])) *
+                                         width;
+        }
+        x0 = qv[0] + (qv[1] - qv[0]) * g / (nx - 1);
         const double bw = d.bw_scale * d.atm_vol * sqrt(t0 > 0.15 ? t0 : 0.15) * pow(n_particles, -0.2);
         const double wc = (hi + 1e-12 - lo) / nb;
         const double *cnt = d.acc, *sv = cnt + nb, *sx = sv + nb, *sxx = sx + nb, *sxv = sxx + nb;
-        double S0 = 0, T0 = 0, Ax = 0, Axx = 0, Axv = 0;
+        double r[5] = {0, 0, 0, 0, 0};
         for (int k = t; k < nb; k += blockDim.x) {
             const double c = lo + (k + 0.5) * wc;
             const double dd = (x0 - c) / bw, w = exp(-0.5 * dd * dd);
-            S0 += w * cnt[k], T0 += w * sv[k];
-            if (d.local_linear) Ax += w * sx[k], Axx += w * sxx[k], Axv += w * sxv[k];
+            r[0] += w * cnt[k], r[1] += w * sv[k];
+            if (d.local_linear) r[2] += w * sx[k], r[3] += w * sxx[k], r[4] += w * sxv[k];
         }
-        s_red[0][t] = S0, s_red[1][t] = T0, s_red[2][t] = Ax, s_red[3][t] = Axx, s_red[4][t] = Axv;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            r[q] = warp_sum(r[q]);
+            if (lane == 0) s_red[q][warp] = r[q];
+        }
         __syncthreads();
-        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-            if (t < s)
-                for (int r = 0; r < 5; ++r) s_red[r][t] += s_red[r][t + s];
-            __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            r[q] = 0.0;
+            for (int w = 0; w < nw; ++w) r[q] += s_red[q][w];
         }
-        S0 = s_red[0][0], T0 = s_red[1][0], Ax = s_red[2][0], Axx = s_red[3][0], Axv = s_red[4][0];
+        const double S0 = r[0], T0 = r[1], Ax = r[2], Axx = r[3], Axv = r[4];
         const double fallback = d.acc[5 * nb] / n_particles;
-        const double nw = S0 > 1e-8 ? T0 / (S0 > 1e-300 ? S0 : 1e-300) : fallback;
-        cond = nw;
+        const double nw_e = S0 > 1e-8 ? T0 / (S0 > 1e-300 ? S0 : 1e-300) : fallback;
+        cond = nw_e;
         if (d.local_linear) {
             const double S1 = Ax - x0 * S0, S2 = Axx - 2 * x0 * Ax + x0 * x0 * S0, T1 = Axv - x0 * T0;
             const double det = S0 * S2 - S1 * S1;
             const bool ok = S0 >= 50 && det > 1e-12 * S0 * fabs(S2);
-            const double ll = ok ? (S2 * T0 - S1 * T1) / det : nw;
-            cond = ll > 1e-8 ? ll : 1e-8;
+            const double lle = ok ? (S2 * T0 - S1 * T1) / det : nw_e;
+            cond = lle > 1e-8 ? lle : 1e-8;
         }
     }
     if (t == 0) {
@@ -225,6 +298,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v, int i) {
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[8], s_max[8];
+    if (blockIdx.x == 0 && threadIdx.x == 0) range_clear(d.range + 2 * (i & 1));  // for step i + 1's min and max
     for (int g = threadIdx.x; g < d.n_x; g += blockDim.x) s_lev[g] = static_cast<R>(d.lev[g]);
     __syncthreads();
     const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -272,14 +346,10 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) mn = m_min(mn, s_min[w]), mx = m_max(mx, s_max[w]);
-        atomicMin(reinterpret_cast<long long*>(&d.range[0]), ordered(static_cast<double>(mn)));
-        atomicMax(reinterpret_cast<long long*>(&d.range[1]), ordered(static_cast<double>(mx)));
+        long long* rg = d.range + 2 * ((i + 1) & 1);
+        atomicMin(&rg[0], ordered(static_cast<double>(mn)));
+        atomicMax(&rg[1], ordered(static_cast<double>(mx)));
     }
-}
-
-__global__ void lev_range_reset(long long* range) {
-    range[0] = 0x7FFFFFFFFFFFFFFFLL;
-    range[1] = static_cast<long long>(0x8000000000000000ULL);
 }
 
 void check_request(const ob_leverage_request& rq) {
@@ -315,32 +385,36 @@ void run_leverage(ob_leverage_request& rq) {
     d.lv_rows = arena.put<double>(rq.lv_rows, static_cast<size_t>(S) * rq.n_lv);
     d.fine = arena.alloc<unsigned>(rq.n_fine);
     d.acc = arena.alloc<double>(5 * static_cast<size_t>(rq.n_bins) + 1);
-    d.range = arena.alloc<long long>(2);
+    d.range = arena.alloc<long long>(4);
     d.x_eval = arena.alloc<double>(rq.n_x);
     d.lev = arena.alloc<double>(rq.n_x);
     d.x_grids = arena.alloc<double>(static_cast<size_t>(S) * rq.n_x);
     d.values = arena.alloc<double>(static_cast<size_t>(S) * rq.n_x);
     R* x = arena.alloc<R>(n);
     R* v = arena.alloc<R>(n);
-    const size_t bin_smem = (5 * static_cast<size_t>(rq.n_bins) + 1) * sizeof(double) + rq.n_fine * sizeof(unsigned);
+    const int nb = rq.n_bins, nf = rq.n_fine, ll = rq.local_linear;
+    const size_t bin_smem = (static_cast<size_t>(nb) + 1) * sizeof(unsigned long long) +
+                            (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0) +
+                            (static_cast<size_t>(nf) + nb) * sizeof(unsigned);
     check_cuda(cudaFuncSetAttribute(lev_bin<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(bin_smem)),
                "cudaFuncSetAttribute");
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lev_bin<R>, 512, bin_smem), "occupancy");
-    const int bin_grid = static_cast<int>(std::max<long long>(
-        1, std::min<long long>(static_cast<long long>(sms) * std::max(1, per_sm), (n + 511) / 512)));
+    // one block an SM (fewer for small particle counts): the partials stay few, each block bins many particles
+    d.n_part = static_cast<int>(std::max<long long>(1, std::min<long long>(sms, (n + 511) / 512)));
+    d.part_u32 = arena.alloc<unsigned>(static_cast<size_t>(d.n_part) * (nf + nb));
+    d.part_i64 = arena.alloc<long long>(static_cast<size_t>(d.n_part) * (nb + 1));
+    d.part_f64 = ll ? arena.alloc<double>(static_cast<size_t>(d.n_part) * 3 * nb) : nullptr;
+    const int n_merge = nf + nb + nb + 1 + (ll ? 3 * nb : 0);
     const unsigned step_grid = static_cast<unsigned>((rq.n_pairs + 255) / 256);
     const double n_particles = 2.0 * static_cast<double>(rq.n_pairs);
     lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256>>>(x, v, n, static_cast<R>(rq.v0), d.range);
     check_cuda(cudaGetLastError(), "lev_init launch");
     for (int i = 0; i < S; ++i) {
         if (i > 0) {
-            lev_reset<<<1, 1024>>>(d);
-            lev_bin<R><<<bin_grid, 512, bin_smem>>>(d, x, v);
+            lev_bin<R><<<d.n_part, 512, bin_smem>>>(d, x, v, i & 1);
+            lev_merge<<<(n_merge + 255) / 256, 256>>>(d);
         }
         lev_regress<<<rq.n_x, 256>>>(d, i, n_particles);
-        lev_range_reset<<<1, 1>>>(d.range);
         lev_step<R><<<step_grid, 256>>>(d, x, v, i);
     }
     check_cuda(cudaGetLastError(), "leverage launches");
