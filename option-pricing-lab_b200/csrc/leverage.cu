@@ -6,16 +6,15 @@
 //   lev_bin        one block an SM: its particles into a private fine histogram (u32) and regression bins (u32
 //                  count, the v sums in 64-bit fixed point, the local-linear moments in FP64) in shared memory, then
 //                  stored whole as the block's partial (no global atomics)
-//   lev_merge      one thread per histogram or bin entry: the blocks' partials added in block order (so the step's
-//                  counts and sums do not depend on the schedule)
-//   lev_regress    one block per grid point g: the quantiles of the fine histogram bound the grid (the reference's
-//                  first-match search, by a block-wide scan of the counts), the Gaussian-kernel regression E[v | x_g]
-//                  (Nadaraya-Watson or local linear) over the bins in FP64, and L_g = clip(sqrt(sigma_loc^2 / E), lmin,
-//                  lmax) with the local variance interpolated on its uniform row; the row and the grid go straight
-//                  into the output tables
-//   lev_step       one thread per antithetic pair: the SLV Euler step with the leverage row staged in shared memory,
-//                  normals from Philox counter (pair, step + 1, 0, 0), the new range of x by block then global min/max
-//                  (two range slots alternate by step, each cleared by the step before its writer)
+//   lev_merge      the blocks' partials added in a fixed order (so the step's counts and sums do not depend on the
+//                  schedule); the last block to finish computes the range of x and the two quantiles of the fine
+//                  histogram that bound the regression grid (the reference's first-match search, by a block scan)
+//   lev_regress    one block per grid point g: the Gaussian-kernel regression E[v | x_g] (Nadaraya-Watson or local
+//                  linear) over the bins in FP64, and L_g = clip(sqrt(sigma_loc^2 / E), lmin, lmax) with the local
+//                  variance interpolated on its uniform row; the row and the grid go straight into the output tables
+//   lev_step       one thread per antithetic pair (grid-stride): the SLV Euler step with the leverage row staged in
+//                  shared memory, normals from Philox counter (pair, step + 1, 0, 0), each block's min and max of the
+//                  new x stored for the next step (no atomics)
 // Particles are float (OB_FP32) or double (OB_FP64); bins, regression and the leverage ratio are FP64 in both (a v
 // enters its block's sum rounded to 2^-37).
 #include <algorithm>
@@ -45,28 +44,22 @@ struct LevDev {
     const double* lv_rows;
     unsigned* fine;            // n_fine
     double* acc;               // 5 n_bins + 1 (the last: sum of v)
-    long long* range;          // 2 slots of the ordered min and max of x (double keys), alternating by step
     int n_part;                // blocks of lev_bin, each with its partial below
     unsigned* part_u32;        // n_part x (n_fine + n_bins): fine histogram, counts
     long long* part_i64;       // n_part x (n_bins + 1): v sums (fixed point), the total v sum
     double* part_f64;          // n_part x 3 n_bins: x, x^2, x v sums (local linear only)
+    int n_step_blocks;         // blocks of lev_step, each with its min and max of the new x
+    double* part_range;        // n_step_blocks x 2
+    double* stats;             // the step's lower and upper quantiles, min and max of x (from lev_merge)
+    unsigned* done;            // lev_merge's finished blocks (the last one computes stats and clears it)
     double* x_eval;            // n_x, the current grid
     double* lev;               // n_x, the current leverage row
     double* x_grids;           // n_steps x n_x
     double* values;            // n_steps x n_x
 };
 
-// Order-preserving map of doubles to signed 64-bit integers, for atomicMin / atomicMax.
-__device__ __forceinline__ long long ordered(double d) {
-    const long long i = __double_as_longlong(d);
-    return i >= 0 ? i : i ^ 0x7FFFFFFFFFFFFFFFLL;
-}
-__device__ __forceinline__ double unordered(long long i) {
-    return __longlong_as_double(i >= 0 ? i : i ^ 0x7FFFFFFFFFFFFFFFLL);
-}
-
-// The v sums of a block are 64-bit fixed point with 2^36 units per unit of v (exact whatever the order of the
-// atomics: |v| may reach 2^27 / particles of a block, far above any variance); the merge adds the blocks' sums in
+// The v sums of a binning block are 64-bit fixed point with 2^36 units per unit of v (exact whatever the order of
+// the atomics: |v| may reach 2^27 / particles of a block, far above any variance); the merge adds the blocks' sums in
 // FP64 in block order.
 constexpr double kFix = 68719476736.0;
 
@@ -76,23 +69,35 @@ __device__ __forceinline__ long long warp_sum_i64(long long v) {
     return v;
 }
 
-__device__ __forceinline__ void range_clear(long long* r) {
-    r[0] = 0x7FFFFFFFFFFFFFFFLL;
-    r[1] = static_cast<long long>(0x8000000000000000ULL);
+// Min and max of x over the last step's blocks, in every thread of the calling block (any multiple of 32 threads).
+__device__ void range_of(const LevDev& d, double& lo, double& hi, double* s_mn, double* s_mx) {
+    double mn = 1.0e300, mx = -1.0e300;
+    for (int b = threadIdx.x; b < d.n_step_blocks; b += blockDim.x)
+        mn = fmin(mn, d.part_range[2 * b]), mx = fmax(mx, d.part_range[2 * b + 1]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_mn[warp] = mn, s_mx[warp] = mx;
+    __syncthreads();
+    lo = s_mn[0], hi = s_mx[0];
+    for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) lo = fmin(lo, s_mn[w]), hi = fmax(hi, s_mx[w]);
+    __syncthreads();
 }
 
 template <typename R>
-__global__ void lev_init(R* x, R* v, long long n, R v0, long long* range) {
+__global__ void lev_init(R* x, R* v, long long n, R v0) {
     const long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (j < n) x[j] = R(0), v[j] = v0;
-    if (j == 0) range[0] = ordered(0.0), range[1] = ordered(0.0), range_clear(range + 2);
 }
 
-// Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU. Slot: the range
-// of the particles' x written by the previous step.
+// Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU.
 template <typename R>
-__global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x, const R* __restrict__ v, int slot) {
+__global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x, const R* __restrict__ v) {
     extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ double s_mn[16], s_mx[16];
     const int nb = d.n_bins, nf = d.n_fine, ll = d.local_linear;
     unsigned long long* s_sv = reinterpret_cast<unsigned long long*>(sm);  // nb, then the total
     double* s_ll = reinterpret_cast<double*>(s_sv + nb + 1);               // 3 nb when local linear
@@ -102,9 +107,9 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     if (ll)
         for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) s_ll[k] = 0.0;
     for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) s_fine[k] = 0u;
-    __syncthreads();
-    const long long* rg = d.range + 2 * slot;
-    const R lo = static_cast<R>(unordered(rg[0])), hi = static_cast<R>(unordered(rg[1]));
+    double lo_d, hi_d;
+    range_of(d, lo_d, hi_d, s_mn, s_mx);  // (its barrier also orders the clearing above)
+    const R lo = static_cast<R>(lo_d), hi = static_cast<R>(hi_d);
     const R wf = (hi - lo) / static_cast<R>(nf), we = (hi + static_cast<R>(1e-12) - lo) / static_cast<R>(nb);
     const long long n = 2 * d.n_pairs;
     long long tot = 0;
@@ -138,30 +143,6 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     }
 }
 
-// The step's histogram and bins: entry e of the fine histogram, counts, v sums (and total), local-linear sums, each
-// the sum of the n_part partials in block order.
-__global__ void __launch_bounds__(256) lev_merge(LevDev d) {
-    const int nb = d.n_bins, nf = d.n_fine, P = d.n_part;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n_u = nf + nb, n_i = nb + 1, n_f = d.local_linear ? 3 * nb : 0;
-    if (e < n_u) {
-        unsigned long long s = 0;
-        for (int b = 0; b < P; ++b) s += d.part_u32[static_cast<long long>(b) * n_u + e];
-        if (e < nf) d.fine[e] = static_cast<unsigned>(s);
-        else d.acc[e - nf] = static_cast<double>(s);
-    } else if (e < n_u + n_i) {
-        const int k = e - n_u;
-        double s = 0.0;
-        for (int b = 0; b < P; ++b) s += static_cast<double>(d.part_i64[static_cast<long long>(b) * n_i + k]) / kFix;
-        d.acc[k < nb ? nb + k : 5 * nb] = s;
-    } else if (e < n_u + n_i + n_f) {
-        const int k = e - n_u - n_i;
-        double s = 0.0;
-        for (int b = 0; b < P; ++b) s += d.part_f64[static_cast<long long>(b) * n_f + k];
-        d.acc[2 * nb + k] = s;
-    }
-}
-
 // Exclusive prefix of x over the block and the block's total (any block size that is a multiple of 32, up to 1024).
 __device__ unsigned long long block_scan(unsigned long long x, unsigned long long* s_warp, unsigned long long& total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -184,6 +165,93 @@ __device__ unsigned long long block_scan(unsigned long long x, unsigned long lon
     return before + inc - x;
 }
 
+// The step's histogram and bins, then its quantiles. Block: 32 entries (one a lane) x 8 warps; warp w adds the
+// partials w, w + 8, ... and the block adds the warps in order, so every entry is the same sum on every run. The last
+// block to finish (a ticket, no waiting) computes the range of x and the quantiles of the merged fine histogram
+// (RC/src/leverage.cpp:26-38: the first fine bin k with a count and (counts before k) + count >= q total, at
+// lo + (k + (q total - before) / count) width), each thread scanning a run of bins after a block scan of the runs'
+// counts. Dynamic shared memory: the fine histogram (n_fine u32).
+__global__ void __launch_bounds__(256) lev_merge(LevDev d) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ double s_part[8][32];
+    __shared__ unsigned long long s_warp[32];
+    __shared__ double s_cum[2][256];
+    __shared__ int s_best[2];
+    __shared__ double s_mn[8], s_mx[8];
+    __shared__ bool s_last;
+    const int nb = d.n_bins, nf = d.n_fine, P = d.n_part;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int e = blockIdx.x * 32 + lane;
+    const int n_u = nf + nb, n_i = nb + 1, n_f = d.local_linear ? 3 * nb : 0;
+    double s = 0.0;
+    if (e < n_u) {
+        unsigned long long c = 0;
+        for (int b = warp; b < P; b += 8) c += d.part_u32[static_cast<long long>(b) * n_u + e];
+        s = static_cast<double>(c);
+    } else if (e < n_u + n_i) {
+        const int k = e - n_u;
+        for (int b = warp; b < P; b += 8) s += static_cast<double>(d.part_i64[static_cast<long long>(b) * n_i + k]) / kFix;
+    } else if (e < n_u + n_i + n_f) {
+        const int k = e - n_u - n_i;
+        for (int b = warp; b < P; b += 8) s += d.part_f64[static_cast<long long>(b) * n_f + k];
+    }
+    s_part[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += s_part[w][lane];
+        if (e < nf) d.fine[e] = static_cast<unsigned>(t);
+        else if (e < n_u) d.acc[e - nf] = t;
+        else if (e < n_u + n_i) d.acc[e - n_u < nb ? nb + (e - n_u) : 5 * nb] = t;
+        else if (e < n_u + n_i + n_f) d.acc[2 * nb + (e - n_u - n_i)] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(d.done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // the last block: the merged histogram is complete
+    unsigned* s_fine = reinterpret_cast<unsigned*>(sm);
+    for (int k = threadIdx.x; k < nf; k += blockDim.x) s_fine[k] = __ldcg(d.fine + k);
+    if (threadIdx.x < 2) s_best[threadIdx.x] = nf;
+    double lo, hi;
+    range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also order the loads above)
+    const int t = threadIdx.x, per = (nf + blockDim.x - 1) / blockDim.x;
+    const int a = min(t * per, nf), b = min(a + per, nf);
+    unsigned long long mine = 0;
+    for (int k = a; k < b; ++k) mine += s_fine[k];
+    unsigned long long total_u;
+    const unsigned long long before = block_scan(mine, s_warp, total_u);
+    const double total = static_cast<double>(total_u);
+    const double q2[2] = {d.q_lo, d.q_hi};
+#pragma unroll
+    for (int qi = 0; qi < 2; ++qi) {
+        const double target = q2[qi] * total;
+        double cum = static_cast<double>(before);
+        for (int k = a; k < b; ++k) {
+            const unsigned c = s_fine[k];
+            const double next = cum + static_cast<double>(c);
+            if (next >= target && c > 0) {
+                atomicMin(&s_best[qi], k);
+                s_cum[qi][t] = cum;
+                break;
+            }
+            cum = next;
+        }
+    }
+    __syncthreads();
+    if (t < 2) {
+        const int kb = s_best[t];
+        const double width = (hi - lo) / static_cast<double>(nf);
+        d.stats[t] = kb >= nf ? hi
+                              : lo + (static_cast<double>(kb) + (q2[t] * total - s_cum[t][kb / per]) /
+                                                                    static_cast<double>(s_fine[kb])) *
+                                         width;
+    }
+    if (t == 0) d.stats[2] = lo, d.stats[3] = hi, *d.done = 0u;
+}
+
 __device__ __forceinline__ double interp_uniform(double x, double a, double b, const double* y, int n) {
     const double u = (x - a) / (b - a) * (n - 1);
     if (!(u > 0)) return y[0];
@@ -194,15 +262,10 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 }
 
 // Grid, regression and leverage of step i; block g computes grid point g. Step 0 uses the reference's initial grid
-// and E[v | x] = v0. The quantiles (RC/src/leverage.cpp:26-38): the first fine bin k with a count and (counts before
-// k) + count >= q total, at lo + (k + (q total - before) / count) width; each thread owns a run of bins, and a block
-// scan of the runs' counts gives every thread the counts before its run.
+// and E[v | x] = v0; later steps read the grid's bounds (the quantiles) and the bins from lev_merge.
 __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_particles) {
-    __shared__ unsigned long long s_warp[32];
-    __shared__ double s_cum[2][256];
-    __shared__ int s_best[2];
     __shared__ double s_red[5][32];
-    const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
+    const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
     const double t0 = d.t0[i], h = d.dt[i];
     double x0, cond;
@@ -210,44 +273,8 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
         x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
         cond = d.v0;
     } else {
-        const long long* rg = d.range + 2 * (i & 1);
-        const double lo = unordered(rg[0]), hi = unordered(rg[1]);
-        const int per = (nf + blockDim.x - 1) / blockDim.x;
-        const int a = min(t * per, nf), b = min(a + per, nf);
-        unsigned long long mine = 0;
-        for (int k = a; k < b; ++k) mine += d.fine[k];
-        if (t < 2) s_best[t] = nf;
-        unsigned long long total_u;
-        const unsigned long long before = block_scan(mine, s_warp, total_u);
-        const double total = static_cast<double>(total_u);
-        const double q2[2] = {d.q_lo, d.q_hi};
-#pragma unroll
-        for (int qi = 0; qi < 2; ++qi) {
-            const double target = q2[qi] * total;
-            double cum = static_cast<double>(before);
-            for (int k = a; k < b; ++k) {
-                const unsigned c = d.fine[k];
-                const double next = cum + static_cast<double>(c);
-                if (next >= target && c > 0) {
-                    atomicMin(&s_best[qi], k);
-                    s_cum[qi][t] = cum;
-                    break;
-                }
-                cum = next;
-            }
-        }
-        __syncthreads();
-        const double width = (hi - lo) / static_cast<double>(nf);
-        double qv[2];
-#pragma unroll
-        for (int qi = 0; qi < 2; ++qi) {
-            const int kb = s_best[qi];
-            qv[qi] = kb >= nf ? hi
-                              : lo + (static_cast<double>(kb) + (q2[qi] * total - s_cum[qi][kb / per]) /
-                                                                    static_cast<double>(d.fine[kb])) *
-                                         width;
-        }
-        x0 = qv[0] + (qv[1] - qv[0]) * g / (nx - 1);
+        const double qa = d.stats[0], qb = d.stats[1], lo = d.stats[2], hi = d.stats[3];
+        x0 = qa + (qb - qa) * g / (nx - 1);
         const double bw = d.bw_scale * d.atm_vol * sqrt(t0 > 0.15 ? t0 : 0.15) * pow(n_particles, -0.2);
         const double wc = (hi + 1e-12 - lo) / nb;
         const double *cnt = d.acc, *sv = cnt + nb, *sx = sv + nb, *sxx = sx + nb, *sxv = sxx + nb;
@@ -294,24 +321,24 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
     }
 }
 
+// The SLV Euler step of every pair (grid-stride), and the block's min and max of the new x into part_range.
 template <typename R>
 __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v, int i) {
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[8], s_max[8];
-    if (blockIdx.x == 0 && threadIdx.x == 0) range_clear(d.range + 2 * (i & 1));  // for step i + 1's min and max
     for (int g = threadIdx.x; g < d.n_x; g += blockDim.x) s_lev[g] = static_cast<R>(d.lev[g]);
     __syncthreads();
-    const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int nx = d.n_x;
     const R h = static_cast<R>(d.dt[i]);
     const R a = static_cast<R>(d.x_eval[0]), b = static_cast<R>(d.x_eval[nx - 1]);
     const R rho = static_cast<R>(d.rho), kappa = static_cast<R>(d.kappa), theta = static_cast<R>(d.theta);
     const R xi = static_cast<R>(d.xi);
+    const R rc = m_sqrt(R(1) - rho * rho);
     R mn = sizeof(R) == 4 ? R(3.0e38f) : R(1.0e300), mx = -mn;
-    if (p < d.n_pairs) {
+    for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; p < d.n_pairs;
+         p += static_cast<long long>(gridDim.x) * blockDim.x) {
         R z0, z1, z2, z3;
         normals4<R>(static_cast<uint64_t>(p), static_cast<uint64_t>(i + 1), 0u, d.k0, d.k1, z0, z1, z2, z3);
-        const R rc = m_sqrt(R(1) - rho * rho);
 #pragma unroll
         for (int leg = 0; leg < 2; ++leg) {
             const long long j = leg ? d.n_pairs + p : p;
@@ -346,9 +373,8 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) mn = m_min(mn, s_min[w]), mx = m_max(mx, s_max[w]);
-        long long* rg = d.range + 2 * ((i + 1) & 1);
-        atomicMin(&rg[0], ordered(static_cast<double>(mn)));
-        atomicMax(&rg[1], ordered(static_cast<double>(mx)));
+        d.part_range[2 * blockIdx.x] = static_cast<double>(mn);
+        d.part_range[2 * blockIdx.x + 1] = static_cast<double>(mx);
     }
 }
 
@@ -385,7 +411,6 @@ void run_leverage(ob_leverage_request& rq) {
     d.lv_rows = arena.put<double>(rq.lv_rows, static_cast<size_t>(S) * rq.n_lv);
     d.fine = arena.alloc<unsigned>(rq.n_fine);
     d.acc = arena.alloc<double>(5 * static_cast<size_t>(rq.n_bins) + 1);
-    d.range = arena.alloc<long long>(4);
     d.x_eval = arena.alloc<double>(rq.n_x);
     d.lev = arena.alloc<double>(rq.n_x);
     d.x_grids = arena.alloc<double>(static_cast<size_t>(S) * rq.n_x);
@@ -396,26 +421,34 @@ void run_leverage(ob_leverage_request& rq) {
     const size_t bin_smem = (static_cast<size_t>(nb) + 1) * sizeof(unsigned long long) +
                             (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0) +
                             (static_cast<size_t>(nf) + nb) * sizeof(unsigned);
+    const size_t merge_smem = static_cast<size_t>(nf) * sizeof(unsigned);
     check_cuda(cudaFuncSetAttribute(lev_bin<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(bin_smem)),
                "cudaFuncSetAttribute");
-    // one block an SM (fewer for small particle counts): the partials stay few, each block bins many particles
+    check_cuda(cudaFuncSetAttribute(lev_merge, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(merge_smem)),
+               "cudaFuncSetAttribute");
+    // one binning block an SM (fewer for small particle counts): the partials stay few, each block bins many particles
     d.n_part = static_cast<int>(std::max<long long>(1, std::min<long long>(sms, (n + 511) / 512)));
     d.part_u32 = arena.alloc<unsigned>(static_cast<size_t>(d.n_part) * (nf + nb));
     d.part_i64 = arena.alloc<long long>(static_cast<size_t>(d.n_part) * (nb + 1));
     d.part_f64 = ll ? arena.alloc<double>(static_cast<size_t>(d.n_part) * 3 * nb) : nullptr;
+    d.n_step_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(4LL * sms, (rq.n_pairs + 255) / 256)));
+    d.part_range = arena.alloc<double>(2 * static_cast<size_t>(d.n_step_blocks));
+    d.stats = arena.alloc<double>(4);
+    d.done = arena.alloc<unsigned>(1);
+    check_cuda(cudaMemset(d.done, 0, sizeof(unsigned)), "cudaMemset");
     const int n_merge = nf + nb + nb + 1 + (ll ? 3 * nb : 0);
-    const unsigned step_grid = static_cast<unsigned>((rq.n_pairs + 255) / 256);
     const double n_particles = 2.0 * static_cast<double>(rq.n_pairs);
-    lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256>>>(x, v, n, static_cast<R>(rq.v0), d.range);
+    lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256>>>(x, v, n, static_cast<R>(rq.v0));
     check_cuda(cudaGetLastError(), "lev_init launch");
     for (int i = 0; i < S; ++i) {
         if (i > 0) {
-            lev_bin<R><<<d.n_part, 512, bin_smem>>>(d, x, v, i & 1);
-            lev_merge<<<(n_merge + 255) / 256, 256>>>(d);
+            lev_bin<R><<<d.n_part, 512, bin_smem>>>(d, x, v);
+            lev_merge<<<(n_merge + 31) / 32, 256, merge_smem>>>(d);
         }
         lev_regress<<<rq.n_x, 256>>>(d, i, n_particles);
-        lev_step<R><<<step_grid, 256>>>(d, x, v, i);
+        lev_step<R><<<d.n_step_blocks, 256>>>(d, x, v, i);
     }
     check_cuda(cudaGetLastError(), "leverage launches");
     check_cuda(cudaMemcpy(rq.x_grids, d.x_grids, static_cast<size_t>(S) * rq.n_x * sizeof(double),
