@@ -3,20 +3,20 @@
 // the particle device of RC/src/leverage.cpp:156-214 / RC/src/leverage_gpu.cu:40-106.
 //
 // Per step i, everything stays on the device (the reference crosses PCIe three times a step):
-//   lev_bin        one block an SM: its particles into a private fine histogram (u32) and regression bins (u32
-//                  count, the v sums in 64-bit fixed point, the local-linear moments in FP64) in shared memory, then
-//                  stored whole as the block's partial (no global atomics)
-//   lev_merge      the blocks' partials added in a fixed order (so the step's counts and sums do not depend on the
-//                  schedule); the last block to finish computes the range of x and the two quantiles of the fine
-//                  histogram that bound the regression grid (the reference's first-match search, by a block scan)
-//   lev_regress    one block per grid point g: the Gaussian-kernel regression E[v | x_g] (Nadaraya-Watson or local
-//                  linear) over the bins in FP64, and L_g = clip(sqrt(sigma_loc^2 / E), lmin, lmax) with the local
-//                  variance interpolated on its uniform row; the row and the grid go straight into the output tables
+//   lev_bin        one block an SM: its particles into a private fine histogram and regression bins in shared
+//                  memory (u32 counts, the v sums in 64-bit fixed point, the local-linear moments in FP64), then its
+//                  non-zero entries added into the step's global histogram and bins (integer atomics: the counts and v
+//                  sums do not depend on the order)
+//   lev_regress    one block per grid point g: the quantiles of the fine histogram bound the grid (the reference's
+//                  first-match search, by a block scan), then the Gaussian-kernel regression E[v | x_g]
+//                  (Nadaraya-Watson or local linear) over the bins in FP64, and L_g = clip(sqrt(sigma_loc^2 / E),
+//                  lmin, lmax) with the local variance interpolated on its uniform row; the row and the grid go
+//                  straight into the output tables
 //   lev_step       one thread per antithetic pair (grid-stride): the SLV Euler step with the leverage row staged in
 //                  shared memory, normals from Philox counter (pair, step + 1, 0, 0), each block's min and max of the
-//                  new x stored for the next step (no atomics)
-// Particles are float (OB_FP32) or double (OB_FP64); bins, regression and the leverage ratio are FP64 in both (a v
-// enters its block's sum rounded to 2^-37).
+//                  new x stored for the next step (no atomics); it also clears the histogram and bins just read
+// Particles are float (OB_FP32) or double (OB_FP64); bins, regression and the leverage ratio are FP64 in both (each v
+// enters the sums rounded to 2^-37).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -42,25 +42,21 @@ struct LevDev {
     const double* lv_lo;
     const double* lv_inv_dx;
     const double* lv_rows;
+    // the step's histogram and bins, added into by every binning block, cleared by the step kernel after use
     unsigned* fine;            // n_fine
-    double* acc;               // 5 n_bins + 1 (the last: sum of v)
-    int n_part;                // blocks of lev_bin, each with its partial below
-    unsigned* part_u32;        // n_part x (n_fine + n_bins): fine histogram, counts
-    long long* part_i64;       // n_part x (n_bins + 1): v sums (fixed point), the total v sum
-    double* part_f64;          // n_part x 3 n_bins: x, x^2, x v sums (local linear only)
+    unsigned* cnt;             // n_bins
+    unsigned long long* sv;    // n_bins + 1: v sums in fixed point, then the sum of all v
+    double* acc_ll;            // 3 n_bins: x, x^2, x v sums (local linear only)
     int n_step_blocks;         // blocks of lev_step, each with its min and max of the new x
     double* part_range;        // n_step_blocks x 2
-    double* stats;             // the step's lower and upper quantiles, min and max of x (from lev_merge)
-    unsigned* done;            // lev_merge's finished blocks (the last one computes stats and clears it)
     double* x_eval;            // n_x, the current grid
     double* lev;               // n_x, the current leverage row
     double* x_grids;           // n_steps x n_x
     double* values;            // n_steps x n_x
 };
 
-// The v sums of a binning block are 64-bit fixed point with 2^36 units per unit of v (exact whatever the order of
-// the atomics: |v| may reach 2^27 / particles of a block, far above any variance); the merge adds the blocks' sums in
-// FP64 in block order.
+// The v sums are 64-bit fixed point with 2^36 units per unit of v: integer additions, so the sums are the same
+// whatever the order of the atomics (|v| may reach 2^27 / particles, far above any variance).
 constexpr double kFix = 68719476736.0;
 
 __device__ __forceinline__ long long warp_sum_i64(long long v) {
@@ -93,7 +89,8 @@ __global__ void lev_init(R* x, R* v, long long n, R v0) {
     if (j < n) x[j] = R(0), v[j] = v0;
 }
 
-// Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU.
+// Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU. A block bins its
+// particles in shared memory, then adds its non-zero entries into the step's global histogram and bins.
 template <typename R>
 __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x, const R* __restrict__ v) {
     extern __shared__ __align__(16) unsigned char sm[];
@@ -133,14 +130,14 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     tot = warp_sum_i64(tot);
     if ((threadIdx.x & 31) == 0) atomicAdd(&s_sv[nb], static_cast<unsigned long long>(tot));
     __syncthreads();
-    unsigned* pu = d.part_u32 + static_cast<long long>(blockIdx.x) * (nf + nb);
-    long long* pi = d.part_i64 + static_cast<long long>(blockIdx.x) * (nb + 1);
-    for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) pu[k] = s_fine[k];
-    for (int k = threadIdx.x; k < nb + 1; k += blockDim.x) pi[k] = static_cast<long long>(s_sv[k]);
-    if (ll) {
-        double* pf = d.part_f64 + static_cast<long long>(blockIdx.x) * 3 * nb;
-        for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) pf[k] = s_ll[k];
-    }
+    for (int k = threadIdx.x; k < nf; k += blockDim.x)
+        if (s_fine[k]) atomicAdd(&d.fine[k], s_fine[k]);
+    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+        if (s_cnt[k]) atomicAdd(&d.cnt[k], s_cnt[k]), atomicAdd(&d.sv[k], s_sv[k]);
+    if (threadIdx.x == 0) atomicAdd(&d.sv[nb], s_sv[nb]);
+    if (ll)
+        for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x)
+            if (s_ll[k] != 0.0) atomicAdd(&d.acc_ll[k], s_ll[k]);
 }
 
 // Exclusive prefix of x over the block and the block's total (any block size that is a multiple of 32, up to 1024).
@@ -165,93 +162,6 @@ __device__ unsigned long long block_scan(unsigned long long x, unsigned long lon
     return before + inc - x;
 }
 
-// The step's histogram and bins, then its quantiles. Block: 32 entries (one a lane) x 8 warps; warp w adds the
-// partials w, w + 8, ... and the block adds the warps in order, so every entry is the same sum on every run. The last
-// block to finish (a ticket, no waiting) computes the range of x and the quantiles of the merged fine histogram
-// (RC/src/leverage.cpp:26-38: the first fine bin k with a count and (counts before k) + count >= q total, at
-// lo + (k + (q total - before) / count) width), each thread scanning a run of bins after a block scan of the runs'
-// counts. Dynamic shared memory: the fine histogram (n_fine u32).
-__global__ void __launch_bounds__(256) lev_merge(LevDev d) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ double s_part[8][32];
-    __shared__ unsigned long long s_warp[32];
-    __shared__ double s_cum[2][256];
-    __shared__ int s_best[2];
-    __shared__ double s_mn[8], s_mx[8];
-    __shared__ bool s_last;
-    const int nb = d.n_bins, nf = d.n_fine, P = d.n_part;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int e = blockIdx.x * 32 + lane;
-    const int n_u = nf + nb, n_i = nb + 1, n_f = d.local_linear ? 3 * nb : 0;
-    double s = 0.0;
-    if (e < n_u) {
-        unsigned long long c = 0;
-        for (int b = warp; b < P; b += 8) c += d.part_u32[static_cast<long long>(b) * n_u + e];
-        s = static_cast<double>(c);
-    } else if (e < n_u + n_i) {
-        const int k = e - n_u;
-        for (int b = warp; b < P; b += 8) s += static_cast<double>(d.part_i64[static_cast<long long>(b) * n_i + k]) / kFix;
-    } else if (e < n_u + n_i + n_f) {
-        const int k = e - n_u - n_i;
-        for (int b = warp; b < P; b += 8) s += d.part_f64[static_cast<long long>(b) * n_f + k];
-    }
-    s_part[warp][lane] = s;
-    __syncthreads();
-    if (warp == 0) {
-        double t = 0.0;
-        for (int w = 0; w < 8; ++w) t += s_part[w][lane];
-        if (e < nf) d.fine[e] = static_cast<unsigned>(t);
-        else if (e < n_u) d.acc[e - nf] = t;
-        else if (e < n_u + n_i) d.acc[e - n_u < nb ? nb + (e - n_u) : 5 * nb] = t;
-        else if (e < n_u + n_i + n_f) d.acc[2 * nb + (e - n_u - n_i)] = t;
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(d.done, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    // the last block: the merged histogram is complete
-    unsigned* s_fine = reinterpret_cast<unsigned*>(sm);
-    for (int k = threadIdx.x; k < nf; k += blockDim.x) s_fine[k] = __ldcg(d.fine + k);
-    if (threadIdx.x < 2) s_best[threadIdx.x] = nf;
-    double lo, hi;
-    range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also order the loads above)
-    const int t = threadIdx.x, per = (nf + blockDim.x - 1) / blockDim.x;
-    const int a = min(t * per, nf), b = min(a + per, nf);
-    unsigned long long mine = 0;
-    for (int k = a; k < b; ++k) mine += s_fine[k];
-    unsigned long long total_u;
-    const unsigned long long before = block_scan(mine, s_warp, total_u);
-    const double total = static_cast<double>(total_u);
-    const double q2[2] = {d.q_lo, d.q_hi};
-#pragma unroll
-    for (int qi = 0; qi < 2; ++qi) {
-        const double target = q2[qi] * total;
-        double cum = static_cast<double>(before);
-        for (int k = a; k < b; ++k) {
-            const unsigned c = s_fine[k];
-            const double next = cum + static_cast<double>(c);
-            if (next >= target && c > 0) {
-                atomicMin(&s_best[qi], k);
-                s_cum[qi][t] = cum;
-                break;
-            }
-            cum = next;
-        }
-    }
-    __syncthreads();
-    if (t < 2) {
-        const int kb = s_best[t];
-        const double width = (hi - lo) / static_cast<double>(nf);
-        d.stats[t] = kb >= nf ? hi
-                              : lo + (static_cast<double>(kb) + (q2[t] * total - s_cum[t][kb / per]) /
-                                                                    static_cast<double>(s_fine[kb])) *
-                                         width;
-    }
-    if (t == 0) d.stats[2] = lo, d.stats[3] = hi, *d.done = 0u;
-}
-
 __device__ __forceinline__ double interp_uniform(double x, double a, double b, const double* y, int n) {
     const double u = (x - a) / (b - a) * (n - 1);
     if (!(u > 0)) return y[0];
@@ -262,10 +172,18 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 }
 
 // Grid, regression and leverage of step i; block g computes grid point g. Step 0 uses the reference's initial grid
-// and E[v | x] = v0; later steps read the grid's bounds (the quantiles) and the bins from lev_merge.
+// and E[v | x] = v0. The grid's bounds are the quantiles of the fine histogram (RC/src/leverage.cpp:26-38: the first
+// fine bin k with a count and (counts before k) + count >= q total, at lo + (k + (q total - before) / count) width),
+// computed in every block from the histogram staged in shared memory (dynamic, n_fine u32): each thread scans a run
+// of bins after a block scan of the runs' counts.
 __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_particles) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ unsigned long long s_warp[32];
+    __shared__ double s_cum[2][256];
+    __shared__ int s_best[2];
     __shared__ double s_red[5][32];
-    const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, t = threadIdx.x;
+    __shared__ double s_mn[8], s_mx[8];
+    const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
     const double t0 = d.t0[i], h = d.dt[i];
     double x0, cond;
@@ -273,16 +191,55 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
         x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
         cond = d.v0;
     } else {
-        const double qa = d.stats[0], qb = d.stats[1], lo = d.stats[2], hi = d.stats[3];
-        x0 = qa + (qb - qa) * g / (nx - 1);
+        unsigned* s_fine = reinterpret_cast<unsigned*>(sm);
+        for (int k = t; k < nf; k += blockDim.x) s_fine[k] = d.fine[k];
+        if (t < 2) s_best[t] = nf;
+        double lo, hi;
+        range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also order the staging above)
+        const int per = (nf + blockDim.x - 1) / blockDim.x;
+        const int a = min(t * per, nf), b = min(a + per, nf);
+        unsigned long long mine = 0;
+        for (int k = a; k < b; ++k) mine += s_fine[k];
+        unsigned long long total_u;
+        const unsigned long long before = block_scan(mine, s_warp, total_u);
+        const double total = static_cast<double>(total_u);
+        const double q2[2] = {d.q_lo, d.q_hi};
+#pragma unroll
+        for (int qi = 0; qi < 2; ++qi) {
+            const double target = q2[qi] * total;
+            double cum = static_cast<double>(before);
+            for (int k = a; k < b; ++k) {
+                const unsigned c = s_fine[k];
+                const double next = cum + static_cast<double>(c);
+                if (next >= target && c > 0) {
+                    atomicMin(&s_best[qi], k);
+                    s_cum[qi][t] = cum;
+                    break;
+                }
+                cum = next;
+            }
+        }
+        __syncthreads();
+        const double width = (hi - lo) / static_cast<double>(nf);
+        double qv[2];
+#pragma unroll
+        for (int qi = 0; qi < 2; ++qi) {
+            const int kb = s_best[qi];
+            qv[qi] = kb >= nf ? hi
+                              : lo + (static_cast<double>(kb) + (q2[qi] * total - s_cum[qi][kb / per]) /
+                                                                    static_cast<double>(s_fine[kb])) *
+                                         width;
+        }
+        x0 = qv[0] + (qv[1] - qv[0]) * g / (nx - 1);
         const double bw = d.bw_scale * d.atm_vol * sqrt(t0 > 0.15 ? t0 : 0.15) * pow(n_particles, -0.2);
         const double wc = (hi + 1e-12 - lo) / nb;
-        const double *cnt = d.acc, *sv = cnt + nb, *sx = sv + nb, *sxx = sx + nb, *sxv = sxx + nb;
+        const double *sx = d.acc_ll, *sxx = sx + nb, *sxv = sxx + nb;
         double r[5] = {0, 0, 0, 0, 0};
         for (int k = t; k < nb; k += blockDim.x) {
             const double c = lo + (k + 0.5) * wc;
             const double dd = (x0 - c) / bw, w = exp(-0.5 * dd * dd);
-            r[0] += w * cnt[k], r[1] += w * sv[k];
+            const double sv = static_cast<double>(static_cast<long long>(d.sv[k])) / kFix;
+            r[0] += w * static_cast<double>(d.cnt[k]), r[1] += w * sv;
             if (d.local_linear) r[2] += w * sx[k], r[3] += w * sxx[k], r[4] += w * sxv[k];
         }
 #pragma unroll
@@ -297,7 +254,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
             for (int w = 0; w < nw; ++w) r[q] += s_red[q][w];
         }
         const double S0 = r[0], T0 = r[1], Ax = r[2], Axx = r[3], Axv = r[4];
-        const double fallback = d.acc[5 * nb] / n_particles;
+        const double fallback = static_cast<double>(static_cast<long long>(d.sv[nb])) / kFix / n_particles;
         const double nw_e = S0 > 1e-8 ? T0 / (S0 > 1e-300 ? S0 : 1e-300) : fallback;
         cond = nw_e;
         if (d.local_linear) {
@@ -321,11 +278,22 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
     }
 }
 
-// The SLV Euler step of every pair (grid-stride), and the block's min and max of the new x into part_range.
+// The SLV Euler step of every pair (grid-stride), and the block's min and max of the new x into part_range. The step's
+// histogram and bins are read (lev_regress is done): the blocks clear them for the next step's binning.
 template <typename R>
 __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v, int i) {
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[8], s_max[8];
+    {
+        const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0;
+        const int stride = gridDim.x * blockDim.x;
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nf + nb + nb + 1 + n_ll; k += stride) {
+            if (k < nf) d.fine[k] = 0u;
+            else if (k < nf + nb) d.cnt[k - nf] = 0u;
+            else if (k < nf + 2 * nb + 1) d.sv[k - nf - nb] = 0ull;
+            else d.acc_ll[k - nf - 2 * nb - 1] = 0.0;
+        }
+    }
     for (int g = threadIdx.x; g < d.n_x; g += blockDim.x) s_lev[g] = static_cast<R>(d.lev[g]);
     __syncthreads();
     const int nx = d.n_x;
@@ -409,45 +377,41 @@ void run_leverage(ob_leverage_request& rq) {
     d.lv_lo = arena.put<double>(rq.lv_lo, S);
     d.lv_inv_dx = arena.put<double>(rq.lv_inv_dx, S);
     d.lv_rows = arena.put<double>(rq.lv_rows, static_cast<size_t>(S) * rq.n_lv);
-    d.fine = arena.alloc<unsigned>(rq.n_fine);
-    d.acc = arena.alloc<double>(5 * static_cast<size_t>(rq.n_bins) + 1);
+    const int nb = rq.n_bins, nf = rq.n_fine, ll = rq.local_linear;
+    d.fine = arena.alloc<unsigned>(nf);
+    d.cnt = arena.alloc<unsigned>(nb);
+    d.sv = arena.alloc<unsigned long long>(nb + 1);
+    d.acc_ll = arena.alloc<double>(3 * static_cast<size_t>(nb));
+    check_cuda(cudaMemset(d.fine, 0, nf * sizeof(unsigned)), "cudaMemset");
+    check_cuda(cudaMemset(d.cnt, 0, nb * sizeof(unsigned)), "cudaMemset");
+    check_cuda(cudaMemset(d.sv, 0, (nb + 1) * sizeof(unsigned long long)), "cudaMemset");
+    check_cuda(cudaMemset(d.acc_ll, 0, 3 * nb * sizeof(double)), "cudaMemset");
     d.x_eval = arena.alloc<double>(rq.n_x);
     d.lev = arena.alloc<double>(rq.n_x);
     d.x_grids = arena.alloc<double>(static_cast<size_t>(S) * rq.n_x);
     d.values = arena.alloc<double>(static_cast<size_t>(S) * rq.n_x);
     R* x = arena.alloc<R>(n);
     R* v = arena.alloc<R>(n);
-    const int nb = rq.n_bins, nf = rq.n_fine, ll = rq.local_linear;
     const size_t bin_smem = (static_cast<size_t>(nb) + 1) * sizeof(unsigned long long) +
                             (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0) +
                             (static_cast<size_t>(nf) + nb) * sizeof(unsigned);
-    const size_t merge_smem = static_cast<size_t>(nf) * sizeof(unsigned);
+    const size_t reg_smem = static_cast<size_t>(nf) * sizeof(unsigned);
     check_cuda(cudaFuncSetAttribute(lev_bin<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(bin_smem)),
                "cudaFuncSetAttribute");
-    check_cuda(cudaFuncSetAttribute(lev_merge, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(merge_smem)),
+    check_cuda(cudaFuncSetAttribute(lev_regress, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(reg_smem)),
                "cudaFuncSetAttribute");
-    // one binning block an SM (fewer for small particle counts): the partials stay few, each block bins many particles
-    d.n_part = static_cast<int>(std::max<long long>(1, std::min<long long>(sms, (n + 511) / 512)));
-    d.part_u32 = arena.alloc<unsigned>(static_cast<size_t>(d.n_part) * (nf + nb));
-    d.part_i64 = arena.alloc<long long>(static_cast<size_t>(d.n_part) * (nb + 1));
-    d.part_f64 = ll ? arena.alloc<double>(static_cast<size_t>(d.n_part) * 3 * nb) : nullptr;
+    // one binning block an SM (fewer for small particle counts): each block bins many particles before it adds
+    const int n_bin_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(sms, (n + 511) / 512)));
     d.n_step_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(4LL * sms, (rq.n_pairs + 255) / 256)));
     d.part_range = arena.alloc<double>(2 * static_cast<size_t>(d.n_step_blocks));
-    d.stats = arena.alloc<double>(4);
-    d.done = arena.alloc<unsigned>(1);
-    check_cuda(cudaMemset(d.done, 0, sizeof(unsigned)), "cudaMemset");
-    const int n_merge = nf + nb + nb + 1 + (ll ? 3 * nb : 0);
     const double n_particles = 2.0 * static_cast<double>(rq.n_pairs);
     lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256>>>(x, v, n, static_cast<R>(rq.v0));
     check_cuda(cudaGetLastError(), "lev_init launch");
     for (int i = 0; i < S; ++i) {
-        if (i > 0) {
-            lev_bin<R><<<d.n_part, 512, bin_smem>>>(d, x, v);
-            lev_merge<<<(n_merge + 31) / 32, 256, merge_smem>>>(d);
-        }
-        lev_regress<<<rq.n_x, 256>>>(d, i, n_particles);
+        if (i > 0) lev_bin<R><<<n_bin_blocks, 512, bin_smem>>>(d, x, v);
+        lev_regress<<<rq.n_x, 256, i > 0 ? reg_smem : 0>>>(d, i, n_particles);
         lev_step<R><<<d.n_step_blocks, 256>>>(d, x, v, i);
     }
     check_cuda(cudaGetLastError(), "leverage launches");
