@@ -68,8 +68,17 @@ __device__ __forceinline__ long long warp_sum_i64(long long v) {
 // Min and max of x over the last step's blocks, in every thread of the calling block (any multiple of 32 threads).
 __device__ void range_of(const LevDev& d, double& lo, double& hi, double* s_mn, double* s_mx) {
     double mn = 1.0e300, mx = -1.0e300;
-    for (int b = threadIdx.x; b < d.n_step_blocks; b += blockDim.x)
-        mn = fmin(mn, d.part_range[2 * b]), mx = fmax(mx, d.part_range[2 * b + 1]);
+    const double2* pr = reinterpret_cast<const double2*>(d.part_range);
+    for (int b0 = threadIdx.x; b0 < d.n_step_blocks; b0 += 4 * blockDim.x) {
+        double2 r[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int b = b0 + j * blockDim.x;
+            r[j] = b < d.n_step_blocks ? pr[b] : make_double2(1.0e300, -1.0e300);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mn = fmin(mn, r[j].x), mx = fmax(mx, r[j].y);
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, off));
@@ -110,22 +119,33 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     const R wf = (hi - lo) / static_cast<R>(nf), we = (hi + static_cast<R>(1e-12) - lo) / static_cast<R>(nb);
     const long long n = 2 * d.n_pairs;
     long long tot = 0;
-    for (long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
-         j += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const R xj = x[j], vj = d.positive_part ? m_max(v[j], R(0)) : v[j];
-        const int f = wf > R(0) ? static_cast<int>((xj - lo) / wf) : 0;
-        atomicAdd(&s_fine[min(max(f, 0), nf - 1)], 1u);
-        const int k = min(max(static_cast<int>((xj - lo) / we), 0), nb - 1);
-        const double xd = static_cast<double>(xj), vd = static_cast<double>(vj);
-        const long long q = __double2ll_rn(vd * kFix);
-        atomicAdd(&s_cnt[k], 1u);
-        atomicAdd(&s_sv[k], static_cast<unsigned long long>(q));
-        if (ll) {
-            atomicAdd(&s_ll[k], xd);
-            atomicAdd(&s_ll[nb + k], xd * xd);
-            atomicAdd(&s_ll[2 * nb + k], xd * vd);
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long j0 = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; j0 < n; j0 += 4 * stride) {
+        // four particles' loads in flight before their atomics
+        R xr[4], vr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long j = j0 + u * stride;
+            xr[u] = j < n ? x[j] : R(0), vr[u] = j < n ? v[j] : R(0);
         }
-        tot += q;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (j0 + u * stride >= n) break;
+            const R xj = xr[u], vj = d.positive_part ? m_max(vr[u], R(0)) : vr[u];
+            const int f = wf > R(0) ? static_cast<int>((xj - lo) / wf) : 0;
+            atomicAdd(&s_fine[min(max(f, 0), nf - 1)], 1u);
+            const int k = min(max(static_cast<int>((xj - lo) / we), 0), nb - 1);
+            const double xd = static_cast<double>(xj), vd = static_cast<double>(vj);
+            const long long q = __double2ll_rn(vd * kFix);
+            atomicAdd(&s_cnt[k], 1u);
+            atomicAdd(&s_sv[k], static_cast<unsigned long long>(q));
+            if (ll) {
+                atomicAdd(&s_ll[k], xd);
+                atomicAdd(&s_ll[nb + k], xd * xd);
+                atomicAdd(&s_ll[2 * nb + k], xd * vd);
+            }
+            tot += q;
+        }
     }
     tot = warp_sum_i64(tot);
     if ((threadIdx.x & 31) == 0) atomicAdd(&s_sv[nb], static_cast<unsigned long long>(tot));
@@ -192,7 +212,22 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
         cond = d.v0;
     } else {
         unsigned* s_fine = reinterpret_cast<unsigned*>(sm);
-        for (int k = t; k < nf; k += blockDim.x) s_fine[k] = d.fine[k];
+        {
+            // staged 16 bytes a load, eight loads in flight a thread (a load-then-store loop would wait on each)
+            const uint4* src = reinterpret_cast<const uint4*>(d.fine);
+            uint4* dst = reinterpret_cast<uint4*>(s_fine);
+            const int n4 = nf / 4;
+            for (int k0 = t; k0 < n4; k0 += 8 * blockDim.x) {
+                uint4 r[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (k0 + j * static_cast<int>(blockDim.x) < n4) r[j] = src[k0 + j * blockDim.x];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (k0 + j * static_cast<int>(blockDim.x) < n4) dst[k0 + j * blockDim.x] = r[j];
+            }
+            for (int k = 4 * n4 + t; k < nf; k += blockDim.x) s_fine[k] = d.fine[k];
+        }
         if (t < 2) s_best[t] = nf;
         double lo, hi;
         range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also order the staging above)
