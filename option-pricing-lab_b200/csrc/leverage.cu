@@ -194,8 +194,8 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 // Grid, regression and leverage of step i; block g computes grid point g. Step 0 uses the reference's initial grid
 // and E[v | x] = v0. The grid's bounds are the quantiles of the fine histogram (RC/src/leverage.cpp:26-38: the first
 // fine bin k with a count and (counts before k) + count >= q total, at lo + (k + (q total - before) / count) width),
-// computed in every block from the histogram staged in shared memory (dynamic, n_fine u32): each thread scans a run
-// of bins after a block scan of the runs' counts.
+// computed in every block from the histogram staged in shared memory (dynamic: n_fine u32 and a word every 32 bins):
+// each thread scans a run of bins after a block scan of the runs' counts.
 __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_particles) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ unsigned long long s_warp[32];
@@ -211,11 +211,12 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
         x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
         cond = d.v0;
     } else {
+        // the histogram in shared memory with a word of padding every 32 bins (bin k at k + k / 32), so that the
+        // threads' runs of consecutive bins sit in different banks
         unsigned* s_fine = reinterpret_cast<unsigned*>(sm);
         {
             // staged 16 bytes a load, eight loads in flight a thread (a load-then-store loop would wait on each)
             const uint4* src = reinterpret_cast<const uint4*>(d.fine);
-            uint4* dst = reinterpret_cast<uint4*>(s_fine);
             const int n4 = nf / 4;
             for (int k0 = t; k0 < n4; k0 += 8 * blockDim.x) {
                 uint4 r[8];
@@ -223,10 +224,15 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
                 for (int j = 0; j < 8; ++j)
                     if (k0 + j * static_cast<int>(blockDim.x) < n4) r[j] = src[k0 + j * blockDim.x];
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    if (k0 + j * static_cast<int>(blockDim.x) < n4) dst[k0 + j * blockDim.x] = r[j];
+                for (int j = 0; j < 8; ++j) {
+                    const int m = 4 * (k0 + j * static_cast<int>(blockDim.x));
+                    if (m < 4 * n4) {
+                        s_fine[m + (m >> 5)] = r[j].x, s_fine[m + 1 + ((m + 1) >> 5)] = r[j].y;
+                        s_fine[m + 2 + ((m + 2) >> 5)] = r[j].z, s_fine[m + 3 + ((m + 3) >> 5)] = r[j].w;
+                    }
+                }
             }
-            for (int k = 4 * n4 + t; k < nf; k += blockDim.x) s_fine[k] = d.fine[k];
+            for (int k = 4 * n4 + t; k < nf; k += blockDim.x) s_fine[k + (k >> 5)] = d.fine[k];
         }
         if (t < 2) s_best[t] = nf;
         double lo, hi;
@@ -234,7 +240,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
         const int per = (nf + blockDim.x - 1) / blockDim.x;
         const int a = min(t * per, nf), b = min(a + per, nf);
         unsigned long long mine = 0;
-        for (int k = a; k < b; ++k) mine += s_fine[k];
+        for (int k = a; k < b; ++k) mine += s_fine[k + (k >> 5)];
         unsigned long long total_u;
         const unsigned long long before = block_scan(mine, s_warp, total_u);
         const double total = static_cast<double>(total_u);
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
             const double target = q2[qi] * total;
             double cum = static_cast<double>(before);
             for (int k = a; k < b; ++k) {
-                const unsigned c = s_fine[k];
+                const unsigned c = s_fine[k + (k >> 5)];
                 const double next = cum + static_cast<double>(c);
                 if (next >= target && c > 0) {
                     atomicMin(&s_best[qi], k);
@@ -262,7 +268,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
             const int kb = s_best[qi];
             qv[qi] = kb >= nf ? hi
                               : lo + (static_cast<double>(kb) + (q2[qi] * total - s_cum[qi][kb / per]) /
-                                                                    static_cast<double>(s_fine[kb])) *
+                                                                    static_cast<double>(s_fine[kb + (kb >> 5)])) *
                                          width;
         }
         x0 = qv[0] + (qv[1] - qv[0]) * g / (nx - 1);
@@ -430,7 +436,7 @@ void run_leverage(ob_leverage_request& rq) {
     const size_t bin_smem = (static_cast<size_t>(nb) + 1) * sizeof(unsigned long long) +
                             (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0) +
                             (static_cast<size_t>(nf) + nb) * sizeof(unsigned);
-    const size_t reg_smem = static_cast<size_t>(nf) * sizeof(unsigned);
+    const size_t reg_smem = (static_cast<size_t>(nf) + nf / 32 + 1) * sizeof(unsigned);
     check_cuda(cudaFuncSetAttribute(lev_bin<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(bin_smem)),
                "cudaFuncSetAttribute");
