@@ -61,6 +61,18 @@ int require_device();
 // ------------------------------------------------------------------------------------------------ device memory
 
 // Owns device allocations for one call or one plan.
+// A non-blocking stream owned by one call, destroyed with it.
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream() { check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate"); }
+    ~Stream() {
+        if (s) cudaStreamDestroy(s);
+    }
+    Stream(const Stream&) = delete;
+    Stream& operator=(const Stream&) = delete;
+    cudaStream_t get() const { return s; }
+};
+
 struct DeviceArena {
     void* ptrs[64] = {};
     int n = 0;

@@ -42,6 +42,7 @@ struct LevDev {
     const double* lv_lo;
     const double* lv_inv_dx;
     const double* lv_rows;
+    const double* bw;          // n_steps: the kernel bandwidth of each step, computed on the host
     // the step's histogram and bins, added into by every binning block, cleared by the step kernel after use
     unsigned* fine;            // n_fine
     unsigned* cnt;             // n_bins
@@ -92,6 +93,10 @@ __device__ void range_of(const LevDev& d, double& lo, double& hi, double* s_mn, 
     __syncthreads();
 }
 
+// Programmatic dependent launch: the step's kernels are launched while the previous one runs, and each waits here,
+// before its first read of the previous kernel's output, until that kernel has finished and its writes are visible.
+__device__ __forceinline__ void wait_previous() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename R>
 __global__ void lev_init(R* x, R* v, long long n, R v0) {
     const long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -113,6 +118,7 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     if (ll)
         for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) s_ll[k] = 0.0;
     for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) s_fine[k] = 0u;
+    wait_previous();
     double lo_d, hi_d;
     range_of(d, lo_d, hi_d, s_mn, s_mx);  // (its barrier also orders the clearing above)
     const R lo = static_cast<R>(lo_d), hi = static_cast<R>(hi_d);
@@ -205,7 +211,8 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
     __shared__ double s_mn[8], s_mx[8];
     const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-    const double t0 = d.t0[i], h = d.dt[i];
+    const double h = d.dt[i];
+    wait_previous();
     double x0, cond;
     if (i == 0) {
         x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
@@ -272,7 +279,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
                                          width;
         }
         x0 = qv[0] + (qv[1] - qv[0]) * g / (nx - 1);
-        const double bw = d.bw_scale * d.atm_vol * sqrt(t0 > 0.15 ? t0 : 0.15) * pow(n_particles, -0.2);
+        const double bw = d.bw[i];
         const double wc = (hi + 1e-12 - lo) / nb;
         const double *sx = d.acc_ll, *sxx = sx + nb, *sxv = sxx + nb;
         double r[5] = {0, 0, 0, 0, 0};
@@ -325,6 +332,7 @@ template <typename R>
 __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v, int i) {
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[8], s_max[8];
+    wait_previous();
     {
         const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0;
         const int stride = gridDim.x * blockDim.x;
@@ -448,20 +456,42 @@ void run_leverage(ob_leverage_request& rq) {
     d.n_step_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(4LL * sms, (rq.n_pairs + 255) / 256)));
     d.part_range = arena.alloc<double>(2 * static_cast<size_t>(d.n_step_blocks));
     const double n_particles = 2.0 * static_cast<double>(rq.n_pairs);
-    lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256>>>(x, v, n, static_cast<R>(rq.v0));
+    // the kernel bandwidth of each step, as RC/src/leverage.cpp:63 computes it
+    std::vector<double> bw(S);
+    for (int i = 0; i < S; ++i)
+        bw[i] = rq.bandwidth_scale * rq.atm_vol * std::sqrt(std::max(rq.t0[i], 0.15)) * std::pow(n_particles, -0.2);
+    d.bw = arena.put<double>(bw.data(), S);
+    Stream stream;
+    cudaStream_t st = stream.get();
+    cudaLaunchAttribute pdl[1];
+    pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    pdl[0].val.programmaticStreamSerializationAllowed = 1;
+    auto config = [&](unsigned grid, unsigned block, size_t smem) {
+        cudaLaunchConfig_t c{};
+        c.gridDim = dim3(grid), c.blockDim = dim3(block), c.dynamicSmemBytes = smem, c.stream = st;
+        c.attrs = pdl, c.numAttrs = 1;
+        return c;
+    };
+    lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(x, v, n, static_cast<R>(rq.v0));
     check_cuda(cudaGetLastError(), "lev_init launch");
+    const cudaLaunchConfig_t c_bin = config(n_bin_blocks, 512, bin_smem);
+    const cudaLaunchConfig_t c_step = config(d.n_step_blocks, 256, 0);
+    const cudaLaunchConfig_t c_reg0 = config(rq.n_x, 256, 0), c_reg = config(rq.n_x, 256, reg_smem);
+    const R* cx = x;
+    const R* cv = v;
     for (int i = 0; i < S; ++i) {
-        if (i > 0) lev_bin<R><<<n_bin_blocks, 512, bin_smem>>>(d, x, v);
-        lev_regress<<<rq.n_x, 256, i > 0 ? reg_smem : 0>>>(d, i, n_particles);
-        lev_step<R><<<d.n_step_blocks, 256>>>(d, x, v, i);
+        if (i > 0) check_cuda(cudaLaunchKernelEx(&c_bin, lev_bin<R>, d, cx, cv), "lev_bin launch");
+        check_cuda(cudaLaunchKernelEx(i > 0 ? &c_reg : &c_reg0, lev_regress, d, i, n_particles), "lev_regress launch");
+        check_cuda(cudaLaunchKernelEx(&c_step, lev_step<R>, d, x, v, i), "lev_step launch");
     }
     check_cuda(cudaGetLastError(), "leverage launches");
-    check_cuda(cudaMemcpy(rq.x_grids, d.x_grids, static_cast<size_t>(S) * rq.n_x * sizeof(double),
-                          cudaMemcpyDeviceToHost),
+    check_cuda(cudaMemcpyAsync(rq.x_grids, d.x_grids, static_cast<size_t>(S) * rq.n_x * sizeof(double),
+                               cudaMemcpyDeviceToHost, st),
                "copy x_grids");
-    check_cuda(cudaMemcpy(rq.values, d.values, static_cast<size_t>(S) * rq.n_x * sizeof(double),
-                          cudaMemcpyDeviceToHost),
+    check_cuda(cudaMemcpyAsync(rq.values, d.values, static_cast<size_t>(S) * rq.n_x * sizeof(double),
+                               cudaMemcpyDeviceToHost, st),
                "copy values");
+    check_cuda(cudaStreamSynchronize(st), "leverage");
     rq.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
 }
 
