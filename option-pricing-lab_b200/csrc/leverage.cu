@@ -45,6 +45,7 @@ struct LevDev {
     const double* bw;          // n_steps: the kernel bandwidth of each step, computed on the host
     // the step's histogram and bins, added into by every binning block, cleared by the step kernel after use
     unsigned* fine;            // n_fine
+    unsigned* chunk;           // (n_fine + 31) / 32: totals of 32-bin chunks of fine
     unsigned* cnt;             // n_bins
     unsigned long long* sv;    // n_bins + 1: v sums in fixed point, then the sum of all v
     double* acc_ll;            // 3 n_bins: x, x^2, x v sums (local linear only)
@@ -158,6 +159,17 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     __syncthreads();
     for (int k = threadIdx.x; k < nf; k += blockDim.x)
         if (s_fine[k]) atomicAdd(&d.fine[k], s_fine[k]);
+    {
+        // the block's 32-bin chunk totals: a warp a chunk, a lane a bin
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_ch = (nf + 31) / 32;
+        for (int c = warp; c < n_ch; c += blockDim.x >> 5) {
+            const int k = 32 * c + lane;
+            unsigned u = k < nf ? s_fine[k] : 0u;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) u += __shfl_xor_sync(0xffffffffu, u, off);
+            if (lane == 0 && u) atomicAdd(&d.chunk[c], u);
+        }
+    }
     for (int k = threadIdx.x; k < nb; k += blockDim.x)
         if (s_cnt[k]) atomicAdd(&d.cnt[k], s_cnt[k]), atomicAdd(&d.sv[k], s_sv[k]);
     if (threadIdx.x == 0) atomicAdd(&d.sv[nb], s_sv[nb]);
@@ -200,13 +212,12 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 // Grid, regression and leverage of step i; block g computes grid point g. Step 0 uses the reference's initial grid
 // and E[v | x] = v0. The grid's bounds are the quantiles of the fine histogram (RC/src/leverage.cpp:26-38: the first
 // fine bin k with a count and (counts before k) + count >= q total, at lo + (k + (q total - before) / count) width),
-// computed in every block from the histogram staged in shared memory (dynamic: n_fine u32 and a word every 32 bins):
-// each thread scans a run of bins after a block scan of the runs' counts.
+// computed in every block from the chunk totals and, for the chunk that holds each quantile, its 32 bins.
 __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_particles) {
-    extern __shared__ __align__(16) unsigned char sm[];
     __shared__ unsigned long long s_warp[32];
     __shared__ double s_cum[2][256];
     __shared__ int s_best[2];
+    __shared__ double s_q[2];
     __shared__ double s_red[5][32];
     __shared__ double s_mn[8], s_mx[8];
     const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
@@ -218,36 +229,17 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
         x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
         cond = d.v0;
     } else {
-        // the histogram in shared memory with a word of padding every 32 bins (bin k at k + k / 32), so that the
-        // threads' runs of consecutive bins sit in different banks
-        unsigned* s_fine = reinterpret_cast<unsigned*>(sm);
-        {
-            // staged 16 bytes a load, eight loads in flight a thread (a load-then-store loop would wait on each)
-            const uint4* src = reinterpret_cast<const uint4*>(d.fine);
-            const int n4 = nf / 4;
-            for (int k0 = t; k0 < n4; k0 += 8 * blockDim.x) {
-                uint4 r[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    if (k0 + j * static_cast<int>(blockDim.x) < n4) r[j] = src[k0 + j * blockDim.x];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int m = 4 * (k0 + j * static_cast<int>(blockDim.x));
-                    if (m < 4 * n4) {
-                        s_fine[m + (m >> 5)] = r[j].x, s_fine[m + 1 + ((m + 1) >> 5)] = r[j].y;
-                        s_fine[m + 2 + ((m + 2) >> 5)] = r[j].z, s_fine[m + 3 + ((m + 3) >> 5)] = r[j].w;
-                    }
-                }
-            }
-            for (int k = 4 * n4 + t; k < nf; k += blockDim.x) s_fine[k + (k >> 5)] = d.fine[k];
-        }
-        if (t < 2) s_best[t] = nf;
-        double lo, hi;
-        range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also order the staging above)
-        const int per = (nf + blockDim.x - 1) / blockDim.x;
-        const int a = min(t * per, nf), b = min(a + per, nf);
+        // Two levels: each thread owns a run of 32-bin chunks and their totals (kept by lev_bin); a block scan of the
+        // runs gives the counts before every chunk; the first chunk with a count that reaches the target holds the
+        // quantile's bin, and the thread owning it scans that chunk's 32 bins.
+        const int n_ch = (nf + 31) / 32, cpt = (n_ch + blockDim.x - 1) / blockDim.x;
+        const int ca = min(t * cpt, n_ch), cb = min(ca + cpt, n_ch);
+        unsigned mine_c[2] = {0u, 0u};  // cpt <= 2 (n_fine <= 16384)
         unsigned long long mine = 0;
-        for (int k = a; k < b; ++k) mine += s_fine[k + (k >> 5)];
+        for (int c = ca; c < cb; ++c) mine_c[c - ca] = d.chunk[c], mine += mine_c[c - ca];
+        if (t < 2) s_best[t] = n_ch;
+        double lo, hi;
+        range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also publish s_best)
         unsigned long long total_u;
         const unsigned long long before = block_scan(mine, s_warp, total_u);
         const double total = static_cast<double>(total_u);
@@ -256,38 +248,69 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
         for (int qi = 0; qi < 2; ++qi) {
             const double target = q2[qi] * total;
             double cum = static_cast<double>(before);
-            for (int k = a; k < b; ++k) {
-                const unsigned c = s_fine[k + (k >> 5)];
-                const double next = cum + static_cast<double>(c);
-                if (next >= target && c > 0) {
-                    atomicMin(&s_best[qi], k);
+            for (int c = ca; c < cb; ++c) {
+                const unsigned tc = mine_c[c - ca];
+                if (tc > 0 && cum + static_cast<double>(tc) >= target) {
+                    atomicMin(&s_best[qi], c);
                     s_cum[qi][t] = cum;
                     break;
                 }
-                cum = next;
+                cum += static_cast<double>(tc);
             }
         }
         __syncthreads();
         const double width = (hi - lo) / static_cast<double>(nf);
-        double qv[2];
 #pragma unroll
         for (int qi = 0; qi < 2; ++qi) {
-            const int kb = s_best[qi];
-            qv[qi] = kb >= nf ? hi
-                              : lo + (static_cast<double>(kb) + (q2[qi] * total - s_cum[qi][kb / per]) /
-                                                                    static_cast<double>(s_fine[kb + (kb >> 5)])) *
-                                         width;
+            const int cw = s_best[qi];
+            if (cw < n_ch && t == cw / cpt) {
+                // the bins of chunk cw: the first with a count and (counts before it) + count >= target
+                const double target = q2[qi] * total;
+                unsigned cc[32];  // the 32 loads issued together, then the search
+#pragma unroll
+                for (int j = 0; j < 32; ++j) cc[j] = 32 * cw + j < nf ? d.fine[32 * cw + j] : 0u;
+                double cum = s_cum[qi][t];
+                int kb = nf;
+                unsigned cb_count = 0u;
+                double before_kb = 0.0;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const unsigned c = cc[j];
+                    if (kb == nf && c > 0 && cum + static_cast<double>(c) >= target)
+                        kb = 32 * cw + j, cb_count = c, before_kb = cum;
+                    cum += static_cast<double>(c);
+                }
+                s_q[qi] = kb >= nf ? hi
+                                   : lo + (static_cast<double>(kb) + (target - before_kb) /
+                                                                         static_cast<double>(cb_count)) *
+                                              width;
+            } else if (cw >= n_ch && t == 0) {
+                s_q[qi] = hi;
+            }
         }
+        __syncthreads();
+        const double qv[2] = {s_q[0], s_q[1]};
         x0 = qv[0] + (qv[1] - qv[0]) * g / (nx - 1);
         const double bw = d.bw[i];
         const double wc = (hi + 1e-12 - lo) / nb;
         const double *sx = d.acc_ll, *sxx = sx + nb, *sxv = sxx + nb;
         double r[5] = {0, 0, 0, 0, 0};
-        for (int k = t; k < nb; k += blockDim.x) {
+        // n_bins <= 512: at most two bins a thread, their loads issued together
+        unsigned cn[2];
+        unsigned long long sq[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int k = t + u * static_cast<int>(blockDim.x);
+            cn[u] = k < nb ? d.cnt[k] : 0u, sq[u] = k < nb ? d.sv[k] : 0ull;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int k = t + u * static_cast<int>(blockDim.x);
+            if (k >= nb) break;
             const double c = lo + (k + 0.5) * wc;
             const double dd = (x0 - c) / bw, w = exp(-0.5 * dd * dd);
-            const double sv = static_cast<double>(static_cast<long long>(d.sv[k])) / kFix;
-            r[0] += w * static_cast<double>(d.cnt[k]), r[1] += w * sv;
+            const double sv = static_cast<double>(static_cast<long long>(sq[u])) / kFix;
+            r[0] += w * static_cast<double>(cn[u]), r[1] += w * sv;
             if (d.local_linear) r[2] += w * sx[k], r[3] += w * sxx[k], r[4] += w * sxv[k];
         }
 #pragma unroll
@@ -334,13 +357,14 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
     __shared__ R s_min[8], s_max[8];
     wait_previous();
     {
-        const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0;
+        const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0, n_ch = (nf + 31) / 32;
         const int stride = gridDim.x * blockDim.x;
-        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nf + nb + nb + 1 + n_ll; k += stride) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nf + nb + nb + 1 + n_ll + n_ch; k += stride) {
             if (k < nf) d.fine[k] = 0u;
             else if (k < nf + nb) d.cnt[k - nf] = 0u;
             else if (k < nf + 2 * nb + 1) d.sv[k - nf - nb] = 0ull;
-            else d.acc_ll[k - nf - 2 * nb - 1] = 0.0;
+            else if (k < nf + 2 * nb + 1 + n_ll) d.acc_ll[k - nf - 2 * nb - 1] = 0.0;
+            else d.chunk[k - nf - 2 * nb - 1 - n_ll] = 0u;
         }
     }
     for (int g = threadIdx.x; g < d.n_x; g += blockDim.x) s_lev[g] = static_cast<R>(d.lev[g]);
@@ -428,6 +452,8 @@ void run_leverage(ob_leverage_request& rq) {
     d.lv_rows = arena.put<double>(rq.lv_rows, static_cast<size_t>(S) * rq.n_lv);
     const int nb = rq.n_bins, nf = rq.n_fine, ll = rq.local_linear;
     d.fine = arena.alloc<unsigned>(nf);
+    d.chunk = arena.alloc<unsigned>((nf + 31) / 32);
+    check_cuda(cudaMemset(d.chunk, 0, (nf + 31) / 32 * sizeof(unsigned)), "cudaMemset");
     d.cnt = arena.alloc<unsigned>(nb);
     d.sv = arena.alloc<unsigned long long>(nb + 1);
     d.acc_ll = arena.alloc<double>(3 * static_cast<size_t>(nb));
@@ -444,12 +470,8 @@ void run_leverage(ob_leverage_request& rq) {
     const size_t bin_smem = (static_cast<size_t>(nb) + 1) * sizeof(unsigned long long) +
                             (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0) +
                             (static_cast<size_t>(nf) + nb) * sizeof(unsigned);
-    const size_t reg_smem = (static_cast<size_t>(nf) + nf / 32 + 1) * sizeof(unsigned);
     check_cuda(cudaFuncSetAttribute(lev_bin<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(bin_smem)),
-               "cudaFuncSetAttribute");
-    check_cuda(cudaFuncSetAttribute(lev_regress, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(reg_smem)),
                "cudaFuncSetAttribute");
     // one binning block an SM (fewer for small particle counts): each block bins many particles before it adds
     const int n_bin_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(sms, (n + 511) / 512)));
@@ -476,12 +498,12 @@ void run_leverage(ob_leverage_request& rq) {
     check_cuda(cudaGetLastError(), "lev_init launch");
     const cudaLaunchConfig_t c_bin = config(n_bin_blocks, 512, bin_smem);
     const cudaLaunchConfig_t c_step = config(d.n_step_blocks, 256, 0);
-    const cudaLaunchConfig_t c_reg0 = config(rq.n_x, 256, 0), c_reg = config(rq.n_x, 256, reg_smem);
+    const cudaLaunchConfig_t c_reg = config(rq.n_x, 256, 0);
     const R* cx = x;
     const R* cv = v;
     for (int i = 0; i < S; ++i) {
         if (i > 0) check_cuda(cudaLaunchKernelEx(&c_bin, lev_bin<R>, d, cx, cv), "lev_bin launch");
-        check_cuda(cudaLaunchKernelEx(i > 0 ? &c_reg : &c_reg0, lev_regress, d, i, n_particles), "lev_regress launch");
+        check_cuda(cudaLaunchKernelEx(&c_reg, lev_regress, d, i, n_particles), "lev_regress launch");
         check_cuda(cudaLaunchKernelEx(&c_step, lev_step<R>, d, x, v, i), "lev_step launch");
     }
     check_cuda(cudaGetLastError(), "leverage launches");
