@@ -264,6 +264,48 @@ typedef struct {
 
 typedef struct ob_batch ob_batch;
 
+/* ---------------------------------------------------------------------------------------------- payoff scripts */
+
+/* A payoff script of the reference's language (packages/structured/src/optlab/structured/script/), compiled on the
+   host into register bytecode (optlab_b200/script.py) and run on every path while it is simulated. `model` is the
+   simulation (its product fields are unused); names follow the script's underlyings. Registers 0 .. n_const - 1
+   hold `consts` (register 0 is 1.0, the top-level mask), the next ones the variables (0 at the start of a path),
+   then temporaries; n_regs <= 128. `code` is n_code instructions of 4 ints (op, d, a, b), event k running
+   instructions event_code[k] .. event_code[k + 1] - 1 at step end event_step[k] (0: the valuation date) with the
+   discount factor event_discount[k] of its payment date (0: no payment counted). Window w (lowest, highest or
+   realised variance, win_func 0, 1, 2) reads name win_name[w] at the step ends fix_step[win_fix0[w] ..
+   win_fix0[w + 1] - 1]; a variance corridor is [win_lower[w], win_upper[w]] (NaN: no bound). smoothing: the
+   relative width of the comparison ramps (0: hard comparisons). */
+typedef struct {
+    ob_mc_request model;
+    int n_code;
+    const int* code;
+    int n_const;
+    const double* consts;
+    int n_regs;
+    int n_events;
+    const int* event_step;
+    const int* event_code;     /* n_events + 1 */
+    const double* event_discount;
+    int n_windows;             /* <= 32 */
+    const int* win_name;
+    const int* win_func;
+    const int* win_fix0;       /* n_windows + 1 */
+    const int* fix_step;
+    const double* win_lower;
+    const double* win_upper;
+    double smoothing;
+} ob_script_request;
+
+/* price and se of the pair-averaged present value; the paths (legs) on which a payment was not finite, a condition
+   undefined where it mattered, or the redemption weights did not add up to one. */
+typedef struct {
+    double price, se;
+    long long n_paths;
+    long long bad_pay, bad_cond, bad_redemption;
+    double kernel_ms;
+} ob_script_result;
+
 /* ---------------------------------------------------------------------------------------------- entry points */
 
 const char* ob_last_error(void);
@@ -343,6 +385,11 @@ int ob_batch_result(ob_batch* batch, double* price, double* se, double* device_m
    max_classes of them 6 ints each in info: model, names, product, trades, tile (pairs per work item), block. */
 int ob_batch_classes(const ob_batch* batch, int max_classes, int* n_classes, int* info);
 int ob_batch_destroy(ob_batch* batch);
+
+/* Payoff scripts: no counterpart in the reference ABI; it replaces the evaluation of a script on paths brought to
+   the host (packages/structured/src/optlab/structured/engine.py:143-153 with script/evaluator.py:123-231): the
+   paths are simulated and the script evaluated on the device, and only the price and its SE come back. */
+int ob_script_price(const ob_script_request* rq, int precision, ob_script_result* res);
 
 #ifdef __cplusplus
 }

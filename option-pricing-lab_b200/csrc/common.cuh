@@ -192,6 +192,8 @@ struct NormalStream {
 
 // ------------------------------------------------------------------------------------------------ math helpers
 
+__device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double m_abs(double x) { return fabs(x); }
 __device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float m_exp(float x) { return expf(x); }

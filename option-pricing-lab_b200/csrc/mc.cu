@@ -271,30 +271,12 @@ struct Packer {
 
 }  // namespace
 
-void check_mc_request(const ob_mc_request& rq) {
+void check_mc_model(const ob_mc_request& rq) {
     if (rq.model != OB_MODEL_PATHS && rq.model != OB_MODEL_HESTON_QE) invalid("model must be 0 or 1");
     if (rq.n_names < 1 || rq.n_names > OB_MAX_NAMES) invalid("n_names must be 1 to 8");
     if (rq.model == OB_MODEL_HESTON_QE && rq.n_names != 1) invalid("the QE model has one name");
     if (rq.n_pairs < 2 || rq.first_pair < 0) invalid("n_pairs must be >= 2 and first_pair >= 0");
     if (rq.n_steps < 1 || !rq.dt || !rq.t0 || !rq.spot) invalid("null time grid or spot");
-    if (rq.product == OB_PRODUCT_LADDER) {
-        if (rq.n_legs < 1 || rq.n_legs > OB_MAX_OUT - 1 || !rq.leg_type || !rq.leg_strike)
-            invalid("ladder: n_legs must be 1 to 31 with leg_type and leg_strike");
-        for (int k = 0; k < rq.n_legs; ++k) {
-            if (rq.leg_type[k] < 0 || rq.leg_type[k] > 3) invalid("leg_type must be 0 to 3");
-            const int bt = rq.leg_barrier ? rq.leg_barrier[k] : 0;
-            if (bt < 0 || bt > 4) invalid("leg_barrier must be 0 to 4");
-            if (bt && !(rq.leg_level && rq.leg_level[k] > 0)) invalid("a barrier leg needs a positive level");
-        }
-    } else if (rq.product == OB_PRODUCT_AUTOCALL) {
-        if (rq.n_obs < 1 || !rq.obs_step || !rq.obs_discount || !rq.trigger) invalid("autocall: null schedule");
-        for (int j = 0; j < rq.n_obs; ++j)
-            if (rq.obs_step[j] < 1 || rq.obs_step[j] > rq.n_steps || (j && rq.obs_step[j] <= rq.obs_step[j - 1]))
-                invalid("obs_step must be increasing in [1, n_steps]");
-        if (!(rq.ki_barrier >= 0) || !(rq.coupon_barrier >= 0)) invalid("barriers must be >= 0");
-    } else {
-        invalid("product must be 0 or 1");
-    }
     if (rq.model == OB_MODEL_PATHS) {
         if (!rq.root || !rq.kind || !rq.cvar || !rq.heston || !rq.log_fwd) invalid("null array");
         for (int a = 0; a < rq.n_names; ++a) {
@@ -318,6 +300,28 @@ void check_mc_request(const ob_mc_request& rq) {
             invalid("Heston parameters out of range");
         for (int i = 1; i < rq.n_steps; ++i)
             if (std::fabs(rq.dt[i] - rq.dt[0]) > 1e-9 * rq.dt[0]) invalid("the QE model needs uniform steps");
+    }
+}
+
+void check_mc_request(const ob_mc_request& rq) {
+    check_mc_model(rq);
+    if (rq.product == OB_PRODUCT_LADDER) {
+        if (rq.n_legs < 1 || rq.n_legs > OB_MAX_OUT - 1 || !rq.leg_type || !rq.leg_strike)
+            invalid("ladder: n_legs must be 1 to 31 with leg_type and leg_strike");
+        for (int k = 0; k < rq.n_legs; ++k) {
+            if (rq.leg_type[k] < 0 || rq.leg_type[k] > 3) invalid("leg_type must be 0 to 3");
+            const int bt = rq.leg_barrier ? rq.leg_barrier[k] : 0;
+            if (bt < 0 || bt > 4) invalid("leg_barrier must be 0 to 4");
+            if (bt && !(rq.leg_level && rq.leg_level[k] > 0)) invalid("a barrier leg needs a positive level");
+        }
+    } else if (rq.product == OB_PRODUCT_AUTOCALL) {
+        if (rq.n_obs < 1 || !rq.obs_step || !rq.obs_discount || !rq.trigger) invalid("autocall: null schedule");
+        for (int j = 0; j < rq.n_obs; ++j)
+            if (rq.obs_step[j] < 1 || rq.obs_step[j] > rq.n_steps || (j && rq.obs_step[j] <= rq.obs_step[j - 1]))
+                invalid("obs_step must be increasing in [1, n_steps]");
+        if (!(rq.ki_barrier >= 0) || !(rq.coupon_barrier >= 0)) invalid("barriers must be >= 0");
+    } else {
+        invalid("product must be 0 or 1");
     }
 }
 

@@ -30,6 +30,7 @@ struct McArgs {
 };
 
 void check_mc_request(const ob_mc_request& rq);
+void check_mc_model(const ob_mc_request& rq);  // the model part of an ob_mc_request (its product unused)
 
 struct McPlan {
     DeviceArena arena;

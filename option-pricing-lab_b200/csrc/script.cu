@@ -1,0 +1,461 @@
+// Payoff scripts on the device: ob_script_price simulates a request's paths (the path engine's step of model.cuh, or
+// Andersen QE for one Heston name) and runs a compiled payoff script on both legs of every pair at its event steps,
+// then reduces the pair-averaged present values into a price and its standard error.
+//
+// The script is the reference's payoff language (packages/structured/src/optlab/structured/script/), compiled on
+// the host (optlab_b200/script.py) into instructions over a register file: the reference evaluates it on arrays of
+// paths with conditions as masks (evaluator.py:123-231): inside an `if`, an assignment is x = m e + (1 - m) x, a
+// payment adds m alive e to the flows, `terminate` multiplies alive by 1 - m, and both branches are evaluated. Read
+// per path, that is straight-line code, so every lane of a warp runs the same instruction stream: the interpreter
+// does not diverge. Each leg has its own register file (constants, variables, temporaries) in local memory; the
+// registers are touched only at event steps, a few dozen times a path, against hundreds of path steps.
+//
+// Windows (lowest, highest, realised variance of one name's fixings) are kept as running states updated at their
+// fixing steps, so nothing of the path is stored. Paths whose script is undefined (a payment that is not finite, a
+// condition that is NaN where it matters, redemption weights that do not add up to one) are counted and reported;
+// the host raises them as the reference does.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mc.cuh"
+
+namespace ob {
+
+namespace {
+
+constexpr int kMaxRegs = 128;
+constexpr int kMaxWindows = 32;
+constexpr double kAnnual = 252.0;  // realised variance: fixings a year (varswap.py:24)
+
+enum ScriptOp : int {
+    kSpot, kWin, kMov, kAdd, kSub, kMul, kDiv, kNeg, kMin, kMax, kAbs, kExp, kLog, kSqrt,
+    kGe, kGt, kLe, kLt, kEq, kAnd, kOr, kNot, kAssign, kPay, kTerm, kCond, kNumOps
+};
+
+template <typename R>
+struct ScriptDev {
+    ModelDev<R> m;
+    int model, n_names, n_steps;
+    const R* lf;        // n_names x (n_steps + 1): ln(F(t_i) / spot)
+    R spot0[OB_MAX_NAMES];
+    QeConsts<R> qe;
+    const int4* code;
+    const double* consts;
+    int n_const, n_regs;
+    const int* event_at;        // n_steps + 1: event index of each step end, or -1
+    const int* event_code;      // n_events + 1
+    const double* event_disc;
+    const unsigned* fix_mask;   // n_steps + 1: windows fixing at each step end
+    int n_windows;
+    const int* win_name;
+    const int* win_func;
+    const int* win_nfix;
+    const double* win_lo;
+    const double* win_hi;
+    R eps;
+    double red_tol;
+    unsigned long long* bad;    // 3 counters: payments, conditions, redemptions
+};
+
+// One leg's state between events.
+template <typename R>
+struct LegState {
+    R reg[kMaxRegs];
+    R wv[kMaxWindows];        // lowest / highest so far, or (variance) the last fixing
+    double wsum[kMaxWindows];  // variance: sum of squared log returns in the corridor
+    int wn[kMaxWindows];       // fixings seen
+    R alive;
+    double pv, red;
+    bool bad_pay, bad_cond;
+};
+
+template <typename R>
+__device__ __forceinline__ R compare(int op, R a, R b, R eps) {
+    if (isnan(a) || isnan(b)) return a + b;  // NaN stays NaN
+    const bool h = op == kGe ? a >= b : op == kGt ? a > b : op == kLe ? a <= b : op == kLt ? a < b : a == b;
+    const R hard = h ? R(1) : R(0);
+    if (eps == R(0) || op == kEq) return hard;
+    const R scale = eps * m_abs(b);
+    if (!(scale > R(0))) return hard;
+    const R d = (op == kGe || op == kGt) ? a - b : b - a;
+    return m_min(m_max(d / scale + R(0.5), R(0)), R(1));
+}
+
+// The script's instructions of one event on one leg. spot(a): the leg's spot of name a at this step.
+template <typename R, typename SpotFn>
+__device__ void run_event(const ScriptDev<R>& d, LegState<R>& s, int c0, int c1, double disc, SpotFn spot) {
+    R* r = s.reg;
+    for (int pc = c0; pc < c1; ++pc) {
+        const int4 in = __ldg(d.code + pc);
+        const int dst = in.y, a = in.z, b = in.w;
+        switch (in.x) {
+            case kSpot: r[dst] = spot(a); break;
+            case kWin: {
+                const int f = d.win_func[a];
+                r[dst] = f == 2 ? static_cast<R>(kAnnual / static_cast<double>(d.win_nfix[a] - 1) * s.wsum[a])
+                                : s.wv[a];
+                break;
+            }
+            case kMov: r[dst] = r[a]; break;
+            case kAdd: r[dst] = r[a] + r[b]; break;
+            case kSub: r[dst] = r[a] - r[b]; break;
+            case kMul: r[dst] = r[a] * r[b]; break;
+            case kDiv: r[dst] = r[a] / r[b]; break;
+            case kNeg: r[dst] = -r[a]; break;
+            case kMin: case kMax: {  // NaN propagates, as NumPy's minimum and maximum
+                const R x = r[a], y = r[b];
+                r[dst] = (isnan(x) || isnan(y)) ? x + y : (in.x == kMin ? (x < y ? x : y) : (x > y ? x : y));
+                break;
+            }
+            case kAbs: r[dst] = m_abs(r[a]); break;
+            case kExp: r[dst] = m_exp(r[a]); break;
+            case kLog: r[dst] = m_log(r[a]); break;
+            case kSqrt: r[dst] = m_sqrt(r[a]); break;
+            case kGe: case kGt: case kLe: case kLt: case kEq: r[dst] = compare(in.x, r[a], r[b], d.eps); break;
+            case kAnd: {  // a certain false operand decides, even where the other one is undefined
+                const R x = r[a], y = r[b];
+                r[dst] = (x == R(0) || y == R(0)) ? R(0) : x * y;
+                break;
+            }
+            case kOr: {
+                const R x = r[a], y = r[b];
+                r[dst] = (x == R(1) || y == R(1)) ? R(1) : x + y - x * y;
+                break;
+            }
+            case kNot: r[dst] = R(1) - r[a]; break;
+            case kAssign: {
+                const R m = r[b], e = r[a], old = r[dst];
+                r[dst] = m == R(1) ? e : (m == R(0) ? old : m * e + (R(1) - m) * old);
+                break;
+            }
+            case kPay: {
+                const R w = r[b] * s.alive, e = r[a];
+                if (w != R(0)) {
+                    if (!isfinite(e)) s.bad_pay = true;
+                    else s.pv += disc * (static_cast<double>(w) * static_cast<double>(e));
+                }
+                if (dst == 2) s.red += static_cast<double>(w);
+                break;
+            }
+            case kTerm: s.alive = s.alive * (R(1) - r[a]); break;
+            case kCond: {
+                R c = r[a];
+                if (isnan(c)) {
+                    if (r[b] * s.alive != R(0)) s.bad_cond = true;
+                    c = R(0);
+                }
+                r[dst] = c;
+                break;
+            }
+            default: break;
+        }
+    }
+}
+
+// The windows fixing at this step, on one leg.
+template <typename R, typename SpotFn>
+__device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, LegState<R>& s, unsigned mask, SpotFn spot) {
+    while (mask) {
+        const int w = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const R S = spot(d.win_name[w]);
+        const int f = d.win_func[w];
+        if (f == 0) {
+            s.wv[w] = m_min(s.wv[w], S);
+        } else if (f == 1) {
+            s.wv[w] = m_max(s.wv[w], S);
+        } else {
+            if (s.wn[w] > 0) {
+                const R prev = s.wv[w];
+                const double lo = d.win_lo[w], hi = d.win_hi[w];
+                const double pd = static_cast<double>(prev);
+                const bool inside = (isnan(lo) || pd >= lo) && (isnan(hi) || pd <= hi);
+                const double rr = static_cast<double>(m_log(S / prev));
+                if (inside) s.wsum[w] += rr * rr;
+            }
+            s.wv[w] = S;
+        }
+        s.wn[w] += 1;
+    }
+}
+
+template <typename R>
+__device__ void leg_init(const ScriptDev<R>& d, LegState<R>& s) {
+    for (int k = 0; k < d.n_regs; ++k) s.reg[k] = k < d.n_const ? static_cast<R>(d.consts[k]) : R(0);
+    for (int w = 0; w < d.n_windows; ++w) {
+        s.wv[w] = d.win_func[w] == 1 ? R(-INFINITY) : R(INFINITY);
+        s.wsum[w] = 0.0, s.wn[w] = 0;
+    }
+    s.alive = R(1), s.pv = 0.0, s.red = 0.0, s.bad_pay = s.bad_cond = false;
+}
+
+template <typename R, int N, int MODEL>
+__global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n_pairs, uint32_t k0, uint32_t k1,
+                                                     double* __restrict__ partial) {
+    __shared__ double wacc[4][2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+    if (threadIdx.x < 8) (&wacc[0][0])[threadIdx.x] = 0.0;
+    __syncthreads();
+    ModelDev<R> m = d.m;
+    m.k0 = k0, m.k1 = k1;
+    const int S = d.n_steps;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n_pairs;
+         base += stride) {
+        const bool active = base + lane < n_pairs;
+        const uint64_t pair = static_cast<uint64_t>(active ? base + lane : n_pairs - 1);
+        LegState<R> leg[2];
+        leg_init(d, leg[0]), leg_init(d, leg[1]);
+        PairDev<R, N> st;
+        NormalStream<R> qrng;
+        R y[2] = {R(0), R(0)}, v[2] = {d.qe.v0, d.qe.v0};
+        if (MODEL == OB_MODEL_HESTON_QE) qrng.init(pair, k0, k1, 0u);
+        else pair_init<R, N>(m, st, pair);
+        for (int i = 0; i <= S; ++i) {
+            if (i > 0) {
+                if (MODEL == OB_MODEL_HESTON_QE) {
+                    const R zv = qrng.next(), zx = qrng.next();
+                    qe_step(d.qe, y[0], v[0], zv, zx);
+                    qe_step(d.qe, y[1], v[1], -zv, -zx);
+                } else {
+                    pair_step<R, N>(m, st, i);
+                }
+            }
+            const unsigned fm = d.fix_mask[i];
+            const int ev = d.event_at[i];
+            if (!fm && ev < 0) continue;
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                auto spot = [&](int a) -> R {
+                    if (MODEL == OB_MODEL_HESTON_QE) return d.spot0[0] * m_exp(y[l]);
+                    R x = R(0);
+#pragma unroll
+                    for (int n = 0; n < N; ++n)
+                        if (n == a) x = st.x[l][n];
+                    return d.spot0[a] * m_exp(d.lf[a * (S + 1) + i] + x);
+                };
+                if (fm) fix_windows(d, leg[l], fm, spot);
+                if (ev >= 0) run_event(d, leg[l], d.event_code[ev], d.event_code[ev + 1], d.event_disc[ev], spot);
+            }
+        }
+        double y_pair = 0.0;
+        if (active) {
+            y_pair = 0.5 * (leg[0].pv + leg[1].pv);
+            unsigned long long bp = 0, bc = 0, br = 0;
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                bp += leg[l].bad_pay, bc += leg[l].bad_cond;
+                br += !(fabs(leg[l].red - 1.0) <= d.red_tol);
+            }
+            if (bp) atomicAdd(&d.bad[0], bp);
+            if (bc) atomicAdd(&d.bad[1], bc);
+            if (br) atomicAdd(&d.bad[2], br);
+        }
+        const double s1 = warp_sum(y_pair), s2 = warp_sum(y_pair * y_pair);
+        if (lane == 0) wacc[warp][0] += s1, wacc[warp][1] += s2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double s = 0.0;
+        for (int w = 0; w < n_warps; ++w) s += wacc[w][threadIdx.x];
+        partial[2 * static_cast<long long>(blockIdx.x) + threadIdx.x] = s;
+    }
+}
+
+// The blocks' totals added in block order by one warp per sum (lane l adds blocks l, l + 32, ...).
+__global__ void script_finalize(const double* __restrict__ partial, int n_blocks, double* __restrict__ sums) {
+    const int lane = threadIdx.x & 31, t = threadIdx.x >> 5;
+    if (t >= 2) return;
+    double s = 0.0;
+    for (int b = lane; b < n_blocks; b += 32) s += partial[2 * static_cast<long long>(b) + t];
+    s = warp_sum(s);
+    if (lane == 0) sums[t] = s;
+}
+
+template <typename R>
+using ScriptFn = void (*)(ScriptDev<R>, long long, uint32_t, uint32_t, double*);
+
+template <typename R>
+ScriptFn<R> pick_script(int model, int n) {
+    if (model == OB_MODEL_HESTON_QE) return script_kernel<R, 1, OB_MODEL_HESTON_QE>;
+    if (n <= 1) return script_kernel<R, 1, OB_MODEL_PATHS>;
+    if (n <= 2) return script_kernel<R, 2, OB_MODEL_PATHS>;
+    if (n <= 4) return script_kernel<R, 4, OB_MODEL_PATHS>;
+    return script_kernel<R, 8, OB_MODEL_PATHS>;
+}
+
+// Every index the device will follow is checked here: registers, names, windows, tags, code ranges and steps.
+void check_script(const ob_script_request& rq) {
+    check_mc_model(rq.model);
+    const int S = rq.model.n_steps, n = rq.model.n_names;
+    if (rq.n_regs < 1 || rq.n_regs > kMaxRegs) invalid("n_regs must be 1 to 128");
+    if (rq.n_const < 1 || rq.n_const > rq.n_regs || !rq.consts) invalid("n_const must be 1 to n_regs");
+    if (rq.n_code < 0 || (rq.n_code > 0 && !rq.code)) invalid("null code");
+    if (rq.n_events < 1 || !rq.event_step || !rq.event_code || !rq.event_discount) invalid("a script needs events");
+    if (rq.n_windows < 0 || rq.n_windows > kMaxWindows) invalid("n_windows must be 0 to 32");
+    if (rq.n_windows && (!rq.win_name || !rq.win_func || !rq.win_fix0 || !rq.fix_step || !rq.win_lower ||
+                         !rq.win_upper))
+        invalid("null window arrays");
+    if (!(rq.smoothing >= 0)) invalid("smoothing must be >= 0");
+    for (int k = 0; k < rq.n_events; ++k) {
+        if (rq.event_step[k] < 0 || rq.event_step[k] > S || (k && rq.event_step[k] <= rq.event_step[k - 1]))
+            invalid("event steps must increase within 0 .. n_steps");
+        if (!(rq.event_discount[k] >= 0)) invalid("event discounts must be >= 0");
+    }
+    for (int k = 0; k <= rq.n_events; ++k)
+        if (rq.event_code[k] < 0 || rq.event_code[k] > rq.n_code || (k && rq.event_code[k] < rq.event_code[k - 1]))
+            invalid("event code ranges must increase within the code");
+    for (int w = 0; w < rq.n_windows; ++w) {
+        if (rq.win_name[w] < 0 || rq.win_name[w] >= n) invalid("a window reads an unknown name");
+        if (rq.win_func[w] < 0 || rq.win_func[w] > 2) invalid("win_func must be 0, 1 or 2");
+        if (rq.win_fix0[w] < 0 || rq.win_fix0[w + 1] <= rq.win_fix0[w]) invalid("a window needs fixings");
+        if (rq.win_func[w] == 2 && rq.win_fix0[w + 1] - rq.win_fix0[w] < 2)
+            invalid("a variance window needs at least two fixings");
+        for (int k = rq.win_fix0[w]; k < rq.win_fix0[w + 1]; ++k)
+            if (rq.fix_step[k] < 0 || rq.fix_step[k] > S || (k > rq.win_fix0[w] && rq.fix_step[k] <= rq.fix_step[k - 1]))
+                invalid("window fixing steps must increase within 0 .. n_steps");
+    }
+    auto reg = [&](int r) {
+        if (r < 0 || r >= rq.n_regs) invalid("an instruction names a register beyond n_regs");
+    };
+    for (int pc = 0; pc < rq.n_code; ++pc) {
+        const int* in = rq.code + 4 * pc;
+        const int op = in[0], d = in[1], a = in[2], b = in[3];
+        if (op < 0 || op >= kNumOps) invalid("unknown instruction");
+        switch (op) {
+            case kSpot:
+                reg(d);
+                if (a < 0 || a >= n) invalid("an instruction reads an unknown name");
+                break;
+            case kWin:
+                reg(d);
+                if (a < 0 || a >= rq.n_windows) invalid("an instruction reads an unknown window");
+                break;
+            case kPay:
+                if (d < 0 || d > 2) invalid("a payment tag must be 0, 1 or 2");
+                reg(a), reg(b);
+                break;
+            case kTerm: reg(a); break;
+            case kMov: case kNeg: case kAbs: case kExp: case kLog: case kSqrt: case kNot: reg(d), reg(a); break;
+            default:
+                reg(d), reg(a), reg(b);
+                if (op == kAssign && d < rq.n_const) invalid("an assignment to a constant register");
+        }
+    }
+}
+
+template <typename R>
+void run_script(const ob_script_request& rq, ob_script_result& res) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const int sms = require_device();
+    DeviceArena arena;
+    const ob_mc_request& mq = rq.model;
+    const int n = mq.n_names, S = mq.n_steps;
+    ScriptDev<R> d{};
+    d.model = mq.model, d.n_names = n, d.n_steps = S;
+    for (int a = 0; a < n; ++a) d.spot0[a] = static_cast<R>(mq.spot[a]);
+    ModelDev<R>& m = d.m;
+    m.n_names = n, m.n_steps = S, m.n_x = mq.n_x, m.same = mq.same, m.mixer = 0;
+    m.dt = arena.put<R>(mq.dt, S);
+    m.t0 = arena.put<R>(mq.t0, S);
+    if (mq.model == OB_MODEL_PATHS) {
+        bool table = false;
+        for (int a = 0; a < n; ++a) {
+            m.has_var |= mq.kind[a] == 2 || mq.kind[a] == 3;
+            m.has_slv |= mq.kind[a] == 3;
+            table |= mq.kind[a] == 1 || mq.kind[a] == 3;
+        }
+        m.root = arena.put<R>(mq.root, static_cast<size_t>(n) * n);
+        m.kind = arena.put<int>(mq.kind, n);
+        m.cvar = arena.put<R>(mq.cvar, n);
+        m.hes = arena.put<R>(mq.heston, 5 * static_cast<size_t>(n));
+        if (table) {
+            m.step_row = arena.put<int>(mq.step_row, static_cast<size_t>(n) * S);
+            m.lo = arena.put<R>(mq.row_lo, mq.n_rows);
+            m.inv_dx = arena.put<R>(mq.row_inv_dx, mq.n_rows);
+            m.table = arena.put<R>(mq.table, static_cast<size_t>(mq.n_rows) * mq.n_x);
+        }
+        d.lf = arena.put<R>(mq.log_fwd, static_cast<size_t>(n) * (S + 1));
+    } else {
+        d.qe = make_qe_consts<R>(mq.heston, mq.r, mq.q, mq.dt[0]);
+    }
+    std::vector<int4> code(static_cast<size_t>(rq.n_code));
+    if (rq.n_code) std::memcpy(code.data(), rq.code, code.size() * sizeof(int4));
+    d.code = arena.put<int4>(code.data(), code.size());
+    d.consts = arena.put<double>(rq.consts, rq.n_const);
+    d.n_const = rq.n_const, d.n_regs = rq.n_regs;
+    std::vector<int> event_at(S + 1, -1);
+    for (int k = 0; k < rq.n_events; ++k) event_at[rq.event_step[k]] = k;
+    d.event_at = arena.put<int>(event_at.data(), event_at.size());
+    d.event_code = arena.put<int>(rq.event_code, rq.n_events + 1);
+    d.event_disc = arena.put<double>(rq.event_discount, rq.n_events);
+    std::vector<unsigned> fix_mask(S + 1, 0u);
+    std::vector<int> nfix(std::max(1, rq.n_windows), 0);
+    for (int w = 0; w < rq.n_windows; ++w) {
+        for (int k = rq.win_fix0[w]; k < rq.win_fix0[w + 1]; ++k) fix_mask[rq.fix_step[k]] |= 1u << w;
+        nfix[w] = rq.win_fix0[w + 1] - rq.win_fix0[w];
+    }
+    d.fix_mask = arena.put<unsigned>(fix_mask.data(), fix_mask.size());
+    d.n_windows = rq.n_windows;
+    if (rq.n_windows) {
+        d.win_name = arena.put<int>(rq.win_name, rq.n_windows);
+        d.win_func = arena.put<int>(rq.win_func, rq.n_windows);
+        d.win_nfix = arena.put<int>(nfix.data(), rq.n_windows);
+        d.win_lo = arena.put<double>(rq.win_lower, rq.n_windows);
+        d.win_hi = arena.put<double>(rq.win_upper, rq.n_windows);
+    }
+    d.eps = static_cast<R>(rq.smoothing);
+    d.red_tol = rq.smoothing == 0.0 ? 1e-12 : (sizeof(R) == 8 ? 1e-9 : 1e-5);
+    d.bad = arena.alloc<unsigned long long>(3);
+    check_cuda(cudaMemset(d.bad, 0, 3 * sizeof(unsigned long long)), "cudaMemset");
+
+    const void* fn = reinterpret_cast<const void*>(pick_script<R>(mq.model, n));
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0), "occupancy");
+    const long long need = (mq.n_pairs + 127) / 128;
+    const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(need, 1LL * sms * std::max(1, per_sm))));
+    double* partial = arena.alloc<double>(2 * static_cast<size_t>(grid));
+    double* sums = arena.alloc<double>(2);
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    const uint32_t k0 = static_cast<uint32_t>(mq.seed), k1 = static_cast<uint32_t>(mq.seed >> 32);
+    check_cuda(cudaEventRecord(e0), "cudaEventRecord");
+    reinterpret_cast<ScriptFn<R>>(const_cast<void*>(fn))<<<grid, 128>>>(d, mq.n_pairs, k0, k1, partial);
+    check_cuda(cudaGetLastError(), "script_kernel launch");
+    script_finalize<<<1, 64>>>(partial, grid, sums);
+    check_cuda(cudaGetLastError(), "script_finalize launch");
+    check_cuda(cudaEventRecord(e1), "cudaEventRecord");
+    double h[2];
+    unsigned long long bad[3];
+    check_cuda(cudaMemcpy(h, sums, sizeof h, cudaMemcpyDeviceToHost), "copy sums");
+    check_cuda(cudaMemcpy(bad, d.bad, sizeof bad, cudaMemcpyDeviceToHost), "copy counts");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0), cudaEventDestroy(e1);
+    const double nn = static_cast<double>(mq.n_pairs), mean = h[0] / nn;
+    res.price = mean;
+    res.se = nn > 1 ? std::sqrt(std::fmax(h[1] / nn - mean * mean, 0.0) / (nn - 1.0)) : 0.0;
+    res.n_paths = 2 * mq.n_pairs;
+    res.bad_pay = static_cast<long long>(bad[0]), res.bad_cond = static_cast<long long>(bad[1]);
+    res.bad_redemption = static_cast<long long>(bad[2]);
+    res.kernel_ms = ms;
+    (void)t_start;
+}
+
+}  // namespace
+}  // namespace ob
+
+extern "C" int ob_script_price(const ob_script_request* rq, int precision, ob_script_result* res) {
+    return ob::guarded([&] {
+        if (!rq || !res) ob::invalid("null argument");
+        if (precision != OB_FP32 && precision != OB_FP64) ob::invalid("precision must be OB_FP32 or OB_FP64");
+        ob::check_script(*rq);
+        *res = ob_script_result{};
+        if (precision == OB_FP32) ob::run_script<float>(*rq, *res);
+        else ob::run_script<double>(*rq, *res);
+    });
+}

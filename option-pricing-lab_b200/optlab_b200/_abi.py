@@ -284,6 +284,41 @@ class ObBatchRequest(C.Structure):
     ]
 
 
+class ObScriptRequest(C.Structure):
+    _fields_ = [
+        ("model", ObMcRequest),
+        ("n_code", C.c_int),
+        ("code", _ip),
+        ("n_const", C.c_int),
+        ("consts", _dp),
+        ("n_regs", C.c_int),
+        ("n_events", C.c_int),
+        ("event_step", _ip),
+        ("event_code", _ip),
+        ("event_discount", _dp),
+        ("n_windows", C.c_int),
+        ("win_name", _ip),
+        ("win_func", _ip),
+        ("win_fix0", _ip),
+        ("fix_step", _ip),
+        ("win_lower", _dp),
+        ("win_upper", _dp),
+        ("smoothing", C.c_double),
+    ]
+
+
+class ObScriptResult(C.Structure):
+    _fields_ = [
+        ("price", C.c_double),
+        ("se", C.c_double),
+        ("n_paths", C.c_longlong),
+        ("bad_pay", C.c_longlong),
+        ("bad_cond", C.c_longlong),
+        ("bad_redemption", C.c_longlong),
+        ("kernel_ms", C.c_double),
+    ]
+
+
 # Every symbol include/optlab_b200.h declares, with its ctypes signature (restype, argtypes).
 SIGNATURES = {
     "ob_last_error": (C.c_char_p, []),
@@ -327,6 +362,7 @@ SIGNATURES = {
     "ob_batch_result": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "ob_batch_classes": (C.c_int, [C.c_void_p, C.c_int, _ip, _ip]),
     "ob_batch_destroy": (C.c_int, [C.c_void_p]),
+    "ob_script_price": (C.c_int, [C.POINTER(ObScriptRequest), C.c_int, C.POINTER(ObScriptResult)]),
 }
 
 _lib: list = []

@@ -60,6 +60,8 @@ PAIRS = {
     "ob_adjoint_result": _abi.ObAdjointResult,
     "ob_batch_trade": _abi.ObBatchTrade,
     "ob_batch_request": _abi.ObBatchRequest,
+    "ob_script_request": _abi.ObScriptRequest,
+    "ob_script_result": _abi.ObScriptResult,
 }
 
 
