@@ -231,7 +231,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage"])
+    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage", "script"])
     ap.add_argument("--trades", type=int, default=512, help="batch workload: trades in the book")
     ap.add_argument("--paths", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -251,6 +251,8 @@ def main():
         return run_batch(args, world, rank)
     if args.workload == "leverage":
         return run_leverage(args, world, rank)
+    if args.workload == "script":
+        return run_script(args, world, rank)
 
     import torch
 
@@ -627,6 +629,89 @@ def run_leverage(args, world, rank):
         "gpu_launches": args.steps * (1 + 5 * s.n_steps),
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "result": {"leverage_at_atm_last_step": float(held.values[-1, s.n_x // 2])},
+    }
+    print(json.dumps(line))
+
+
+def phoenix_script(ph, steps_per_year: int) -> str:
+    """The local-vol Phoenix of the default workload written in the payoff language."""
+    n_obs = int(round(ph.years * ph.obs_per_year))
+    lines = ["underlying X", "param S0 = 100", f"param cb = {ph.coupon_barrier!r}", f"param cpn = {ph.coupon!r}",
+             f"param call = {ph.trigger!r}", f"param ki = {ph.ki_barrier!r}", f"param K = {ph.put_strike!r}"]
+    for j in range(1, n_obs + 1):
+        t = j / ph.obs_per_year
+        lines.append(f"event t={t!r} pay t={t!r}")
+        if j == 1:
+            lines.append("  missed = 0")
+        lines += ["  perf = X / S0", "  if perf >= cb then", "    pay cpn * (1 + missed) as coupon", "    missed = 0",
+                  "  else", "    missed = missed + 1", "  end"]
+        if j < n_obs:
+            lines += ["  if perf >= call then", "    pay 1 as redemption", "    terminate", "  end"]
+        else:
+            n_fix = int(round(ph.years * steps_per_year))
+            lines += [f"  knocked = lowest(X, t=0, t={t!r}, n={n_fix}) < ki * S0", "  if knocked then",
+                      "    pay 1 - max(K - perf, 0) as redemption", "  else", "    pay 1 as redemption", "  end"]
+        lines.append("end")
+    return "\n".join(lines) + "\n"
+
+
+def run_script(args, world, rank):
+    """The default workload's Phoenix (2^20 paths x 756 steps of local vol, FP32 paths, FP64 sums) written as a payoff
+    script and run by the device's script interpreter (ob_script_price), beside the fused Phoenix kernel on the same
+    paths: what a general script costs against the specialised kernel. Units: path-steps."""
+    import torch
+
+    from optlab_b200 import engine, workloads
+    from optlab_b200 import script as sc
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    ph = workloads.Phoenix()
+    held = workloads.lv_phoenix(n_paths=args.paths or 2**20, phoenix=ph)
+    comp = sc.compile_script(phoenix_script(ph, 252))
+    req = sc.script_request(comp, held, lambda t: float(np.exp(-0.02 * t)))
+    units = workloads.path_steps(held)
+    for _ in range(args.warmup):
+        sc.run(req, "fp32")
+    ms, wall = [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            r = sc.run(req, "fp32")
+            wall.append(time.perf_counter() - t)
+            ms.append(r.kernel_ms)
+    fused = engine.mc_price(held, "fp32")
+    t_ms = statistics.median(ms)
+    clk = clocks.summary()
+    line = {
+        "metric": "path-steps/s",
+        "value": units / (t_ms / 1e3),
+        "unit": "path-steps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded SSVI surface; the default workload's Phoenix as a script)",
+        "config": {"workload": "script_phoenix", "n_paths": 2 * held.struct.n_pairs, "n_steps": held.struct.n_steps,
+                   "instructions": int(comp.code.shape[0]), "registers": int(comp.n_regs),
+                   "l2": "no flush: one call holds uploads, kernel and read-back"},
+        "fused_kernel": {"ms_per_step": fused.kernel_ms, "price": fused.price[0],
+                         "script_over_fused_time": t_ms / fused.kernel_ms},
+        "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": "Gwarp-inst/s", "frac": None,
+                     "traffic": None, "note": "the path step of the generic engine plus the interpreter at events"},
+        "cpu_baseline": None,
+        "e2e": {"value": units / statistics.median(wall), "unit": "path-steps/s",
+                "h2d_bytes_per_step": int(req.struct.n_code * 16 + held.struct.n_rows * held.struct.n_x * 8),
+                "d2h_bytes_per_step": 5 * 8},
+        "gpu_launches": 2 * args.steps,
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "result": {"price": r.price, "se": r.se, "fused_price": fused.price[0], "fused_se": fused.se[0]},
     }
     print(json.dumps(line))
 

@@ -64,7 +64,7 @@ struct ScriptDev {
 template <typename R>
 struct LegState {
     R reg[kMaxRegs];
-    R wv[kMaxWindows];        // lowest / highest so far, or (variance) the last fixing
+    R wv[kMaxWindows];        // lowest / highest ln(S / spot0) so far, or (variance) the last one
     double wsum[kMaxWindows];  // variance: sum of squared log returns in the corridor
     int wn[kMaxWindows];       // fixings seen
     R alive;
@@ -96,7 +96,7 @@ __device__ void run_event(const ScriptDev<R>& d, LegState<R>& s, int c0, int c1,
             case kWin: {
                 const int f = d.win_func[a];
                 r[dst] = f == 2 ? static_cast<R>(kAnnual / static_cast<double>(d.win_nfix[a] - 1) * s.wsum[a])
-                                : s.wv[a];
+                                : d.spot0[d.win_name[a]] * m_exp(s.wv[a]);
                 break;
             }
             case kMov: r[dst] = r[a]; break;
@@ -155,28 +155,29 @@ __device__ void run_event(const ScriptDev<R>& d, LegState<R>& s, int c0, int c1,
     }
 }
 
-// The windows fixing at this step, on one leg.
-template <typename R, typename SpotFn>
-__device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, LegState<R>& s, unsigned mask, SpotFn spot) {
+// The windows fixing at this step, on one leg. logp(a): ln(S_a / spot0_a) of name a at this step. A window keeps the
+// extreme (or, for the variance, the last) of ln(S / spot0): S is increasing in it, so the lowest and highest spots
+// are spot0 exp(extreme), and the log returns are differences of it; no exp or log is taken at the fixings.
+template <typename R, typename LogFn>
+__device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, LegState<R>& s, unsigned mask, LogFn logp) {
     while (mask) {
         const int w = __ffs(mask) - 1;
         mask &= mask - 1;
-        const R S = spot(d.win_name[w]);
+        const R y = logp(d.win_name[w]);
         const int f = d.win_func[w];
         if (f == 0) {
-            s.wv[w] = m_min(s.wv[w], S);
+            s.wv[w] = m_min(s.wv[w], y);
         } else if (f == 1) {
-            s.wv[w] = m_max(s.wv[w], S);
+            s.wv[w] = m_max(s.wv[w], y);
         } else {
             if (s.wn[w] > 0) {
                 const R prev = s.wv[w];
-                const double lo = d.win_lo[w], hi = d.win_hi[w];
-                const double pd = static_cast<double>(prev);
+                const double lo = d.win_lo[w], hi = d.win_hi[w], pd = static_cast<double>(prev);
                 const bool inside = (isnan(lo) || pd >= lo) && (isnan(hi) || pd <= hi);
-                const double rr = static_cast<double>(m_log(S / prev));
+                const double rr = static_cast<double>(y - prev);
                 if (inside) s.wsum[w] += rr * rr;
             }
-            s.wv[w] = S;
+            s.wv[w] = y;
         }
         s.wn[w] += 1;
     }
@@ -229,15 +230,16 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
             if (!fm && ev < 0) continue;
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
-                auto spot = [&](int a) -> R {
-                    if (MODEL == OB_MODEL_HESTON_QE) return d.spot0[0] * m_exp(y[l]);
+                auto logp = [&](int a) -> R {
+                    if (MODEL == OB_MODEL_HESTON_QE) return y[l];
                     R x = R(0);
 #pragma unroll
                     for (int n = 0; n < N; ++n)
                         if (n == a) x = st.x[l][n];
-                    return d.spot0[a] * m_exp(d.lf[a * (S + 1) + i] + x);
+                    return d.lf[a * (S + 1) + i] + x;
                 };
-                if (fm) fix_windows(d, leg[l], fm, spot);
+                auto spot = [&](int a) -> R { return d.spot0[a] * m_exp(logp(a)); };
+                if (fm) fix_windows(d, leg[l], fm, logp);
                 if (ev >= 0) run_event(d, leg[l], d.event_code[ev], d.event_code[ev + 1], d.event_disc[ev], spot);
             }
         }
@@ -404,8 +406,17 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
         d.win_name = arena.put<int>(rq.win_name, rq.n_windows);
         d.win_func = arena.put<int>(rq.win_func, rq.n_windows);
         d.win_nfix = arena.put<int>(nfix.data(), rq.n_windows);
-        d.win_lo = arena.put<double>(rq.win_lower, rq.n_windows);
-        d.win_hi = arena.put<double>(rq.win_upper, rq.n_windows);
+        // the corridor as bounds on ln(S / spot0) of the window's name (NaN: no bound)
+        std::vector<double> llo(rq.n_windows), lhi(rq.n_windows);
+        for (int w = 0; w < rq.n_windows; ++w) {
+            const double s0 = mq.spot[rq.win_name[w]];
+            auto bound = [&](double b) {
+                return std::isnan(b) ? b : (b > 0 ? std::log(b / s0) : -INFINITY);  // no positive spot is <= 0
+            };
+            llo[w] = bound(rq.win_lower[w]), lhi[w] = bound(rq.win_upper[w]);
+        }
+        d.win_lo = arena.put<double>(llo.data(), llo.size());
+        d.win_hi = arena.put<double>(lhi.data(), lhi.size());
     }
     d.eps = static_cast<R>(rq.smoothing);
     d.red_tol = rq.smoothing == 0.0 ? 1e-12 : (sizeof(R) == 8 ? 1e-9 : 1e-5);
