@@ -682,7 +682,15 @@ def run_script(args, world, rank):
             r = sc.run(req, "fp32")
             wall.append(time.perf_counter() - t)
             ms.append(r.kernel_ms)
-    fused = engine.mc_price(held, "fp32")
+    plan = engine.McPlan(held, "fp32")  # the fused kernel on the same pairs, warmed as the script was
+    for _ in range(args.warmup):
+        plan.run(held.struct.n_pairs, 0, held.struct.seed)
+    plan.result()
+    fused_ms = []
+    for _ in range(args.steps):
+        plan.run(held.struct.n_pairs, 0, held.struct.seed)
+        fused = plan.result()
+        fused_ms.append(fused.kernel_ms)
     t_ms = statistics.median(ms)
     clk = clocks.summary()
     line = {
@@ -701,8 +709,8 @@ def run_script(args, world, rank):
         "config": {"workload": "script_phoenix", "n_paths": 2 * held.struct.n_pairs, "n_steps": held.struct.n_steps,
                    "instructions": int(comp.code.shape[0]), "registers": int(comp.n_regs),
                    "l2": "no flush: one call holds uploads, kernel and read-back"},
-        "fused_kernel": {"ms_per_step": fused.kernel_ms, "price": fused.price[0],
-                         "script_over_fused_time": t_ms / fused.kernel_ms},
+        "fused_kernel": {"ms_per_step": statistics.median(fused_ms), "price": fused.price[0],
+                         "script_over_fused_time": t_ms / statistics.median(fused_ms)},
         "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": "Gwarp-inst/s", "frac": None,
                      "traffic": None, "note": "the path step of the generic engine plus the interpreter at events"},
         "cpu_baseline": None,

@@ -267,6 +267,205 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
     }
 }
 
+// Every name local vol (kind 1), N names: the fused kernel's layout and stepping (fused.cuh) with the script at the
+// step ends. Shared memory holds per step {-dt/2, sqrt(dt), dt}, per step and name {lo, inv_dx, log-forward, row},
+// the correlation root, the table as (y, dy) pairs, and per step end the event to run and the windows fixing there.
+// Normals come in batches of G steps of whole Philox blocks; the correlated z is computed once a pair and used with
+// both signs. Block totals as in script_kernel.
+struct LvOffsets {
+    int step, name_step, root, table2, sched, lf0;
+};
+
+template <typename R>
+struct LvArgs {
+    LvOffsets off;
+    const unsigned char* blob;
+    int smem_blob;
+    R top;
+};
+
+template <typename R, int N>
+__global__ void __launch_bounds__(256) script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0,
+                                                        uint32_t k1, double* __restrict__ partial) {
+    constexpr int C = N;
+    constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);
+    constexpr int NB = C * G / 4;
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ double wacc[8][2];
+    {
+        const int4* src = reinterpret_cast<const int4*>(a.blob);
+        int4* dst = reinterpret_cast<int4*>(sm);
+        for (int t = threadIdx.x; t < a.smem_blob / 16; t += blockDim.x) dst[t] = src[t];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+    if (threadIdx.x < 16) (&wacc[0][0])[threadIdx.x] = 0.0;
+    __syncthreads();
+    const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
+    const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
+    const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
+    const Pair2<R>* s_tab = reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
+    const int2* s_sched = reinterpret_cast<const int2*>(sm + a.off.sched);  // (event, window mask) per step end
+    const R* s_lf0 = reinterpret_cast<const R*>(sm + a.off.lf0);
+    const int S = d.n_steps;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n_pairs;
+         base += stride) {
+        const bool active = base + lane < n_pairs;
+        const uint64_t pair = static_cast<uint64_t>(active ? base + lane : n_pairs - 1);
+        LegState<R> leg[2];
+        leg_init(d, leg[0]), leg_init(d, leg[1]);
+        R x0[N], x1[N], y0[N], y1[N];
+#pragma unroll
+        for (int n = 0; n < N; ++n) x0[n] = x1[n] = R(0), y0[n] = y1[n] = s_lf0[n];
+        auto observe = [&](int i) {
+            const int2 sc = s_sched[i];
+            if (!sc.y && sc.x < 0) return;
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                auto logp = [&](int nm) -> R {
+                    R v = R(0);
+#pragma unroll
+                    for (int n = 0; n < N; ++n)
+                        if (n == nm) v = l ? y1[n] : y0[n];
+                    return v;
+                };
+                auto spot = [&](int nm) -> R { return d.spot0[nm] * m_exp(logp(nm)); };
+                if (sc.y) fix_windows(d, leg[l], static_cast<unsigned>(sc.y), logp);
+                if (sc.x >= 0) run_event(d, leg[l], d.event_code[sc.x], d.event_code[sc.x + 1], d.event_disc[sc.x], spot);
+            }
+        };
+        observe(0);
+        for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) {
+            R z[C * G];
+#pragma unroll
+            for (int k = 0; k < NB; ++k)
+                normals4<R>(pair, static_cast<uint64_t>(b) * NB + k, 0u, k0, k1, z[4 * k], z[4 * k + 1], z[4 * k + 2],
+                            z[4 * k + 3]);
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int i = i0 + g;
+                if (G > 1 && i > S) break;
+                const StepRec<R> st = s_step[i - 1];
+                R zc[N];
+#pragma unroll
+                for (int n = 0; n < N; ++n) {
+                    R acc = R(0);
+#pragma unroll
+                    for (int m = 0; m < N; ++m) acc += s_root[n * N + m] * z[g * C + m];
+                    zc[n] = acc;
+                }
+#pragma unroll
+                for (int n = 0; n < N; ++n) {
+                    const NameStep<R> ns = s_ns[(i - 1) * N + n];
+                    R u0 = (x0[n] - ns.lo) * ns.inv_dx, u1 = (x1[n] - ns.lo) * ns.inv_dx;
+                    u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
+                    const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
+                    const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
+                    const Pair2<R> p0 = s_tab[ns.row + j0], p1 = s_tab[ns.row + j1];
+                    const R v0 = p0.a + f0 * p0.b, v1 = p1.a + f1 * p1.b;
+                    x0[n] += v0 * st.hdt + (m_sqrt(v0) * st.sdt) * zc[n];
+                    x1[n] += v1 * st.hdt + (m_sqrt(v1) * st.sdt) * (-zc[n]);
+                    y0[n] = x0[n] + ns.lf, y1[n] = x1[n] + ns.lf;
+                }
+                observe(i);
+            }
+        }
+        double y_pair = 0.0;
+        if (active) {
+            y_pair = 0.5 * (leg[0].pv + leg[1].pv);
+            unsigned long long bp = 0, bc = 0, br = 0;
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                bp += leg[l].bad_pay, bc += leg[l].bad_cond;
+                br += !(fabs(leg[l].red - 1.0) <= d.red_tol);
+            }
+            if (bp) atomicAdd(&d.bad[0], bp);
+            if (bc) atomicAdd(&d.bad[1], bc);
+            if (br) atomicAdd(&d.bad[2], br);
+        }
+        const double s1 = warp_sum(y_pair), s2 = warp_sum(y_pair * y_pair);
+        if (lane == 0) wacc[warp][0] += s1, wacc[warp][1] += s2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double s = 0.0;
+        for (int w = 0; w < n_warps; ++w) s += wacc[w][threadIdx.x];
+        partial[2 * static_cast<long long>(blockIdx.x) + threadIdx.x] = s;
+    }
+}
+
+template <typename R>
+using ScriptLvFn = void (*)(ScriptDev<R>, LvArgs<R>, long long, uint32_t, uint32_t, double*);
+
+template <typename R>
+ScriptLvFn<R> pick_lv(int n) {
+    switch (n) {
+        case 1: return script_lv_kernel<R, 1>;
+        case 2: return script_lv_kernel<R, 2>;
+        case 3: return script_lv_kernel<R, 3>;
+        case 4: return script_lv_kernel<R, 4>;
+        case 5: return script_lv_kernel<R, 5>;
+        default: return nullptr;
+    }
+}
+
+// The staged blob of the local-vol path, or false when it does not apply (a name not local vol, more than five
+// names, or more than the shared-memory budget: 110 KB in float, 220 KB in double).
+template <typename R>
+bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, DeviceArena& arena, LvArgs<R>& a) {
+    const ob_mc_request& q = rq.model;
+    const int n = q.n_names, S = q.n_steps;
+    if (q.model != OB_MODEL_PATHS || n > 5) return false;
+    for (int k = 0; k < n; ++k)
+        if (q.kind[k] != 1) return false;
+    std::vector<unsigned char> blob;
+    auto put = [&](const void* src, size_t bytes) {
+        const size_t at = (blob.size() + 15) & ~static_cast<size_t>(15);
+        blob.resize(at + ((bytes + 15) & ~static_cast<size_t>(15)), 0);
+        if (bytes) std::memcpy(blob.data() + at, src, bytes);
+        return static_cast<int>(at);
+    };
+    std::vector<StepRec<R>> steps(S);
+    for (int i = 0; i < S; ++i) {
+        std::memset(&steps[i], 0, sizeof steps[i]);
+        steps[i].hdt = static_cast<R>(-0.5 * q.dt[i]), steps[i].sdt = static_cast<R>(std::sqrt(q.dt[i]));
+        steps[i].dt = static_cast<R>(q.dt[i]), steps[i].obs = -1;
+    }
+    a.off.step = put(steps.data(), steps.size() * sizeof(StepRec<R>));
+    std::vector<NameStep<R>> ns(static_cast<size_t>(S) * n);
+    for (int i = 1; i <= S; ++i)
+        for (int k = 0; k < n; ++k) {
+            NameStep<R>& r = ns[static_cast<size_t>(i - 1) * n + k];
+            std::memset(&r, 0, sizeof r);
+            const int row = q.step_row[static_cast<size_t>(k) * S + (i - 1)];
+            r.lf = static_cast<R>(q.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
+            r.lo = static_cast<R>(q.row_lo[row]), r.inv_dx = static_cast<R>(q.row_inv_dx[row]);
+            r.row = row * (q.n_x - 1);
+        }
+    a.off.name_step = put(ns.data(), ns.size() * sizeof(NameStep<R>));
+    std::vector<R> root(static_cast<size_t>(n) * n), lf0(n);
+    for (size_t k = 0; k < root.size(); ++k) root[k] = static_cast<R>(q.root[k]);
+    for (int k = 0; k < n; ++k) lf0[k] = static_cast<R>(q.log_fwd[static_cast<size_t>(k) * (S + 1)]);
+    a.off.root = put(root.data(), root.size() * sizeof(R));
+    a.off.lf0 = put(lf0.data(), lf0.size() * sizeof(R));
+    std::vector<Pair2<R>> tab(static_cast<size_t>(q.n_rows) * (q.n_x - 1));
+    for (int r = 0; r < q.n_rows; ++r)
+        for (int k = 0; k + 1 < q.n_x; ++k) {
+            const double* row = q.table + static_cast<size_t>(r) * q.n_x;
+            tab[static_cast<size_t>(r) * (q.n_x - 1) + k] = {static_cast<R>(row[k]), static_cast<R>(row[k + 1] - row[k])};
+        }
+    a.off.table2 = put(tab.data(), tab.size() * sizeof(Pair2<R>));
+    a.off.sched = put(sched.data(), sched.size() * sizeof(int2));
+    const size_t budget = sizeof(R) == 4 ? (110u << 10) : (220u << 10);
+    if (blob.size() > budget) return false;
+    a.smem_blob = static_cast<int>((blob.size() + 15) & ~static_cast<size_t>(15));
+    unsigned char* dblob = arena.alloc<unsigned char>(std::max<size_t>(16, blob.size()));
+    check_cuda(cudaMemcpy(dblob, blob.data(), blob.size(), cudaMemcpyHostToDevice), "copy blob");
+    a.blob = dblob;
+    a.top = static_cast<R>(q.n_x - 1) - static_cast<R>(1e-4);
+    return true;
+}
+
 // The blocks' totals added in block order by one warp per sum (lane l adds blocks l, l + 32, ...).
 __global__ void script_finalize(const double* __restrict__ partial, int n_blocks, double* __restrict__ sums) {
     const int lane = threadIdx.x & 31, t = threadIdx.x >> 5;
@@ -423,10 +622,20 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     d.bad = arena.alloc<unsigned long long>(3);
     check_cuda(cudaMemset(d.bad, 0, 3 * sizeof(unsigned long long)), "cudaMemset");
 
-    const void* fn = reinterpret_cast<const void*>(pick_script<R>(mq.model, n));
+    std::vector<int2> sched(S + 1);
+    for (int i = 0; i <= S; ++i) sched[i] = make_int2(event_at[i], static_cast<int>(fix_mask[i]));
+    LvArgs<R> lv{};
+    const bool fast = pack_lv<R>(rq, sched, arena, lv);
+    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n))
+                          : reinterpret_cast<const void*>(pick_script<R>(mq.model, n));
+    const int block = fast ? 256 : 128;
+    const size_t smem = fast ? static_cast<size_t>(lv.smem_blob) : 0;
+    if (fast)
+        check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                   "cudaFuncSetAttribute");
     int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0), "occupancy");
-    const long long need = (mq.n_pairs + 127) / 128;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem), "occupancy");
+    const long long need = (mq.n_pairs + block - 1) / block;
     const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(need, 1LL * sms * std::max(1, per_sm))));
     double* partial = arena.alloc<double>(2 * static_cast<size_t>(grid));
     double* sums = arena.alloc<double>(2);
@@ -435,7 +644,10 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
     const uint32_t k0 = static_cast<uint32_t>(mq.seed), k1 = static_cast<uint32_t>(mq.seed >> 32);
     check_cuda(cudaEventRecord(e0), "cudaEventRecord");
-    reinterpret_cast<ScriptFn<R>>(const_cast<void*>(fn))<<<grid, 128>>>(d, mq.n_pairs, k0, k1, partial);
+    if (fast)
+        reinterpret_cast<ScriptLvFn<R>>(const_cast<void*>(fn))<<<grid, block, smem>>>(d, lv, mq.n_pairs, k0, k1, partial);
+    else
+        reinterpret_cast<ScriptFn<R>>(const_cast<void*>(fn))<<<grid, block>>>(d, mq.n_pairs, k0, k1, partial);
     check_cuda(cudaGetLastError(), "script_kernel launch");
     script_finalize<<<1, 64>>>(partial, grid, sums);
     check_cuda(cudaGetLastError(), "script_finalize launch");
