@@ -287,7 +287,7 @@ typedef struct {
     const int* event_step;
     const int* event_code;     /* n_events + 1 */
     const double* event_discount;
-    int n_windows;             /* <= 32 */
+    int n_windows;             /* <= 8 */
     const int* win_name;
     const int* win_func;
     const int* win_fix0;       /* n_windows + 1 */

@@ -27,7 +27,7 @@ namespace ob {
 namespace {
 
 constexpr int kMaxRegs = 128;
-constexpr int kMaxWindows = 32;
+constexpr int kMaxWindows = 8;  // windows held in registers (kernels for up to 2 and up to 8)
 constexpr double kAnnual = 252.0;  // realised variance: fixings a year (varswap.py:24)
 
 enum ScriptOp : int {
@@ -60,16 +60,22 @@ struct ScriptDev {
     unsigned long long* bad;    // 3 counters: payments, conditions, redemptions
 };
 
-// One leg's state between events.
+// One leg's state between events (its register file lives in local memory: it is touched only at events).
 template <typename R>
 struct LegState {
     R reg[kMaxRegs];
-    R wv[kMaxWindows];        // lowest / highest ln(S / spot0) so far, or (variance) the last one
-    double wsum[kMaxWindows];  // variance: sum of squared log returns in the corridor
-    int wn[kMaxWindows];       // fixings seen
     R alive;
     double pv, red;
     bool bad_pay, bad_cond;
+};
+
+// One leg's windows, read and written only by loops unrolled over NW so that they stay in registers: they change at
+// every fixing, which is every step for a daily window. v: the lowest / highest ln(S / spot0) so far, or (variance)
+// the last one (NaN before the first fixing); s: the variance's sum of squared log returns in its corridor.
+template <typename R, int NW>
+struct WinState {
+    R v[NW];
+    double s[NW];
 };
 
 template <typename R>
@@ -85,8 +91,9 @@ __device__ __forceinline__ R compare(int op, R a, R b, R eps) {
 }
 
 // The script's instructions of one event on one leg. spot(a): the leg's spot of name a at this step.
-template <typename R, typename SpotFn>
-__device__ void run_event(const ScriptDev<R>& d, LegState<R>& s, int c0, int c1, double disc, SpotFn spot) {
+template <typename R, int NW, typename SpotFn>
+__device__ __noinline__ void run_event(const ScriptDev<R>& d, LegState<R>& s, const WinState<R, NW>& win, int c0, int c1,
+                          double disc, SpotFn spot) {
     R* r = s.reg;
     for (int pc = c0; pc < c1; ++pc) {
         const int4 in = __ldg(d.code + pc);
@@ -94,9 +101,13 @@ __device__ void run_event(const ScriptDev<R>& d, LegState<R>& s, int c0, int c1,
         switch (in.x) {
             case kSpot: r[dst] = spot(a); break;
             case kWin: {
-                const int f = d.win_func[a];
-                r[dst] = f == 2 ? static_cast<R>(kAnnual / static_cast<double>(d.win_nfix[a] - 1) * s.wsum[a])
-                                : d.spot0[d.win_name[a]] * m_exp(s.wv[a]);
+                R v = R(0);
+                double sum = 0.0;
+#pragma unroll
+                for (int w = 0; w < NW; ++w)
+                    if (w == a) v = win.v[w], sum = win.s[w];
+                r[dst] = d.win_func[a] == 2 ? static_cast<R>(kAnnual / static_cast<double>(d.win_nfix[a] - 1) * sum)
+                                            : d.spot0[d.win_name[a]] * m_exp(v);
                 break;
             }
             case kMov: r[dst] = r[a]; break;
@@ -158,42 +169,47 @@ __device__ void run_event(const ScriptDev<R>& d, LegState<R>& s, int c0, int c1,
 // The windows fixing at this step, on one leg. logp(a): ln(S_a / spot0_a) of name a at this step. A window keeps the
 // extreme (or, for the variance, the last) of ln(S / spot0): S is increasing in it, so the lowest and highest spots
 // are spot0 exp(extreme), and the log returns are differences of it; no exp or log is taken at the fixings.
-template <typename R, typename LogFn>
-__device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, LegState<R>& s, unsigned mask, LogFn logp) {
-    while (mask) {
-        const int w = __ffs(mask) - 1;
-        mask &= mask - 1;
+template <typename R, int NW, typename LogFn>
+__device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, WinState<R, NW>& win, unsigned mask, LogFn logp) {
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        if (!((mask >> w) & 1u)) continue;
         const R y = logp(d.win_name[w]);
         const int f = d.win_func[w];
         if (f == 0) {
-            s.wv[w] = m_min(s.wv[w], y);
+            win.v[w] = m_min(win.v[w], y);
         } else if (f == 1) {
-            s.wv[w] = m_max(s.wv[w], y);
+            win.v[w] = m_max(win.v[w], y);
         } else {
-            if (s.wn[w] > 0) {
-                const R prev = s.wv[w];
+            const R prev = win.v[w];
+            if (!isnan(prev)) {
                 const double lo = d.win_lo[w], hi = d.win_hi[w], pd = static_cast<double>(prev);
                 const bool inside = (isnan(lo) || pd >= lo) && (isnan(hi) || pd <= hi);
                 const double rr = static_cast<double>(y - prev);
-                if (inside) s.wsum[w] += rr * rr;
+                if (inside) win.s[w] += rr * rr;
             }
-            s.wv[w] = y;
+            win.v[w] = y;
         }
-        s.wn[w] += 1;
+    }
+}
+
+template <typename R, int NW>
+__device__ __forceinline__ void win_init(const ScriptDev<R>& d, WinState<R, NW>& win) {
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const int f = w < d.n_windows ? d.win_func[w] : 0;
+        win.v[w] = f == 0 ? R(INFINITY) : (f == 1 ? R(-INFINITY) : R(NAN));
+        win.s[w] = 0.0;
     }
 }
 
 template <typename R>
 __device__ void leg_init(const ScriptDev<R>& d, LegState<R>& s) {
     for (int k = 0; k < d.n_regs; ++k) s.reg[k] = k < d.n_const ? static_cast<R>(d.consts[k]) : R(0);
-    for (int w = 0; w < d.n_windows; ++w) {
-        s.wv[w] = d.win_func[w] == 1 ? R(-INFINITY) : R(INFINITY);
-        s.wsum[w] = 0.0, s.wn[w] = 0;
-    }
     s.alive = R(1), s.pv = 0.0, s.red = 0.0, s.bad_pay = s.bad_cond = false;
 }
 
-template <typename R, int N, int MODEL>
+template <typename R, int N, int MODEL, int NW>
 __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n_pairs, uint32_t k0, uint32_t k1,
                                                      double* __restrict__ partial) {
     __shared__ double wacc[4][2];
@@ -210,6 +226,8 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
         const uint64_t pair = static_cast<uint64_t>(active ? base + lane : n_pairs - 1);
         LegState<R> leg[2];
         leg_init(d, leg[0]), leg_init(d, leg[1]);
+        WinState<R, NW> win[2];
+        win_init(d, win[0]), win_init(d, win[1]);
         PairDev<R, N> st;
         NormalStream<R> qrng;
         R y[2] = {R(0), R(0)}, v[2] = {d.qe.v0, d.qe.v0};
@@ -239,8 +257,9 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
                     return d.lf[a * (S + 1) + i] + x;
                 };
                 auto spot = [&](int a) -> R { return d.spot0[a] * m_exp(logp(a)); };
-                if (fm) fix_windows(d, leg[l], fm, logp);
-                if (ev >= 0) run_event(d, leg[l], d.event_code[ev], d.event_code[ev + 1], d.event_disc[ev], spot);
+                if (fm) fix_windows(d, win[l], fm, logp);
+                if (ev >= 0)
+                    run_event(d, leg[l], win[l], d.event_code[ev], d.event_code[ev + 1], d.event_disc[ev], spot);
             }
         }
         double y_pair = 0.0;
@@ -284,21 +303,21 @@ struct LvArgs {
     R top;
 };
 
-template <typename R, int N>
-__global__ void __launch_bounds__(256) script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0,
+template <typename R, int N, int NW>
+__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0,
                                                         uint32_t k1, double* __restrict__ partial) {
     constexpr int C = N;
     constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);
     constexpr int NB = C * G / 4;
     extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ double wacc[8][2];
+    __shared__ double wacc[16][2];
     {
         const int4* src = reinterpret_cast<const int4*>(a.blob);
         int4* dst = reinterpret_cast<int4*>(sm);
         for (int t = threadIdx.x; t < a.smem_blob / 16; t += blockDim.x) dst[t] = src[t];
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
-    if (threadIdx.x < 16) (&wacc[0][0])[threadIdx.x] = 0.0;
+    if (threadIdx.x < 32) (&wacc[0][0])[threadIdx.x] = 0.0;
     __syncthreads();
     const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
     const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
@@ -314,6 +333,8 @@ __global__ void __launch_bounds__(256) script_lv_kernel(ScriptDev<R> d, LvArgs<R
         const uint64_t pair = static_cast<uint64_t>(active ? base + lane : n_pairs - 1);
         LegState<R> leg[2];
         leg_init(d, leg[0]), leg_init(d, leg[1]);
+        WinState<R, NW> win[2];
+        win_init(d, win[0]), win_init(d, win[1]);
         R x0[N], x1[N], y0[N], y1[N];
 #pragma unroll
         for (int n = 0; n < N; ++n) x0[n] = x1[n] = R(0), y0[n] = y1[n] = s_lf0[n];
@@ -330,8 +351,9 @@ __global__ void __launch_bounds__(256) script_lv_kernel(ScriptDev<R> d, LvArgs<R
                     return v;
                 };
                 auto spot = [&](int nm) -> R { return d.spot0[nm] * m_exp(logp(nm)); };
-                if (sc.y) fix_windows(d, leg[l], static_cast<unsigned>(sc.y), logp);
-                if (sc.x >= 0) run_event(d, leg[l], d.event_code[sc.x], d.event_code[sc.x + 1], d.event_disc[sc.x], spot);
+                if (sc.y) fix_windows(d, win[l], static_cast<unsigned>(sc.y), logp);
+                if (sc.x >= 0)
+                    run_event(d, leg[l], win[l], d.event_code[sc.x], d.event_code[sc.x + 1], d.event_disc[sc.x], spot);
             }
         };
         observe(0);
@@ -397,16 +419,22 @@ __global__ void __launch_bounds__(256) script_lv_kernel(ScriptDev<R> d, LvArgs<R
 template <typename R>
 using ScriptLvFn = void (*)(ScriptDev<R>, LvArgs<R>, long long, uint32_t, uint32_t, double*);
 
-template <typename R>
-ScriptLvFn<R> pick_lv(int n) {
+template <typename R, int NW>
+ScriptLvFn<R> pick_lv_nw(int n) {
     switch (n) {
-        case 1: return script_lv_kernel<R, 1>;
-        case 2: return script_lv_kernel<R, 2>;
-        case 3: return script_lv_kernel<R, 3>;
-        case 4: return script_lv_kernel<R, 4>;
-        case 5: return script_lv_kernel<R, 5>;
+        case 1: return script_lv_kernel<R, 1, NW>;
+        case 2: return script_lv_kernel<R, 2, NW>;
+        case 3: return script_lv_kernel<R, 3, NW>;
+        case 4: return script_lv_kernel<R, 4, NW>;
+        case 5: return script_lv_kernel<R, 5, NW>;
         default: return nullptr;
     }
+}
+
+// Kernels for up to 2 windows (most products: a knock-in window or two) and up to 8.
+template <typename R>
+ScriptLvFn<R> pick_lv(int n, int n_windows) {
+    return n_windows <= 2 ? pick_lv_nw<R, 2>(n) : pick_lv_nw<R, kMaxWindows>(n);
 }
 
 // The staged blob of the local-vol path, or false when it does not apply (a name not local vol, more than five
@@ -479,13 +507,18 @@ __global__ void script_finalize(const double* __restrict__ partial, int n_blocks
 template <typename R>
 using ScriptFn = void (*)(ScriptDev<R>, long long, uint32_t, uint32_t, double*);
 
+template <typename R, int NW>
+ScriptFn<R> pick_script_nw(int model, int n) {
+    if (model == OB_MODEL_HESTON_QE) return script_kernel<R, 1, OB_MODEL_HESTON_QE, NW>;
+    if (n <= 1) return script_kernel<R, 1, OB_MODEL_PATHS, NW>;
+    if (n <= 2) return script_kernel<R, 2, OB_MODEL_PATHS, NW>;
+    if (n <= 4) return script_kernel<R, 4, OB_MODEL_PATHS, NW>;
+    return script_kernel<R, 8, OB_MODEL_PATHS, NW>;
+}
+
 template <typename R>
-ScriptFn<R> pick_script(int model, int n) {
-    if (model == OB_MODEL_HESTON_QE) return script_kernel<R, 1, OB_MODEL_HESTON_QE>;
-    if (n <= 1) return script_kernel<R, 1, OB_MODEL_PATHS>;
-    if (n <= 2) return script_kernel<R, 2, OB_MODEL_PATHS>;
-    if (n <= 4) return script_kernel<R, 4, OB_MODEL_PATHS>;
-    return script_kernel<R, 8, OB_MODEL_PATHS>;
+ScriptFn<R> pick_script(int model, int n, int n_windows) {
+    return n_windows <= 2 ? pick_script_nw<R, 2>(model, n) : pick_script_nw<R, kMaxWindows>(model, n);
 }
 
 // Every index the device will follow is checked here: registers, names, windows, tags, code ranges and steps.
@@ -496,7 +529,7 @@ void check_script(const ob_script_request& rq) {
     if (rq.n_const < 1 || rq.n_const > rq.n_regs || !rq.consts) invalid("n_const must be 1 to n_regs");
     if (rq.n_code < 0 || (rq.n_code > 0 && !rq.code)) invalid("null code");
     if (rq.n_events < 1 || !rq.event_step || !rq.event_code || !rq.event_discount) invalid("a script needs events");
-    if (rq.n_windows < 0 || rq.n_windows > kMaxWindows) invalid("n_windows must be 0 to 32");
+    if (rq.n_windows < 0 || rq.n_windows > kMaxWindows) invalid("n_windows must be 0 to 8");
     if (rq.n_windows && (!rq.win_name || !rq.win_func || !rq.win_fix0 || !rq.fix_step || !rq.win_lower ||
                          !rq.win_upper))
         invalid("null window arrays");
@@ -626,9 +659,9 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     for (int i = 0; i <= S; ++i) sched[i] = make_int2(event_at[i], static_cast<int>(fix_mask[i]));
     LvArgs<R> lv{};
     const bool fast = pack_lv<R>(rq, sched, arena, lv);
-    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n))
-                          : reinterpret_cast<const void*>(pick_script<R>(mq.model, n));
-    const int block = fast ? 256 : 128;
+    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n, rq.n_windows))
+                          : reinterpret_cast<const void*>(pick_script<R>(mq.model, n, rq.n_windows));
+    const int block = fast ? 512 : 128;
     const size_t smem = fast ? static_cast<size_t>(lv.smem_blob) : 0;
     if (fast)
         check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),

@@ -674,7 +674,7 @@ _ARITH = {"+": "add", "-": "sub", "*": "mul", "/": "div"}
 _CMP = {">=": "ge", ">": "gt", "<=": "le", "<": "lt", "==": "eq"}
 WIN_FUNC = {"lowest": 0, "highest": 1, "variance": 2}
 MAX_REGS = 128
-MAX_WINDOWS = 32
+MAX_WINDOWS = 8
 
 
 @dataclass
