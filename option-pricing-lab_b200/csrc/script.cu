@@ -55,6 +55,7 @@ struct ScriptDev {
     const int* win_nfix;
     const double* win_lo;
     const double* win_hi;
+    const R* win_spot0;
     R eps;
     double red_tol;
     unsigned long long* bad;    // 3 counters: payments, conditions, redemptions
@@ -90,16 +91,28 @@ __device__ __forceinline__ R compare(int op, R a, R b, R eps) {
     return m_min(m_max(d / scale + R(0.5), R(0)), R(1));
 }
 
-// The script's instructions of one event on one leg. spot(a): the leg's spot of name a at this step.
-template <typename R, int NW, typename SpotFn>
-__device__ __noinline__ void run_event(const ScriptDev<R>& d, LegState<R>& s, const WinState<R, NW>& win, int c0, int c1,
-                          double disc, SpotFn spot) {
+// What the interpreter reads besides a leg's state, passed by value so that no state of the kernel's step loop has
+// its address taken (the step loop keeps its paths and windows in registers).
+template <typename R>
+struct EvCtx {
+    const int4* code;
+    const int* win_func;
+    const int* win_nfix;
+    const R* win_spot0;  // the spot of each window's name at the valuation date
+    R eps;
+};
+
+// The script's instructions of one event on one leg: sp[a] is the leg's spot of name a at this step, win a copy of
+// the leg's windows. Out of line: it runs a few dozen times a path, and inlined it would crowd the step loop.
+template <typename R, int NW>
+__device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, NW> win, const R* sp, int c0, int c1,
+                                       double disc) {
     R* r = s.reg;
     for (int pc = c0; pc < c1; ++pc) {
         const int4 in = __ldg(d.code + pc);
         const int dst = in.y, a = in.z, b = in.w;
         switch (in.x) {
-            case kSpot: r[dst] = spot(a); break;
+            case kSpot: r[dst] = sp[a]; break;
             case kWin: {
                 R v = R(0);
                 double sum = 0.0;
@@ -107,7 +120,7 @@ __device__ __noinline__ void run_event(const ScriptDev<R>& d, LegState<R>& s, co
                 for (int w = 0; w < NW; ++w)
                     if (w == a) v = win.v[w], sum = win.s[w];
                 r[dst] = d.win_func[a] == 2 ? static_cast<R>(kAnnual / static_cast<double>(d.win_nfix[a] - 1) * sum)
-                                            : d.spot0[d.win_name[a]] * m_exp(v);
+                                            : d.win_spot0[a] * m_exp(v);
                 break;
             }
             case kMov: r[dst] = r[a]; break;
@@ -193,6 +206,13 @@ __device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, WinState<R, N
     }
 }
 
+template <typename R>
+__device__ __forceinline__ EvCtx<R> ev_ctx(const ScriptDev<R>& d) {
+    EvCtx<R> c;
+    c.code = d.code, c.win_func = d.win_func, c.win_nfix = d.win_nfix, c.win_spot0 = d.win_spot0, c.eps = d.eps;
+    return c;
+}
+
 template <typename R, int NW>
 __device__ __forceinline__ void win_init(const ScriptDev<R>& d, WinState<R, NW>& win) {
 #pragma unroll
@@ -256,10 +276,14 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
                         if (n == a) x = st.x[l][n];
                     return d.lf[a * (S + 1) + i] + x;
                 };
-                auto spot = [&](int a) -> R { return d.spot0[a] * m_exp(logp(a)); };
                 if (fm) fix_windows(d, win[l], fm, logp);
-                if (ev >= 0)
-                    run_event(d, leg[l], win[l], d.event_code[ev], d.event_code[ev + 1], d.event_disc[ev], spot);
+                if (ev >= 0) {
+                    R sp[N];
+#pragma unroll
+                    for (int n = 0; n < N; ++n) sp[n] = n < d.n_names ? d.spot0[n] * m_exp(logp(n)) : R(0);
+                    run_event<R, NW>(ev_ctx(d), leg[l], win[l], sp, d.event_code[ev], d.event_code[ev + 1],
+                                     d.event_disc[ev]);
+                }
             }
         }
         double y_pair = 0.0;
@@ -350,10 +374,14 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
                         if (n == nm) v = l ? y1[n] : y0[n];
                     return v;
                 };
-                auto spot = [&](int nm) -> R { return d.spot0[nm] * m_exp(logp(nm)); };
                 if (sc.y) fix_windows(d, win[l], static_cast<unsigned>(sc.y), logp);
-                if (sc.x >= 0)
-                    run_event(d, leg[l], win[l], d.event_code[sc.x], d.event_code[sc.x + 1], d.event_disc[sc.x], spot);
+                if (sc.x >= 0) {
+                    R sp[N];
+#pragma unroll
+                    for (int n = 0; n < N; ++n) sp[n] = d.spot0[n] * m_exp(l ? y1[n] : y0[n]);
+                    run_event<R, NW>(ev_ctx(d), leg[l], win[l], sp, d.event_code[sc.x], d.event_code[sc.x + 1],
+                                     d.event_disc[sc.x]);
+                }
             }
         };
         observe(0);
@@ -649,6 +677,9 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
         }
         d.win_lo = arena.put<double>(llo.data(), llo.size());
         d.win_hi = arena.put<double>(lhi.data(), lhi.size());
+        std::vector<double> ws0(rq.n_windows);
+        for (int w = 0; w < rq.n_windows; ++w) ws0[w] = mq.spot[rq.win_name[w]];
+        d.win_spot0 = arena.put<R>(ws0.data(), ws0.size());
     }
     d.eps = static_cast<R>(rq.smoothing);
     d.red_tol = rq.smoothing == 0.0 ? 1e-12 : (sizeof(R) == 8 ? 1e-9 : 1e-5);
