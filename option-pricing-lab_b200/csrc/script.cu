@@ -182,13 +182,28 @@ __device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, N
 // The windows fixing at this step, on one leg. logp(a): ln(S_a / spot0_a) of name a at this step. A window keeps the
 // extreme (or, for the variance, the last) of ln(S / spot0): S is increasing in it, so the lowest and highest spots
 // are spot0 exp(extreme), and the log returns are differences of it; no exp or log is taken at the fixings.
+// Each window's function and name, packed (function | name << 2), loaded once a thread into registers.
+template <int NW>
+struct WinMeta {
+    int fn[NW];
+};
+
+template <typename R, int NW>
+__device__ __forceinline__ WinMeta<NW> win_meta(const ScriptDev<R>& d) {
+    WinMeta<NW> m;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) m.fn[w] = w < d.n_windows ? (d.win_func[w] | (d.win_name[w] << 2)) : 0;
+    return m;
+}
+
 template <typename R, int NW, typename LogFn>
-__device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, WinState<R, NW>& win, unsigned mask, LogFn logp) {
+__device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, const WinMeta<NW>& meta, WinState<R, NW>& win,
+                                            unsigned mask, LogFn logp) {
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
         if (!((mask >> w) & 1u)) continue;
-        const R y = logp(d.win_name[w]);
-        const int f = d.win_func[w];
+        const int f = meta.fn[w] & 3;
+        const R y = logp(meta.fn[w] >> 2);
         if (f == 0) {
             win.v[w] = m_min(win.v[w], y);
         } else if (f == 1) {
@@ -239,6 +254,7 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
     ModelDev<R> m = d.m;
     m.k0 = k0, m.k1 = k1;
     const int S = d.n_steps;
+    const WinMeta<NW> meta = win_meta<R, NW>(d);
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n_pairs;
          base += stride) {
@@ -276,7 +292,7 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
                         if (n == a) x = st.x[l][n];
                     return d.lf[a * (S + 1) + i] + x;
                 };
-                if (fm) fix_windows(d, win[l], fm, logp);
+                if (fm) fix_windows(d, meta, win[l], fm, logp);
                 if (ev >= 0) {
                     R sp[N];
 #pragma unroll
@@ -350,6 +366,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
     const int2* s_sched = reinterpret_cast<const int2*>(sm + a.off.sched);  // (event, window mask) per step end
     const R* s_lf0 = reinterpret_cast<const R*>(sm + a.off.lf0);
     const int S = d.n_steps;
+    const WinMeta<NW> meta = win_meta<R, NW>(d);
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n_pairs;
          base += stride) {
@@ -374,7 +391,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
                         if (n == nm) v = l ? y1[n] : y0[n];
                     return v;
                 };
-                if (sc.y) fix_windows(d, win[l], static_cast<unsigned>(sc.y), logp);
+                if (sc.y) fix_windows(d, meta, win[l], static_cast<unsigned>(sc.y), logp);
                 if (sc.x >= 0) {
                     R sp[N];
 #pragma unroll
