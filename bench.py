@@ -11,7 +11,9 @@ device-timed steps (CUDA events on the launching stream), max over ranks. `e2e` 
 call with host inputs (`optlab_b200.engine.mc_price`: upload, kernel, read-back). Ranks (torchrun) each take their own
 range of pairs (first_pair = rank x pairs): weak scaling, no collective in the timed steps, and one FP64 all-reduce
 of the sums after them (optlab_b200.shard). `--workload adjoint` times the Greeks of the worst-of autocall (FP32
-adjoint against FP64 bump-and-revalue); `--workload batch` the batched revaluation of a 512-trade book.
+adjoint against FP64 bump-and-revalue); `--workload batch` the batched revaluation of a 512-trade book;
+`--workload leverage` the SLV leverage calibration; `--workload script` the default Phoenix written as a payoff script
+and run by the device's script interpreter.
 
 `--impl reference` times the reference's CPU implementation of the same workload instead: its path engine
 (optlab::api::paths, compiled from the reference's sources into oracle/_ref) writing the 12 quarterly columns and the
