@@ -295,7 +295,22 @@ typedef struct {
     const double* win_lower;
     const double* win_upper;
     double smoothing;
+    /* The issuer's call (`call pay`, instruction "call" with d = call index, a = amount, b = mask): call_mode 0 never
+       calls; 1 records a pilot: for every path (pair p's legs at p and n_pairs + p), per event its discounted flows
+       before and after its call statement, then per call its mask, the alive mass, the amount and the n_state state
+       values, into the host array `record` (2 n_pairs x (2 n_events + n_calls (3 + n_state)) doubles); 2 applies
+       fitted rules: the issuer calls where the rule's continuation of the state is above the amount. A rule is
+       OB_RULE_STRIDE doubles: valid, n_poly, n_knots, mean[4], scale[4], powers[25][4], knot variable[25],
+       knot[25], coefficients[50] (the polynomials', then the hinges'). */
+    int n_calls;
+    const int* call_state;     /* n_calls x 4: registers of each call's state */
+    int n_state;               /* <= 4 */
+    int call_mode;
+    const double* rules;
+    double* record;
 } ob_script_request;
+
+#define OB_RULE_STRIDE 224
 
 /* price and se of the pair-averaged present value; the paths (legs) on which a payment was not finite, a condition
    undefined where it mattered, or the redemption weights did not add up to one. */

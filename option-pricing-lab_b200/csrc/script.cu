@@ -29,10 +29,12 @@ namespace {
 constexpr int kMaxRegs = 128;
 constexpr int kMaxWindows = 8;  // windows held in registers (kernels for up to 2 and up to 8)
 constexpr double kAnnual = 252.0;  // realised variance: fixings a year (varswap.py:24)
+constexpr int kMaxState = 4;       // state variables of an issuer's call
+constexpr int kMaxPoly = 25, kMaxKnots = 25;  // a rule's polynomial terms and hinges
 
 enum ScriptOp : int {
     kSpot, kWin, kMov, kAdd, kSub, kMul, kDiv, kNeg, kMin, kMax, kAbs, kExp, kLog, kSqrt,
-    kGe, kGt, kLe, kLt, kEq, kAnd, kOr, kNot, kAssign, kPay, kTerm, kCond, kNumOps
+    kGe, kGt, kLe, kLt, kEq, kAnd, kOr, kNot, kAssign, kPay, kTerm, kCond, kCall, kNumOps
 };
 
 template <typename R>
@@ -59,6 +61,11 @@ struct ScriptDev {
     R eps;
     double red_tol;
     unsigned long long* bad;    // 3 counters: payments, conditions, redemptions
+    // the issuer's call
+    int n_events, n_calls, n_state, call_mode, rec_stride;
+    const int* call_state;      // n_calls x 4 registers
+    const double* rules;        // n_calls x OB_RULE_STRIDE
+    double* record;             // call_mode 1: 2 n_pairs x rec_stride
 };
 
 // One leg's state between events (its register file lives in local memory: it is touched only at events).
@@ -100,7 +107,35 @@ struct EvCtx {
     const int* win_nfix;
     const R* win_spot0;  // the spot of each window's name at the valuation date
     R eps;
+    int call_mode, n_state, n_events, k;  // k: the event
+    const int* call_state;
+    const double* rules;
+    double* rec;         // this leg's record (call_mode 1), or null
 };
+
+// A fitted rule's continuation of the state (exercise: the polynomial terms, then the hinges max(z_v - knot, 0), on
+// the state normalised by the rule's mean and scale).
+__device__ double continuation(const double* rule, const double* state, int n_state) {
+    const int n_poly = static_cast<int>(rule[1]), n_knots = static_cast<int>(rule[2]);
+    double z[kMaxState];
+#pragma unroll
+    for (int j = 0; j < kMaxState; ++j) z[j] = j < n_state ? (state[j] - rule[3 + j]) / rule[7 + j] : 0.0;
+    const double* coef = rule + 161;
+    double cont = 0.0;
+    for (int t = 0; t < n_poly; ++t) {
+        double term = 1.0;
+        for (int j = 0; j < n_state; ++j) {
+            const int p = static_cast<int>(rule[11 + 4 * t + j]);
+            for (int e = 0; e < p; ++e) term *= z[j];
+        }
+        cont += coef[t] * term;
+    }
+    for (int q = 0; q < n_knots; ++q) {
+        const double h = z[static_cast<int>(rule[111 + q])] - rule[136 + q];
+        cont += coef[n_poly + q] * (h > 0.0 ? h : 0.0);
+    }
+    return cont;
+}
 
 // The script's instructions of one event on one leg: sp[a] is the leg's spot of name a at this step, win a copy of
 // the leg's windows. Out of line: it runs a few dozen times a path, and inlined it would crowd the step loop.
@@ -108,6 +143,8 @@ template <typename R, int NW>
 __device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, NW> win, const R* sp, int c0, int c1,
                                        double disc) {
     R* r = s.reg;
+    bool after = false;  // past this event's call statement
+    double pre = 0.0, post = 0.0;
     for (int pc = c0; pc < c1; ++pc) {
         const int4 in = __ldg(d.code + pc);
         const int dst = in.y, a = in.z, b = in.w;
@@ -158,10 +195,40 @@ __device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, N
             case kPay: {
                 const R w = r[b] * s.alive, e = r[a];
                 if (w != R(0)) {
-                    if (!isfinite(e)) s.bad_pay = true;
-                    else s.pv += disc * (static_cast<double>(w) * static_cast<double>(e));
+                    if (!isfinite(e)) {
+                        s.bad_pay = true;
+                    } else {
+                        const double paid = disc * (static_cast<double>(w) * static_cast<double>(e));
+                        s.pv += paid;
+                        if (after) post += paid;
+                        else pre += paid;
+                    }
                 }
                 if (dst == 2) s.red += static_cast<double>(w);
+                break;
+            }
+            case kCall: {
+                double st[kMaxState];
+#pragma unroll
+                for (int j = 0; j < kMaxState; ++j)
+                    st[j] = j < d.n_state ? static_cast<double>(r[d.call_state[4 * dst + j]]) : 0.0;
+                const R m = r[b], amt = r[a];
+                if (d.call_mode == 1 && d.rec) {
+                    double* c = d.rec + 2 * d.n_events + dst * (3 + d.n_state);
+                    c[0] = static_cast<double>(m), c[1] = static_cast<double>(s.alive), c[2] = static_cast<double>(amt);
+                    for (int j = 0; j < d.n_state; ++j) c[3 + j] = st[j];
+                    after = true;
+                } else if (d.call_mode == 2) {
+                    const double* rule = d.rules + static_cast<long long>(dst) * OB_RULE_STRIDE;
+                    const bool call = rule[0] != 0.0 && continuation(rule, st, d.n_state) > static_cast<double>(amt);
+                    const R md = call ? m : R(0), w = md * s.alive;
+                    if (w != R(0)) {
+                        if (!isfinite(amt)) s.bad_pay = true;
+                        else s.pv += disc * (static_cast<double>(w) * static_cast<double>(amt));
+                    }
+                    s.red += static_cast<double>(w);
+                    s.alive = s.alive * (R(1) - md);
+                }
                 break;
             }
             case kTerm: s.alive = s.alive * (R(1) - r[a]); break;
@@ -177,6 +244,7 @@ __device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, N
             default: break;
         }
     }
+    if (d.call_mode == 1 && d.rec) d.rec[2 * d.k] = pre, d.rec[2 * d.k + 1] = post;
 }
 
 // The windows fixing at this step, on one leg. logp(a): ln(S_a / spot0_a) of name a at this step. A window keeps the
@@ -222,10 +290,20 @@ __device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, const WinMeta
 }
 
 template <typename R>
-__device__ __forceinline__ EvCtx<R> ev_ctx(const ScriptDev<R>& d) {
+__device__ __forceinline__ EvCtx<R> ev_ctx(const ScriptDev<R>& d, int k, double* rec) {
     EvCtx<R> c;
     c.code = d.code, c.win_func = d.win_func, c.win_nfix = d.win_nfix, c.win_spot0 = d.win_spot0, c.eps = d.eps;
+    c.call_mode = d.call_mode, c.n_state = d.n_state, c.n_events = d.n_events, c.k = k;
+    c.call_state = d.call_state, c.rules = d.rules, c.rec = rec;
     return c;
+}
+
+// The record of one leg of one pair (pair p's legs are paths p and n_pairs + p), or null.
+template <typename R>
+__device__ __forceinline__ double* leg_record(const ScriptDev<R>& d, long long p, long long n_pairs, int l,
+                                              bool active) {
+    if (d.call_mode != 1 || !active) return nullptr;
+    return d.record + static_cast<long long>(d.rec_stride) * (l ? n_pairs + p : p);
 }
 
 template <typename R, int NW>
@@ -297,8 +375,8 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
                     R sp[N];
 #pragma unroll
                     for (int n = 0; n < N; ++n) sp[n] = n < d.n_names ? d.spot0[n] * m_exp(logp(n)) : R(0);
-                    run_event<R, NW>(ev_ctx(d), leg[l], win[l], sp, d.event_code[ev], d.event_code[ev + 1],
-                                     d.event_disc[ev]);
+                    run_event<R, NW>(ev_ctx(d, ev, leg_record(d, base + lane, n_pairs, l, active)), leg[l], win[l], sp,
+                                     d.event_code[ev], d.event_code[ev + 1], d.event_disc[ev]);
                 }
             }
         }
@@ -396,8 +474,8 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
                     R sp[N];
 #pragma unroll
                     for (int n = 0; n < N; ++n) sp[n] = d.spot0[n] * m_exp(l ? y1[n] : y0[n]);
-                    run_event<R, NW>(ev_ctx(d), leg[l], win[l], sp, d.event_code[sc.x], d.event_code[sc.x + 1],
-                                     d.event_disc[sc.x]);
+                    run_event<R, NW>(ev_ctx(d, sc.x, leg_record(d, base + lane, n_pairs, l, active)), leg[l], win[l],
+                                     sp, d.event_code[sc.x], d.event_code[sc.x + 1], d.event_disc[sc.x]);
                 }
             }
         };
@@ -597,6 +675,35 @@ void check_script(const ob_script_request& rq) {
             if (rq.fix_step[k] < 0 || rq.fix_step[k] > S || (k > rq.win_fix0[w] && rq.fix_step[k] <= rq.fix_step[k - 1]))
                 invalid("window fixing steps must increase within 0 .. n_steps");
     }
+    if (rq.n_calls < 0 || rq.n_state < 0 || rq.n_state > kMaxState) invalid("n_calls >= 0 and n_state 0 to 4");
+    if (rq.call_mode < 0 || rq.call_mode > 2) invalid("call_mode must be 0, 1 or 2");
+    if (rq.n_calls && !rq.call_state) invalid("null call_state");
+    if (rq.call_mode == 1 && rq.n_calls && !rq.record) invalid("call_mode 1 needs a record array");
+    if (rq.call_mode == 2 && rq.n_calls && !rq.rules) invalid("call_mode 2 needs rules");
+    for (int c = 0; c < rq.n_calls; ++c)
+        for (int j = 0; j < rq.n_state; ++j)
+            if (rq.call_state[4 * c + j] < 0 || rq.call_state[4 * c + j] >= rq.n_regs)
+                invalid("a call's state names a register beyond n_regs");
+    if (rq.call_mode == 2)
+        for (int c = 0; c < rq.n_calls; ++c) {
+            const double* r = rq.rules + static_cast<long long>(c) * OB_RULE_STRIDE;
+            if (r[0] == 0.0) continue;
+            const double np = r[1], nk = r[2];
+            if (!(np >= 0 && np <= kMaxPoly && nk >= 0 && nk <= kMaxKnots) || np != std::floor(np) ||
+                nk != std::floor(nk))
+                invalid("a rule has 0 to 25 polynomial terms and 0 to 25 hinges");
+            for (int t = 0; t < static_cast<int>(np); ++t)
+                for (int j = 0; j < rq.n_state; ++j) {
+                    const double pw = r[11 + 4 * t + j];
+                    if (!(pw >= 0 && pw <= 3) || pw != std::floor(pw)) invalid("rule powers must be 0 to 3");
+                }
+            for (int q = 0; q < static_cast<int>(nk); ++q) {
+                const double v = r[111 + q];
+                if (!(v >= 0 && v < rq.n_state) || v != std::floor(v)) invalid("a hinge names an unknown state");
+            }
+            for (int j = 0; j < rq.n_state; ++j)
+                if (!(r[7 + j] != 0.0)) invalid("a rule's scales must not be 0");
+        }
     auto reg = [&](int r) {
         if (r < 0 || r >= rq.n_regs) invalid("an instruction names a register beyond n_regs");
     };
@@ -618,6 +725,10 @@ void check_script(const ob_script_request& rq) {
                 reg(a), reg(b);
                 break;
             case kTerm: reg(a); break;
+            case kCall:
+                if (d < 0 || d >= rq.n_calls) invalid("a call instruction names an unknown call");
+                reg(a), reg(b);
+                break;
             case kMov: case kNeg: case kAbs: case kExp: case kLog: case kSqrt: case kNot: reg(d), reg(a); break;
             default:
                 reg(d), reg(a), reg(b);
@@ -698,6 +809,17 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
         for (int w = 0; w < rq.n_windows; ++w) ws0[w] = mq.spot[rq.win_name[w]];
         d.win_spot0 = arena.put<R>(ws0.data(), ws0.size());
     }
+    d.n_events = rq.n_events, d.n_calls = rq.n_calls, d.n_state = rq.n_state, d.call_mode = rq.call_mode;
+    d.rec_stride = 2 * rq.n_events + rq.n_calls * (3 + rq.n_state);
+    if (rq.n_calls) {
+        d.call_state = arena.put<int>(rq.call_state, 4 * static_cast<size_t>(rq.n_calls));
+        if (rq.call_mode == 2) d.rules = arena.put<double>(rq.rules, static_cast<size_t>(rq.n_calls) * OB_RULE_STRIDE);
+    }
+    const size_t rec_count = rq.call_mode == 1 ? static_cast<size_t>(2 * mq.n_pairs) * d.rec_stride : 0;
+    if (rec_count) {
+        d.record = arena.alloc<double>(rec_count);
+        check_cuda(cudaMemset(d.record, 0, rec_count * sizeof(double)), "cudaMemset");
+    }
     d.eps = static_cast<R>(rq.smoothing);
     d.red_tol = rq.smoothing == 0.0 ? 1e-12 : (sizeof(R) == 8 ? 1e-9 : 1e-5);
     d.bad = arena.alloc<unsigned long long>(3);
@@ -737,6 +859,8 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     unsigned long long bad[3];
     check_cuda(cudaMemcpy(h, sums, sizeof h, cudaMemcpyDeviceToHost), "copy sums");
     check_cuda(cudaMemcpy(bad, d.bad, sizeof bad, cudaMemcpyDeviceToHost), "copy counts");
+    if (rec_count) check_cuda(cudaMemcpy(rq.record, d.record, rec_count * sizeof(double), cudaMemcpyDeviceToHost),
+                              "copy record");
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0), cudaEventDestroy(e1);

@@ -304,7 +304,16 @@ class ObScriptRequest(C.Structure):
         ("win_lower", _dp),
         ("win_upper", _dp),
         ("smoothing", C.c_double),
+        ("n_calls", C.c_int),
+        ("call_state", _ip),
+        ("n_state", C.c_int),
+        ("call_mode", C.c_int),
+        ("rules", _dp),
+        ("record", _dp),
     ]
+
+
+OB_RULE_STRIDE = 224
 
 
 class ObScriptResult(C.Structure):

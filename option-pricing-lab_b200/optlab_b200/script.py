@@ -11,9 +11,12 @@ on every path: inside an `if`, `x = e` becomes `x = m e + (1 - m) x`, `pay e` ad
 clip((a - b) / (eps |b|) + 1/2, 0, 1). The device keeps that reading, so every path runs the same instructions
 (no divergence), and accumulates the present value of the flows (discount factors of the payment dates).
 
-Not on the device: the issuer's call (`call pay`, which needs an exercise policy fitted across paths), variance
-corridors whose bounds are not constants, and fixings before the valuation date; `compile_script` refuses them with
-a `ScriptError`.
+The issuer's call (`call pay`) runs in one of three modes: never called (the script's flows as written, the
+reference's policy NEVER), recording a pilot (each event's flows before and after its call, and at the call its mask,
+the alive mass, the amount and the state: what optlab_b200.exercise fits a Longstaff-Schwartz policy on), or applying
+a fitted policy (the issuer calls where the regression's continuation is above the amount). Not on the device:
+variance corridors whose bounds are not constants, fixings before the valuation date, calls decided on more than
+four state variables; `compile_script` refuses them with a `ScriptError`.
 """
 
 from __future__ import annotations
@@ -26,7 +29,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from ._abi import OB_MODEL_HESTON_QE, ObScriptRequest, ObScriptResult, check, load
+from ._abi import OB_MODEL_HESTON_QE, OB_RULE_STRIDE, ObScriptRequest, ObScriptResult, check, load
 from .engine import precision_code
 
 try:  # the reference's error class, so that callers catching it catch ours
@@ -669,12 +672,13 @@ def build_timeline(p: Program, valuation=None) -> Timeline:
 # Opcodes of the device program (csrc/script.cu). An instruction is four ints: op, d, a, b (registers or indices).
 OP = {name: k for k, name in enumerate((
     "spot", "win", "mov", "add", "sub", "mul", "div", "neg", "min", "max", "abs", "exp", "log", "sqrt",
-    "ge", "gt", "le", "lt", "eq", "and", "or", "not", "assign", "pay", "term", "cond"))}
+    "ge", "gt", "le", "lt", "eq", "and", "or", "not", "assign", "pay", "term", "cond", "call"))}
 _ARITH = {"+": "add", "-": "sub", "*": "mul", "/": "div"}
 _CMP = {">=": "ge", ">": "gt", "<=": "le", "<": "lt", "==": "eq"}
 WIN_FUNC = {"lowest": 0, "highest": 1, "variance": 2}
 MAX_REGS = 128
 MAX_WINDOWS = 8
+MAX_STATE = 4  # variables an issuer's call is decided on (the regression's state)
 
 
 @dataclass
@@ -694,6 +698,7 @@ class Compiled:
     windows: list  # (name index, func, fixing times, lower, upper)
     smoothing: float
     params: dict
+    calls: list = field(default_factory=list)  # per `call pay`: (event index, registers of its state)
 
 
 class _Emitter:
@@ -707,6 +712,8 @@ class _Emitter:
         self.top = 0
         self.max_top = 0
         self.smooth = smoothing
+        self.calls: list = []
+        self.event = 0
 
     def const(self, v: float) -> int:
         v = float(v)
@@ -737,6 +744,10 @@ class _Emitter:
             self.collect(node.expr)
         elif isinstance(node, (Pay, IssuerCall)):
             self.collect(node.expr)
+            if isinstance(node, IssuerCall):
+                for n in self.p.states:
+                    if n in self.params:
+                        self.const(self.params[n])
         elif isinstance(node, If):
             self.collect(node.cond)
             for s in node.body + node.orelse:
@@ -816,8 +827,14 @@ class _Emitter:
             elif isinstance(s, Terminate):
                 self.emit("term", 0, mask)
             elif isinstance(s, IssuerCall):
-                raise ScriptError("the issuer's call ('call pay') needs an exercise policy fitted across paths: "
-                                  "it is not evaluated on the device", s.line, s.col)
+                e = self.expr(s.expr)
+                names = self.p.states or [u[0] for u in self.p.underlyings]
+                if len(names) > MAX_STATE:
+                    raise ScriptError(f"the issuer's call is decided on at most {MAX_STATE} state variables on the "
+                                      f"device, found {len(names)}", s.line, s.col)
+                regs = [self.expr(Name(n, s.line, s.col)) for n in names]
+                self.emit("call", len(self.calls), e, mask)
+                self.calls.append((self.event, regs))
             elif isinstance(s, If):
                 c = self.expr(s.cond)
                 cd = self.temp()
@@ -888,13 +905,14 @@ def compile_script(text: str, params: dict | None = None, smoothing: float = 0.0
             em.collect(s)
     em.layout()
     starts = []
-    for ev in p.events:
+    for k, ev in enumerate(p.events):
         starts.append(len(em.code))
+        em.event = k
         em.block(ev.body, 0, {})
     starts.append(len(em.code))
     code = np.array(em.code, dtype=np.int32).reshape(-1, 4) if em.code else np.zeros((0, 4), np.int32)
     return Compiled(p, tl, names, np.array(em.consts, float), em.max_top, code, np.array(starts, np.int32),
-                    tl.event_times, tl.pay_times, windows, float(smoothing), values)
+                    tl.event_times, tl.pay_times, windows, float(smoothing), values, em.calls)
 
 
 # ----------------------------------------------------------------------------------------------------------- device
@@ -917,10 +935,12 @@ class ScriptHeld:
     compiled: Compiled
 
 
-def script_request(compiled: Compiled, sim, discount) -> ScriptHeld:
+def script_request(compiled: Compiled, sim, discount, call_mode: int = 0, rules=None) -> ScriptHeld:
     """The device request of a compiled script on a simulation: `sim` is an mc_request (Held) whose model part
     (model, names in the script's underlying order, grid, tables, spots, log-forwards) is simulated, its product part
-    ignored; `discount(t)` gives the discount factor of a payment at t. Every observation time must be a step end."""
+    ignored; `discount(t)` gives the discount factor of a payment at t. Every observation time must be a step end.
+    call_mode: 0 the issuer never calls, 1 record a pilot (the held `record` array, filled by `run`), 2 apply
+    `rules` ((n_calls, OB_RULE_STRIDE), optlab_b200.exercise.Policy.pack)."""
     s = sim.struct
     S = s.n_steps
     if s.n_names != len(compiled.names):
@@ -948,6 +968,19 @@ def script_request(compiled: Compiled, sim, discount) -> ScriptHeld:
         win_fix0=np.array(win_fix0, np.int32), fix_step=np.array(fix_step, np.int32),
         win_lower=np.array(lo, np.float64), win_upper=np.array(hi, np.float64),
     )
+    n_calls = len(compiled.calls)
+    n_state = len(compiled.calls[0][1]) if n_calls else 0
+    cs = np.full((max(n_calls, 1), 4), 0, np.int32)
+    for c, (_, regs) in enumerate(compiled.calls):
+        cs[c, : len(regs)] = regs
+    arrays["call_state"] = np.ascontiguousarray(cs.ravel() if n_calls else np.zeros(0, np.int32))
+    if call_mode == 2:
+        rules = np.ascontiguousarray(rules, np.float64)
+        if rules.shape != (n_calls, OB_RULE_STRIDE):
+            raise ValueError(f"rules must be ({n_calls}, {OB_RULE_STRIDE})")
+        arrays["rules"] = rules.ravel()
+    if call_mode == 1:
+        arrays["record"] = np.zeros((2 * s.n_pairs, 2 * len(ev_step) + n_calls * (3 + n_state)))
     r = ObScriptRequest()
     r.model = s
     r.n_code = compiled.code.shape[0]
@@ -956,6 +989,7 @@ def script_request(compiled: Compiled, sim, discount) -> ScriptHeld:
     r.n_events = len(ev_step)
     r.n_windows = len(win_name)
     r.smoothing = compiled.smoothing
+    r.n_calls, r.n_state, r.call_mode = n_calls, n_state, int(call_mode)
     for k, a in arrays.items():
         ctype = C.c_int if a.dtype == np.int32 else C.c_double
         setattr(r, k, a.ctypes.data_as(C.POINTER(ctype)) if a.size else None)

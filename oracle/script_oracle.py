@@ -21,6 +21,7 @@ from optlab_b200.script import (
     Binary,
     Call,
     If,
+    IssuerCall,
     Name,
     Num,
     Pay,
@@ -28,8 +29,8 @@ from optlab_b200.script import (
     Unary,
     Window,
     build_timeline,
-    validate,
     parse,
+    validate,
 )
 
 _FUNCS = {"min": np.minimum, "max": np.maximum, "abs": np.abs, "exp": np.exp, "log": np.log, "sqrt": np.sqrt}
@@ -76,23 +77,36 @@ class ScriptOracle:
         self.eps = float(smoothing)
         self.discount = discount or (lambda t: 1.0)
 
-    def run(self, n_paths, spot, fixings):
+    def run(self, n_paths, spot, fixings, mode="never", rules=None):
+        """mode: "never" (the issuer never calls), "record" (the pilot's record of every call: the result's "pre",
+        "post", "mask", "alive", "amount", "state"), or "apply" (the issuer calls where rules[c] (a Rule, or None:
+        never) continues above the amount, paying the amount as redemption and terminating; exercise.py:71-122)."""
         self.n, self.spot, self.fixings = n_paths, spot, fixings
+        self.mode, self.rules = mode, rules
         self.vars = {}
         self.alive = np.ones(n_paths)
         self.pv = np.zeros(n_paths)
         self.red = np.zeros(n_paths)
         self.bad_pay = np.zeros(n_paths, bool)
         self.bad_cond = np.zeros(n_paths, bool)
+        n_ev = len(self.program.events)
+        self.pre, self.post = np.zeros((n_ev, n_paths)), np.zeros((n_ev, n_paths))
+        self.calls = []  # (mask, alive, amount, state) of each call, in order
         with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
             for k, ev in enumerate(self.program.events):
+                self.k, self.after = k, False
                 self.t_obs = float(self.timeline.event_times[k])
                 t_pay = self.timeline.pay_times[k]
                 self.disc = float(self.discount(t_pay)) if t_pay is not None and t_pay > 0 else 0.0
                 self.block(ev.body, 1.0)
         tol = 1e-12 if self.eps == 0 else 1e-9
         bad_red = ~(np.abs(self.red - 1.0) <= tol)
-        return {"pv": self.pv, "bad_pay": self.bad_pay, "bad_cond": self.bad_cond, "bad_redemption": bad_red}
+        out = {"pv": self.pv, "bad_pay": self.bad_pay, "bad_cond": self.bad_cond, "bad_redemption": bad_red,
+               "pre": self.pre, "post": self.post}
+        if self.calls:
+            out.update(mask=np.array([c[0] for c in self.calls]), alive=np.array([c[1] for c in self.calls]),
+                       amount=np.array([c[2] for c in self.calls]), state=np.array([c[3] for c in self.calls]))
+        return out
 
     def block(self, body, m):
         for s in body:
@@ -110,10 +124,16 @@ class ScriptOracle:
                 self.bad_pay |= live & ~np.isfinite(e)
                 paid = np.where(live & np.isfinite(e), w * e, 0.0)
                 self.pv = self.pv + self.disc * paid
+                if self.after:
+                    self.post[self.k] += self.disc * paid
+                else:
+                    self.pre[self.k] += self.disc * paid
                 if s.tag == "redemption":
                     self.red = self.red + w
             elif isinstance(s, Terminate):
                 self.alive = self.alive * (1.0 - m)
+            elif isinstance(s, IssuerCall):
+                self.issuer_call(s, m)
             elif isinstance(s, If):
                 c = np.broadcast_to(np.asarray(self.expr(s.cond), float), (self.n,))
                 undefined = np.isnan(c)
@@ -124,6 +144,25 @@ class ScriptOracle:
                     self.block(s.orelse, m * (1.0 - c))
             else:
                 raise TypeError(f"not evaluated by the oracle: {s!r}")
+
+    def issuer_call(self, s, m):
+        names = self.program.states or [u[0] for u in self.program.underlyings]
+        amount = np.broadcast_to(np.asarray(self.expr(s.expr), float), (self.n,))
+        state = np.stack([np.broadcast_to(np.asarray(self.expr(Name(x)), float), (self.n,)) for x in names], axis=1)
+        mask = np.broadcast_to(np.asarray(m, float), (self.n,))
+        c = len(self.calls)
+        self.calls.append((mask.copy(), self.alive.copy(), amount.copy(), state.copy()))
+        if self.mode == "record":
+            self.after = True
+        elif self.mode == "apply":
+            rule = self.rules[c]
+            decide = np.zeros(self.n) if rule is None else (rule.continuation(state) > amount).astype(float)
+            md = mask * decide
+            w = md * self.alive
+            self.bad_pay |= (w != 0) & ~np.isfinite(amount)
+            self.pv = self.pv + self.disc * np.where((w != 0) & np.isfinite(amount), w * amount, 0.0)
+            self.red = self.red + w
+            self.alive = self.alive * (1.0 - md)
 
     def expr(self, e):
         if isinstance(e, Num):

@@ -1,6 +1,8 @@
 """Writes tests/golden/script_cases.json: payoff scripts of this repository's tests, evaluated by the reference's own
 script pipeline (optlab.structured.script: parse, validate, build_timeline, Evaluator) on seeded synthetic fixings,
-with each path's present value (cashflows.py:30-41, flat discount exp(-r t)).
+with each path's present value (cashflows.py:30-41, flat discount exp(-r t)); and tests/golden/script_callable.json:
+a callable note's pilot record, the policy the reference fits on it (optlab.structured.exercise.fit) and that policy
+applied to other paths.
 
 The fixings are lognormal paths of every underlying on the script's simulation times (the valuation date is the
 spot); the fake scenario answers `spot(name, t)` and `fixings(name, times)` from them. A case whose evaluation the
@@ -184,6 +186,39 @@ event t=1 pay t=1
 end
 """
 
+CALLABLE = """
+underlying SPX
+param S0 = 100
+param cpn = 0.015
+state perf, low
+event t=0.25 pay t=0.25
+  perf = SPX / S0
+  low = lowest(SPX, t=0, t=0.25, n=12) / S0
+  pay cpn as coupon
+  call pay 1
+end
+event t=0.5 pay t=0.5
+  perf = SPX / S0
+  low = min(low, lowest(SPX, t=0.25, t=0.5, n=12) / S0)
+  pay cpn as coupon
+  call pay 1
+end
+event t=0.75 pay t=0.75
+  perf = SPX / S0
+  pay cpn as coupon
+  call pay 1 + cpn
+end
+event t=1 pay t=1
+  perf = SPX / S0
+  pay cpn as coupon
+  if perf < 0.7 then
+    pay perf as redemption
+  else
+    pay 1 as redemption
+  end
+end
+"""
+
 CASES = [
     ("phoenix", PHOENIX, {}, 0.0, None, {"SPX": 100.0}),
     ("phoenix_smooth", PHOENIX, {"cpn": 0.025}, 0.01, None, {"SPX": 100.0}),
@@ -254,6 +289,60 @@ def main(ref_root: str = "/root/reference") -> None:
         out["cases"].append(case)
     (HERE / "script_cases.json").write_text(json.dumps(out))
     print("wrote", HERE / "script_cases.json", [c["name"] + ("*" if "refused" in c else "") for c in out["cases"]])
+    callable_case(rng)
+
+
+def callable_case(rng) -> None:
+    """tests/golden/script_callable.json: the reference's pilot record and fitted policy (exercise.fit) of a
+    callable note on 600 pilot paths, and its policy applied to 300 other paths (Policy.apply)."""
+    from optlab.structured import exercise
+    from optlab.structured.script.evaluator import Evaluator
+    from optlab.structured.script.parser import parse
+    from optlab.structured.script.timeline import Clock, build_timeline
+    from optlab.structured.script.validate import validate
+
+    program = validate(parse(CALLABLE))
+    tl = build_timeline(program, Clock(None))
+    times = np.asarray(tl.sim_times, float)
+    dts = np.diff(np.concatenate([[0.0], times]))
+
+    def paths(n):
+        z = rng.standard_normal((n, len(times)))
+        return {"SPX": 100.0 * np.exp(np.cumsum(-0.5 * 0.3**2 * dts + 0.3 * np.sqrt(dts) * z, axis=1))}
+
+    pilot, pricing = paths(600), paths(300)
+    disc = lambda t: float(np.exp(-R * t))  # noqa: E731
+    out = Evaluator(program, tl, {}, 0.0).run(Scenario(times, pilot, {"SPX": 100.0}))
+    ex = out.exercise
+    n = 600
+    pre = [disc(ev.t_pay) * sum((np.broadcast_to(f, (n,)) for f in ev.pre.values()), np.zeros(n)) for ev in ex.events]
+    post = [disc(ev.t_pay) * sum((np.broadcast_to(f, (n,)) for f in ev.post.values()), np.zeros(n))
+            for ev in ex.events]
+    calls = [ex.calls[k] for k in sorted(ex.calls)]
+    policy = exercise.fit(out, disc)
+    priced = Evaluator(program, tl, {}, 0.0).run(Scenario(times, pricing, {"SPX": 100.0}))
+    priced = policy.apply(priced)
+    pv = np.zeros(300)
+    for (t, _tag), f in priced.flows.items():
+        if t is not None and t > 0:
+            pv = pv + disc(t) * f
+    rules = []
+    for k in sorted(ex.calls):
+        r = policy.rules[k]
+        rules.append(None if r is None else {"mean": r.mean, "scale": r.scale, "powers": r.powers,
+                                             "knots": r.knots, "coef": r.coef})
+    case = {
+        "script": CALLABLE, "times": times.tolist(), "spot0": {"SPX": 100.0},
+        "pilot": {k: v.tolist() for k, v in pilot.items()}, "pricing": {k: v.tolist() for k, v in pricing.items()},
+        "record": {"pre": np.array(pre).tolist(), "post": np.array(post).tolist(),
+                   "mask": [np.broadcast_to(c.mask, (n,)).tolist() for c in calls],
+                   "alive": [np.broadcast_to(c.alive, (n,)).tolist() for c in calls],
+                   "amount": [np.broadcast_to(c.amount, (n,)).tolist() for c in calls],
+                   "state": [np.asarray(c.state).tolist() for c in calls]},
+        "rules": rules, "in_sample": policy.in_sample, "pv": np.broadcast_to(pv, (300,)).tolist(),
+    }
+    (HERE / "script_callable.json").write_text(json.dumps(case))
+    print("wrote", HERE / "script_callable.json", "in-sample", policy.in_sample, "priced", pv.mean())
 
 
 if __name__ == "__main__":

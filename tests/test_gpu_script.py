@@ -175,3 +175,82 @@ def test_an_undefined_payment_is_reported_as_the_reference_reports_it():
     sim, _ = _simulation(comp, case["spot0"], local_vol=False)
     with pytest.raises(sc.ScriptError, match="not finite"):
         sc.run(sc.script_request(comp, sim, _disc), "fp64")
+
+
+CALLABLE = json.loads((Path(__file__).resolve().parent / "golden" / "script_callable.json").read_text())["script"]
+
+
+def _oracle_run(text, comp, sim, grid, oracle, **kw):
+    """The oracle evaluator on the C oracle's paths of `sim` (as _oracle_price), any mode."""
+    case = {"script": text, "params": {}, "smoothing": 0.0, "valuation": None}
+    _, _, res = _oracle_price_mode(case, comp, sim, grid, oracle, **kw)
+    return res
+
+
+def _oracle_price_mode(case, comp, sim, grid, oracle, **kw):
+    from script_oracle import ScriptOracle
+
+    s = sim.struct
+    arrays = {k: np.ctypeslib.as_array(getattr(s, k), shape=(m,)).copy() for k, m in (
+        ("dt", s.n_steps), ("t0", s.n_steps), ("root", s.n_names**2), ("kind", s.n_names), ("cvar", s.n_names),
+        ("heston", 5 * s.n_names), ("log_fwd", s.n_names * (s.n_steps + 1)), ("spot", s.n_names))}
+    steps = np.searchsorted(grid, comp.timeline.sim_times - 1e-12)
+    fwd = arrays["spot"][:, None] * np.exp(arrays["log_fwd"].reshape(s.n_names, -1)[:, steps])
+    kw_p = dict(dt=arrays["dt"], t0=arrays["t0"], obs_step=steps, root=arrays["root"].reshape(s.n_names, -1),
+                kind=arrays["kind"], cvar=arrays["cvar"], heston=arrays["heston"], same=1, fwd=fwd,
+                n_pairs=s.n_pairs, seed=s.seed)
+    if s.n_rows:
+        kw_p.update(step_row=np.ctypeslib.as_array(s.step_row, shape=(s.n_names * s.n_steps,)).copy(),
+                    lo=np.ctypeslib.as_array(s.row_lo, shape=(s.n_rows,)).copy(),
+                    inv_dx=np.ctypeslib.as_array(s.row_inv_dx, shape=(s.n_rows,)).copy(),
+                    table=np.ctypeslib.as_array(s.table, shape=(s.n_rows * s.n_x,)).copy(), n_x=s.n_x)
+    held = paths_request(**kw_p)
+    oracle.paths(held)
+    out = np.ctypeslib.as_array(held.struct.out, shape=(s.n_names, len(steps), 2 * s.n_pairs))
+    times = comp.timeline.sim_times
+    spot0 = dict(zip(comp.names, arrays["spot"]))
+
+    def col(name, t):
+        if t <= 0:
+            return np.full(2 * s.n_pairs, spot0[name])
+        return out[comp.names.index(name), int(np.argmin(np.abs(times - t)))]
+
+    o = ScriptOracle(case["script"], case["params"], case["smoothing"], case["valuation"], _disc)
+    res = o.run(2 * s.n_pairs, col, lambda name, ts: np.stack([col(name, t) for t in ts], axis=1), **kw)
+    y = 0.5 * (res["pv"][: s.n_pairs] + res["pv"][s.n_pairs:])
+    return y.mean(), y.std(ddof=1) / np.sqrt(len(y)), res
+
+
+def _callable_sim(comp, n_pairs, seed):
+    return _simulation(comp, {"SPX": 100.0}, n_pairs=n_pairs, seed=seed)
+
+
+def test_the_device_pilot_record_is_the_oracles(oracle):
+    from optlab_b200 import exercise
+
+    comp = sc.compile_script(CALLABLE)
+    sim, grid = _callable_sim(comp, 2**11, 29)
+    held = sc.script_request(comp, sim, _disc, call_mode=1)
+    sc.run(held, "fp64")
+    rec = exercise.PilotRecord.from_device(held.keep[1]["record"], len(comp.event_times), len(comp.calls), 2)
+    want = _oracle_run(CALLABLE, comp, sim, grid, oracle, mode="record")
+    for k in ("pre", "post", "mask", "alive", "amount", "state"):
+        assert np.allclose(getattr(rec, k), want[k], rtol=1e-10, atol=1e-13), k
+
+
+def test_an_issuer_call_policy_prices_as_the_oracle_applies_it(oracle):
+    """The policy fitted on the device's pilot, applied by the device on other pairs and by the oracle evaluator on
+    the oracle's paths of those pairs: FP64 prices within 1e-9 (a decision on the boundary may flip in the last
+    bits of the continuation)."""
+    from optlab_b200 import exercise
+
+    comp = sc.compile_script(CALLABLE)
+    sim, grid = _callable_sim(comp, 2**12, 31)
+    result, policy = exercise.price(comp, lambda n, seed: _callable_sim(comp, n, seed)[0], 2**12, 31, _disc, "fp64")
+    assert all(r is not None for r in policy.rules) and policy.pilot_paths == 20000
+    want, se, res = _oracle_price_mode({"script": CALLABLE, "params": {}, "smoothing": 0.0, "valuation": None}, comp,
+                                       sim, grid, oracle, mode="apply", rules=policy.rules)
+    assert abs(result.price - want) <= 1e-9 * abs(want), (result.price, want)
+    never = sc.run(sc.script_request(comp, sim, _disc), "fp64")
+    assert result.price < never.price  # the issuer's option is worth something to the issuer
+    assert result.bad_redemption == 0

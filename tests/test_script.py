@@ -163,8 +163,9 @@ def test_bad_scripts_are_refused_with_the_references_messages(text, message):
 
 
 def test_what_the_device_does_not_evaluate_is_refused():
-    call = "underlying A\nevent t=1 pay t=1\n  call pay 1\n  pay 1 as redemption\nend\n"
-    with pytest.raises(sc.ScriptError, match="issuer's call"):
+    call = ("underlying A\nstate a, b, c, d, e\nevent t=1 pay t=1\n  a = 1\n  b = 1\n  c = 1\n  d = 1\n  e = 1\n"
+            "  call pay 1\n  pay 1 as redemption\nend\n")
+    with pytest.raises(sc.ScriptError, match="at most 4 state variables"):
         sc.compile_script(call)
     corridor = ("underlying A\nevent t=1 pay t=1\n  x = A\n  v = variance(A, t=0, t=1, n=4, x, 200)\n"
                 "  pay v as upside\n  pay 1 as redemption\nend\n")
