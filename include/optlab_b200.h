@@ -231,6 +231,7 @@ typedef struct {
     double coupon_barrier, coupon, ki_barrier, put_strike;
     int memory, ki_daily;
     double discount;
+    int corr_root0; /* local vol, 2 to 5 names: the first of its n_corr moved roots in the root pool, n_names^2 each */
 } ob_batch_trade;
 
 /* The batch: trades, pools and scenarios. Every trade steps by dt; a local-vol table row j of a trade is the
@@ -238,7 +239,14 @@ typedef struct {
    scenarios of each trade: the base, then n_spot relative spot moves (evaluated on the base simulation: the local vol
    is in log-moneyness, so a spot move scales the paths), then n_vol moves of local volatility sigma(k) + shift +
    tilt k (floored at 1 %), each a simulation on the same random numbers (Heston trades do not move under them, as
-   the reference's Heston model ignores the surface). */
+   the reference's Heston model ignores the surface). After those, n_carry (at most 4) moves of the carry on the base
+   simulation: carry_rate moves the rate in the forward and the discounting, carry_div the dividend yield (with repo)
+   in the forward only, so that a path moves by exp((carry_rate - carry_div) t) at time t and a payment at t
+   (the ladder's last step, an autocall's observation step) is discounted by exp(-carry_rate t) more
+   (packages/risk/src/optlab/risk/engine.py:8-11). Last, n_corr moves of the correlation, each a simulation of the
+   multi-name local-vol trades on the moved root at corr_root0 (single-name and Heston trades do not move). The
+   outputs of a trade: base, spot moves, carry moves, vol moves, correlation moves; the base simulation holds at most
+   32 of them (1 + n_spot + n_carry). */
 typedef struct {
     int n_trades;
     const ob_batch_trade* trades;
@@ -260,7 +268,13 @@ typedef struct {
     int n_vol;
     const double* vol_shift;
     const double* vol_tilt;
+    int n_carry;
+    const double* carry_rate;
+    const double* carry_div;
+    int n_corr;
 } ob_batch_request;
+
+#define OB_BATCH_MAX_CARRY 4 /* carry moves of a batch */
 
 typedef struct ob_batch ob_batch;
 
@@ -389,7 +403,8 @@ int ob_adjoint_plan_destroy(ob_adjoint_plan* plan);
    the fastest (budget_ms bounds its time; 0: the defaults); capture records one run (every class's persistent kernel
    on its own stream, then the reduction) as a CUDA graph; launch replays it on `stream` (or runs the kernels directly
    without a capture); run_per_trade runs the same work as one launch per trade simulation, the comparison; result
-   waits and writes price and se (n_trades x (1 + n_spot + n_vol), row-major) and the last run's device time. */
+   waits and writes price and se (n_trades x (1 + n_spot + n_carry + n_vol + n_corr), row-major) and the last run's
+   device time. */
 int ob_batch_create(const ob_batch_request* rq, int precision, ob_batch** batch);
 int ob_batch_tune(ob_batch* batch, int budget_ms);
 int ob_batch_capture(ob_batch* batch, void* stream);

@@ -1,5 +1,5 @@
-// Batched risk revaluation: a book of trades of uneven sizes, each revalued under spot and volatility scenarios, in
-// one replay of a CUDA graph of persistent kernels.
+// Batched risk revaluation: a book of trades of uneven sizes, each revalued under spot, carry, volatility and
+// correlation scenarios, in one replay of a CUDA graph of persistent kernels.
 //
 // What the reference does one simulation at a time (packages/risk/src/optlab/risk/engine.py:382-425,563-644: spot
 // shocks share the base simulation as path factors, every vol or skew shock re-simulates on the group's seed) runs
@@ -8,7 +8,11 @@
 // streams inside one graph, so that large and small trades fill the GPU together. A base simulation evaluates the base
 // and every spot scenario at once: the path keeps its observation log-performances and extremes, and a spot move is
 // a shift of them (the local vol is in log-moneyness). A vol scenario reads the table as (sigma + shift + tilt k)^2,
-// floored at 1 % vol, on the same random numbers. Each tile writes its own partial sums, and a last kernel adds the
+// floored at 1 % vol, on the same random numbers. A carry scenario (a move of the rate, discounting included, or of
+// the dividend yield) also rides on the base simulation, as the reference's forward ratio F'(t) / F(t) (:8-11): the
+// path keeps its extremes and daily low again under each carry's drift (Delta t per step), and the payments take
+// the moved discount. A correlation scenario re-simulates the multi-name local-vol trades on a moved root, on the
+// same random numbers. Each tile writes its own partial sums, and a last kernel adds the
 // tiles of each (trade, scenario) in order, so the results do not depend on the schedule. Tiles and block sizes
 // are chosen per class by ob_batch_tune, which times candidates on the class's own work.
 #include <algorithm>
@@ -25,7 +29,8 @@ namespace ob {
 namespace {
 
 constexpr int kBatchMaxObs = 64;
-constexpr int kBatchMaxOut = 32;  // 1 + spot scenarios per base simulation
+constexpr int kBatchMaxOut = 32;  // 1 + spot + carry scenarios per base simulation
+constexpr int kBatchMaxCarry = OB_BATCH_MAX_CARRY;
 
 template <typename R>
 struct BTrade {
@@ -38,7 +43,9 @@ struct BTrade {
     int has_coupon, memory, ki_daily;
     R ln_cb, ln_ki;
     double coupon, put_strike, discount;
-    int slot0;  // first partial slot of its base simulation
+    int slot0;       // first partial slot of its base simulation
+    int corr_root0;  // its moved roots, one per correlation scenario
+    double carry_df[kBatchMaxCarry];  // the ladder's payment under each carry: exp(-rate move T)
 };
 
 template <typename R>
@@ -60,7 +67,9 @@ struct BDev {
     const R* ln_spot;     // n_spot: ln(1 + spot move)
     const R* vol_shift;
     const R* vol_tilt;
-    int n_spot, n_exp, n_x;
+    const double* obs_carry_df;  // n_carry x observation pool: exp(-rate move t_obs)
+    R carry_dt[kBatchMaxCarry];  // per carry: the drift move (rate - dividend) times dt
+    int n_spot, n_carry, n_vol, n_obs_pool, n_exp, n_x;
     R hdt, sdt, dt, top;
     double* slots;        // partial sums: per tile, 2 x outputs
     const int* sim_slot;  // per (trade, simulation): first slot
@@ -74,17 +83,18 @@ struct Rec;
 template <typename R>
 struct Rec<R, OB_PRODUCT_LADDER> {
     R last, hi, lo;
+    R hc[kBatchMaxCarry], lc[kBatchMaxCarry];  // extremes under each carry's drift
 };
 template <typename R>
 struct Rec<R, OB_PRODUCT_AUTOCALL> {
     R low;
+    R lowc[kBatchMaxCarry];  // daily low under each carry's drift
     R obs[kBatchMaxObs];
 };
 
+// The legs' undiscounted sum at a terminal log performance and extremes.
 template <typename R>
-__device__ __forceinline__ double ladder_value(const BDev<R>& d, const BTrade<R>& t, const Rec<R, OB_PRODUCT_LADDER>& r,
-                                               R shift) {
-    const R lpT = r.last + shift, hi = r.hi + shift, lo = r.lo + shift;
+__device__ __forceinline__ double ladder_legs(const BDev<R>& d, const BTrade<R>& t, R lpT, R hi, R lo) {
     const R U = m_exp(lpT);
     double v = 0.0;
     for (int k = 0; k < t.n_legs; ++k) {
@@ -99,19 +109,32 @@ __device__ __forceinline__ double ladder_value(const BDev<R>& d, const BTrade<R>
             pay = R(0);
         v += static_cast<double>(pay);
     }
-    return t.discount * v;
+    return v;
+}
+
+// c < 0: the recorded path shifted by a spot move; c >= 0: under carry c (no spot move).
+template <typename R>
+__device__ __forceinline__ double ladder_value(const BDev<R>& d, const BTrade<R>& t, const Rec<R, OB_PRODUCT_LADDER>& r,
+                                               R shift, int c) {
+    if (c < 0) return t.discount * ladder_legs(d, t, r.last + shift, r.hi + shift, r.lo + shift);
+    const R lpT = r.last + d.carry_dt[c] * static_cast<R>(t.n_steps);
+    return t.discount * t.carry_df[c] * ladder_legs(d, t, lpT, r.hc[c], r.lc[c]);
 }
 
 // The Phoenix of the fused kernel (coupon with memory, call before the last date, knock-in put at the last), on the
-// recorded observations shifted by a spot move.
+// recorded observations shifted by a spot move (c < 0) or moved by carry c.
 template <typename R>
 __device__ __forceinline__ double autocall_value(const BDev<R>& d, const BTrade<R>& t,
-                                                 const Rec<R, OB_PRODUCT_AUTOCALL>& r, R shift) {
+                                                 const Rec<R, OB_PRODUCT_AUTOCALL>& r, R shift, int c) {
     double pv = 0.0;
     int missed = 0;
     for (int j = 0; j < t.n_obs; ++j) {
-        const R lp = r.obs[j] + shift;
-        const double D = d.obs_disc[t.obs0 + j];
+        R lp = r.obs[j] + shift;
+        double D = d.obs_disc[t.obs0 + j];
+        if (c >= 0) {
+            lp += d.carry_dt[c] * static_cast<R>(d.obs_step[t.obs0 + j]);
+            D *= d.obs_carry_df[c * d.n_obs_pool + t.obs0 + j];
+        }
         if (t.has_coupon) {
             if (lp >= t.ln_cb) {
                 pv += D * t.coupon * (t.memory ? 1 + missed : 1);
@@ -123,7 +146,7 @@ __device__ __forceinline__ double autocall_value(const BDev<R>& d, const BTrade<
         if (j < t.n_obs - 1) {
             if (lp >= d.ln_trig[t.obs0 + j]) return pv + D;
         } else {
-            const R low = m_min(r.low + shift, shift);  // the start (perf 1 + move) is part of the window
+            const R low = m_min((c < 0 ? r.low : r.lowc[c]) + shift, shift);  // the start is part of the window
             const bool ki = t.ki_daily ? low < t.ln_ki : lp < t.ln_ki;
             const double perf = static_cast<double>(m_exp(lp));
             const double put = t.put_strike - perf > 0.0 ? t.put_strike - perf : 0.0;
@@ -134,32 +157,28 @@ __device__ __forceinline__ double autocall_value(const BDev<R>& d, const BTrade<
 }
 
 template <typename R>
-__device__ __forceinline__ double value(const BDev<R>& d, const BTrade<R>& t, const Rec<R, OB_PRODUCT_LADDER>& r, R s) {
-    return ladder_value(d, t, r, s);
+__device__ __forceinline__ double value(const BDev<R>& d, const BTrade<R>& t, const Rec<R, OB_PRODUCT_LADDER>& r, R s,
+                                        int c) {
+    return ladder_value(d, t, r, s, c);
 }
 template <typename R>
 __device__ __forceinline__ double value(const BDev<R>& d, const BTrade<R>& t, const Rec<R, OB_PRODUCT_AUTOCALL>& r,
-                                        R s) {
-    return autocall_value(d, t, r, s);
+                                        R s, int c) {
+    return autocall_value(d, t, r, s, c);
 }
 
-template <typename R, int PRODUCT>
-__device__ __forceinline__ void rec_init(Rec<R, PRODUCT>& r);
-template <>
-__device__ __forceinline__ void rec_init<float, OB_PRODUCT_LADDER>(Rec<float, OB_PRODUCT_LADDER>& r) {
-    r.last = 0.f, r.hi = -1e30f, r.lo = 1e30f;
+template <typename R>
+__device__ __forceinline__ void rec_init(Rec<R, OB_PRODUCT_LADDER>& r) {
+    const R big = static_cast<R>(sizeof(R) == 4 ? 1e30 : 1e300);
+    r.last = R(0), r.hi = -big, r.lo = big;
+#pragma unroll
+    for (int c = 0; c < kBatchMaxCarry; ++c) r.hc[c] = -big, r.lc[c] = big;
 }
-template <>
-__device__ __forceinline__ void rec_init<double, OB_PRODUCT_LADDER>(Rec<double, OB_PRODUCT_LADDER>& r) {
-    r.last = 0.0, r.hi = -1e300, r.lo = 1e300;
-}
-template <>
-__device__ __forceinline__ void rec_init<float, OB_PRODUCT_AUTOCALL>(Rec<float, OB_PRODUCT_AUTOCALL>& r) {
-    r.low = 0.f;
-}
-template <>
-__device__ __forceinline__ void rec_init<double, OB_PRODUCT_AUTOCALL>(Rec<double, OB_PRODUCT_AUTOCALL>& r) {
-    r.low = 0.0;
+template <typename R>
+__device__ __forceinline__ void rec_init(Rec<R, OB_PRODUCT_AUTOCALL>& r) {
+    r.low = R(0);
+#pragma unroll
+    for (int c = 0; c < kBatchMaxCarry; ++c) r.lowc[c] = R(0);
 }
 
 // Step end i of one leg, with lp the worst log performance and j the observation ending there (-1: none).
@@ -171,6 +190,23 @@ template <typename R>
 __device__ __forceinline__ void rec_step(Rec<R, OB_PRODUCT_AUTOCALL>& r, R lp, int j) {
     r.low = m_min(r.low, lp);
     if (j >= 0) r.obs[j] = lp;
+}
+
+// The first nc carry moves at step end i: the log performance lp + Delta_c i dt.
+template <typename R>
+__device__ __forceinline__ void rec_carry(Rec<R, OB_PRODUCT_LADDER>& r, R lp, R fi, const BDev<R>& d, int nc) {
+#pragma unroll
+    for (int c = 0; c < kBatchMaxCarry; ++c)
+        if (c < nc) {
+            const R l = lp + d.carry_dt[c] * fi;
+            r.hc[c] = m_max(r.hc[c], l), r.lc[c] = m_min(r.lc[c], l);
+        }
+}
+template <typename R>
+__device__ __forceinline__ void rec_carry(Rec<R, OB_PRODUCT_AUTOCALL>& r, R lp, R fi, const BDev<R>& d, int nc) {
+#pragma unroll
+    for (int c = 0; c < kBatchMaxCarry; ++c)
+        if (c < nc) r.lowc[c] = m_min(r.lowc[c], lp + d.carry_dt[c] * fi);
 }
 
 template <typename R, int N, bool QE, int PRODUCT>
@@ -190,14 +226,18 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
         if (it >= n_items) break;
         const int4 item = items[it];
         const BTrade<R>& t = d.trades[item.x];
+        // sim 0: the base (with spot and carry moves); 1..n_vol: vol moves; after those: correlation moves
         const int sim = item.y, tile = item.z;
-        const int n_out = sim == 0 ? 1 + d.n_spot : 1;
+        const int nc = sim == 0 ? d.n_carry : 0;
+        const int n_out = sim == 0 ? 1 + d.n_spot + nc : 1;
+        const bool shocked = sim > 0 && sim <= d.n_vol;
         for (int k = threadIdx.x; k < 8 * 2 * kBatchMaxOut; k += blockDim.x) (&wacc[0][0])[k] = 0.0;
-        if (!QE)
-            for (int k = threadIdx.x; k < N * N; k += blockDim.x) s_root[k] = d.root[t.root0 + k];
+        if (!QE) {
+            const int root = sim > d.n_vol ? t.corr_root0 + (sim - 1 - d.n_vol) * N * N : t.root0;
+            for (int k = threadIdx.x; k < N * N; k += blockDim.x) s_root[k] = d.root[root + k];
+        }
         __syncthreads();
-        const R vs = sim > 0 ? d.vol_shift[sim - 1] : R(0), vt = sim > 0 ? d.vol_tilt[sim - 1] : R(0);
-        const bool shocked = sim > 0;
+        const R vs = shocked ? d.vol_shift[sim - 1] : R(0), vt = shocked ? d.vol_tilt[sim - 1] : R(0);
         const long long p0 = static_cast<long long>(tile) * d.tile;
         const long long p1 = min(p0 + d.tile, t.n_pairs);
         const int S = t.n_steps;
@@ -208,7 +248,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
 #pragma unroll
             for (int n = 0; n < N; ++n) x0[n] = x1[n] = R(0);
             Rec<R, PRODUCT> r0, r1;
-            rec_init<R, PRODUCT>(r0), rec_init<R, PRODUCT>(r1);
+            rec_init(r0), rec_init(r1);
             int next_obs = 0;
             for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) {
                 R z[C * G];
@@ -262,14 +302,23 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
                         j = next_obs++;
                     rec_step(r0, lp0, j);
                     rec_step(r1, lp1, j);
+                    if (nc) rec_carry(r0, lp0, static_cast<R>(i), d, nc), rec_carry(r1, lp1, static_cast<R>(i), d, nc);
                 }
             }
-            for (int o = 0; o < n_out; ++o) {
+            for (int o = 0; o < 1 + (sim == 0 ? d.n_spot : 0); ++o) {
                 const R sh = o == 0 ? R(0) : d.ln_spot[o - 1];
-                const double y = active ? 0.5 * (value(d, t, r0, sh) + value(d, t, r1, sh)) : 0.0;
+                const double y = active ? 0.5 * (value(d, t, r0, sh, -1) + value(d, t, r1, sh, -1)) : 0.0;
                 const double s1 = warp_sum(y), s2 = warp_sum(y * y);
                 if (lane == 0) wacc[warp][o] += s1, wacc[warp][kBatchMaxOut + o] += s2;
             }
+#pragma unroll
+            for (int c = 0; c < kBatchMaxCarry; ++c)
+                if (c < nc) {
+                    const int o = 1 + d.n_spot + c;
+                    const double y = active ? 0.5 * (value(d, t, r0, R(0), c) + value(d, t, r1, R(0), c)) : 0.0;
+                    const double s1 = warp_sum(y), s2 = warp_sum(y * y);
+                    if (lane == 0) wacc[warp][o] += s1, wacc[warp][kBatchMaxOut + o] += s2;
+                }
         }
         __syncthreads();
         double* out = d.slots + (static_cast<long long>(d.sim_slot[item.w]) + tile) * 2 * kBatchMaxOut;
@@ -353,7 +402,7 @@ struct BLayout {
 struct Batch {
     DeviceArena arena;
     int precision = OB_FP32, sms = 0;
-    int n_trades = 0, n_spot = 0, n_vol = 0;
+    int n_trades = 0, n_spot = 0, n_vol = 0, n_carry = 0, n_corr = 0;
     std::vector<ob_batch_trade> trades;
     std::vector<BClass> classes;
     std::vector<int> class_of_trade;
@@ -374,6 +423,11 @@ struct Batch {
     template <typename R>
     void build(const ob_batch_request& rq);
     void simulations();
+    // per trade: its base, then under local vol one per vol move, then (2 names or more) one per correlation move
+    int sims_of(int i) const {
+        const ob_batch_trade& t = trades[i];
+        return t.model == OB_MODEL_PATHS ? 1 + n_vol + (t.n_names > 1 ? n_corr : 0) : 1;
+    }
     void layout(BLayout& L, const std::vector<int>& tiles, int only_class = -1, int max_sims = 0);
     template <typename R>
     void launch_class(const BLayout& L, int ci, cudaStream_t st, const int4* items, int n_items, int* counter,
@@ -417,6 +471,12 @@ void check_batch(const ob_batch_request& rq) {
     if (!(rq.dt > 0) || rq.n_exp < 1 || rq.n_x < 2 || !(rq.horizon > 0)) invalid("bad step or table grid");
     if (rq.n_spot < 0 || rq.n_spot + 1 > kBatchMaxOut || (rq.n_spot && !rq.spot_shift)) invalid("n_spot must be 0 to 31");
     if (rq.n_vol < 0 || (rq.n_vol && (!rq.vol_shift || !rq.vol_tilt))) invalid("bad vol scenarios");
+    if (rq.n_carry < 0 || rq.n_carry > kBatchMaxCarry || (rq.n_carry && (!rq.carry_rate || !rq.carry_div)))
+        invalid("n_carry must be 0 to 4, with its moves");
+    if (1 + rq.n_spot + rq.n_carry > kBatchMaxOut) invalid("1 + n_spot + n_carry must be at most 32");
+    for (int k = 0; k < rq.n_carry; ++k)
+        if (!std::isfinite(rq.carry_rate[k]) || !std::isfinite(rq.carry_div[k])) invalid("carry moves must be finite");
+    if (rq.n_corr < 0) invalid("n_corr must be 0 or more");
     for (int k = 0; k < rq.n_spot; ++k)
         if (!(rq.spot_shift[k] > -1.0)) invalid("a spot move must be above -100 %");
     for (int i = 0; i < rq.n_trades; ++i) {
@@ -428,6 +488,7 @@ void check_batch(const ob_batch_request& rq) {
         if (t.model == OB_MODEL_PATHS) {
             if (!rq.table || !rq.row_lo || !rq.row_inv_dx || !rq.root) invalid("local-vol trades need the pools");
             if (t.table_row0 < 0 || t.root0 < 0) invalid("bad pool offsets");
+            if (rq.n_corr && t.n_names > 1 && t.corr_root0 < 0) invalid("bad moved-root offset");
         } else {
             const double* h = t.heston;
             if (!(h[0] >= 0 && h[1] > 0 && h[2] > 0 && h[3] > 0 && std::fabs(h[4]) <= 1))
@@ -455,11 +516,12 @@ void check_batch(const ob_batch_request& rq) {
 
 template <typename R>
 void Batch::build(const ob_batch_request& rq) {
-    n_trades = rq.n_trades, n_spot = rq.n_spot, n_vol = rq.n_vol;
+    n_trades = rq.n_trades, n_spot = rq.n_spot, n_vol = rq.n_vol, n_carry = rq.n_carry, n_corr = rq.n_corr;
     trades.assign(rq.trades, rq.trades + rq.n_trades);
     BDev<R>& d = dev<R>();
     d = BDev<R>{};
-    d.n_spot = n_spot, d.n_exp = rq.n_exp, d.n_x = rq.n_x;
+    d.n_spot = n_spot, d.n_carry = n_carry, d.n_vol = n_vol, d.n_exp = rq.n_exp, d.n_x = rq.n_x;
+    for (int c = 0; c < n_carry; ++c) d.carry_dt[c] = static_cast<R>((rq.carry_rate[c] - rq.carry_div[c]) * rq.dt);
     d.hdt = static_cast<R>(-0.5 * rq.dt), d.sdt = static_cast<R>(std::sqrt(rq.dt)), d.dt = static_cast<R>(rq.dt);
     d.top = static_cast<R>(rq.n_x - 1) - static_cast<R>(1e-4);
     int max_steps = 1, max_row = 0, max_root = 0, max_leg = 0, max_obs = 0;
@@ -468,6 +530,8 @@ void Batch::build(const ob_batch_request& rq) {
         if (t.model == OB_MODEL_PATHS) {
             max_row = std::max(max_row, t.table_row0 + t.n_names * rq.n_exp);
             max_root = std::max(max_root, t.root0 + t.n_names * t.n_names);
+            if (n_corr && t.n_names > 1)
+                max_root = std::max(max_root, t.corr_root0 + n_corr * t.n_names * t.n_names);
         }
         if (t.product == OB_PRODUCT_LADDER) max_leg = std::max(max_leg, t.leg0 + t.n_legs);
         else max_obs = std::max(max_obs, t.obs0 + t.n_obs);
@@ -513,6 +577,14 @@ void Batch::build(const ob_batch_request& rq) {
         d.obs_step = arena.put<int>(rq.obs_step, max_obs);
         d.ln_trig = arena.put<R>(trig.data(), trig.size());
         d.obs_disc = arena.put<double>(rq.obs_discount, max_obs);
+        d.n_obs_pool = max_obs;
+        if (n_carry) {
+            std::vector<double> df(static_cast<size_t>(n_carry) * max_obs);
+            for (int c = 0; c < n_carry; ++c)
+                for (int k = 0; k < max_obs; ++k)
+                    df[static_cast<size_t>(c) * max_obs + k] = std::exp(-rq.carry_rate[c] * rq.obs_step[k] * rq.dt);
+            d.obs_carry_df = arena.put<double>(df.data(), df.size());
+        }
     }
     if (n_spot) {
         std::vector<R> ls(n_spot);
@@ -540,6 +612,8 @@ void Batch::build(const ob_batch_request& rq) {
         b.ln_cb = t.coupon_barrier > 0 ? static_cast<R>(std::log(t.coupon_barrier)) : R(-1e30);
         b.ln_ki = t.ki_barrier > 0 ? static_cast<R>(std::log(t.ki_barrier)) : R(-1e30);
         b.coupon = t.coupon, b.put_strike = t.put_strike, b.discount = t.discount;
+        b.corr_root0 = t.corr_root0;
+        for (int c = 0; c < n_carry; ++c) b.carry_df[c] = std::exp(-rq.carry_rate[c] * t.n_steps * rq.dt);
         const auto key = std::make_tuple(t.model == OB_MODEL_HESTON_QE, t.n_names, t.product);
         auto f = cls.find(key);
         if (f == cls.end()) {
@@ -565,14 +639,13 @@ void Batch::build(const ob_batch_request& rq) {
 template void Batch::build<float>(const ob_batch_request&);
 template void Batch::build<double>(const ob_batch_request&);
 
-// The simulations: per trade its base, then (local vol) one per vol scenario.
+// The simulations of each trade (sims_of) and their outputs: the base carries the base, spot and carry moves.
 void Batch::simulations() {
     sim_of_trade.assign(n_trades, 0);
     sim_outs.clear();
     for (int i = 0; i < n_trades; ++i) {
         sim_of_trade[i] = static_cast<int>(sim_outs.size());
-        const int n_sim = trades[i].model == OB_MODEL_PATHS ? 1 + n_vol : 1;
-        for (int s = 0; s < n_sim; ++s) sim_outs.push_back(s == 0 ? 1 + n_spot : 1);
+        for (int s = 0; s < sims_of(i); ++s) sim_outs.push_back(s == 0 ? 1 + n_spot + n_carry : 1);
     }
     n_sims = static_cast<int>(sim_outs.size());
     d_sim_outs = arena.put<int>(sim_outs.data(), sim_outs.size());
@@ -596,8 +669,7 @@ void Batch::layout(BLayout& L, const std::vector<int>& tiles, int only_class, in
                    static_cast<double>(trades[b].n_steps) * trades[b].n_pairs;
         });
         for (int t : order)
-            for (int s = 0; s < (trades[t].model == OB_MODEL_PATHS ? 1 + n_vol : 1); ++s)
-                sims.push_back(sim_of_trade[t] + s);
+            for (int s = 0; s < sims_of(t); ++s) sims.push_back(sim_of_trade[t] + s);
         if (static_cast<int>(sims.size()) > max_sims) {
             std::fill(keep.begin(), keep.end(), 0);
             for (int k = 0; k < max_sims; ++k)
@@ -607,8 +679,7 @@ void Batch::layout(BLayout& L, const std::vector<int>& tiles, int only_class, in
     for (int i = 0; i < n_trades; ++i) {
         const int tile = tiles[class_of_trade[i]];
         const int tl = static_cast<int>((trades[i].n_pairs + tile - 1) / tile);
-        const int n_sim = trades[i].model == OB_MODEL_PATHS ? 1 + n_vol : 1;
-        for (int s = 0; s < n_sim; ++s) {
+        for (int s = 0; s < sims_of(i); ++s) {
             const int sim = sim_of_trade[i] + s;
             L.sim_slot[sim] = L.n_slots, L.sim_tiles[sim] = keep[sim] ? tl : 0;
             if (only_class < 0 || class_of_trade[i] == only_class) L.n_slots += L.sim_tiles[sim];
@@ -630,8 +701,7 @@ void Batch::layout(BLayout& L, const std::vector<int>& tiles, int only_class, in
         });
         std::vector<int4> items;
         for (int t : order) {
-            const int n_sim = trades[t].model == OB_MODEL_PATHS ? 1 + n_vol : 1;
-            for (int s = 0; s < n_sim; ++s)
+            for (int s = 0; s < sims_of(t); ++s)
                 for (int k = 0; k < L.sim_tiles[sim_of_trade[t] + s]; ++k)
                     items.push_back(make_int4(t, s, k, sim_of_trade[t] + s));
         }
@@ -827,8 +897,7 @@ int ob_batch_run_per_trade(ob_batch* batch, void* stream) {
         if (L.pt_items.empty()) {
             std::vector<int4> items;
             for (int t = 0; t < b.n_trades; ++t) {
-                const int n_sim = b.trades[t].model == OB_MODEL_PATHS ? 1 + b.n_vol : 1;
-                for (int s = 0; s < n_sim; ++s) {
+                for (int s = 0; s < b.sims_of(t); ++s) {
                     const int sim = b.sim_of_trade[t] + s;
                     L.pt_first.push_back(static_cast<int>(items.size()));
                     L.pt_count.push_back(L.sim_tiles[sim]);
@@ -867,7 +936,7 @@ int ob_batch_result(ob_batch* batch, double* price, double* se, double* device_m
         ob::check_cuda(cudaMemcpy(sums.data(), b.last_layout->d_sums, sums.size() * sizeof(double),
                                   cudaMemcpyDeviceToHost),
                        "copy");
-        const int per = 1 + b.n_spot + b.n_vol;
+        const int per = 1 + b.n_spot + b.n_carry + b.n_vol + b.n_corr;
         for (int t = 0; t < b.n_trades; ++t) {
             const double n = static_cast<double>(b.trades[t].n_pairs);
             auto est = [&](int sim, int o, double& m, double& s) {
@@ -876,13 +945,15 @@ int ob_batch_result(ob_batch* batch, double* price, double* se, double* device_m
                 m = s1 / n;
                 s = n > 1 ? std::sqrt(std::fmax(s2 / n - m * m, 0.0) / (n - 1.0)) : 0.0;
             };
-            const int s0 = b.sim_of_trade[t];
-            for (int o = 0; o < 1 + b.n_spot; ++o) est(s0, o, price[t * per + o], se[t * per + o]);
-            for (int v = 0; v < b.n_vol; ++v) {
-                double& p = price[t * per + 1 + b.n_spot + v];
-                double& e = se[t * per + 1 + b.n_spot + v];
-                if (b.trades[t].model == OB_MODEL_PATHS) est(s0 + 1 + v, 0, p, e);
-                else p = price[t * per], e = se[t * per];  // the Heston model ignores the surface
+            const int s0 = b.sim_of_trade[t], n_sim = b.sims_of(t);
+            const int on_base = 1 + b.n_spot + b.n_carry;
+            for (int o = 0; o < on_base; ++o) est(s0, o, price[t * per + o], se[t * per + o]);
+            // vol then correlation moves: their own simulations, or the base where the trade does not move
+            for (int v = 0; v < b.n_vol + b.n_corr; ++v) {
+                double& p = price[t * per + on_base + v];
+                double& e = se[t * per + on_base + v];
+                if (1 + v < n_sim) est(s0 + 1 + v, 0, p, e);
+                else p = price[t * per], e = se[t * per];
             }
         }
         if (device_ms) {

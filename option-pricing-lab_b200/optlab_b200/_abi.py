@@ -14,6 +14,7 @@ from pathlib import Path
 OB_OK, OB_EINVAL, OB_ENODEV, OB_ECUDA, OB_ETIMEOUT, OB_ENOMEM = 0, 1, 2, 3, 4, 5
 OB_FP32, OB_FP64 = 0, 1
 OB_MAX_NAMES, OB_MAX_WINDOWS, OB_MAX_OUT = 8, 2, 32
+OB_BATCH_MAX_CARRY = 4
 OB_MODEL_PATHS, OB_MODEL_HESTON_QE = 0, 1
 OB_PRODUCT_LADDER, OB_PRODUCT_AUTOCALL = 0, 1
 BARRIER = {"none": 0, "up-out": 1, "down-out": 2, "up-in": 3, "down-in": 4}
@@ -254,6 +255,7 @@ class ObBatchTrade(C.Structure):
         ("memory", C.c_int),
         ("ki_daily", C.c_int),
         ("discount", C.c_double),
+        ("corr_root0", C.c_int),
     ]
 
 
@@ -281,6 +283,10 @@ class ObBatchRequest(C.Structure):
         ("n_vol", C.c_int),
         ("vol_shift", _dp),
         ("vol_tilt", _dp),
+        ("n_carry", C.c_int),
+        ("carry_rate", _dp),
+        ("carry_div", _dp),
+        ("n_corr", C.c_int),
     ]
 
 

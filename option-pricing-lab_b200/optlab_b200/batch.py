@@ -1,16 +1,18 @@
-"""Batched risk revaluation: a seeded book of uneven trades, each revalued under spot, parallel-vol and skew scenarios,
-in one replay of a CUDA graph of persistent kernels (csrc/batch.cu through ob_batch_*).
+"""Batched risk revaluation: a seeded book of uneven trades, each revalued under spot, carry, parallel-vol, skew and
+correlation scenarios, in one replay of a CUDA graph of persistent kernels (csrc/batch.cu through ob_batch_*).
 
 The reference revalues a book group by group and scenario by scenario (packages/risk/src/optlab/risk/engine.py:382-425:
-every shock that moves the model is its own simulation on the group's seed; :563-644: shocks that move only the spot
-share the base simulation as factors on its paths). `Batch` keeps that split: per trade one base simulation carries
-the base and every spot move, and each vol or skew move is one more simulation on the same random numbers; all of
-them are work items of the same launch.
+every shock that moves the model is its own simulation on the group's seed; :563-644: shocks that move only the spot,
+the forwards or the discounting share the base simulation as factors on its paths, :8-11). `Batch` keeps that split:
+per trade one base simulation carries the base, every spot move and every carry move (rates or dividends), and each
+vol, skew or correlation move is one more simulation on the same random numbers; all of them are work items of the
+same launch.
 
 `sample_book` draws the benchmark's book: 512 trades of 1 to 5 names, 1 to 5 years of daily steps, 2^14 to 2^18 paths,
 European, barrier or autocall payoffs (worst-of with several names), under Heston QE or local vol of per-name SSVI
-surfaces, with 60 scenarios: 20 spot moves of +-1..20 %, 20 parallel moves of local vol of +-1..10 points, 20 skew
-tilts of +-1..10 points per unit of log-moneyness.
+surfaces, with 66 scenarios: 20 spot moves of +-1..20 %, 4 carry moves (rates +-1 %, dividend yield +-1 %), 20
+parallel moves of local vol of +-1..10 points, 20 skew tilts of +-1..10 points per unit of log-moneyness, and 2
+moves of every pairwise correlation by +-0.10.
 """
 
 from __future__ import annotations
@@ -33,13 +35,15 @@ from ._abi import (
     load,
 )
 from .engine import precision_code
-from .models import correlation_root
+from .models import correlation_root, nearest_correlation
 from .surfaces import SSVI, LocalVarGrid
 
 _STEPS = np.array([0.01, 0.02, 0.03, 0.04, 0.05, 0.075, 0.10, 0.125, 0.15, 0.20])
 SPOT_MOVES = np.concatenate([-_STEPS[::-1], _STEPS])
 VOL_SHIFTS = np.concatenate([-np.arange(10, 0, -1), np.arange(1, 11)]) / 100.0
 SKEW_TILTS = VOL_SHIFTS.copy()
+CARRY_MOVES = ((0.01, 0.0), (-0.01, 0.0), (0.0, 0.01), (0.0, -0.01))  # (rate, dividend yield)
+CORR_MOVES = (-0.10, 0.10)
 MAX_OBS = 64
 MAX_SPOT = 31
 
@@ -75,11 +79,16 @@ class Book:
     spot_shift: np.ndarray
     vol_shift: np.ndarray
     vol_tilt: np.ndarray
+    carry_rate: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    carry_div: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    corr_move: np.ndarray = field(default_factory=lambda: np.zeros(0))  # each trade's moved roots at corr_root0
     struct: ObBatchRequest = field(init=False)
 
+    _DOUBLES = ("table", "row_lo", "row_inv_dx", "root", "leg_strike", "leg_level", "obs_trigger", "obs_discount",
+                "spot_shift", "vol_shift", "vol_tilt", "carry_rate", "carry_div", "corr_move")
+
     def __post_init__(self):
-        for k in ("table", "row_lo", "row_inv_dx", "root", "leg_strike", "leg_level", "obs_trigger", "obs_discount",
-                  "spot_shift", "vol_shift", "vol_tilt"):
+        for k in self._DOUBLES:
             setattr(self, k, _arr(getattr(self, k), np.float64).ravel())
         for k in ("leg_type", "leg_barrier", "obs_step"):
             setattr(self, k, _arr(getattr(self, k), np.int32).ravel())
@@ -88,14 +97,13 @@ class Book:
         s.n_trades = len(self.trades)
         s.trades = self._trades
         s.dt, s.horizon, s.n_exp, s.n_x = self.dt, self.horizon, self.n_exp, self.n_x
-        for k in ("table", "row_lo", "row_inv_dx", "root", "leg_strike", "leg_level", "obs_trigger", "obs_discount",
-                  "spot_shift", "vol_shift", "vol_tilt"):
+        for k in self._DOUBLES[:-1]:
             a = getattr(self, k)
             setattr(s, k, a.ctypes.data_as(_dp) if a.size else None)
         for k in ("leg_type", "leg_barrier", "obs_step"):
             a = getattr(self, k)
             setattr(s, k, a.ctypes.data_as(_ip) if a.size else None)
-        s.n_spot, s.n_vol = len(self.spot_shift), len(self.vol_shift)
+        s.n_spot, s.n_vol, s.n_carry, s.n_corr = self.n_spot, self.n_vol, self.n_carry, self.n_corr
         self.struct = s
 
     @property
@@ -111,17 +119,32 @@ class Book:
         return len(self.vol_shift)
 
     @property
+    def n_carry(self) -> int:
+        return len(self.carry_rate)
+
+    @property
+    def n_corr(self) -> int:
+        return len(self.corr_move)
+
+    @property
     def n_scenarios(self) -> int:
-        return 1 + self.n_spot + self.n_vol
+        """Values per trade: base, spot moves, carry moves, vol moves, correlation moves."""
+        return 1 + self.n_spot + self.n_carry + self.n_vol + self.n_corr
+
+    def sims_of(self, t) -> int:
+        """A trade's simulations: the base, and under local vol one per vol move and (2 names or more) one per
+        correlation move."""
+        if t.model != OB_MODEL_PATHS:
+            return 1
+        return 1 + self.n_vol + (self.n_corr if t.n_names > 1 else 0)
 
     def simulations(self) -> int:
-        """Simulations of one revaluation: per trade the base, and under local vol one per vol scenario."""
-        return sum(1 + (self.n_vol if t.model == OB_MODEL_PATHS else 0) for t in self.trades)
+        """Simulations of one revaluation."""
+        return sum(self.sims_of(t) for t in self.trades)
 
     def path_steps(self) -> int:
         """Name-path-steps of one revaluation: 2 paths per pair x steps x names over every simulation."""
-        return sum(2 * t.n_pairs * t.n_steps * t.n_names * (1 + (self.n_vol if t.model == OB_MODEL_PATHS else 0))
-                   for t in self.trades)
+        return sum(2 * t.n_pairs * t.n_steps * t.n_names * self.sims_of(t) for t in self.trades)
 
     def revaluations(self) -> int:
         """(trade, scenario) values of one revaluation."""
@@ -139,15 +162,32 @@ def _surfaces(rng, n_names, horizon, n_exp, n_x):
     return grids
 
 
+def moved_corr(corr, move: float) -> np.ndarray:
+    """The correlation matrix with every pair moved by `move`, clipped to +-0.999, repaired to the nearest correlation
+    matrix when it is no longer positive definite (packages/risk/src/optlab/risk/shocks.py:337-359)."""
+    c = np.array(corr, dtype=float)
+    if not move:
+        return c
+    c = np.clip(c + move * (1.0 - np.eye(len(c))), -0.999, 0.999)
+    np.fill_diagonal(c, 1.0)
+    try:
+        np.linalg.cholesky(c)
+        return c
+    except np.linalg.LinAlgError:
+        return nearest_correlation(c)
+
+
 def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), years=(1, 5), steps_per_year: int = 252,
                 max_names: int = 5, heston_share: float = 0.25, n_surfaces: int = 16, n_exp: int = 40, n_x: int = 200,
-                spot_moves=SPOT_MOVES, vol_shifts=VOL_SHIFTS, skew_tilts=SKEW_TILTS) -> Book:
+                spot_moves=SPOT_MOVES, vol_shifts=VOL_SHIFTS, skew_tilts=SKEW_TILTS, carry_moves=CARRY_MOVES,
+                corr_moves=CORR_MOVES) -> Book:
     """A seeded book of uneven trades. Each trade: Heston QE (one name, heston_share of the book) or local vol of
     1..max_names consecutive names of a pool of per-name surfaces; maturity a whole number of years in `years`, one
     step a day; 2^k paths with k uniform in paths_log2; a European ladder (1 to 3 calls or puts), a barrier option
     (up-and-out or up-and-in call, down-and-in or down-and-out put), or a Phoenix autocall (quarterly or monthly),
-    each on the worst performance of its names. Scenarios: the spot moves, then the parallel vol shifts, then the
-    skew tilts (a vol scenario is a (shift, tilt) pair: (s, 0) or (0, t))."""
+    each on the worst performance of its names. Scenarios: the spot moves, the carry moves ((rate, dividend yield)
+    pairs), the parallel vol shifts, then the skew tilts (a vol scenario is a (shift, tilt) pair: (s, 0) or (0, t)),
+    then the correlation moves (every pair of a multi-name trade; its moved roots follow its root in the pool)."""
     rng = np.random.default_rng(seed)
     horizon = float(years[1])
     dt = 1.0 / steps_per_year
@@ -179,6 +219,10 @@ def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), year
             corr = np.full((n, n), rho) + (1.0 - rho) * np.eye(n)
             t.root0 = sum(len(x) for x in root)
             root.append(np.asarray(correlation_root(corr), dtype=float).ravel())
+            t.corr_root0 = sum(len(x) for x in root)
+            if n > 1:
+                for m in corr_moves:
+                    root.append(np.asarray(correlation_root(moved_corr(corr, m)), dtype=float).ravel())
             t.heston[:] = [0.04, 1.0, 0.04, 0.5, 0.0]
         if product in ("european", "barrier"):
             t.product = OB_PRODUCT_LADDER
@@ -217,6 +261,7 @@ def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), year
         labels.append(f"{'heston' if heston else 'lv'}-{n}-{product}-{T}y-2^{k}")
     legs_flat = [x for rows in legs for x in rows] or [(0, 0.0, 0, 0.0)]
     obs_flat = [x for rows in obs for x in rows] or [(1, 0.0, 1.0)]
+    carry = np.asarray(carry_moves, float).reshape(-1, 2)
     vs = np.concatenate([np.asarray(vol_shifts, float), np.zeros(len(skew_tilts))])
     vt = np.concatenate([np.zeros(len(vol_shifts)), np.asarray(skew_tilts, float)])
     return Book(
@@ -240,6 +285,9 @@ def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), year
         spot_shift=np.asarray(spot_moves, float),
         vol_shift=vs,
         vol_tilt=vt,
+        carry_rate=carry[:, 0],
+        carry_div=carry[:, 1],
+        corr_move=np.asarray(corr_moves, float),
     )
 
 
@@ -266,7 +314,8 @@ class Batch:
         check(load().ob_batch_run_per_trade(self._p, _stream(stream)))
 
     def result(self):
-        """(price, se) as (n_trades, 1 + n_spot + n_vol) arrays, and the last run's device time in ms."""
+        """(price, se) as (n_trades, n_scenarios) arrays (base, spot, carry, vol, correlation moves), and the last
+        run's device time in ms."""
         b = self.book
         price = np.empty((b.n_trades, b.n_scenarios))
         se = np.empty_like(price)

@@ -674,7 +674,11 @@ int or_mc_price(const ob_mc_request* rq, int n_threads, ob_mc_result* res) {
  * move as a shift ln(1 + move) of every performance (the reference's path factors, packages/risk/src/optlab/risk/
  * engine.py:585-590), a vol move as the local-variance rows rebuilt as (max(sigma + shift + tilt k, 0.01))^2 at each
  * node k, the Heston model unmoved by it (its parameters do not depend on the surface,
- * packages/structured/src/optlab/structured/context.py:163-164). price and se: 1 + n_spot + n_vol values. */
+ * packages/structured/src/optlab/structured/context.py:163-164), a carry move as the log-forward rebuilt with
+ * r + carry_rate and q + carry_div and every payment at time t discounted by exp(-carry_rate t) more (the forward
+ * ratio and discount move of packages/risk/src/optlab/risk/engine.py:8-11 and curves.py:109-112; a Heston trade's
+ * drift moves the same way), a correlation move as the trade's moved root (multi-name local vol; the others do not
+ * move). price and se: 1 + n_spot + n_carry + n_vol + n_corr values, in that order. */
 int or_batch_trade(const ob_batch_request* b, int trade, int n_threads, double* price, double* se) {
     if (!b || trade < 0 || trade >= b->n_trades || !price || !se) return fail("bad batch trade");
     const ob_batch_trade* t = &b->trades[trade];
@@ -684,12 +688,13 @@ int or_batch_trade(const ob_batch_request* b, int trade, int n_threads, double* 
     double* t0 = (double*)malloc(sizeof(double) * S);
     double* lf = (double*)malloc(sizeof(double) * N * (S + 1));
     int* step_row = (int*)malloc(sizeof(int) * N * S);
+    double* odisc = (double*)malloc(sizeof(double) * (t->product == OB_PRODUCT_AUTOCALL ? t->n_obs : 1));
     double* table = (double*)malloc(sizeof(double) * (lv ? N * E * X : 1));
     double* lo = (double*)malloc(sizeof(double) * N * E);
     double* inv = (double*)malloc(sizeof(double) * N * E);
     double spot[OB_MAX_NAMES], cvar[OB_MAX_NAMES], hes[5 * OB_MAX_NAMES];
     int kind[OB_MAX_NAMES];
-    if (!dt || !t0 || !lf || !step_row || !table || !lo || !inv) return fail("out of memory");
+    if (!dt || !t0 || !lf || !step_row || !odisc || !table || !lo || !inv) return fail("out of memory");
     for (int i = 0; i < S; ++i) {
         dt[i] = b->dt, t0[i] = i * b->dt;
         int j = 0;
@@ -724,12 +729,27 @@ int or_batch_trade(const ob_batch_request* b, int trade, int n_threads, double* 
         rq.ki_daily = t->ki_daily;
     }
     int st = OB_OK;
-    const int n_sc = 1 + b->n_spot + b->n_vol;
+    const int n_sc = 1 + b->n_spot + b->n_carry + b->n_vol + b->n_corr;
     for (int sc = 0; sc < n_sc && st == OB_OK; ++sc) {
-        const int vol = sc > b->n_spot ? sc - 1 - b->n_spot : -1;
-        if (vol >= 0 && !lv) { /* the Heston model ignores the surface */
+        const int c0 = 1 + b->n_spot, v0 = c0 + b->n_carry, r0 = v0 + b->n_vol;
+        const int carry = sc >= c0 && sc < v0 ? sc - c0 : -1;
+        const int vol = sc >= v0 && sc < r0 ? sc - v0 : -1;
+        const int corr = sc >= r0 ? sc - r0 : -1;
+        if ((vol >= 0 && !lv) || (corr >= 0 && (!lv || N < 2))) { /* a move the trade's model does not see */
             price[sc] = price[0], se[sc] = se[0];
             continue;
+        }
+        const double dr = carry >= 0 ? b->carry_rate[carry] : 0.0, dq = carry >= 0 ? b->carry_div[carry] : 0.0;
+        rq.r = t->r + dr, rq.q = t->q + dq;
+        for (int a = 0; a < N; ++a)
+            for (int i = 0; i <= S; ++i) lf[a * (S + 1) + i] = (rq.r - rq.q) * (i * b->dt);
+        if (lv) rq.root = b->root + (corr >= 0 ? t->corr_root0 + corr * N * N : t->root0);
+        if (t->product == OB_PRODUCT_LADDER) {
+            rq.discount = t->discount * exp(-dr * S * b->dt);
+        } else {
+            for (int j = 0; j < t->n_obs; ++j)
+                odisc[j] = b->obs_discount[t->obs0 + j] * exp(-dr * b->obs_step[t->obs0 + j] * b->dt);
+            rq.obs_discount = odisc;
         }
         if (lv)
             for (int r = 0; r < N * E; ++r) {
@@ -750,7 +770,7 @@ int or_batch_trade(const ob_batch_request* b, int trade, int n_threads, double* 
         st = mc_price_shifted(&rq, shift, 1, n_threads, &res);
         if (st == OB_OK) price[sc] = res.price[0], se[sc] = res.se[0];
     }
-    free(dt), free(t0), free(lf), free(step_row), free(table), free(lo), free(inv);
+    free(dt), free(t0), free(lf), free(step_row), free(odisc), free(table), free(lo), free(inv);
     return st;
 }
 

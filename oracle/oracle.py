@@ -88,9 +88,9 @@ class Oracle:
         return res.price[0], res.se[0]
 
     def batch_trade(self, book, trade: int, threads: int = 0):
-        """(price, se) of one trade of a batch under each of its scenarios (base, spot moves, vol moves), each
-        scenario its own simulation on the trade's seed."""
-        n = 1 + book.n_spot + book.n_vol
+        """(price, se) of one trade of a batch under each of its scenarios (base, spot, carry, vol and correlation
+        moves), each scenario its own simulation on the trade's seed."""
+        n = book.n_scenarios
         price, se = np.empty(n), np.empty(n)
         self._check(self.lib.or_batch_trade(C.byref(book.struct), int(trade), int(threads) or _cores(),
                                             price.ctypes.data_as(_dp), se.ctypes.data_as(_dp)))

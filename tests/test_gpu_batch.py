@@ -1,6 +1,7 @@
-"""Batched revaluation on the GPU: every (trade, scenario) of a seeded book against the oracle's own simulation of it
-(FP64 within 1e-10 relative, FP32 within 4 standard errors), the graph replay deterministic and equal to a direct
-run, the autotuned and per-trade launches equal up to the order of the sums."""
+"""Batched revaluation on the GPU: every (trade, scenario) of a seeded book (spot, carry, vol, skew and correlation
+moves) against the oracle's own simulation of it (FP64 within 1e-10 relative, FP32 within 4 standard errors), the
+graph replay deterministic and equal to a direct run, the autotuned and per-trade launches equal up to the order of
+the sums."""
 
 import numpy as np
 import pytest
@@ -87,12 +88,35 @@ def test_heston_trades_do_not_move_under_vol_scenarios_and_local_vol_trades_do(b
     with Batch(book, "fp64") as b:
         b.launch()
         price = b.result()[0]
-    vol = slice(1 + book.n_spot, None)
+    v0 = 1 + book.n_spot + book.n_carry
+    vol, corr = slice(v0, v0 + book.n_vol), slice(v0 + book.n_vol, None)
+    carry = slice(1 + book.n_spot, v0)
+    assert book.n_carry == 4 and book.n_corr == 2
     for i, t in enumerate(book.trades):
         if t.model == OB_MODEL_HESTON_QE:
             assert np.all(price[i, vol] == price[i, 0])
+        if t.model == OB_MODEL_HESTON_QE or t.n_names == 1:
+            assert np.all(price[i, corr] == price[i, 0])
+        elif price[i, 0] != 0:
+            assert np.all(price[i, corr] != price[i, 0])
+        if price[i, 0] != 0:
+            assert np.all(price[i, carry] != price[i, 0])  # every trade's forwards and discounting move
     lv = [i for i, t in enumerate(book.trades) if t.model == OB_MODEL_PATHS]
     assert lv and any(np.any(price[i, vol] != price[i, 0]) for i in lv)
+
+
+def test_rate_up_lowers_a_call_ladder_less_than_its_discount_and_dividends_move_the_other_way(book):
+    """Under a 1 % rate rise a call gains forward and loses discount; a 1 % dividend rise only lowers the forward:
+    the carry outputs keep the signs of rho and dividend sensitivity on the calls of the book."""
+    with Batch(book, "fp64") as b:
+        b.launch()
+        price = b.result()[0]
+    c0 = 1 + book.n_spot
+    for i, t in enumerate(book.trades):
+        if t.product != 0 or t.n_legs != 1 or book.leg_type[t.leg0] != 1 or book.leg_barrier[t.leg0] != 0:
+            continue
+        assert price[i, c0 + 2] < price[i, 0] < price[i, c0 + 3]  # dividends up / down
+        assert price[i, c0 + 1] < price[i, 0] < price[i, c0]  # rates down / up
 
 
 def test_a_book_of_every_name_count_and_long_schedules_matches_the_oracle(oracle):
