@@ -461,11 +461,11 @@ def run_adjoint(args, world, rank):
 
 
 def run_batch(args, world, rank):
-    """cfg4: the seeded book (512 trades, 66 scenarios: spot, carry, vol, skew and correlation moves) revalued by one
-    replay of the captured graph, FP32 paths with FP64 sums; against the same simulations as one launch per trade
-    simulation. Units: name-path-steps simulated (2 paths per pair x steps x names, over the base, vol-scenario and
-    correlation-scenario simulations; spot and carry moves ride on the base simulation). One rank: the book is one job
-    (more GPUs would split its trades)."""
+    """cfg4: the seeded book (512 trades, 60 scenarios: spot, vol and skew moves) revalued by one replay of the
+    captured graph, FP32 paths with FP64 sums; against the same simulations as one launch per trade simulation.
+    Units: name-path-steps simulated (2 paths per pair x steps x names, over the base and the vol-scenario
+    simulations; spot moves ride on the base simulation). One rank: the book is one job (more GPUs would split its
+    trades)."""
     import torch
 
     from optlab_b200.batch import Batch, sample_book

@@ -10,9 +10,9 @@ same launch.
 
 `sample_book` draws the benchmark's book: 512 trades of 1 to 5 names, 1 to 5 years of daily steps, 2^14 to 2^18 paths,
 European, barrier or autocall payoffs (worst-of with several names), under Heston QE or local vol of per-name SSVI
-surfaces, with 66 scenarios: 20 spot moves of +-1..20 %, 4 carry moves (rates +-1 %, dividend yield +-1 %), 20
-parallel moves of local vol of +-1..10 points, 20 skew tilts of +-1..10 points per unit of log-moneyness, and 2
-moves of every pairwise correlation by +-0.10.
+surfaces, with 60 scenarios: 20 spot moves of +-1..20 %, 20 parallel moves of local vol of +-1..10 points, 20 skew
+tilts of +-1..10 points per unit of log-moneyness. Carry moves (CARRY_MOVES: rates +-1 %, dividend yield +-1 %) and
+correlation moves (CORR_MOVES: every pair +-0.10) are added on request.
 """
 
 from __future__ import annotations
@@ -179,8 +179,8 @@ def moved_corr(corr, move: float) -> np.ndarray:
 
 def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), years=(1, 5), steps_per_year: int = 252,
                 max_names: int = 5, heston_share: float = 0.25, n_surfaces: int = 16, n_exp: int = 40, n_x: int = 200,
-                spot_moves=SPOT_MOVES, vol_shifts=VOL_SHIFTS, skew_tilts=SKEW_TILTS, carry_moves=CARRY_MOVES,
-                corr_moves=CORR_MOVES) -> Book:
+                spot_moves=SPOT_MOVES, vol_shifts=VOL_SHIFTS, skew_tilts=SKEW_TILTS, carry_moves=(),
+                corr_moves=()) -> Book:
     """A seeded book of uneven trades. Each trade: Heston QE (one name, heston_share of the book) or local vol of
     1..max_names consecutive names of a pool of per-name surfaces; maturity a whole number of years in `years`, one
     step a day; 2^k paths with k uniform in paths_log2; a European ladder (1 to 3 calls or puts), a barrier option

@@ -6,15 +6,17 @@ import pytest
 
 from optlab_b200 import _abi
 from optlab_b200._abi import OB_MODEL_HESTON_QE, OB_MODEL_PATHS, OB_PRODUCT_AUTOCALL, OB_PRODUCT_LADDER
-from optlab_b200.batch import Batch, moved_corr, sample_book
+from optlab_b200.batch import CARRY_MOVES, CORR_MOVES, Batch, moved_corr, sample_book
 from optlab_b200.models import correlation_root
 from optlab_b200.requests import mc_request
 
 
 def test_the_benchmark_book_has_the_stated_mix():
     b = sample_book()
-    assert b.n_trades == 512 and b.n_spot == 20 and b.n_vol == 40 and b.n_carry == 4 and b.n_corr == 2
-    assert b.n_scenarios == 67
+    assert b.n_trades == 512 and b.n_spot == 20 and b.n_vol == 40 and b.n_carry == 0 and b.n_corr == 0
+    assert b.n_scenarios == 61
+    wide = sample_book(n_trades=8, carry_moves=CARRY_MOVES, corr_moves=CORR_MOVES)
+    assert wide.n_carry == 4 and wide.n_corr == 2 and wide.n_scenarios == 67
     t = b.trades
     names = np.array([x.n_names for x in t])
     paths = np.array([2 * x.n_pairs for x in t])

@@ -7,14 +7,15 @@ import numpy as np
 import pytest
 
 from optlab_b200._abi import OB_MODEL_HESTON_QE, OB_MODEL_PATHS
-from optlab_b200.batch import Batch, sample_book
+from optlab_b200.batch import CARRY_MOVES, CORR_MOVES, Batch, sample_book
 
 pytestmark = pytest.mark.gpu
 
 
 def _book(seed=3, n=20, **kw):
     args = dict(n_trades=n, seed=seed, paths_log2=(10, 12), years=(1, 2), steps_per_year=52, n_surfaces=8,
-                spot_moves=[-0.2, -0.05, 0.05, 0.2], vol_shifts=[-0.05, 0.05], skew_tilts=[-0.1, 0.1])
+                spot_moves=[-0.2, -0.05, 0.05, 0.2], vol_shifts=[-0.05, 0.05], skew_tilts=[-0.1, 0.1],
+                carry_moves=CARRY_MOVES, corr_moves=CORR_MOVES)
     args.update(kw)
     return sample_book(**args)
 
