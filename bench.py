@@ -402,6 +402,7 @@ def run_adjoint(args, world, rank):
     n_greeks = w.held.struct.n_names * (1 + len(w.node_T) * len(w.node_k))
     s = w.held.struct
     units = 2 * s.n_pairs * s.n_steps * s.n_names
+    states = s.n_steps * s.n_names * 2 * s.n_pairs * 4  # FP32 states the forward keeps when it keeps every step
     plan = AdjointPlan(w.held, 0.005, "fp32")
     for _ in range(args.warmup):
         autocall_greeks(w.held, nodes, 0.005, plan=plan)
@@ -442,7 +443,9 @@ def run_adjoint(args, world, rank):
         "dtype": "f32",
         "data": "synthetic (seeded SSVI surfaces)",
         "config": {"workload": "adjoint_worst_of", "n_paths": 2 * s.n_pairs, "n_steps": s.n_steps, "names": s.n_names,
-                   "nodes_per_name": [len(w.node_T), len(w.node_k)], "smoothing": 0.005},
+                   "nodes_per_name": [len(w.node_T), len(w.node_k)], "smoothing": 0.005,
+                   "states_kept": "every step" if states <= 24 * 2**30 else "every fourth step",
+                   "states_bytes": states},
         "adjoint": {"forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
                     "path_steps_per_s": 2 * units / (t_adj), "price": g32["price"], "price_se": g32["price_se"]},
         "bump_and_revalue_fp64": {"revaluation_ms": t_rev * 1e3, "revaluations": n_reval,

@@ -197,10 +197,14 @@ typedef struct ob_mc_plan ob_mc_plan;
 
 /* An autocall under the path engine's local vol (every name kind 1, 1 to 4 names, pairs 0 .. n_pairs - 1) with its
    digitals smoothed as ramps of relative width `smoothing` (the reference's risk engine uses 0.005 for Greeks,
-   packages/risk/src/optlab/risk/greeks.py:430; 0 gives the exact payoff). */
+   packages/risk/src/optlab/risk/greeks.py:430; 0 gives the exact payoff). checkpoint: the steps between the states
+   the forward pass keeps for the backward one: 1 (every step: the backward recomputes nothing), 4 (every fourth:
+   the backward recomputes each 4-step segment, a quarter of the memory), 0 (every step while those states take at
+   most 24 GiB, else every fourth). */
 typedef struct {
     ob_mc_request base;
     double smoothing;
+    int checkpoint;
 } ob_adjoint_request;
 
 typedef struct {

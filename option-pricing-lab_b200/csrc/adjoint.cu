@@ -17,9 +17,18 @@
 // adj_backward  one thread per pair again, segments of kCk steps from the last to the first: restart from the
 //               checkpoint, recompute the segment's states and normals, then walk it backwards carrying dV/dx per
 //               name and leg, injecting the observation sensitivities where they were taken, and adding
-//               dV/d(variance) x (1 - w, w) into the two table entries each step read. The gradient of the whole
-//               table (every name's rows) lives in shared memory for the whole kernel (float in the float build,
-//               double in the double one) and is added to the caller's per-batch gradient at the end.
+//               dV/d(variance) x (1 - w, w) into the two table entries each step read. Each block adds into its own
+//               copy of the whole table's gradient (every name's rows; float in the float build, double in the
+//               double one) in global memory, small enough to stay in L2 (148 x 2 blocks x 120 x 200 floats =
+//               28 MB), by reductions that return nothing: the float add of a shared-memory atomic is a
+//               compare-and-swap loop, a global reduction is one instruction the warp does not wait for (the
+//               backward took half the time with it). At the end the block adds its copy into the caller's
+//               per-batch gradient.
+// adj_backward_dense  the same reverse sweep when the forward stored the state after every step (when those
+//               states fit in the dense budget): nothing is recomputed. A step from x to x' read the variance v at x
+//               and moved by v (-dt/2) + sqrt(v dt) z, so its noise term is d = x' - x - v (-dt/2) and
+//               dx'/dv = -dt/2 + d / (2 v): no normals are drawn again. Each segment's states are loaded while
+//               the previous segment is swept (two register buffers).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -38,10 +47,12 @@ constexpr int kAdjBatches = OB_ADJ_BATCHES;
 template <typename R>
 struct AdjArgs {
     int n_names, n_steps, n_obs, n_x, n_rows, n_seg;
+    int n_ck;                  // states stored by the forward: every kCk-th step but the last segment's, or all
     long long n_pairs;
     uint32_t k0, k1;
     const StepRec<R>* steps;   // n_steps
     const NameStep<R>* ns;     // n_steps x n_names
+    const int* row_ix;         // n_steps x n_names: the table row read (gradient entry of pair idx: idx + row)
     const R* root;             // n x n
     const Pair2<R>* table;     // n_rows x (n_x - 1): (y_i, y_i+1 - y_i)
     const R* trig;             // n_obs, in performance (<= 0: no call)
@@ -50,7 +61,7 @@ struct AdjArgs {
     double coupon;
     int memory, has_coupon, ki_daily;
     // forward outputs, backward inputs
-    R* ckpt;                   // (n_seg - 1) x n x 2 x n_pairs: x at grid points kCk, 2 kCk, ...
+    R* ckpt;                   // n_ck x n x 2 x n_pairs: x at grid points CK, 2 CK, ... (CK = kCk, or 1 when dense)
     R* dobs;                   // n_obs x 2 x n_pairs: d(pair value) / d(log perf) at each observation
     unsigned char* who;        // n_obs x 2 x n_pairs: the name that was the worst there
     R* dki;                    // 2 x n_pairs: d(pair value) / d(lowest log perf)
@@ -58,6 +69,7 @@ struct AdjArgs {
     unsigned char* ki_name;    // 2 x n_pairs
     double* partial;           // per block: price sum and square, then per name delta sum and square
     double* grad;              // kAdjBatches x n_rows x n_x
+    R* priv;                   // per backward block: its n_rows x n_x gradient, zeroed before each backward
     unsigned long long* batch_pairs;  // kAdjBatches
 };
 
@@ -217,7 +229,7 @@ __device__ __forceinline__ void batch_normals(const AdjArgs<R>& a, uint64_t pair
         }
 }
 
-template <typename R, int N, bool STORE>
+template <typename R, int N, bool STORE, int CK>
 __global__ void __launch_bounds__(256) adj_forward(AdjArgs<R> a) {
     constexpr int G = Batch<N>::G;
     __shared__ double wacc[8][2 + 2 * N];
@@ -265,8 +277,8 @@ __global__ void __launch_bounds__(256) adj_forward(AdjArgs<R> a) {
                     if (wv[leg] < low[leg]) low[leg] = wv[leg], lstep[leg] = i, lname[leg] = wn[leg];
                     if (st.obs >= 0) lpo[leg][st.obs] = wv[leg], wo[leg][st.obs] = static_cast<unsigned char>(wn[leg]);
                 }
-                if (STORE && i % kCk == 0 && i / kCk < a.n_seg && active) {
-                    const long long c = i / kCk - 1;
+                if (STORE && i % CK == 0 && i / CK <= a.n_ck && active) {
+                    const long long c = i / CK - 1;
 #pragma unroll
                     for (int n = 0; n < N; ++n)
 #pragma unroll
@@ -322,20 +334,36 @@ __global__ void __launch_bounds__(256) adj_forward(AdjArgs<R> a) {
     }
 }
 
+// A reduction into the block's gradient copy (the result unused: no return value is waited for).
 template <typename T>
-__device__ __forceinline__ void shared_add(T* p, T v) {
+__device__ __forceinline__ void grad_add(T* p, T v) {
     atomicAdd(p, v);
+}
+
+// The block's gradient copy added into the caller's gradient of batch blockIdx % kAdjBatches, and its pair count.
+template <typename R>
+__device__ __forceinline__ void flush_gradient(const AdjArgs<R>& a, const R* sg, unsigned long long mine) {
+    __syncthreads();
+    const int tab_n = a.n_rows * a.n_x;
+    const int batch = blockIdx.x % kAdjBatches;
+    double* out = a.grad + static_cast<long long>(batch) * tab_n;
+    for (int t = threadIdx.x; t < tab_n; t += blockDim.x) {
+        const double v = static_cast<double>(__ldcg(sg + t));  // from L2, where the reductions were made
+        if (v != 0.0) atomicAdd(out + t, v);
+    }
+    __shared__ unsigned long long s_cnt;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    atomicAdd(&s_cnt, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(a.batch_pairs + batch, s_cnt);
 }
 
 template <typename R, int N>
 __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
     constexpr int G = Batch<N>::G;
     using GT = R;  // gradient accumulators: float in the float build, double in the double one
-    extern __shared__ __align__(16) unsigned char sm[];
-    GT* sg = reinterpret_cast<GT*>(sm);
-    const int tab_n = a.n_rows * a.n_x;
-    for (int t = threadIdx.x; t < tab_n; t += blockDim.x) sg[t] = GT(0);
-    __syncthreads();
+    GT* sg = a.priv + static_cast<long long>(blockIdx.x) * a.n_rows * a.n_x;
     const int lane = threadIdx.x & 31;
     const long long P = a.n_pairs;
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
@@ -416,6 +444,7 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     const NameStep<R> ns = a.ns[(i - 1) * N + n];
+                    const int rix = __ldg(a.row_ix + (i - 1) * N + n);
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
@@ -424,11 +453,10 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
                         const R c = st.hdt + st.sdt * z / (R(2) * sv);  // d x_i / d var
                         const R vb = xb[leg][n] * c;
                         if (vb != R(0)) {
-                            // table entry (row, i) sits at pair index row * (n_x - 1) + i: recover (row, i)
-                            const int row = r.idx / (a.n_x - 1), col = r.idx - row * (a.n_x - 1);
-                            GT* gr = sg + row * a.n_x + col;
-                            shared_add(gr, static_cast<GT>(vb * (R(1) - r.w)));
-                            shared_add(gr + 1, static_cast<GT>(vb * r.w));
+                            // pair index row (n_x - 1) + i is table entry row n_x + i
+                            GT* gr = sg + r.idx + rix;
+                            grad_add(gr, static_cast<GT>(vb * (R(1) - r.w)));
+                            grad_add(gr + 1, static_cast<GT>(vb * r.w));
                         }
                         xb[leg][n] += vb * r.dvdx;
                     }
@@ -436,20 +464,101 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
             }
         }
     }
-    __syncthreads();
-    const int batch = blockIdx.x % kAdjBatches;
-    double* out = a.grad + static_cast<long long>(batch) * tab_n;
-    for (int t = threadIdx.x; t < tab_n; t += blockDim.x) {
-        const double v = static_cast<double>(sg[t]);
-        if (v != 0.0) atomicAdd(out + t, v);
+    flush_gradient(a, sg, mine);  // pairs of this block: the count of each batch makes its mean
+}
+
+template <typename R, int N>
+__device__ __forceinline__ void dense_segment(const AdjArgs<R>& a, long long p, int s, R (&xs)[kCk + 1][2][N]) {
+    const long long P = a.n_pairs;
+#pragma unroll
+    for (int g = 0; g <= kCk; ++g) {
+        const int i = s * kCk + g;  // grid point
+        if (i > a.n_steps) break;
+#pragma unroll
+        for (int n = 0; n < N; ++n)
+#pragma unroll
+            for (int leg = 0; leg < 2; ++leg)
+                xs[g][leg][n] = i == 0 ? R(0) : a.ckpt[((static_cast<long long>(i - 1) * N + n) * 2 + leg) * P + p];
     }
-    // pairs of this block (the count of each batch makes its mean)
-    __shared__ unsigned long long s_cnt;
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    atomicAdd(&s_cnt, mine);
-    __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(a.batch_pairs + batch, s_cnt);
+}
+
+template <typename R, int N>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1) adj_backward_dense(AdjArgs<R> a) {
+    using GT = R;
+    GT* sg = a.priv + static_cast<long long>(blockIdx.x) * a.n_rows * a.n_x;
+    const int lane = threadIdx.x & 31;
+    const long long P = a.n_pairs;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    unsigned long long mine = 0;
+    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < P;
+         base += stride) {
+        const bool active = base + lane < P;
+        if (!active) continue;  // no block-wide synchronisation below: inactive lanes may leave
+        const long long p = base + lane;
+        ++mine;
+        const int kstep[2] = {a.ki_step[p], a.ki_step[P + p]};
+        const int kname[2] = {a.ki_name[p], a.ki_name[P + p]};
+        const R kd[2] = {a.dki[p], a.dki[P + p]};
+        R xb[2][N];
+#pragma unroll
+        for (int n = 0; n < N; ++n) xb[0][n] = xb[1][n] = R(0);
+        R cur[kCk + 1][2][N], nxt[kCk + 1][2][N];
+        dense_segment<R, N>(a, p, a.n_seg - 1, cur);
+        for (int s = a.n_seg - 1; s >= 0; --s) {
+            if (s > 0) dense_segment<R, N>(a, p, s - 1, nxt);
+            const int i_first = s * kCk + 1;
+            const int len = min(kCk, a.n_steps - s * kCk);
+#pragma unroll
+            for (int g = kCk - 1; g >= 0; --g) {
+                if (g >= len) continue;
+                const int i = i_first + g;
+                const StepRec<R> st = a.steps[i - 1];
+                if (st.obs >= 0) {
+#pragma unroll
+                    for (int leg = 0; leg < 2; ++leg) {
+                        const long long o = (static_cast<long long>(st.obs) * 2 + leg) * P + p;
+                        const R d = a.dobs[o];
+                        const int w = a.who[o];
+#pragma unroll
+                        for (int n = 0; n < N; ++n)
+                            if (w == n) xb[leg][n] += d;
+                    }
+                }
+#pragma unroll
+                for (int leg = 0; leg < 2; ++leg)
+                    if (kstep[leg] == i) {
+#pragma unroll
+                        for (int n = 0; n < N; ++n)
+                            if (kname[leg] == n) xb[leg][n] += kd[leg];
+                    }
+#pragma unroll
+                for (int n = 0; n < N; ++n) {
+                    const NameStep<R> ns = a.ns[(i - 1) * N + n];
+                    const int rix = __ldg(a.row_ix + (i - 1) * N + n);
+#pragma unroll
+                    for (int leg = 0; leg < 2; ++leg) {
+                        const LvStep<R> r = lv_read(a, ns, cur[g][leg][n]);
+                        const R d = cur[g + 1][leg][n] - cur[g][leg][n] - r.var * st.hdt;  // sqrt(v dt) z
+                        const R c = st.hdt + d / (R(2) * r.var);                            // d x_i / d var
+                        const R vb = xb[leg][n] * c;
+                        if (vb != R(0)) {
+                            GT* gr = sg + r.idx + rix;  // pair index row (n_x - 1) + i is entry row n_x + i
+                            grad_add(gr, static_cast<GT>(vb * (R(1) - r.w)));
+                            grad_add(gr + 1, static_cast<GT>(vb * r.w));
+                        }
+                        xb[leg][n] += vb * r.dvdx;
+                    }
+                }
+            }
+#pragma unroll
+            for (int g = 0; g <= kCk; ++g)
+#pragma unroll
+                for (int n = 0; n < N; ++n)
+#pragma unroll
+                    for (int leg = 0; leg < 2; ++leg) cur[g][leg][n] = nxt[g][leg][n];
+        }
+    }
+    flush_gradient(a, sg, mine);
 }
 
 // (y_i, y_i+1 - y_i) pairs of the caller's FP64 table.
@@ -470,7 +579,7 @@ struct AdjPlan {
     int precision = OB_FP32, n = 1, sms = 0, n_out = 0;
     long long n_pairs = 0;
     int grid_f = 0, grid_b = 0;
-    size_t smem_b = 0;
+    size_t priv_bytes = 0;
     AdjArgs<float> af{};
     AdjArgs<double> ad{};
     double spot[OB_MAX_NAMES] = {};
@@ -479,6 +588,7 @@ struct AdjPlan {
     bool backward = false;
     cudaStream_t last = nullptr;
     int tab_n = 0;
+    bool dense = false;  // the forward stores every step's state and the backward recomputes nothing
 
     template <typename R>
     AdjArgs<R>& args();
@@ -505,10 +615,14 @@ namespace {
 
 template <typename R, int N>
 void pick(AdjPlan& p) {
-    p.kf = reinterpret_cast<const void*>(adj_forward<R, N, false>);
-    p.kfs = reinterpret_cast<const void*>(adj_forward<R, N, true>);
-    p.kb = reinterpret_cast<const void*>(adj_backward<R, N>);
+    p.kf = reinterpret_cast<const void*>(adj_forward<R, N, false, kCk>);
+    p.kfs = p.dense ? reinterpret_cast<const void*>(adj_forward<R, N, true, 1>)
+                    : reinterpret_cast<const void*>(adj_forward<R, N, true, kCk>);
+    p.kb = p.dense ? reinterpret_cast<const void*>(adj_backward_dense<R, N>)
+                   : reinterpret_cast<const void*>(adj_backward<R, N>);
 }
+
+constexpr double kDenseBudget = 24.0 * (1ull << 30);  // bytes of stored states below which every step is stored
 
 void check_adjoint(const ob_adjoint_request& r) {
     const ob_mc_request& rq = r.base;
@@ -521,6 +635,7 @@ void check_adjoint(const ob_adjoint_request& r) {
     if (rq.n_obs > kMaxObs) invalid("the adjoint takes at most 64 observations");
     if (rq.first_pair != 0) invalid("the adjoint runs pairs 0 .. n_pairs - 1");
     if (!(r.smoothing >= 0.0 && r.smoothing < 1.0)) invalid("smoothing must be in [0, 1)");
+    if (r.checkpoint != 0 && r.checkpoint != 1 && r.checkpoint != kCk) invalid("checkpoint must be 0, 1 or 4");
     if (rq.ki_barrier <= 0 || rq.coupon_barrier < 0) invalid("the adjoint needs a knock-in barrier above 0");
 }
 
@@ -552,11 +667,13 @@ void AdjPlan::build(const ob_adjoint_request& r) {
     }
     for (int j = 0; j < rq.n_obs; ++j) steps[rq.obs_step[j] - 1].obs = j;
     std::vector<NameStep<R>> ns(static_cast<size_t>(S) * n);
+    std::vector<int> row_ix(static_cast<size_t>(S) * n);
     for (int i = 1; i <= S; ++i)
         for (int k = 0; k < n; ++k) {
             NameStep<R>& e = ns[static_cast<size_t>(i - 1) * n + k];
             std::memset(&e, 0, sizeof e);
             const int row = rq.step_row[static_cast<size_t>(k) * S + (i - 1)];
+            row_ix[static_cast<size_t>(i - 1) * n + k] = row;
             e.lo = static_cast<R>(rq.row_lo[row]);
             e.inv_dx = static_cast<R>(rq.row_inv_dx[row]);
             e.lf = static_cast<R>(rq.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
@@ -567,6 +684,7 @@ void AdjPlan::build(const ob_adjoint_request& r) {
     for (int j = 0; j < rq.n_obs; ++j) trig[j] = rq.trigger[j] > 0 ? static_cast<R>(rq.trigger[j]) : R(0);
     a.steps = arena.put<StepRec<R>>(steps.data(), steps.size());
     a.ns = arena.put<NameStep<R>>(ns.data(), ns.size());
+    a.row_ix = arena.put<int>(row_ix.data(), row_ix.size());
     a.root = arena.put<R>(root.data(), root.size());
     a.trig = arena.put<R>(trig.data(), trig.size());
     a.disc = arena.put<double>(rq.obs_discount, rq.n_obs);
@@ -577,7 +695,10 @@ void AdjPlan::build(const ob_adjoint_request& r) {
     check_cuda(cudaGetLastError(), "adj_table launch");
     a.table = tab;
     const long long P = rq.n_pairs;
-    a.ckpt = arena.alloc<R>(static_cast<size_t>(std::max(1, a.n_seg - 1)) * n * 2 * P);
+    const double dense_bytes = static_cast<double>(S) * n * 2 * P * sizeof(R);
+    dense = r.checkpoint == 1 || (r.checkpoint == 0 && dense_bytes <= kDenseBudget);
+    a.n_ck = dense ? S : a.n_seg - 1;
+    a.ckpt = arena.alloc<R>(static_cast<size_t>(std::max(1, a.n_ck)) * n * 2 * P);
     a.dobs = arena.alloc<R>(static_cast<size_t>(rq.n_obs) * 2 * P);
     a.who = arena.alloc<unsigned char>(static_cast<size_t>(rq.n_obs) * 2 * P);
     a.dki = arena.alloc<R>(2 * static_cast<size_t>(P));
@@ -591,17 +712,15 @@ void AdjPlan::build(const ob_adjoint_request& r) {
         default: pick<R, 4>(*this); break;
     }
     tab_n = rq.n_rows * rq.n_x;
-    smem_b = static_cast<size_t>(tab_n) * sizeof(R);
-    if (smem_b > (200u << 10)) invalid("the tables are too large for the adjoint's shared-memory gradient (200 KB)");
-    check_cuda(cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_b)),
-               "cudaFuncSetAttribute");
     int per_f = 0, per_b = 0;
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_f, kfs, 256, 0), "occupancy");
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_b, kb, 256, smem_b), "occupancy");
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_b, kb, 256, 0), "occupancy");
     const long long need = (P + 255) / 256;
     grid_f = static_cast<int>(std::max<long long>(1, std::min<long long>(need, static_cast<long long>(sms) * std::max(1, per_f))));
     grid_b = static_cast<int>(std::max<long long>(1, std::min<long long>(need, static_cast<long long>(sms) * std::max(1, per_b))));
     a.partial = arena.alloc<double>(static_cast<size_t>(grid_f) * (2 + 2 * n));
+    priv_bytes = static_cast<size_t>(grid_b) * tab_n * sizeof(R);
+    a.priv = arena.alloc<R>(static_cast<size_t>(grid_b) * tab_n);
     for (int k = 0; k < n; ++k) spot[k] = rq.spot[k];
 }
 
@@ -637,12 +756,14 @@ void AdjPlan::run(const double* d_table, double* d_grad, cudaStream_t st) {
         check_cuda(cudaMemsetAsync(d_grad, 0, gbytes, st), "cudaMemsetAsync");
         if (precision == OB_FP32) {
             check_cuda(cudaMemsetAsync(af.batch_pairs, 0, kAdjBatches * sizeof(unsigned long long), st), "memset");
+            check_cuda(cudaMemsetAsync(af.priv, 0, priv_bytes, st), "cudaMemsetAsync");
             using B = void (*)(AdjArgs<float>);
-            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, 256, smem_b, st>>>(af);
+            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, 256, 0, st>>>(af);
         } else {
             check_cuda(cudaMemsetAsync(ad.batch_pairs, 0, kAdjBatches * sizeof(unsigned long long), st), "memset");
+            check_cuda(cudaMemsetAsync(ad.priv, 0, priv_bytes, st), "cudaMemsetAsync");
             using B = void (*)(AdjArgs<double>);
-            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, 256, smem_b, st>>>(ad);
+            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, 256, 0, st>>>(ad);
         }
         check_cuda(cudaGetLastError(), "adj_backward launch");
     }

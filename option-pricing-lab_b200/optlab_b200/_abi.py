@@ -215,7 +215,7 @@ OB_ADJ_BATCHES = 32
 
 
 class ObAdjointRequest(C.Structure):
-    _fields_ = [("base", ObMcRequest), ("smoothing", C.c_double)]
+    _fields_ = [("base", ObMcRequest), ("smoothing", C.c_double), ("checkpoint", C.c_int)]
 
 
 class ObAdjointResult(C.Structure):

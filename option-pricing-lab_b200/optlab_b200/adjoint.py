@@ -24,13 +24,16 @@ from .engine import precision_code
 
 
 class AdjointPlan:
-    """A local-vol autocall request (OB_MODEL_PATHS, kinds 1, OB_PRODUCT_AUTOCALL) uploaded for adjoint runs."""
+    """A local-vol autocall request (OB_MODEL_PATHS, kinds 1, OB_PRODUCT_AUTOCALL) uploaded for adjoint runs.
+    checkpoint: the steps between the states the forward keeps for the backward (1: every step, the backward
+    recomputes nothing; 4: every fourth, a quarter of the memory; 0: every step up to 24 GiB of states)."""
 
-    def __init__(self, held, smoothing: float = 0.005, precision="fp32"):
+    def __init__(self, held, smoothing: float = 0.005, precision="fp32", checkpoint: int = 0):
         self._held = held
         rq = ObAdjointRequest()
         rq.base = held.struct
         rq.smoothing = float(smoothing)
+        rq.checkpoint = int(checkpoint)
         self._rq = rq
         self._p = C.c_void_p()
         check(load().ob_adjoint_plan_create(C.byref(rq), precision_code(precision), C.byref(self._p)))
@@ -122,7 +125,8 @@ def hats(points, nodes) -> np.ndarray:
 class VegaNodes:
     """Tent bumps of local volatility on node_T x node_k per name, for the rows of each name in a stacked table.
 
-    row_name[r] is the name a table row belongs to, row_T[r] its expiry, row_lo / row_inv_dx its log-strike grid."""
+    row_name[r] is the name a table row belongs to, row_T[r] its expiry, row_lo / row_inv_dx its log-strike grid.
+    The weights live on `device` (default: the current CUDA device when there is one, else the CPU)."""
 
     row_name: np.ndarray
     row_T: np.ndarray
@@ -131,9 +135,15 @@ class VegaNodes:
     n_x: int
     node_T: np.ndarray
     node_k: np.ndarray
+    device: object = None
 
     def __post_init__(self):
-        dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else torch.device("cpu")
+        if self.device is not None:
+            dev = torch.device(self.device)
+        elif torch.cuda.is_available():
+            dev = torch.device("cuda", torch.cuda.current_device())
+        else:
+            dev = torch.device("cpu")
         k = self.row_lo[:, None] + np.arange(self.n_x)[None, :] / self.row_inv_dx[:, None]
         self.phi = torch.tensor(hats(self.row_T, self.node_T), dtype=torch.float64, device=dev)  # (rows, E)
         psi = hats(k.ravel(), self.node_k).reshape(k.shape[0], self.n_x, -1)

@@ -150,3 +150,10 @@ def test_a_missing_device_is_an_engine_error_not_a_crash():
         pytest.skip("a device is present")
     with pytest.raises(_abi.EngineError, match="no CUDA device"):
         engine.mc_price(workloads.lv_phoenix(n_paths=64), "fp32")
+
+
+def test_an_adjoint_checkpoint_interval_other_than_0_1_or_4_is_refused():
+    from optlab_b200.adjoint import AdjointPlan
+
+    with pytest.raises(_abi.EngineError, match="checkpoint must be 0, 1 or 4"):
+        AdjointPlan(workloads.worst_of(n_paths=2**10, years=1.0).held, 0.005, "fp32", checkpoint=2)

@@ -146,3 +146,21 @@ def test_autograd_vegas_are_the_contracted_table_gradient():
         direct = nodes.contract(plan.gradient, _base(w)).cpu().numpy()
     assert np.allclose(g["vega"], direct, rtol=1e-12, atol=1e-15)
     assert g["vega"].shape == (3, 10, 15)
+
+
+@pytest.mark.parametrize("precision,rel", [("fp64", 1e-9), ("fp32", 2e-4)])
+def test_stored_states_and_recomputed_segments_give_the_same_greeks(precision, rel):
+    """checkpoint=1 stores every step and the backward recovers each step's noise from the stored states;
+    checkpoint=4 recomputes 4-step segments from their checkpoints and redraws the normals: the same gradient."""
+    w = _wo(n_paths=2**13)
+    nodes = _nodes(w)
+    with AdjointPlan(w.held, EPS, precision, checkpoint=1) as dense, \
+            AdjointPlan(w.held, EPS, precision, checkpoint=4) as sparse:
+        gd = autocall_greeks(w.held, nodes, EPS, plan=dense)
+        gs = autocall_greeks(w.held, nodes, EPS, plan=sparse)
+        bd, bs = dense.batch_pairs, sparse.batch_pairs
+    assert gd["price"] == gs["price"] and np.array_equal(gd["delta"], gs["delta"])
+    assert torch.equal(bd, bs)
+    scale = np.abs(gs["vega"]).max()
+    assert np.abs(gd["vega"] - gs["vega"]).max() <= rel * scale, np.abs(gd["vega"] - gs["vega"]).max() / scale
+

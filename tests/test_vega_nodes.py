@@ -10,7 +10,7 @@ from optlab_b200.adjoint import VegaNodes, hats
 
 def _nodes():
     w = workloads.worst_of(n_paths=64, years=1.0)
-    return w, VegaNodes(w.row_name, w.row_T, w.row_lo, w.row_inv_dx, w.n_x, w.node_T, w.node_k)
+    return w, VegaNodes(w.row_name, w.row_T, w.row_lo, w.row_inv_dx, w.n_x, w.node_T, w.node_k, device="cpu")
 
 
 def test_tent_weights_interpolate_and_sum_to_one():
