@@ -326,6 +326,18 @@ typedef struct {
     int call_mode;
     const double* rules;
     double* record;
+    /* Branched continuations (the inner paths of the issuer's dual bound, packages/structured/src/optlab/structured/
+       exercise.py:294-380): with branch = 1, one local-vol name and the staged local-vol kernel, pair p continues
+       outer path o = p / branch_pairs: up to step end branch_step both its legs follow that path's draws (path o of
+       an outer simulation of branch_outer pairs on branch_seed: pair o of it for o < branch_outer, else the
+       antithetic leg of pair o - branch_outer), after it the pair draws its own on the model's seed. pair_value
+       (host, n_pairs doubles, may be NULL; also without branch) receives each pair's average present value. */
+    int branch;
+    int branch_step;
+    long long branch_outer;
+    long long branch_pairs;
+    unsigned long long branch_seed;
+    double* pair_value;
 } ob_script_request;
 
 #define OB_RULE_STRIDE 224

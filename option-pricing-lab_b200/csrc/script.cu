@@ -66,6 +66,12 @@ struct ScriptDev {
     const int* call_state;      // n_calls x 4 registers
     const double* rules;        // n_calls x OB_RULE_STRIDE
     double* record;             // call_mode 1: 2 n_pairs x rec_stride
+    // branched continuations: up to step end branch_step, pair p follows outer path p / branch_pairs of an outer
+    // simulation of branch_outer pairs on the key (bk0, bk1)
+    int branch_step;
+    long long branch_outer, branch_pairs;
+    uint32_t bk0, bk1;
+    double* pair_value;         // n_pairs: each pair's average present value, or null
 };
 
 // One leg's state between events (its register file lives in local memory: it is touched only at events).
@@ -383,6 +389,7 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
         double y_pair = 0.0;
         if (active) {
             y_pair = 0.5 * (leg[0].pv + leg[1].pv);
+            if (d.pair_value) d.pair_value[base + lane] = y_pair;
             unsigned long long bp = 0, bc = 0, br = 0;
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
@@ -421,9 +428,12 @@ struct LvArgs {
     R top;
 };
 
-template <typename R, int N, int NW>
-__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0,
-                                                        uint32_t k1, double* __restrict__ partial) {
+// BRANCH: the pairs continue the paths of an outer simulation after step end d.branch_step (one leg per outer path:
+// before the branch both legs take the outer path's normals, the outer antithetic leg's with the sign flipped).
+template <typename R, int N, int NW, bool BRANCH>
+__global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
+    script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0, uint32_t k1,
+                     double* __restrict__ partial) {
     constexpr int C = N;
     constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);
     constexpr int NB = C * G / 4;
@@ -450,6 +460,13 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
          base += stride) {
         const bool active = base + lane < n_pairs;
         const uint64_t pair = static_cast<uint64_t>(active ? base + lane : n_pairs - 1);
+        uint64_t opair = 0;
+        R osign = R(1);
+        if (BRANCH) {
+            const long long o = static_cast<long long>(pair) / d.branch_pairs;  // the outer path continued
+            opair = static_cast<uint64_t>(o < d.branch_outer ? o : o - d.branch_outer);
+            osign = o < d.branch_outer ? R(1) : R(-1);
+        }
         LegState<R> leg[2];
         leg_init(d, leg[0]), leg_init(d, leg[1]);
         WinState<R, NW> win[2];
@@ -482,21 +499,34 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
         observe(0);
         for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) {
             R z[C * G];
+            const bool own = !BRANCH || i0 + G - 1 > d.branch_step;  // a step of the batch draws its own normals
+            if (own) {
 #pragma unroll
-            for (int k = 0; k < NB; ++k)
-                normals4<R>(pair, static_cast<uint64_t>(b) * NB + k, 0u, k0, k1, z[4 * k], z[4 * k + 1], z[4 * k + 2],
-                            z[4 * k + 3]);
+                for (int k = 0; k < NB; ++k)
+                    normals4<R>(pair, static_cast<uint64_t>(b) * NB + k, 0u, k0, k1, z[4 * k], z[4 * k + 1],
+                                z[4 * k + 2], z[4 * k + 3]);
+            }
+            R zo[BRANCH ? C * G : 1];
+            if (BRANCH && i0 <= d.branch_step) {  // a step of the batch follows the outer path
+#pragma unroll
+                for (int k = 0; k < NB; ++k)
+                    normals4<R>(opair, static_cast<uint64_t>(b) * NB + k, 0u, d.bk0, d.bk1, zo[4 * k], zo[4 * k + 1],
+                                zo[4 * k + 2], zo[4 * k + 3]);
+            }
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int i = i0 + g;
                 if (G > 1 && i > S) break;
                 const StepRec<R> st = s_step[i - 1];
+                const bool before = BRANCH && i <= d.branch_step;
+                const R* zs = before ? &zo[g * C] : &z[g * C];
+                const R sg0 = before ? osign : R(1), sg1 = before ? osign : R(-1);  // the legs' signs
                 R zc[N];
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     R acc = R(0);
 #pragma unroll
-                    for (int m = 0; m < N; ++m) acc += s_root[n * N + m] * z[g * C + m];
+                    for (int m = 0; m < N; ++m) acc += s_root[n * N + m] * zs[m];
                     zc[n] = acc;
                 }
 #pragma unroll
@@ -508,8 +538,13 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
                     const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
                     const Pair2<R> p0 = s_tab[ns.row + j0], p1 = s_tab[ns.row + j1];
                     const R v0 = p0.a + f0 * p0.b, v1 = p1.a + f1 * p1.b;
-                    x0[n] += v0 * st.hdt + (m_sqrt(v0) * st.sdt) * zc[n];
-                    x1[n] += v1 * st.hdt + (m_sqrt(v1) * st.sdt) * (-zc[n]);
+                    if (BRANCH) {
+                        x0[n] += v0 * st.hdt + (m_sqrt(v0) * st.sdt) * (sg0 * zc[n]);
+                        x1[n] += v1 * st.hdt + (m_sqrt(v1) * st.sdt) * (sg1 * zc[n]);
+                    } else {
+                        x0[n] += v0 * st.hdt + (m_sqrt(v0) * st.sdt) * zc[n];
+                        x1[n] += v1 * st.hdt + (m_sqrt(v1) * st.sdt) * (-zc[n]);
+                    }
                     y0[n] = x0[n] + ns.lf, y1[n] = x1[n] + ns.lf;
                 }
                 observe(i);
@@ -518,6 +553,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1) script_lv_kernel(
         double y_pair = 0.0;
         if (active) {
             y_pair = 0.5 * (leg[0].pv + leg[1].pv);
+            if (d.pair_value) d.pair_value[base + lane] = y_pair;
             unsigned long long bp = 0, bc = 0, br = 0;
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
@@ -543,21 +579,22 @@ template <typename R>
 using ScriptLvFn = void (*)(ScriptDev<R>, LvArgs<R>, long long, uint32_t, uint32_t, double*);
 
 template <typename R, int NW>
-ScriptLvFn<R> pick_lv_nw(int n) {
+ScriptLvFn<R> pick_lv_nw(int n, bool branch) {
+    if (branch) return n == 1 ? script_lv_kernel<R, 1, NW, true> : nullptr;  // the dual bound is single-name
     switch (n) {
-        case 1: return script_lv_kernel<R, 1, NW>;
-        case 2: return script_lv_kernel<R, 2, NW>;
-        case 3: return script_lv_kernel<R, 3, NW>;
-        case 4: return script_lv_kernel<R, 4, NW>;
-        case 5: return script_lv_kernel<R, 5, NW>;
+        case 1: return script_lv_kernel<R, 1, NW, false>;
+        case 2: return script_lv_kernel<R, 2, NW, false>;
+        case 3: return script_lv_kernel<R, 3, NW, false>;
+        case 4: return script_lv_kernel<R, 4, NW, false>;
+        case 5: return script_lv_kernel<R, 5, NW, false>;
         default: return nullptr;
     }
 }
 
 // Kernels for up to 2 windows (most products: a knock-in window or two) and up to 8.
 template <typename R>
-ScriptLvFn<R> pick_lv(int n, int n_windows) {
-    return n_windows <= 2 ? pick_lv_nw<R, 2>(n) : pick_lv_nw<R, kMaxWindows>(n);
+ScriptLvFn<R> pick_lv(int n, int n_windows, bool branch) {
+    return n_windows <= 2 ? pick_lv_nw<R, 2>(n, branch) : pick_lv_nw<R, kMaxWindows>(n, branch);
 }
 
 // The staged blob of the local-vol path, or false when it does not apply (a name not local vol, more than five
@@ -674,6 +711,14 @@ void check_script(const ob_script_request& rq) {
         for (int k = rq.win_fix0[w]; k < rq.win_fix0[w + 1]; ++k)
             if (rq.fix_step[k] < 0 || rq.fix_step[k] > S || (k > rq.win_fix0[w] && rq.fix_step[k] <= rq.fix_step[k - 1]))
                 invalid("window fixing steps must increase within 0 .. n_steps");
+    }
+    if (rq.branch != 0 && rq.branch != 1) invalid("branch must be 0 or 1");
+    if (rq.branch) {
+        if (n != 1 || rq.model.model != OB_MODEL_PATHS || rq.model.kind[0] != 1)
+            invalid("a branched run continues one local-vol name");
+        if (rq.branch_step < 0 || rq.branch_step > S) invalid("branch_step must be within 0 .. n_steps");
+        if (rq.branch_outer < 1 || rq.branch_pairs < 1 || rq.model.n_pairs != 2 * rq.branch_outer * rq.branch_pairs)
+            invalid("a branched run has branch_pairs pairs for each of the 2 branch_outer outer paths");
     }
     if (rq.n_calls < 0 || rq.n_state < 0 || rq.n_state > kMaxState) invalid("n_calls >= 0 and n_state 0 to 4");
     if (rq.call_mode < 0 || rq.call_mode > 2) invalid("call_mode must be 0, 1 or 2");
@@ -820,6 +865,10 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
         d.record = arena.alloc<double>(rec_count);
         check_cuda(cudaMemset(d.record, 0, rec_count * sizeof(double)), "cudaMemset");
     }
+    d.branch_step = rq.branch ? rq.branch_step : -1;
+    d.branch_outer = rq.branch_outer, d.branch_pairs = rq.branch_pairs;
+    d.bk0 = static_cast<uint32_t>(rq.branch_seed), d.bk1 = static_cast<uint32_t>(rq.branch_seed >> 32);
+    if (rq.pair_value) d.pair_value = arena.alloc<double>(static_cast<size_t>(mq.n_pairs));
     d.eps = static_cast<R>(rq.smoothing);
     d.red_tol = rq.smoothing == 0.0 ? 1e-12 : (sizeof(R) == 8 ? 1e-9 : 1e-5);
     d.bad = arena.alloc<unsigned long long>(3);
@@ -829,7 +878,8 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     for (int i = 0; i <= S; ++i) sched[i] = make_int2(event_at[i], static_cast<int>(fix_mask[i]));
     LvArgs<R> lv{};
     const bool fast = pack_lv<R>(rq, sched, arena, lv);
-    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n, rq.n_windows))
+    if (rq.branch && !fast) invalid("a branched run needs the staged local-vol kernel (its tables too large)");
+    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n, rq.n_windows, rq.branch != 0))
                           : reinterpret_cast<const void*>(pick_script<R>(mq.model, n, rq.n_windows));
     const int block = fast ? 512 : 128;
     const size_t smem = fast ? static_cast<size_t>(lv.smem_blob) : 0;
@@ -861,6 +911,10 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     check_cuda(cudaMemcpy(bad, d.bad, sizeof bad, cudaMemcpyDeviceToHost), "copy counts");
     if (rec_count) check_cuda(cudaMemcpy(rq.record, d.record, rec_count * sizeof(double), cudaMemcpyDeviceToHost),
                               "copy record");
+    if (rq.pair_value)
+        check_cuda(cudaMemcpy(rq.pair_value, d.pair_value, static_cast<size_t>(mq.n_pairs) * sizeof(double),
+                              cudaMemcpyDeviceToHost),
+                   "copy pair values");
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0), cudaEventDestroy(e1);

@@ -316,6 +316,12 @@ class ObScriptRequest(C.Structure):
         ("call_mode", C.c_int),
         ("rules", _dp),
         ("record", _dp),
+        ("branch", C.c_int),
+        ("branch_step", C.c_int),
+        ("branch_outer", C.c_longlong),
+        ("branch_pairs", C.c_longlong),
+        ("branch_seed", C.c_ulonglong),
+        ("pair_value", _dp),
     ]
 
 

@@ -184,3 +184,91 @@ def price(compiled, make_sim, n_pairs: int, seed: int, discount, precision="fp32
     policy = fit(rec, [k for k, _ in compiled.calls], pay_d)
     held = sc.script_request(compiled, make_sim(n_pairs, seed), discount, call_mode=2, rules=policy.pack(n_state))
     return sc.run(held, precision), policy
+
+
+DUAL_OUTER_KEY = 0xD0A1B0D5  # the dual bound's outer paths draw on seed ^ this
+DUAL_INNER_KEY = 0x1A2B3C4D  # the continuations from call c draw on seed ^ this ^ (c + 1)
+
+
+def decisions(policy: Policy, rec: PilotRecord) -> np.ndarray:
+    """(calls, paths): 1 where the policy calls at a call the path reaches, the rule's continuation of the state
+    above the amount (exercise.py: Policy.decisions); 0 at calls without a rule."""
+    out = np.zeros_like(rec.amount)
+    for c, rule in enumerate(policy.rules):
+        if rule is not None:
+            out[c] = (rule.continuation(rec.state[c]) > rec.amount[c]).astype(float)
+    return out
+
+
+def dual_recursion(pre, post, mask, alive, amount, decide, call_events, call_discount, H, price0):
+    """The martingale dual of the issuer's (minimising) problem, exercise.py:353-372. pre, post: (events, paths)
+    discounted flows of the uncalled outer paths before and after each event's call statement; mask, alive, amount,
+    decide: (calls, paths); call_events[c]: the event of call c, call_discount[c] the discount factor of its
+    payment; H[c]: (paths,) the policy's value from call c on, not called at c or before (mean of the
+    continuations). Returns per path min_j (G_j - M_j), G_j the note's flows if called at call j (never: the last
+    H), M the martingale of the policy's value started at price0."""
+    pv = pre + post
+    n = pv.shape[1]
+    M = np.zeros(n)
+    best = np.full(n, np.inf)
+    previous = np.full(n, float(price0))
+    for c, k in enumerate(call_events):
+        reach = mask[c] * alive[c]
+        g = np.where(reach > 0, pv[:k].sum(axis=0) + pre[k] + call_discount[c] * reach * amount[c], np.inf)
+        called = decide[c] * (reach > 0)
+        level = np.where(called > 0, g, H[c])
+        M = M + level - previous
+        best = np.minimum(best, g - M)
+        previous = H[c]
+    return np.minimum(best, previous - M)
+
+
+def dual_bound(compiled, make_sim, policy: Policy, price0: float, price_se: float, seed: int, discount,
+               n_outer: int = 1000, n_inner: int = 200, precision="fp64") -> dict:
+    """Andersen-Broadie for the issuer, who minimises (exercise.py:294-380): the note's value is at least
+    E[min_j (G_j - M_j)], G_j the note's flows if called at call date j, M the martingale of the policy's own value,
+    whose conditional expectations come from n_inner continuations of each of n_outer outer paths branched at each
+    call date. On the device: the outer paths are a recorded uncalled run (call mode 1, n_outer / 2 antithetic
+    pairs on seed ^ DUAL_OUTER_KEY); the continuations from call c are one branched run (n_outer x n_inner / 2
+    pairs, each following its outer path's draws up to the call's step end, its own after it) that applies the
+    policy after c and never at c or before, and returns each pair's value. price0 and price_se are the policy's
+    price and SE (the pricing run's). A single local-vol name (the reference's bound needs a model without a
+    variance process and a single name); returns lower, lower_se, gap, gap_se, outer, inner (the SE of the gap on
+    the outer pairs' averages)."""
+    if not compiled.calls:
+        raise ValueError("no dual bound without an issuer call")
+    if len(compiled.names) != 1:
+        raise ValueError("no dual bound for a basket")
+    n_outer += n_outer % 2
+    n_inner += n_inner % 2
+    P, per = n_outer // 2, n_inner // 2
+    n_state = len(compiled.calls[0][1])
+    n_ev = len(compiled.event_times)
+    outer_seed = (seed ^ DUAL_OUTER_KEY) & (2**64 - 1)
+    outer = sc.script_request(compiled, make_sim(P, outer_seed), discount, call_mode=1)
+    s = outer.struct.model
+    if s.model != 0 or s.kind[0] != 1:
+        raise ValueError("no dual bound for a model with a variance process (local vol only)")
+    sc.run(outer, precision)
+    rec = PilotRecord.from_device(outer.keep[1]["record"], n_ev, len(compiled.calls), n_state)
+    ev_step = outer.keep[1]["event_step"]
+    pay_d = [float(discount(t)) if t is not None and t > 0 else 0.0 for t in compiled.pay_times]
+    call_events = [k for k, _ in compiled.calls]
+    call_disc = [pay_d[k] if pay_d[k] > 0 else 1.0 for k in call_events]
+    packed = policy.pack(n_state)
+    H = []
+    for c, k in enumerate(call_events):
+        rules = packed.copy()
+        rules[: c + 1] = 0.0  # not called at c nor before
+        inner_seed = (seed ^ DUAL_INNER_KEY ^ (c + 1)) & (2**64 - 1)
+        inner = sc.script_request(compiled, make_sim(n_outer * per, inner_seed), discount, call_mode=2, rules=rules,
+                                  branch=(int(ev_step[k]), P, per, outer_seed))
+        sc.run(inner, precision)
+        H.append(inner.keep[1]["pair_value"].reshape(n_outer, per).mean(axis=1))
+    best = dual_recursion(rec.pre, rec.post, rec.mask, rec.alive, rec.amount, decisions(policy, rec), call_events,
+                          call_disc, H, price0)
+    pairs = 0.5 * (best[:P] + best[P:])
+    gap = float(price0 - pairs.mean())
+    gap_se = float(pairs.std(ddof=1) / np.sqrt(P))
+    return {"lower": float(price0) - gap, "lower_se": float(np.hypot(price_se, gap_se)), "gap": gap,
+            "gap_se": gap_se, "outer": n_outer, "inner": n_inner}

@@ -935,12 +935,16 @@ class ScriptHeld:
     compiled: Compiled
 
 
-def script_request(compiled: Compiled, sim, discount, call_mode: int = 0, rules=None) -> ScriptHeld:
+def script_request(compiled: Compiled, sim, discount, call_mode: int = 0, rules=None, pair_values: bool = False,
+                   branch=None) -> ScriptHeld:
     """The device request of a compiled script on a simulation: `sim` is an mc_request (Held) whose model part
     (model, names in the script's underlying order, grid, tables, spots, log-forwards) is simulated, its product part
     ignored; `discount(t)` gives the discount factor of a payment at t. Every observation time must be a step end.
     call_mode: 0 the issuer never calls, 1 record a pilot (the held `record` array, filled by `run`), 2 apply
-    `rules` ((n_calls, OB_RULE_STRIDE), optlab_b200.exercise.Policy.pack)."""
+    `rules` ((n_calls, OB_RULE_STRIDE), optlab_b200.exercise.Policy.pack). pair_values: keep each pair's average
+    present value (the held `pair_value` array). branch = (step, outer_pairs, pairs_per_outer, outer_seed): the
+    pairs continue the paths of an outer simulation of outer_pairs pairs on outer_seed after step end `step`
+    (pairs_per_outer pairs a path, path o < outer_pairs being leg 0 of outer pair o, the others leg 1)."""
     s = sim.struct
     S = s.n_steps
     if s.n_names != len(compiled.names):
@@ -981,6 +985,8 @@ def script_request(compiled: Compiled, sim, discount, call_mode: int = 0, rules=
         arrays["rules"] = rules.ravel()
     if call_mode == 1:
         arrays["record"] = np.zeros((2 * s.n_pairs, 2 * len(ev_step) + n_calls * (3 + n_state)))
+    if pair_values or branch is not None:
+        arrays["pair_value"] = np.zeros(s.n_pairs)
     r = ObScriptRequest()
     r.model = s
     r.n_code = compiled.code.shape[0]
@@ -990,6 +996,10 @@ def script_request(compiled: Compiled, sim, discount, call_mode: int = 0, rules=
     r.n_windows = len(win_name)
     r.smoothing = compiled.smoothing
     r.n_calls, r.n_state, r.call_mode = n_calls, n_state, int(call_mode)
+    if branch is not None:
+        step, outer, per, seed = branch
+        r.branch, r.branch_step, r.branch_outer, r.branch_pairs, r.branch_seed = 1, int(step), int(outer), int(per), \
+            int(seed) & (2**64 - 1)
     for k, a in arrays.items():
         ctype = C.c_int if a.dtype == np.int32 else C.c_double
         setattr(r, k, a.ctypes.data_as(C.POINTER(ctype)) if a.size else None)

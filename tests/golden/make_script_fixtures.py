@@ -2,7 +2,10 @@
 script pipeline (optlab.structured.script: parse, validate, build_timeline, Evaluator) on seeded synthetic fixings,
 with each path's present value (cashflows.py:30-41, flat discount exp(-r t)); and tests/golden/script_callable.json:
 a callable note's pilot record, the policy the reference fits on it (optlab.structured.exercise.fit) and that policy
-applied to other paths.
+applied to other paths; and tests/golden/script_dual.json: the reference's dual bound of a callable reverse convertible
+under Black-Scholes (optlab.structured.exercise.dual_bound) on 40 outer paths with 16 continuations each, with the
+outer paths and continuations it drew, the policy it used and its result, plus the reference's PDE value of the note
+(tests/helpers/_callable_refs.py: callable_note) and the reference's bound at 1000 x 200.
 
 The fixings are lognormal paths of every underlying on the script's simulation times (the valuation date is the
 spot); the fake scenario answers `spot(name, t)` and `fixings(name, times)` from them. A case whose evaluation the
@@ -343,6 +346,106 @@ def callable_case(rng) -> None:
     }
     (HERE / "script_callable.json").write_text(json.dumps(case))
     print("wrote", HERE / "script_callable.json", "in-sample", policy.in_sample, "priced", pv.mean())
+    dual_case(rng)
+
+
+CALLABLE_RC = """
+underlying SPX
+param c = 0.06
+event t=0.5 pay t=0.5
+  pay c * 0.5 as coupon
+  call pay 1
+end
+event t=1 pay t=1
+  pay c * 0.5 as coupon
+  call pay 1
+end
+event t=1.5 pay t=1.5
+  pay c * 0.5 as coupon
+  call pay 1
+end
+event t=2 pay t=2
+  pay c * 0.5 as coupon
+  pay min(SPX / 100, 1) as redemption
+end
+"""
+DUAL_R, DUAL_Q, DUAL_VOL = 0.04, 0.01, 0.2
+
+
+def dual_case(rng) -> None:
+    """tests/golden/script_dual.json (see the module docstring)."""
+    import optlab.core.models as core_models
+    from optlab.core import BlackScholesModel, Market
+    from optlab.structured import exercise
+    from optlab.structured.script.evaluator import Evaluator
+    from optlab.structured.script.parser import parse
+    from optlab.structured.script.timeline import Clock, build_timeline
+    from optlab.structured.script.validate import validate
+
+    sys.path.insert(0, str(Path(exercise.__file__).resolve().parents[5] / "tests" / "helpers"))
+    from _callable_refs import callable_note
+
+    program = validate(parse(CALLABLE_RC))
+    tl = build_timeline(program, Clock(None))
+    times = np.asarray(tl.sim_times, float)
+    dts = np.diff(np.concatenate([[0.0], times]))
+    model, market = BlackScholesModel(DUAL_VOL), Market.flat(100.0, DUAL_R, DUAL_Q)
+    disc = lambda t: float(np.exp(-DUAL_R * t))  # noqa: E731
+
+    def paths(n):
+        z = rng.standard_normal((n, len(times)))
+        drift = (DUAL_R - DUAL_Q - 0.5 * DUAL_VOL**2) * dts
+        return 100.0 * np.exp(np.cumsum(drift + DUAL_VOL * np.sqrt(dts) * z, axis=1))
+
+    def pvs(out):
+        pv = np.zeros(out.n_paths)
+        for (t, _tag), f in out.flows.items():
+            if t is not None and t > 0:
+                pv = pv + disc(t) * f
+        return pv
+
+    from optlab.structured.scenario import Scenario as RefScenario
+
+    pilot = Evaluator(program, tl, {}, 0.0, True).run(RefScenario("SPX", times, paths(4000), 100.0))
+    policy = exercise.fit(pilot, disc)
+    priced = policy.apply(Evaluator(program, tl, {}, 0.0, True).run(RefScenario("SPX", times, paths(4000), 100.0)))
+    pv = pvs(priced)
+    price0, price_se = float(pv.mean()), float(pv.std(ddof=1) / np.sqrt(len(pv)))
+    drawn = {"outer": None, "tails": []}
+    simulate, continued = core_models.simulate, exercise._continued
+
+    def keep_outer(*a, **k):
+        drawn["outer"] = simulate(*a, **k)
+        return drawn["outer"]
+
+    def keep_tail(*a, **k):
+        tail = continued(*a, **k)
+        drawn["tails"].append(tail)
+        return tail
+
+    core_models.simulate, exercise._continued = keep_outer, keep_tail
+    try:
+        small = exercise.dual_bound(model, market, "SPX", tl, program, {}, 100.0, None, policy, disc, price0,
+                                    price_se, 11, n_outer=40, n_inner=16)
+    finally:
+        core_models.simulate, exercise._continued = simulate, continued
+    big = exercise.dual_bound(model, market, "SPX", tl, program, {}, 100.0, None, policy, disc, price0, price_se, 11,
+                              n_outer=1000, n_inner=200)
+    pde = callable_note(lambda p: np.minimum(p, 1.0), 2.0, [(t, 0.03) for t in (0.5, 1.0, 1.5, 2.0)],
+                        [(0.5, 1.0), (1.0, 1.0), (1.5, 1.0)], r=DUAL_R, q=DUAL_Q, vol=DUAL_VOL)
+    rules = []
+    for k in sorted(pilot.exercise.calls):
+        r = policy.rules[k]
+        rules.append(None if r is None else {"mean": r.mean, "scale": r.scale, "powers": r.powers,
+                                             "knots": r.knots, "coef": r.coef})
+    case = {
+        "script": CALLABLE_RC, "times": times.tolist(), "spot0": {"SPX": 100.0}, "r": DUAL_R, "q": DUAL_Q,
+        "vol": DUAL_VOL, "rules": rules, "price0": price0, "price_se": price_se,
+        "outer": drawn["outer"].tolist(), "tails": [t.tolist() for t in drawn["tails"]], "n_inner": 16,
+        "small": small, "big": big, "pde": float(pde),
+    }
+    (HERE / "script_dual.json").write_text(json.dumps(case))
+    print("wrote", HERE / "script_dual.json", "price0", price0, "small", small, "big", big, "pde", pde)
 
 
 if __name__ == "__main__":
