@@ -43,7 +43,7 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0
 # Executed warp instructions per path-step of the dominant kernel, measured by ncu (smsp__inst_executed.sum of one
 # launch divided by its path-steps) and recorded under profiles/. The issue roofline below multiplies it by the live
 # path-step rate. A launch's instruction count does not depend on timing, so a profiled launch gives it exactly.
-INST_PER_PATH_STEP = {"lv_phoenix": 1.582, "heston_qe": 20.3}
+INST_PER_PATH_STEP = {"lv_phoenix": 1.496, "heston_qe": 20.3}
 # DRAM bytes (read + written) of one profiled launch of the dominant kernel: the packed inputs, read once from HBM
 # and then from L2; the loop keeps its state in registers, so the figure does not grow with the path count.
 DRAM_PER_LAUNCH = {"lv_phoenix": 119296, "heston_qe": 44288}

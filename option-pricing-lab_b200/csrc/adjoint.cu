@@ -190,7 +190,7 @@ __device__ __forceinline__ Pair2<double> load_pair(const Pair2<double>* p) {
 template <typename R>
 __device__ __forceinline__ LvStep<R> lv_read(const AdjArgs<R>& a, const NameStep<R>& ns, R x) {
     LvStep<R> s;
-    R u = (x - ns.lo) * ns.inv_dx;
+    R u = table_u(ns, x);
     const bool inside = u > R(0) && u < a.top;
     u = m_min(m_max(u, R(0)), a.top);
     const int j = static_cast<int>(u);
@@ -674,7 +674,7 @@ void AdjPlan::build(const ob_adjoint_request& r) {
             std::memset(&e, 0, sizeof e);
             const int row = rq.step_row[static_cast<size_t>(k) * S + (i - 1)];
             row_ix[static_cast<size_t>(i - 1) * n + k] = row;
-            e.lo = static_cast<R>(rq.row_lo[row]);
+            e.org = name_step_org<R>(rq.row_lo[row], rq.row_inv_dx[row]);
             e.inv_dx = static_cast<R>(rq.row_inv_dx[row]);
             e.lf = static_cast<R>(rq.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
             e.row = row * (rq.n_x - 1);

@@ -114,6 +114,11 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
     const R* s_trig = reinterpret_cast<const R*>(sm + a.off.ln_trig);
     const double* s_disc = reinterpret_cast<const double*>(sm + a.off.obs_disc);
     const int S = a.n_steps;
+    // the correlation root: in registers for one or two names, read from shared memory for more (registers spill)
+    constexpr bool kRootRegs = N <= 2;
+    R rt[kRootRegs ? N * N : 1];
+#pragma unroll
+    for (int k = 0; k < (kRootRegs ? N * N : 0); ++k) rt[k] = s_root[k];
 
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n_pairs;
@@ -157,7 +162,7 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                     for (int n = 0; n < N; ++n) {
                         R acc = R(0);
 #pragma unroll
-                        for (int b = 0; b < N; ++b) acc += s_root[n * N + b] * zs[b];
+                        for (int b = 0; b < N; ++b) acc += (kRootRegs ? rt[n * N + b] : s_root[n * N + b]) * zs[b];
                         zc[n] = acc;
                     }
                     if (VAR) {
@@ -167,21 +172,21 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                             if (a.same) {
                                 R acc = R(0);
 #pragma unroll
-                                for (int b = 0; b < N; ++b) acc += s_root[n * N + b] * zr[b];
+                                for (int b = 0; b < N; ++b) acc += (kRootRegs ? rt[n * N + b] : s_root[n * N + b]) * zr[b];
                                 wc[n] = acc;
                             } else {
                                 wc[n] = zr[n];
                             }
                         }
                     }
-                    R w0 = R(1e30), w1 = R(1e30);
+                    R w0 = R(0), w1 = R(0);  // the worst log performance: the first name's, then the minimum
 #pragma unroll
                     for (int n = 0; n < N; ++n) {
                         const NameStep<R> ns = s_ns[(i - 1) * N + n];
                         R var0, var1, vp0 = R(0), vp1 = R(0);
                         if (VAR) vp0 = m_max(v0[n], R(0)), vp1 = m_max(v1[n], R(0));
                         if (TABLE) {
-                            R u0 = (x0[n] - ns.lo) * ns.inv_dx, u1 = (x1[n] - ns.lo) * ns.inv_dx;
+                            R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
                             u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
                             const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
                             const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
@@ -197,9 +202,11 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                             v0[n] += h[1] * (h[2] - vp0) * st.dt + h[3] * (m_sqrt(vp0) * st.sdt) * zv;
                             v1[n] += h[1] * (h[2] - vp1) * st.dt + h[3] * (m_sqrt(vp1) * st.sdt) * (-zv);
                         }
-                        x0[n] += var0 * st.hdt + (m_sqrt(var0) * st.sdt) * zc[n];
-                        x1[n] += var1 * st.hdt + (m_sqrt(var1) * st.sdt) * (-zc[n]);
-                        w0 = m_min(w0, x0[n] + ns.lf), w1 = m_min(w1, x1[n] + ns.lf);
+                        const R zd = st.sdt * zc[n];  // sqrt(dt) z, the legs' +-
+                        x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
+                        x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
+                        if (n == 0) w0 = x0[n] + ns.lf, w1 = x1[n] + ns.lf;
+                        else w0 = m_min(w0, x0[n] + ns.lf), w1 = m_min(w1, x1[n] + ns.lf);
                     }
                     lp0 = w0, lp1 = w1;
                 }
@@ -413,7 +420,7 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
                 r.lf = static_cast<R>(rq.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
                 if (table) {
                     const int row = rq.step_row[static_cast<size_t>(k) * S + (i - 1)];
-                    r.lo = static_cast<R>(rq.row_lo[row]);
+                    r.org = name_step_org<R>(rq.row_lo[row], rq.row_inv_dx[row]);
                     r.inv_dx = static_cast<R>(rq.row_inv_dx[row]);
                     r.row = row * (rq.n_x - 1);
                 }

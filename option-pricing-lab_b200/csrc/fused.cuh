@@ -15,18 +15,33 @@
 
 namespace ob {
 
+// org is the row's origin in the form its interpolation coordinate u = table_u(step, x) uses: -lo inv_dx in float
+// (u = x inv_dx + org, one multiply-add), lo in double (u = (x - lo) inv_dx, the reference's order).
 template <typename R>
 struct alignas(16) NameStep;
 template <>
 struct alignas(16) NameStep<float> {
-    float lo, inv_dx, lf;
+    float org, inv_dx, lf;
     int row;  // first (y_i, y_i+1) pair of the step's table row
 };
 template <>
 struct alignas(16) NameStep<double> {
-    double lo, inv_dx, lf;
+    double org, inv_dx, lf;
     int row, pad;
 };
+
+__host__ __device__ inline float name_step_org(double lo, double inv_dx, float*) {
+    return static_cast<float>(-lo * inv_dx);
+}
+__host__ __device__ inline double name_step_org(double lo, double, double*) { return lo; }
+// The origin to store for a row starting at lo with 1 / dx = inv_dx.
+template <typename R>
+__host__ __device__ inline R name_step_org(double lo, double inv_dx) {
+    return name_step_org(lo, inv_dx, static_cast<R*>(nullptr));
+}
+
+__device__ __forceinline__ float table_u(const NameStep<float>& s, float x) { return fmaf(x, s.inv_dx, s.org); }
+__device__ __forceinline__ double table_u(const NameStep<double>& s, double x) { return (x - s.org) * s.inv_dx; }
 
 // One table interval: the value at its left point and the increment to the right one, so that an interpolation is
 // one multiply-add (y + w dy, the reference's y_i (1 - w) + y_i+1 w up to rounding).

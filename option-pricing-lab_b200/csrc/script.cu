@@ -455,6 +455,11 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
     const R* s_lf0 = reinterpret_cast<const R*>(sm + a.off.lf0);
     const int S = d.n_steps;
     const WinMeta<NW> meta = win_meta<R, NW>(d);
+    // the correlation root: in registers for one or two names, read from shared memory for more (registers spill)
+    constexpr bool kRootRegs = N <= 2;
+    R rt[kRootRegs ? N * N : 1];
+#pragma unroll
+    for (int k = 0; k < (kRootRegs ? N * N : 0); ++k) rt[k] = s_root[k];
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n_pairs;
          base += stride) {
@@ -526,25 +531,24 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
                 for (int n = 0; n < N; ++n) {
                     R acc = R(0);
 #pragma unroll
-                    for (int m = 0; m < N; ++m) acc += s_root[n * N + m] * zs[m];
+                    for (int m = 0; m < N; ++m) acc += (kRootRegs ? rt[n * N + m] : s_root[n * N + m]) * zs[m];
                     zc[n] = acc;
                 }
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     const NameStep<R> ns = s_ns[(i - 1) * N + n];
-                    R u0 = (x0[n] - ns.lo) * ns.inv_dx, u1 = (x1[n] - ns.lo) * ns.inv_dx;
+                    R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
                     u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
                     const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
                     const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
                     const Pair2<R> p0 = s_tab[ns.row + j0], p1 = s_tab[ns.row + j1];
                     const R v0 = p0.a + f0 * p0.b, v1 = p1.a + f1 * p1.b;
-                    if (BRANCH) {
-                        x0[n] += v0 * st.hdt + (m_sqrt(v0) * st.sdt) * (sg0 * zc[n]);
-                        x1[n] += v1 * st.hdt + (m_sqrt(v1) * st.sdt) * (sg1 * zc[n]);
-                    } else {
-                        x0[n] += v0 * st.hdt + (m_sqrt(v0) * st.sdt) * zc[n];
-                        x1[n] += v1 * st.hdt + (m_sqrt(v1) * st.sdt) * (-zc[n]);
-                    }
+                    // sqrt(dt) z with the legs' signs (+1, -1 but before a branch), the step's multiply-add written
+                    // out: the same arithmetic in every instantiation, so a branch at step 0 is an ordinary run bit
+                    // for bit
+                    const R zd = st.sdt * zc[n], z0 = sg0 * zd, z1 = sg1 * zd;
+                    x0[n] += m_fma(m_sqrt(v0), z0, v0 * st.hdt);
+                    x1[n] += m_fma(m_sqrt(v1), z1, v1 * st.hdt);
                     y0[n] = x0[n] + ns.lf, y1[n] = x1[n] + ns.lf;
                 }
                 observe(i);
@@ -627,7 +631,7 @@ bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, Device
             std::memset(&r, 0, sizeof r);
             const int row = q.step_row[static_cast<size_t>(k) * S + (i - 1)];
             r.lf = static_cast<R>(q.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
-            r.lo = static_cast<R>(q.row_lo[row]), r.inv_dx = static_cast<R>(q.row_inv_dx[row]);
+            r.org = name_step_org<R>(q.row_lo[row], q.row_inv_dx[row]), r.inv_dx = static_cast<R>(q.row_inv_dx[row]);
             r.row = row * (q.n_x - 1);
         }
     a.off.name_step = put(ns.data(), ns.size() * sizeof(NameStep<R>));
