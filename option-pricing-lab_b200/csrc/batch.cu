@@ -7,8 +7,10 @@
 // kernel per trade class (local vol with N = 1..5 names or Heston QE, ladder or autocall), the kernels on their own
 // streams inside one graph, so that large and small trades fill the GPU together. A base simulation evaluates the base
 // and every spot scenario at once: the path keeps its observation log-performances and extremes, and a spot move is
-// a shift of them (the local vol is in log-moneyness). A vol scenario reads the table as (sigma + shift + tilt k)^2,
-// floored at 1 % vol, on the same random numbers. A carry scenario (a move of the rate, discounting included, or of
+// a shift of them (the local vol is in log-moneyness). A vol scenario reads its own copy of the tables, made once on
+// the host with every node moved to (sigma + shift + tilt k)^2, floored at 1 % vol (1 + n_vol copies of the pool,
+// 42 MB in float for the benchmark's book: L2-sized), on the same random numbers; the step is then the fused
+// kernel's (one table read, one multiply-add). A carry scenario (a move of the rate, discounting included, or of
 // the dividend yield) also rides on the base simulation, as the reference's forward ratio F'(t) / F(t) (:8-11): the
 // path keeps its extremes and daily low again under each carry's drift (Delta t per step), and the payments take
 // the moved discount. A correlation scenario re-simulates the multi-name local-vol trades on a moved root, on the
@@ -51,9 +53,9 @@ struct BTrade {
 template <typename R>
 struct BDev {
     const BTrade<R>* trades;
-    const Pair2<R>* sig;  // pool rows x (n_x - 1): (sigma_i, sigma_i+1)
-    const R* row_lo;
-    const R* row_dx;      // 1 / inv_dx
+    const Pair2<R>* tab;  // (1 + n_vol) x pool rows x (n_x - 1): (var_i, var_i+1 - var_i), base then each vol move
+    long long tab_stride; // pool rows x (n_x - 1)
+    const R* row_org;     // the row's origin in table_u's form (name_step_org)
     const R* row_inv_dx;
     const int* row_of;    // step -> expiry row
     const R* root;
@@ -65,8 +67,6 @@ struct BDev {
     const R* ln_trig;
     const double* obs_disc;
     const R* ln_spot;     // n_spot: ln(1 + spot move)
-    const R* vol_shift;
-    const R* vol_tilt;
     const double* obs_carry_df;  // n_carry x observation pool: exp(-rate move t_obs)
     R carry_dt[kBatchMaxCarry];  // per carry: the drift move (rate - dividend) times dt
     int n_spot, n_carry, n_vol, n_obs_pool, n_exp, n_x;
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
             for (int k = threadIdx.x; k < N * N; k += blockDim.x) s_root[k] = d.root[root + k];
         }
         __syncthreads();
-        const R vs = shocked ? d.vol_shift[sim - 1] : R(0), vt = shocked ? d.vol_tilt[sim - 1] : R(0);
+        const Pair2<R>* tab = d.tab + (shocked ? sim : 0) * d.tab_stride;
         const long long p0 = static_cast<long long>(tile) * d.tile;
         const long long p1 = min(p0 + d.tile, t.n_pairs);
         const int S = t.n_steps;
@@ -275,23 +275,19 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
 #pragma unroll
                             for (int m = 0; m < N; ++m) zc += s_root[n * N + m] * z[g * C + m];
                             const int row = t.row0 + n * d.n_exp + erow;
-                            const R lo = d.row_lo[row], inv = d.row_inv_dx[row];
+                            const R org = d.row_org[row], inv = d.row_inv_dx[row];
+                            const Pair2<R>* trow = tab + static_cast<long long>(row) * (d.n_x - 1);
+                            const R zd = d.sdt * zc;  // sqrt(dt) z, the legs' +-
 #pragma unroll
                             for (int leg = 0; leg < 2; ++leg) {
                                 R& x = leg ? x1[n] : x0[n];
-                                R u = (x - lo) * inv;
+                                R u = table_u(org, inv, x);
                                 u = m_min(m_max(u, R(0)), d.top);
                                 const int j = static_cast<int>(u);
                                 const R w = u - static_cast<R>(j);
-                                const Pair2<R> s = d.sig[row * (d.n_x - 1) + j];
-                                R s0 = s.a, s1 = s.b;
-                                if (shocked) {
-                                    const R k = lo + static_cast<R>(j) * d.row_dx[row];
-                                    s0 = m_max(s0 + vs + vt * k, R(0.01));
-                                    s1 = m_max(s1 + vs + vt * (k + d.row_dx[row]), R(0.01));
-                                }
-                                const R var = s0 * s0 + w * (s1 * s1 - s0 * s0);
-                                x += var * d.hdt + (m_sqrt(var) * d.sdt) * (leg ? -zc : zc);
+                                const Pair2<R> p = trow[j];
+                                const R var = p.a + w * p.b;
+                                x += m_fma(leg ? -m_sqrt(var) : m_sqrt(var), zd, var * d.hdt);
                                 if (leg) lp1 = m_min(lp1, x + lf);
                                 else lp0 = m_min(lp0, x + lf);
                             }
@@ -546,19 +542,30 @@ void Batch::build(const ob_batch_request& rq) {
     }
     d.row_of = arena.put<int>(row_of.data(), row_of.size());
     if (max_row > 0) {
-        std::vector<Pair2<R>> sig(static_cast<size_t>(max_row) * (rq.n_x - 1));
-        std::vector<R> dx(max_row);
-        for (int r = 0; r < max_row; ++r) {
-            for (int k = 0; k + 1 < rq.n_x; ++k)
-                sig[static_cast<size_t>(r) * (rq.n_x - 1) + k] = {
-                    static_cast<R>(std::sqrt(rq.table[static_cast<size_t>(r) * rq.n_x + k])),
-                    static_cast<R>(std::sqrt(rq.table[static_cast<size_t>(r) * rq.n_x + k + 1]))};
-            dx[r] = static_cast<R>(1.0 / rq.row_inv_dx[r]);
-        }
-        d.sig = arena.put<Pair2<R>>(sig.data(), sig.size());
-        d.row_lo = arena.put<R>(rq.row_lo, max_row);
+        // the base tables, then each vol move's: every node's variance (sigma + shift + tilt k)^2, sigma floored at
+        // 1 % (the oracle rebuilds its rows the same way), as (var_i, var_i+1 - var_i) pairs
+        const int nx = rq.n_x;
+        d.tab_stride = static_cast<long long>(max_row) * (nx - 1);
+        std::vector<Pair2<R>> tab(static_cast<size_t>(1 + n_vol) * d.tab_stride);
+        std::vector<double> v(nx);
+        for (int s = 0; s <= n_vol; ++s)
+            for (int r = 0; r < max_row; ++r) {
+                const double dx = 1.0 / rq.row_inv_dx[r];
+                for (int k = 0; k < nx; ++k) {
+                    v[k] = rq.table[static_cast<size_t>(r) * nx + k];
+                    if (s > 0) {
+                        const double sg = std::sqrt(v[k]) + rq.vol_shift[s - 1] + rq.vol_tilt[s - 1] * (rq.row_lo[r] + k * dx);
+                        v[k] = sg > 0.01 ? sg * sg : 0.01 * 0.01;
+                    }
+                }
+                Pair2<R>* out = tab.data() + s * d.tab_stride + static_cast<long long>(r) * (nx - 1);
+                for (int k = 0; k + 1 < nx; ++k) out[k] = {static_cast<R>(v[k]), static_cast<R>(v[k + 1] - v[k])};
+            }
+        d.tab = arena.put<Pair2<R>>(tab.data(), tab.size());
+        std::vector<R> org(max_row);
+        for (int r = 0; r < max_row; ++r) org[r] = name_step_org<R>(rq.row_lo[r], rq.row_inv_dx[r]);
+        d.row_org = arena.put<R>(org.data(), org.size());
         d.row_inv_dx = arena.put<R>(rq.row_inv_dx, max_row);
-        d.row_dx = arena.put<R>(dx.data(), dx.size());
         d.root = arena.put<R>(rq.root, max_root);
     }
     if (max_leg > 0) {
@@ -590,10 +597,6 @@ void Batch::build(const ob_batch_request& rq) {
         std::vector<R> ls(n_spot);
         for (int k = 0; k < n_spot; ++k) ls[k] = static_cast<R>(std::log1p(rq.spot_shift[k]));
         d.ln_spot = arena.put<R>(ls.data(), ls.size());
-    }
-    if (n_vol) {
-        d.vol_shift = arena.put<R>(rq.vol_shift, n_vol);
-        d.vol_tilt = arena.put<R>(rq.vol_tilt, n_vol);
     }
     std::vector<BTrade<R>> bt(n_trades);
     std::map<std::tuple<bool, int, int>, int> cls;

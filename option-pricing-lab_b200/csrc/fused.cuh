@@ -40,8 +40,12 @@ __host__ __device__ inline R name_step_org(double lo, double inv_dx) {
     return name_step_org(lo, inv_dx, static_cast<R*>(nullptr));
 }
 
-__device__ __forceinline__ float table_u(const NameStep<float>& s, float x) { return fmaf(x, s.inv_dx, s.org); }
-__device__ __forceinline__ double table_u(const NameStep<double>& s, double x) { return (x - s.org) * s.inv_dx; }
+__device__ __forceinline__ float table_u(float org, float inv_dx, float x) { return fmaf(x, inv_dx, org); }
+__device__ __forceinline__ double table_u(double org, double inv_dx, double x) { return (x - org) * inv_dx; }
+template <typename R>
+__device__ __forceinline__ R table_u(const NameStep<R>& s, R x) {
+    return table_u(s.org, s.inv_dx, x);
+}
 
 // One table interval: the value at its left point and the increment to the right one, so that an interpolation is
 // one multiply-add (y + w dy, the reference's y_i (1 - w) + y_i+1 w up to rounding).
