@@ -145,7 +145,9 @@ __device__ double continuation(const double* rule, const double* state, int n_st
 
 // The script's instructions of one event on one leg: sp[a] is the leg's spot of name a at this step, win a copy of
 // the leg's windows. Out of line: it runs a few dozen times a path, and inlined it would crowd the step loop.
-template <typename R, int NW>
+// CALLS: the script has issuer calls; without them the interpreter keeps no call bookkeeping, whose registers would
+// spill in the dispatch loop of every script (a third slower on the Phoenix).
+template <typename R, int NW, bool CALLS>
 __device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, NW> win, const R* sp, int c0, int c1,
                                        double disc) {
     R* r = s.reg;
@@ -206,37 +208,42 @@ __device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, N
                     } else {
                         const double paid = disc * (static_cast<double>(w) * static_cast<double>(e));
                         s.pv += paid;
-                        if (after) post += paid;
-                        else pre += paid;
+                        if (CALLS) {
+                            if (after) post += paid;
+                            else pre += paid;
+                        }
                     }
                 }
                 if (dst == 2) s.red += static_cast<double>(w);
                 break;
             }
-            case kCall: {
-                double st[kMaxState];
+            case kCall:
+                if (CALLS) {
+                    double st[kMaxState];
 #pragma unroll
-                for (int j = 0; j < kMaxState; ++j)
-                    st[j] = j < d.n_state ? static_cast<double>(r[d.call_state[4 * dst + j]]) : 0.0;
-                const R m = r[b], amt = r[a];
-                if (d.call_mode == 1 && d.rec) {
-                    double* c = d.rec + 2 * d.n_events + dst * (3 + d.n_state);
-                    c[0] = static_cast<double>(m), c[1] = static_cast<double>(s.alive), c[2] = static_cast<double>(amt);
-                    for (int j = 0; j < d.n_state; ++j) c[3 + j] = st[j];
-                    after = true;
-                } else if (d.call_mode == 2) {
-                    const double* rule = d.rules + static_cast<long long>(dst) * OB_RULE_STRIDE;
-                    const bool call = rule[0] != 0.0 && continuation(rule, st, d.n_state) > static_cast<double>(amt);
-                    const R md = call ? m : R(0), w = md * s.alive;
-                    if (w != R(0)) {
-                        if (!isfinite(amt)) s.bad_pay = true;
-                        else s.pv += disc * (static_cast<double>(w) * static_cast<double>(amt));
+                    for (int j = 0; j < kMaxState; ++j)
+                        st[j] = j < d.n_state ? static_cast<double>(r[d.call_state[4 * dst + j]]) : 0.0;
+                    const R m = r[b], amt = r[a];
+                    if (d.call_mode == 1 && d.rec) {
+                        double* c = d.rec + 2 * d.n_events + dst * (3 + d.n_state);
+                        c[0] = static_cast<double>(m), c[1] = static_cast<double>(s.alive);
+                        c[2] = static_cast<double>(amt);
+                        for (int j = 0; j < d.n_state; ++j) c[3 + j] = st[j];
+                        after = true;
+                    } else if (d.call_mode == 2) {
+                        const double* rule = d.rules + static_cast<long long>(dst) * OB_RULE_STRIDE;
+                        const bool call =
+                            rule[0] != 0.0 && continuation(rule, st, d.n_state) > static_cast<double>(amt);
+                        const R md = call ? m : R(0), w = md * s.alive;
+                        if (w != R(0)) {
+                            if (!isfinite(amt)) s.bad_pay = true;
+                            else s.pv += disc * (static_cast<double>(w) * static_cast<double>(amt));
+                        }
+                        s.red += static_cast<double>(w);
+                        s.alive = s.alive * (R(1) - md);
                     }
-                    s.red += static_cast<double>(w);
-                    s.alive = s.alive * (R(1) - md);
                 }
                 break;
-            }
             case kTerm: s.alive = s.alive * (R(1) - r[a]); break;
             case kCond: {
                 R c = r[a];
@@ -250,7 +257,7 @@ __device__ __noinline__ void run_event(EvCtx<R> d, LegState<R>& s, WinState<R, N
             default: break;
         }
     }
-    if (d.call_mode == 1 && d.rec) d.rec[2 * d.k] = pre, d.rec[2 * d.k + 1] = post;
+    if (CALLS && d.call_mode == 1 && d.rec) d.rec[2 * d.k] = pre, d.rec[2 * d.k + 1] = post;
 }
 
 // The windows fixing at this step, on one leg. logp(a): ln(S_a / spot0_a) of name a at this step. A window keeps the
@@ -381,7 +388,7 @@ __global__ void __launch_bounds__(128) script_kernel(ScriptDev<R> d, long long n
                     R sp[N];
 #pragma unroll
                     for (int n = 0; n < N; ++n) sp[n] = n < d.n_names ? d.spot0[n] * m_exp(logp(n)) : R(0);
-                    run_event<R, NW>(ev_ctx(d, ev, leg_record(d, base + lane, n_pairs, l, active)), leg[l], win[l], sp,
+                    run_event<R, NW, true>(ev_ctx(d, ev, leg_record(d, base + lane, n_pairs, l, active)), leg[l], win[l], sp,
                                      d.event_code[ev], d.event_code[ev + 1], d.event_disc[ev]);
                 }
             }
@@ -430,7 +437,7 @@ struct LvArgs {
 
 // BRANCH: the pairs continue the paths of an outer simulation after step end d.branch_step (one leg per outer path:
 // before the branch both legs take the outer path's normals, the outer antithetic leg's with the sign flipped).
-template <typename R, int N, int NW, bool BRANCH>
+template <typename R, int N, int NW, bool BRANCH, bool CALLS>
 __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
     script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0, uint32_t k1,
                      double* __restrict__ partial) {
@@ -496,7 +503,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
                     R sp[N];
 #pragma unroll
                     for (int n = 0; n < N; ++n) sp[n] = d.spot0[n] * m_exp(l ? y1[n] : y0[n]);
-                    run_event<R, NW>(ev_ctx(d, sc.x, leg_record(d, base + lane, n_pairs, l, active)), leg[l], win[l],
+                    run_event<R, NW, CALLS>(ev_ctx(d, sc.x, leg_record(d, base + lane, n_pairs, l, active)), leg[l], win[l],
                                      sp, d.event_code[sc.x], d.event_code[sc.x + 1], d.event_disc[sc.x]);
                 }
             }
@@ -582,23 +589,28 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
 template <typename R>
 using ScriptLvFn = void (*)(ScriptDev<R>, LvArgs<R>, long long, uint32_t, uint32_t, double*);
 
-template <typename R, int NW>
-ScriptLvFn<R> pick_lv_nw(int n, bool branch) {
-    if (branch) return n == 1 ? script_lv_kernel<R, 1, NW, true> : nullptr;  // the dual bound is single-name
+template <typename R, int NW, bool CALLS>
+ScriptLvFn<R> pick_lv_calls(int n) {
     switch (n) {
-        case 1: return script_lv_kernel<R, 1, NW, false>;
-        case 2: return script_lv_kernel<R, 2, NW, false>;
-        case 3: return script_lv_kernel<R, 3, NW, false>;
-        case 4: return script_lv_kernel<R, 4, NW, false>;
-        case 5: return script_lv_kernel<R, 5, NW, false>;
+        case 1: return script_lv_kernel<R, 1, NW, false, CALLS>;
+        case 2: return script_lv_kernel<R, 2, NW, false, CALLS>;
+        case 3: return script_lv_kernel<R, 3, NW, false, CALLS>;
+        case 4: return script_lv_kernel<R, 4, NW, false, CALLS>;
+        case 5: return script_lv_kernel<R, 5, NW, false, CALLS>;
         default: return nullptr;
     }
 }
 
+template <typename R, int NW>
+ScriptLvFn<R> pick_lv_nw(int n, bool branch, bool calls) {
+    if (branch) return n == 1 ? script_lv_kernel<R, 1, NW, true, true> : nullptr;  // the dual bound: one name
+    return calls ? pick_lv_calls<R, NW, true>(n) : pick_lv_calls<R, NW, false>(n);
+}
+
 // Kernels for up to 2 windows (most products: a knock-in window or two) and up to 8.
 template <typename R>
-ScriptLvFn<R> pick_lv(int n, int n_windows, bool branch) {
-    return n_windows <= 2 ? pick_lv_nw<R, 2>(n, branch) : pick_lv_nw<R, kMaxWindows>(n, branch);
+ScriptLvFn<R> pick_lv(int n, int n_windows, bool branch, bool calls) {
+    return n_windows <= 2 ? pick_lv_nw<R, 2>(n, branch, calls) : pick_lv_nw<R, kMaxWindows>(n, branch, calls);
 }
 
 // The staged blob of the local-vol path, or false when it does not apply (a name not local vol, more than five
@@ -883,7 +895,7 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     LvArgs<R> lv{};
     const bool fast = pack_lv<R>(rq, sched, arena, lv);
     if (rq.branch && !fast) invalid("a branched run needs the staged local-vol kernel (its tables too large)");
-    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n, rq.n_windows, rq.branch != 0))
+    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n, rq.n_windows, rq.branch != 0, rq.n_calls > 0))
                           : reinterpret_cast<const void*>(pick_script<R>(mq.model, n, rq.n_windows));
     const int block = fast ? 512 : 128;
     const size_t smem = fast ? static_cast<size_t>(lv.smem_blob) : 0;
