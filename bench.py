@@ -43,7 +43,27 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0
 # Executed warp instructions per path-step of the dominant kernel, measured by ncu (smsp__inst_executed.sum of one
 # launch divided by its path-steps) and recorded under profiles/. The issue roofline below multiplies it by the live
 # path-step rate. A launch's instruction count does not depend on timing, so a profiled launch gives it exactly.
-INST_PER_PATH_STEP = {"lv_phoenix": 1.496, "heston_qe": 20.3}
+INST_PER_PATH_STEP = {"lv_phoenix": 1.496, "heston_qe": 20.3, "script": 2.903,
+                      # the 12 class kernels of one revaluation of the 32-trade book: 404.1 G over 2.49e11 path-steps
+                      "batch": 1.623}
+# Warp instructions of one leverage calibration at 2^18 particles x 504 steps: lev_bin 4.24 M x 503 + lev_regress
+# 1.44 M x 504 + lev_step 1.70 M x 504 (ncu, one launch of each).
+LEV_INST_PER_CALIBRATION = 4.24e6 * 503 + 1.44e6 * 504 + 1.70e6 * 504
+
+
+def issue_roofline(warp_inst_per_s: float | None, note: str) -> dict:
+    """The issue roofline of a bench line: achieved warp instructions per second (None: not measured for this size)
+    against SMs x 4 schedulers x the measured max SM clock."""
+    import torch
+
+    peaks, peak_kind = load_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    peak = props.multi_processor_count * 4 * sm_max * 1e6 / 1e9
+    achieved = warp_inst_per_s / 1e9 if warp_inst_per_s is not None else None
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gwarp-inst/s",
+            "frac": achieved / peak if achieved is not None else None, "traffic": None,
+            "note": f"{note}; peak = SMs x 4 schedulers x max SM clock ({sm_max:.0f} MHz, {peak_kind})"}
 # DRAM bytes (read + written) of one profiled launch of the dominant kernel: the packed inputs, read once from HBM
 # and then from L2; the loop keeps its state in registers, so the figure does not grow with the path count.
 DRAM_PER_LAUNCH = {"lv_phoenix": 119296, "heston_qe": 44288}
@@ -551,8 +571,9 @@ def run_batch(args, world, rank):
         "per_trade_launches": {"ms_per_step": t_pt * 1e3, "path_steps_per_s": units / t_pt,
                                "speedup_of_graph": t_pt / t_step, "launches": n_sims},
         "autotune": {"seconds": t_tune, "create_seconds": t_create, "classes": shapes},
-        "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": "Gwarp-inst/s", "frac": None,
-                     "traffic": None, "note": "see the lv_phoenix line: the same FP32/SFU issue-bound stepping"},
+        "roofline": issue_roofline(INST_PER_PATH_STEP["batch"] * units / t_step,
+                                   "FP32/SFU issue-bound stepping as the fused kernels; achieved = ncu warp "
+                                   "instructions per path-step of the class kernels (32-trade book) x live rate"),
         "cpu_baseline": cpu,
         "e2e": {"value": units / statistics.median(e2e), "unit": "path-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": n_sims * 32 * 2 * 8, "seconds_per_call": statistics.median(e2e)},
@@ -628,12 +649,14 @@ def run_leverage(args, world, rank):
         "config": {"workload": "slv_leverage", "particles": 2 * s.n_pairs, "n_steps": s.n_steps, "n_x": s.n_x,
                    "n_bins": s.n_bins, "n_fine": s.n_fine, "lv_row_points": s.n_lv,
                    "l2": "particles (2 MB) stay in L2 by design: the calibration is latency-bound"},
-        "roofline": {"bound": "latency", "achieved": None, "peak": None, "unit": "us per time step", "frac": None,
-                     "traffic": None, "note": "504 dependent steps of 5 small launches each"},
+        "roofline": dict(issue_roofline(
+            LEV_INST_PER_CALIBRATION / (ms / 1e3) if 2 * s.n_pairs == 2**18 and s.n_steps == 504 else None,
+            "504 dependent steps of 3 small launches (bin, regress, step): latency-bound, so the issue rate is low; "
+            "achieved = ncu warp instructions of a calibration / its measured time"), bound="latency"),
         "cpu_baseline": cpu,
         "e2e": {"value": units / statistics.median(wall), "unit": "path-steps/s",
                 "h2d_bytes_per_step": s.n_steps * (s.n_lv + 4) * 8, "d2h_bytes_per_step": 2 * s.n_steps * s.n_x * 8},
-        "gpu_launches": args.steps * (1 + 5 * s.n_steps),
+        "gpu_launches": args.steps * 3 * s.n_steps,  # lev_init, then per step bin (not at step 0), regress, step
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "result": {"leverage_at_atm_last_step": float(held.values[-1, s.n_x // 2])},
     }
@@ -718,8 +741,10 @@ def run_script(args, world, rank):
                    "l2": "no flush: one call holds uploads, kernel and read-back"},
         "fused_kernel": {"ms_per_step": statistics.median(fused_ms), "price": fused.price[0],
                          "script_over_fused_time": t_ms / statistics.median(fused_ms)},
-        "roofline": {"bound": "issue", "achieved": None, "peak": None, "unit": "Gwarp-inst/s", "frac": None,
-                     "traffic": None, "note": "the path step of the generic engine plus the interpreter at events"},
+        "roofline": issue_roofline(
+            INST_PER_PATH_STEP["script"] * units / (t_ms / 1e3) if held.struct.n_pairs == 2**19 else None,
+            "the local-vol step plus the interpreter at events; achieved = ncu warp instructions per path-step x "
+            "live rate"),
         "cpu_baseline": None,
         "e2e": {"value": units / statistics.median(wall), "unit": "path-steps/s",
                 "h2d_bytes_per_step": int(req.struct.n_code * 16 + held.struct.n_rows * held.struct.n_x * 8),
