@@ -19,9 +19,11 @@
 // enters the sums rounded to 2^-37).
 //
 // The 3 x 504 launches are a few microseconds of GPU work each, so launching them one by one makes the host the
-// bound on a slow CPU (measured: 54.8 us a step against 28.6 us of kernels). The steps are therefore captured into
-// CUDA graphs of 4, 8, 16, ... up to kGraphSteps steps (programmatic dependent launches inside them), each launched
-// as soon as it is instantiated, while the host captures the next: the GPU runs the chunks back to back.
+// bound on a slow CPU (measured: 54.8 us a step against 28.6 us of kernels). The kernels therefore take the step
+// index from a device counter (set by lev_init, advanced by lev_bin once the previous step is done) rather than as
+// an argument, so every step after the first is the same three launches: they are captured once as a CUDA graph of
+// kGraphSteps steps (programmatic dependent launches inside it) and the graph is replayed, with one more graph for
+// the remaining steps. The host then issues a few dozen graph launches instead of 1,500 kernel launches.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -33,7 +35,7 @@ namespace ob {
 
 namespace {
 
-constexpr int kGraphSteps = 64;  // time steps per captured graph; the first ones are shorter, so the GPU starts early
+constexpr int kGraphSteps = 16;  // time steps per replayed graph
 
 // Instantiated graphs, destroyed when the calibration ends (after its stream has been synchronised, or on an error).
 struct GraphExecs {
@@ -70,6 +72,7 @@ struct LevDev {
     double* lev;               // n_x, the current leverage row
     double* x_grids;           // n_steps x n_x
     double* values;            // n_steps x n_x
+    int* step;                 // the current step: 0 from lev_init, advanced by lev_bin before the step's regression
 };
 
 // The v sums are 64-bit fixed point with 2^36 units per unit of v: integer additions, so the sums are the same
@@ -114,10 +117,14 @@ __device__ void range_of(const LevDev& d, double& lo, double& hi, double* s_mn, 
 __device__ __forceinline__ void wait_previous() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 template <typename R>
-__global__ void lev_init(R* x, R* v, long long n, R v0) {
+__global__ void lev_init(R* x, R* v, long long n, R v0, int* step) {
     const long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (j < n) x[j] = R(0), v[j] = v0;
+    if (j == 0) *step = 0;
 }
+
+// The step index, read after the wait for the previous kernel (which may have advanced it), from L2.
+__device__ __forceinline__ int current_step(const LevDev& d) { return __ldcg(d.step); }
 
 // Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU. A block bins its
 // particles in shared memory, then adds its non-zero entries into the step's global histogram and bins.
@@ -135,6 +142,7 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
         for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) s_ll[k] = 0.0;
     for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) s_fine[k] = 0u;
     wait_previous();
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(d.step, 1);  // the previous step is done: this is the next
     double lo_d, hi_d;
     range_of(d, lo_d, hi_d, s_mn, s_mx);  // (its barrier also orders the clearing above)
     const R lo = static_cast<R>(lo_d), hi = static_cast<R>(hi_d);
@@ -228,7 +236,7 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 // and E[v | x] = v0. The grid's bounds are the quantiles of the fine histogram (RC/src/leverage.cpp:26-38: the first
 // fine bin k with a count and (counts before k) + count >= q total, at lo + (k + (q total - before) / count) width),
 // computed in every block from the chunk totals and, for the chunk that holds each quantile, its 32 bins.
-__global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_particles) {
+__global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles) {
     __shared__ unsigned long long s_warp[32];
     __shared__ double s_cum[2][256];
     __shared__ int s_best[2];
@@ -237,8 +245,9 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
     __shared__ double s_mn[8], s_mx[8];
     const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-    const double h = d.dt[i];
     wait_previous();
+    const int i = current_step(d);
+    const double h = d.dt[i];
     double x0, cond;
     if (i == 0) {
         x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
@@ -367,10 +376,11 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, int i, double n_par
 // The SLV Euler step of every pair (grid-stride), and the block's min and max of the new x into part_range. The step's
 // histogram and bins are read (lev_regress is done): the blocks clear them for the next step's binning.
 template <typename R>
-__global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v, int i) {
+__global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v) {
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[8], s_max[8];
     wait_previous();
+    const int i = current_step(d);
     {
         const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0, n_ch = (nf + 31) / 32;
         const int stride = gridDim.x * blockDim.x;
@@ -482,6 +492,7 @@ void run_leverage(ob_leverage_request& rq) {
     d.values = arena.alloc<double>(static_cast<size_t>(S) * rq.n_x);
     R* x = arena.alloc<R>(n);
     R* v = arena.alloc<R>(n);
+    d.step = arena.alloc<int>(1);
     const size_t bin_smem = (static_cast<size_t>(nb) + 1) * sizeof(unsigned long long) +
                             (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0) +
                             (static_cast<size_t>(nf) + nb) * sizeof(unsigned);
@@ -509,8 +520,15 @@ void run_leverage(ob_leverage_request& rq) {
         c.attrs = pdl, c.numAttrs = 1;
         return c;
     };
-    lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(x, v, n, static_cast<R>(rq.v0));
+    lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(x, v, n, static_cast<R>(rq.v0), d.step);
     check_cuda(cudaGetLastError(), "lev_init launch");
+    const R* cx = x;
+    const R* cv = v;
+    // step 0 (no binning: the particles all start at x = 0), launched directly
+    const cudaLaunchConfig_t c_reg0 = config(rq.n_x, 256, 0), c_step0 = config(d.n_step_blocks, 256, 0);
+    check_cuda(cudaLaunchKernelEx(&c_reg0, lev_regress, d, n_particles), "lev_regress launch");
+    check_cuda(cudaLaunchKernelEx(&c_step0, lev_step<R>, d, x, v), "lev_step launch");
+    // the other steps: graphs of kGraphSteps steps, replayed, and one of the remainder
     Stream capture;
     const cudaStream_t cs = capture.get();
     auto on = [&](cudaLaunchConfig_t c) {
@@ -520,16 +538,14 @@ void run_leverage(ob_leverage_request& rq) {
     const cudaLaunchConfig_t c_bin = on(config(n_bin_blocks, 512, bin_smem));
     const cudaLaunchConfig_t c_step = on(config(d.n_step_blocks, 256, 0));
     const cudaLaunchConfig_t c_reg = on(config(rq.n_x, 256, 0));
-    const R* cx = x;
-    const R* cv = v;
     GraphExecs execs;
-    for (int i0 = 0, len = 4; i0 < S; i0 += len, len = std::min(2 * len, kGraphSteps)) {
+    auto make_graph = [&](int steps) {
         check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
         cudaError_t e = cudaSuccess;
-        for (int i = i0; i < std::min(S, i0 + len) && e == cudaSuccess; ++i) {
-            if (i > 0) e = cudaLaunchKernelEx(&c_bin, lev_bin<R>, d, cx, cv);
-            if (e == cudaSuccess) e = cudaLaunchKernelEx(&c_reg, lev_regress, d, i, n_particles);
-            if (e == cudaSuccess) e = cudaLaunchKernelEx(&c_step, lev_step<R>, d, x, v, i);
+        for (int k = 0; k < steps && e == cudaSuccess; ++k) {
+            e = cudaLaunchKernelEx(&c_bin, lev_bin<R>, d, cx, cv);
+            if (e == cudaSuccess) e = cudaLaunchKernelEx(&c_reg, lev_regress, d, n_particles);
+            if (e == cudaSuccess) e = cudaLaunchKernelEx(&c_step, lev_step<R>, d, x, v);
         }
         cudaGraph_t g = nullptr;
         const cudaError_t e_end = cudaStreamEndCapture(cs, &g);
@@ -542,8 +558,14 @@ void run_leverage(ob_leverage_request& rq) {
         cudaGraphDestroy(g);
         check_cuda(e_inst, "cudaGraphInstantiate (leverage)");
         execs.v.push_back(ge);
-        check_cuda(cudaGraphLaunch(ge, st), "cudaGraphLaunch (leverage)");
+        return ge;
+    };
+    const int rest = S - 1, full = rest / kGraphSteps, tail = rest % kGraphSteps;
+    if (full) {
+        const cudaGraphExec_t ge = make_graph(kGraphSteps);
+        for (int r = 0; r < full; ++r) check_cuda(cudaGraphLaunch(ge, st), "cudaGraphLaunch (leverage)");
     }
+    if (tail) check_cuda(cudaGraphLaunch(make_graph(tail), st), "cudaGraphLaunch (leverage)");
     check_cuda(cudaMemcpyAsync(rq.x_grids, d.x_grids, static_cast<size_t>(S) * rq.n_x * sizeof(double),
                                cudaMemcpyDeviceToHost, st),
                "copy x_grids");
