@@ -177,18 +177,8 @@ struct LvStep {
     int idx;  // index of the (y_i, dy_i) pair: row offset + i
 };
 
-// Read-only loads of a table pair through the non-coherent cache.
-__device__ __forceinline__ Pair2<float> load_pair(const Pair2<float>* p) {
-    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
-    return {v.x, v.y};
-}
-__device__ __forceinline__ Pair2<double> load_pair(const Pair2<double>* p) {
-    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
-    return {v.x, v.y};
-}
-
 template <typename R>
-__device__ __forceinline__ LvStep<R> lv_read(const AdjArgs<R>& a, const NameStep<R>& ns, R x) {
+__device__ __forceinline__ LvStep<R> lv_read(const AdjArgs<R>& a, const Pair2<R>* tab, const NameStep<R>& ns, R x) {
     LvStep<R> s;
     R u = table_u(ns, x);
     const bool inside = u > R(0) && u < a.top;
@@ -196,10 +186,28 @@ __device__ __forceinline__ LvStep<R> lv_read(const AdjArgs<R>& a, const NameStep
     const int j = static_cast<int>(u);
     s.w = u - static_cast<R>(j);
     s.idx = ns.row + j;
-    const Pair2<R> y = load_pair(a.table + s.idx);
+    const Pair2<R> y = tab[s.idx];
     s.var = y.a + s.w * y.b;
     s.dvdx = inside ? y.b * ns.inv_dx : R(0);
     return s;
+}
+
+// ST (float tables up to kStageBytes): the whole table staged in the block's shared memory, read there by every step
+// of the forward pass (1024-thread blocks, one an SM, so the warps stay as many); otherwise read from global memory
+// through L1.
+constexpr size_t kStageBytes = 200u << 10;
+
+template <typename R, bool ST>
+__device__ __forceinline__ const Pair2<R>* stage_table(const AdjArgs<R>& a, unsigned char* dyn) {
+    if (!ST) return a.table;
+    const int n16 = a.n_rows * (a.n_x - 1) * static_cast<int>(sizeof(Pair2<R>)) / 16;
+    const int4* src = reinterpret_cast<const int4*>(a.table);
+    int4* dst = reinterpret_cast<int4*>(dyn);
+    for (int k = threadIdx.x; k < n16; k += blockDim.x) dst[k] = __ldg(src + k);
+    if (threadIdx.x == 0 && (a.n_rows * (a.n_x - 1)) % 2)  // an odd count of 8-byte float pairs: the last one
+        reinterpret_cast<Pair2<R>*>(dyn)[a.n_rows * (a.n_x - 1) - 1] = a.table[a.n_rows * (a.n_x - 1) - 1];
+    __syncthreads();
+    return reinterpret_cast<const Pair2<R>*>(dyn);
 }
 
 template <int N>
@@ -229,12 +237,14 @@ __device__ __forceinline__ void batch_normals(const AdjArgs<R>& a, uint64_t pair
         }
 }
 
-template <typename R, int N, bool STORE, int CK>
-__global__ void __launch_bounds__(256) adj_forward(AdjArgs<R> a) {
+template <typename R, int N, bool STORE, int CK, bool ST>
+__global__ void __launch_bounds__(ST ? 1024 : 256) adj_forward(AdjArgs<R> a) {
     constexpr int G = Batch<N>::G;
-    __shared__ double wacc[8][2 + 2 * N];
+    __shared__ double wacc[32][2 + 2 * N];
+    extern __shared__ __align__(16) unsigned char dyn[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int t = threadIdx.x; t < 8 * (2 + 2 * N); t += blockDim.x) (&wacc[0][0])[t] = 0.0;
+    for (int t = threadIdx.x; t < 32 * (2 + 2 * N); t += blockDim.x) (&wacc[0][0])[t] = 0.0;
+    const Pair2<R>* tab = stage_table<R, ST>(a, dyn);
     __syncthreads();
     const long long P = a.n_pairs;
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
@@ -266,7 +276,7 @@ __global__ void __launch_bounds__(256) adj_forward(AdjArgs<R> a) {
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
-                        const LvStep<R> s = lv_read(a, ns, x[leg][n]);
+                        const LvStep<R> s = lv_read(a, tab, ns, x[leg][n]);
                         x[leg][n] += s.var * st.hdt + (m_sqrt(s.var) * st.sdt) * z;
                         const R lp = x[leg][n] + ns.lf;
                         if (lp < wv[leg]) wv[leg] = lp, wn[leg] = n;
@@ -364,6 +374,7 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
     constexpr int G = Batch<N>::G;
     using GT = R;  // gradient accumulators: float in the float build, double in the double one
     GT* sg = a.priv + static_cast<long long>(blockIdx.x) * a.n_rows * a.n_x;
+    const Pair2<R>* tab = a.table;
     const int lane = threadIdx.x & 31;
     const long long P = a.n_pairs;
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
@@ -411,7 +422,7 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
-                        const LvStep<R> r = lv_read(a, ns, xs[g][leg][n]);
+                        const LvStep<R> r = lv_read(a, tab, ns, xs[g][leg][n]);
                         xs[g + 1][leg][n] = xs[g][leg][n] + r.var * st.hdt + (m_sqrt(r.var) * st.sdt) * z;
                     }
                 }
@@ -448,7 +459,7 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
-                        const LvStep<R> r = lv_read(a, ns, xs[g][leg][n]);
+                        const LvStep<R> r = lv_read(a, tab, ns, xs[g][leg][n]);
                         const R sv = m_sqrt(r.var);
                         const R c = st.hdt + st.sdt * z / (R(2) * sv);  // d x_i / d var
                         const R vb = xb[leg][n] * c;
@@ -486,6 +497,7 @@ template <typename R, int N>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1) adj_backward_dense(AdjArgs<R> a) {
     using GT = R;
     GT* sg = a.priv + static_cast<long long>(blockIdx.x) * a.n_rows * a.n_x;
+    const Pair2<R>* tab = a.table;  // (staging it in shared memory measured no faster: the state loads bound it)
     const int lane = threadIdx.x & 31;
     const long long P = a.n_pairs;
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
@@ -537,7 +549,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1) adj_backward_dens
                     const int rix = __ldg(a.row_ix + (i - 1) * N + n);
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
-                        const LvStep<R> r = lv_read(a, ns, cur[g][leg][n]);
+                        const LvStep<R> r = lv_read(a, tab, ns, cur[g][leg][n]);
                         const R d = cur[g + 1][leg][n] - cur[g][leg][n] - r.var * st.hdt;  // sqrt(v dt) z
                         const R c = st.hdt + d / (R(2) * r.var);                            // d x_i / d var
                         const R vb = xb[leg][n] * c;
@@ -589,6 +601,9 @@ struct AdjPlan {
     cudaStream_t last = nullptr;
     int tab_n = 0;
     bool dense = false;  // the forward stores every step's state and the backward recomputes nothing
+    bool staged = false; // the table is staged in shared memory (float tables up to kStageBytes)
+    int block_f = 256, block_b = 256;
+    size_t smem = 0;     // dynamic shared memory of the staged forward kernels
 
     template <typename R>
     AdjArgs<R>& args();
@@ -613,13 +628,20 @@ AdjArgs<double>& AdjPlan::args<double>() {
 
 namespace {
 
-template <typename R, int N>
-void pick(AdjPlan& p) {
-    p.kf = reinterpret_cast<const void*>(adj_forward<R, N, false, kCk>);
-    p.kfs = p.dense ? reinterpret_cast<const void*>(adj_forward<R, N, true, 1>)
-                    : reinterpret_cast<const void*>(adj_forward<R, N, true, kCk>);
+template <typename R, int N, bool ST>
+void pick_st(AdjPlan& p) {
+    p.kf = reinterpret_cast<const void*>(adj_forward<R, N, false, kCk, ST>);
+    p.kfs = p.dense ? reinterpret_cast<const void*>(adj_forward<R, N, true, 1, ST>)
+                    : reinterpret_cast<const void*>(adj_forward<R, N, true, kCk, ST>);
     p.kb = p.dense ? reinterpret_cast<const void*>(adj_backward_dense<R, N>)
                    : reinterpret_cast<const void*>(adj_backward<R, N>);
+}
+
+// Staged tables for float only (double tables of the benchmark's size do not fit a block's shared memory).
+template <typename R, int N>
+void pick(AdjPlan& p) {
+    if (sizeof(R) == 4 && p.staged) pick_st<R, N, true>(p);
+    else pick_st<R, N, false>(p);
 }
 
 constexpr double kDenseBudget = 24.0 * (1ull << 30);  // bytes of stored states below which every step is stored
@@ -705,19 +727,31 @@ void AdjPlan::build(const ob_adjoint_request& r) {
     a.ki_step = arena.alloc<int>(2 * static_cast<size_t>(P));
     a.ki_name = arena.alloc<unsigned char>(2 * static_cast<size_t>(P));
     a.batch_pairs = arena.alloc<unsigned long long>(kAdjBatches);
+    const size_t tab_bytes = static_cast<size_t>(rq.n_rows) * (rq.n_x - 1) * sizeof(Pair2<R>);
+    staged = sizeof(R) == 4 && tab_bytes <= kStageBytes;
+    smem = staged ? tab_bytes : 0;
+    block_f = staged ? 1024 : 256;
     switch (n) {
         case 1: pick<R, 1>(*this); break;
         case 2: pick<R, 2>(*this); break;
         case 3: pick<R, 3>(*this); break;
         default: pick<R, 4>(*this); break;
     }
+    const size_t smem_b = 0;
+    if (staged) {
+        check_cuda(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                   "cudaFuncSetAttribute");
+        check_cuda(cudaFuncSetAttribute(kfs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                   "cudaFuncSetAttribute");
+    }
     tab_n = rq.n_rows * rq.n_x;
     int per_f = 0, per_b = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_f, kfs, 256, 0), "occupancy");
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_b, kb, 256, 0), "occupancy");
-    const long long need = (P + 255) / 256;
-    grid_f = static_cast<int>(std::max<long long>(1, std::min<long long>(need, static_cast<long long>(sms) * std::max(1, per_f))));
-    grid_b = static_cast<int>(std::max<long long>(1, std::min<long long>(need, static_cast<long long>(sms) * std::max(1, per_b))));
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_f, kfs, block_f, smem), "occupancy");
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_b, kb, block_b, smem_b), "occupancy");
+    grid_f = static_cast<int>(std::max<long long>(
+        1, std::min<long long>((P + block_f - 1) / block_f, static_cast<long long>(sms) * std::max(1, per_f))));
+    grid_b = static_cast<int>(std::max<long long>(
+        1, std::min<long long>((P + block_b - 1) / block_b, static_cast<long long>(sms) * std::max(1, per_b))));
     a.partial = arena.alloc<double>(static_cast<size_t>(grid_f) * (2 + 2 * n));
     priv_bytes = static_cast<size_t>(grid_b) * tab_n * sizeof(R);
     a.priv = arena.alloc<R>(static_cast<size_t>(grid_b) * tab_n);
@@ -738,7 +772,7 @@ void AdjPlan::run(const double* d_table, double* d_grad, cudaStream_t st) {
         }
         af.grad = d_grad;
         using F = void (*)(AdjArgs<float>);
-        reinterpret_cast<F>(const_cast<void*>(grad ? kfs : kf))<<<grid_f, 256, 0, st>>>(af);
+        reinterpret_cast<F>(const_cast<void*>(grad ? kfs : kf))<<<grid_f, block_f, smem, st>>>(af);
     } else {
         if (d_table) {
             const int cells = ad.n_rows * (ad.n_x - 1);
@@ -747,7 +781,7 @@ void AdjPlan::run(const double* d_table, double* d_grad, cudaStream_t st) {
         }
         ad.grad = d_grad;
         using F = void (*)(AdjArgs<double>);
-        reinterpret_cast<F>(const_cast<void*>(grad ? kfs : kf))<<<grid_f, 256, 0, st>>>(ad);
+        reinterpret_cast<F>(const_cast<void*>(grad ? kfs : kf))<<<grid_f, block_f, smem, st>>>(ad);
     }
     check_cuda(cudaGetLastError(), "adj_forward launch");
     check_cuda(cudaEventRecord(e1, st), "cudaEventRecord");
@@ -758,12 +792,12 @@ void AdjPlan::run(const double* d_table, double* d_grad, cudaStream_t st) {
             check_cuda(cudaMemsetAsync(af.batch_pairs, 0, kAdjBatches * sizeof(unsigned long long), st), "memset");
             check_cuda(cudaMemsetAsync(af.priv, 0, priv_bytes, st), "cudaMemsetAsync");
             using B = void (*)(AdjArgs<float>);
-            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, 256, 0, st>>>(af);
+            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, block_b, 0, st>>>(af);
         } else {
             check_cuda(cudaMemsetAsync(ad.batch_pairs, 0, kAdjBatches * sizeof(unsigned long long), st), "memset");
             check_cuda(cudaMemsetAsync(ad.priv, 0, priv_bytes, st), "cudaMemsetAsync");
             using B = void (*)(AdjArgs<double>);
-            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, 256, 0, st>>>(ad);
+            reinterpret_cast<B>(const_cast<void*>(kb))<<<grid_b, block_b, 0, st>>>(ad);
         }
         check_cuda(cudaGetLastError(), "adj_backward launch");
     }
