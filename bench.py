@@ -45,7 +45,9 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0
 # path-step rate. A launch's instruction count does not depend on timing, so a profiled launch gives it exactly.
 INST_PER_PATH_STEP = {"lv_phoenix": 1.496, "heston_qe": 20.3, "script": 2.903,
                       # the 12 class kernels of one revaluation of the 32-trade book: 404.1 G over 2.49e11 path-steps
-                      "batch": 1.623}
+                      "batch": 1.623,
+                      # the drop-in path engine's local-vol kernel on the Phoenix model (12 columns + a daily window)
+                      "paths": 2.639}
 # Warp instructions of one leverage calibration at 2^18 particles x 504 steps: lev_bin 4.24 M x 503 + lev_regress
 # 1.44 M x 504 + lev_step 1.70 M x 504 (ncu, one launch of each).
 LEV_INST_PER_CALIBRATION = 4.24e6 * 503 + 1.44e6 * 504 + 1.70e6 * 504
@@ -166,16 +168,41 @@ def input_bytes(held) -> int:
 # ---------------------------------------------------------------------------------------------------- CPU baseline
 
 
+def phoenix_paths_request(n_paths: int, seed: int = 7):
+    """The local-vol Phoenix's model as a drop-in paths request (the reference's `run()`): the 12 quarterly columns
+    and one daily window (lowest, highest) of the name, for n_paths paths; returns (request, Phoenix, market)."""
+    from optlab_b200 import workloads
+    from optlab_b200.requests import paths_request
+
+    held, _, _ = build_workload("lv_phoenix", n_paths)
+    s = held.struct
+    ph = workloads.Phoenix()
+    obs_step, _ = ph.schedule(252)
+    n_steps = s.n_steps
+    all_obs = np.arange(0, n_steps + 1, dtype=np.int32)  # every step end (and t = 0) for the daily window
+    col_of = np.full(len(all_obs), -1, np.int32)
+    col_of[obs_step] = np.arange(len(obs_step), dtype=np.int32)
+    m = workloads.FlatMarket(100.0, 0.02, 0.01)
+    dt = np.ctypeslib.as_array(s.dt, shape=(n_steps,)).copy()
+    t_end = np.concatenate([[0.0], np.cumsum(dt)])
+    g = workloads.lv_grid()
+    t0 = t_end[:-1]
+    rq = paths_request(
+        dt=dt, t0=t0, obs_step=all_obs, root=[[1.0]], kind=[1], cvar=[0.0], heston=[0.0, 1, 1, 0, 0], same=1,
+        fwd=m.F(t_end)[None, :], n_pairs=n_paths // 2, seed=seed, step_row=g.row_of(t0), lo=g.lo, inv_dx=g.inv_dx,
+        table=g.rows, n_x=g.n_x, col_of=col_of, n_keep=len(obs_step), win_lo=[0], win_hi=[n_steps],
+    )
+    return rq, ph, m
+
+
 def cpu_reference_sample(name: str, n_paths: int, threads: int):
     """Time the reference's CPU implementation of the workload on n_paths paths: (seconds, kind, cores, detail)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     from oracle import Oracle, Reference, reference_available
 
     from optlab_b200 import workloads
-    from optlab_b200.requests import paths_request
 
-    held, _, _ = build_workload(name, n_paths)
-    s = held.struct
+    held, _, _ = build_workload("lv_phoenix" if name == "paths" else name, n_paths)
     kind = "reference" if reference_available() else "port"
     if name == "heston_qe":
         if kind == "reference":
@@ -194,30 +221,19 @@ def cpu_reference_sample(name: str, n_paths: int, threads: int):
         Oracle().mc_price(held, threads)
         return time.perf_counter() - t, kind, threads, "oracle port (C, double)"
     # local-vol Phoenix: the reference's path engine writes the quarterly columns and the daily window, then the
-    # payoff is evaluated on the columns (the reference's structured engine does this in NumPy).
-    ph = workloads.Phoenix()
-    obs_step, _ = ph.schedule(252)
-    n_steps = s.n_steps
-    all_obs = np.arange(0, n_steps + 1, dtype=np.int32)  # every step end (and t = 0) for the daily window
-    col_of = np.full(len(all_obs), -1, np.int32)
-    col_of[obs_step] = np.arange(len(obs_step), dtype=np.int32)
-    m = workloads.FlatMarket(100.0, 0.02, 0.01)
-    dt = np.ctypeslib.as_array(s.dt, shape=(n_steps,)).copy()
-    t_end = np.concatenate([[0.0], np.cumsum(dt)])
-    g = workloads.lv_grid()
-    t0 = t_end[:-1]
-    rq = paths_request(
-        dt=dt, t0=t0, obs_step=all_obs, root=[[1.0]], kind=[1], cvar=[0.0], heston=[0.0, 1, 1, 0, 0], same=1,
-        fwd=m.F(t_end)[None, :], n_pairs=n_paths // 2, seed=7, step_row=g.row_of(t0), lo=g.lo, inv_dx=g.inv_dx,
-        table=g.rows, n_x=g.n_x, col_of=col_of, n_keep=len(obs_step), win_lo=[0], win_hi=[n_steps],
-    )
+    # payoff is evaluated on the columns (the reference's structured engine does this in NumPy); the paths workload
+    # is the path engine alone.
+    rq, ph, m = phoenix_paths_request(n_paths)
+    n_obs = len(ph.schedule(252)[0])
     t = time.perf_counter()
     if kind == "reference":
         Reference().paths(rq, threads)
     else:
         Oracle().paths(rq, threads)
+    if name == "paths":
+        return time.perf_counter() - t, kind, threads, "reference path engine (12 columns + daily window)"
     out = next(a for a in rq.keep if isinstance(a, np.ndarray) and a.ndim == 3)[0]
-    phoenix_payoff(out[: len(obs_step)].T / 100.0, out[len(obs_step)] / 100.0, ph, m)
+    phoenix_payoff(out[:n_obs].T / 100.0, out[n_obs] / 100.0, ph, m)
     return time.perf_counter() - t, kind, threads, "reference path engine (columns + daily window) + payoff on columns"
 
 
@@ -253,7 +269,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lv_phoenix", choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage", "script"])
+    ap.add_argument("--workload", default="lv_phoenix",
+                    choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage", "script", "paths"])
     ap.add_argument("--trades", type=int, default=512, help="batch workload: trades in the book")
     ap.add_argument("--paths", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -275,6 +292,8 @@ def main():
         return run_leverage(args, world, rank)
     if args.workload == "script":
         return run_script(args, world, rank)
+    if args.workload == "paths":
+        return run_paths(args, world, rank)
 
     import torch
 
@@ -764,6 +783,70 @@ def ctypes_sizeof_trade() -> int:
     return ctypes.sizeof(ObBatchTrade)
 
 
+def run_paths(args, world, rank):
+    """The drop-in path engine (the reference's `run()`, `ob_paths`): the local-vol Phoenix's model, 2^20 paths x 756
+    steps, its 12 quarterly spot columns and one daily window (lowest and highest spot) written for every path and
+    copied back to the host (2^20 x 14 doubles = 117 MB). `value`: path-steps per second of the kernel, timed by CUDA
+    events inside the engine (inputs on the device); `e2e`: the whole call from host arrays (upload, kernel, the
+    columns back), by the host clock. One rank: the call is one job."""
+    import torch
+
+    from optlab_b200 import engine
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if rank != 0:
+        return
+    n_paths = args.paths or 2**20
+    rq, _, _ = phoenix_paths_request(n_paths)
+    s = rq.struct
+    units = 2 * s.n_pairs * s.n_steps * s.n_names
+    for _ in range(args.warmup):
+        engine.paths(rq, "fp32")
+    kern, wall = [], []
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            k_ms, _ = engine.paths(rq, "fp32")
+            wall.append(time.perf_counter() - t)
+            kern.append(k_ms)
+    t_k = statistics.median(kern) / 1e3
+    out_bytes = 2 * s.n_pairs * s.n_names * s.n_cols * 8
+    in_bytes = input_bytes(rq) - out_bytes
+    cpu = None
+    if not args.no_cpu_baseline:
+        n_s = 2**18
+        secs, kind, cores, detail = cpu_reference_sample("paths", n_s, os.cpu_count() or 1)
+        cpu = {"value": n_s * s.n_steps / secs, "unit": "path-steps/s", "cores": cores, "kind": kind,
+               "sample": f"{n_s} paths x {s.n_steps} steps ({detail})"}
+    clk = clocks.summary()
+    ipu = INST_PER_PATH_STEP.get("paths")
+    line = {
+        "metric": "path-steps/s",
+        "value": units / t_k,
+        "unit": "path-steps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_k * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded SSVI surface)",
+        "config": {"workload": "paths", "n_paths": 2 * s.n_pairs, "n_steps": s.n_steps, "columns": s.n_cols,
+                   "output_bytes": out_bytes, "l2": "each call uploads its inputs and writes 117 MB of columns"},
+        "roofline": issue_roofline(ipu * units / t_k if ipu and n_paths == 2**20 else None,
+                                   "the local-vol step plus the column and window stores; achieved = ncu warp "
+                                   "instructions per path-step x live rate"),
+        "cpu_baseline": cpu,
+        "e2e": {"value": units / statistics.median(wall), "unit": "path-steps/s", "h2d_bytes_per_step": int(in_bytes),
+                "d2h_bytes_per_step": int(out_bytes)},
+        "gpu_launches": args.steps,
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+    }
+    print(json.dumps(line))
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -775,7 +858,9 @@ def run_reference(args, world, rank):
     for _ in range(args.steps):
         s, kind, cores, detail = cpu_reference_sample(args.workload, n_s, threads)
         secs.append(s)
-    _, _, config = build_workload(args.workload, None)
+    _, _, config = build_workload("lv_phoenix" if args.workload == "paths" else args.workload, None)
+    if args.workload == "paths":
+        config = dict(config, workload="paths", product="12 quarterly columns + a daily window (no payoff)")
     n_units = n_s * config["n_steps"]
     tot = sum(secs)
     value = n_units * args.steps / tot

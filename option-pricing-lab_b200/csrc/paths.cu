@@ -2,12 +2,21 @@
 // RC/src/paths_gpu.cu:76-167). One thread per antithetic pair, state in registers, the spot columns and window
 // extremes written in the reference's layout (out[(a n_cols + c) 2 n_pairs + row], pair p at row p, its antithetic
 // at n_pairs + p), in float or double. The request is checked as RC/src/requests.cpp:168-207 does.
+//
+// Baskets of one to five names all in local vol without a mixer (the common case: every local-vol quote) run a
+// specialised kernel, paths_lv_kernel: the fused kernels' step (per-step records, correlation root and the table as
+// (y, dy) pairs staged in shared memory, normals drawn in batches of whole Philox blocks; the same stream order as
+// the generic engine), and per step end the observations taken there, read from a staged schedule. Columns and
+// window extremes are the reference's S = F_j exp(x) at each observation (kept columns written, window extremes
+// compared on S), so a window's extremes equal those of the full columns bit for bit. Other requests run the generic
+// kernel, which follows RC/include/optlab_cuda/paths.hpp step for step.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
-#include "model.cuh"
+#include "fused.cuh"
 
 namespace ob {
 
@@ -81,6 +90,134 @@ __global__ void __launch_bounds__(256) paths_kernel(PathsDev<R> s) {
     }
 }
 
+// Offsets of the staged blob of paths_lv_kernel (bytes).
+struct PathsLvOffsets {
+    int step, name_step, root, table2, sched, col, fwd;
+};
+
+template <typename R>
+struct PathsLvArgs {
+    PathsLvOffsets off;
+    const unsigned char* blob;
+    int smem_blob;
+    int n_steps, n_obs, n_cols, n_keep, n_win;
+    int win_lo[2], win_hi[2];
+    long long n_pairs, first_pair, rows;
+    uint32_t k0, k1;
+    R top;
+    double* out;
+};
+
+// Observation j of both legs: the kept column and the windows that hold it, on S = F_j exp(x) as the reference.
+template <typename R, int N>
+__device__ __forceinline__ void lv_record(const PathsLvArgs<R>& a, const int* s_col, const R* s_fwd, int j, long long p,
+                                          bool active, const R (&x0)[N], const R (&x1)[N], R (&lo)[2][N][2],
+                                          R (&hi)[2][N][2]) {
+    const int c = s_col[j];
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+        const R f = s_fwd[n * a.n_obs + j];
+        const R S0 = f * m_exp(x0[n]), S1 = f * m_exp(x1[n]);
+        double* base = a.out + static_cast<long long>(n) * a.n_cols * a.rows;
+        if (c >= 0 && active) {
+            base[c * a.rows + p] = static_cast<double>(S0);
+            base[c * a.rows + a.n_pairs + p] = static_cast<double>(S1);
+        }
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            if (w >= a.n_win || j < a.win_lo[w] || j > a.win_hi[w]) continue;
+            if (j == a.win_lo[w]) {
+                lo[0][n][w] = hi[0][n][w] = S0, lo[1][n][w] = hi[1][n][w] = S1;
+            } else {
+                lo[0][n][w] = m_min(lo[0][n][w], S0), hi[0][n][w] = m_max(hi[0][n][w], S0);
+                lo[1][n][w] = m_min(lo[1][n][w], S1), hi[1][n][w] = m_max(hi[1][n][w], S1);
+            }
+            if (j == a.win_hi[w] && active) {
+                const long long cl = a.n_keep + 2 * w, ch = cl + 1;
+                base[cl * a.rows + p] = static_cast<double>(lo[0][n][w]);
+                base[ch * a.rows + p] = static_cast<double>(hi[0][n][w]);
+                base[cl * a.rows + a.n_pairs + p] = static_cast<double>(lo[1][n][w]);
+                base[ch * a.rows + a.n_pairs + p] = static_cast<double>(hi[1][n][w]);
+            }
+        }
+    }
+}
+
+// 512-thread blocks for one or two names, 256 for more (registers); one float name fits two blocks an SM (32 warps).
+template <int N>
+constexpr int lv_block() {
+    return N <= 2 ? 512 : 256;
+}
+
+template <typename R, int N>
+__global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 1) paths_lv_kernel(PathsLvArgs<R> a) {
+    constexpr int C = N;
+    constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);  // steps per batch of whole Philox blocks
+    constexpr int NB = C * G / 4;
+    extern __shared__ __align__(16) unsigned char sm[];
+    {
+        const int4* src = reinterpret_cast<const int4*>(a.blob);
+        int4* dst = reinterpret_cast<int4*>(sm);
+        for (int t = threadIdx.x; t < a.smem_blob / 16; t += blockDim.x) dst[t] = src[t];
+    }
+    __syncthreads();
+    const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
+    const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
+    const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
+    const Pair2<R>* s_tab = reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
+    const int2* s_sched = reinterpret_cast<const int2*>(sm + a.off.sched);  // observations [x, y) at each step end
+    const int* s_col = reinterpret_cast<const int*>(sm + a.off.col);
+    const R* s_fwd = reinterpret_cast<const R*>(sm + a.off.fwd);
+    const int S = a.n_steps;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < a.n_pairs;
+         base += stride) {
+        const int lane = threadIdx.x & 31;
+        const bool active = base + lane < a.n_pairs;
+        const long long p = active ? base + lane : a.n_pairs - 1;
+        const uint64_t pair = static_cast<uint64_t>(a.first_pair + p);
+        R x0[N], x1[N], lo[2][N][2], hi[2][N][2];
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            x0[n] = x1[n] = R(0);
+#pragma unroll
+            for (int w = 0; w < 2; ++w) lo[0][n][w] = lo[1][n][w] = hi[0][n][w] = hi[1][n][w] = R(0);
+        }
+        for (int j = s_sched[0].x; j < s_sched[0].y; ++j) lv_record<R, N>(a, s_col, s_fwd, j, p, active, x0, x1, lo, hi);
+        for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) {
+            R z[C * G];
+#pragma unroll
+            for (int k = 0; k < NB; ++k)
+                normals4<R>(pair, static_cast<uint64_t>(b) * NB + k, 0u, a.k0, a.k1, z[4 * k], z[4 * k + 1],
+                            z[4 * k + 2], z[4 * k + 3]);
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                const int i = i0 + g;
+                if (G > 1 && i > S) break;
+                const StepRec<R> st = s_step[i - 1];
+#pragma unroll
+                for (int n = 0; n < N; ++n) {
+                    R zc = R(0);
+#pragma unroll
+                    for (int m = 0; m < N; ++m) zc += s_root[n * N + m] * z[g * C + m];
+                    const NameStep<R> ns = s_ns[(i - 1) * N + n];
+                    R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
+                    u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
+                    const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
+                    const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
+                    const Pair2<R> y0 = s_tab[ns.row + j0], y1 = s_tab[ns.row + j1];
+                    const R v0 = y0.a + f0 * y0.b, v1 = y1.a + f1 * y1.b;
+                    const R zd = st.sdt * zc;  // sqrt(dt) z, the legs' +-
+                    x0[n] += m_fma(m_sqrt(v0), zd, v0 * st.hdt);
+                    x1[n] += m_fma(-m_sqrt(v1), zd, v1 * st.hdt);
+                }
+                const int2 ob = s_sched[i];
+                for (int j = ob.x; j < ob.y; ++j) lv_record<R, N>(a, s_col, s_fwd, j, p, active, x0, x1, lo, hi);
+            }
+        }
+    }
+}
+
 void check_request(const ob_paths_request& c) {
     if (c.n_names < 1 || c.n_names > OB_MAX_NAMES) invalid("n_names must be 1 to 8");
     if (c.n_pairs < 1 || c.first_pair < 0) invalid("n_pairs must be >= 1 and first_pair >= 0");
@@ -121,6 +258,86 @@ void check_request(const ob_paths_request& c) {
         if (c.win_lo[w] < 0 || c.win_hi[w] < c.win_lo[w] || c.win_hi[w] >= c.n_obs) invalid("bad window");
 }
 
+// The staged blob of paths_lv_kernel, or false when the request is not for it (a name not in local vol, a mixer,
+// more than five names, or a blob beyond the shared-memory budget: 110 KB in float, 200 KB in double).
+template <typename R>
+bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>& a) {
+    const int n = h.n_names, S = h.n_steps;
+    if (h.mixer || n > 5 || S < 1) return false;
+    for (int k = 0; k < n; ++k)
+        if (h.kind[k] != 1) return false;
+    std::vector<unsigned char> blob;
+    auto put = [&](const void* src, size_t bytes) {
+        const size_t at = (blob.size() + 15) & ~static_cast<size_t>(15);
+        blob.resize(at + ((bytes + 15) & ~static_cast<size_t>(15)), 0);
+        if (bytes) std::memcpy(blob.data() + at, src, bytes);
+        return static_cast<int>(at);
+    };
+    std::vector<StepRec<R>> steps(S);
+    for (int i = 0; i < S; ++i) {
+        std::memset(&steps[i], 0, sizeof steps[i]);
+        steps[i].hdt = static_cast<R>(-0.5 * h.dt[i]), steps[i].sdt = static_cast<R>(std::sqrt(h.dt[i]));
+        steps[i].dt = static_cast<R>(h.dt[i]), steps[i].obs = -1;
+    }
+    a.off.step = put(steps.data(), steps.size() * sizeof(StepRec<R>));
+    std::vector<NameStep<R>> ns(static_cast<size_t>(S) * n);
+    for (int i = 0; i < S; ++i)
+        for (int k = 0; k < n; ++k) {
+            NameStep<R>& r = ns[static_cast<size_t>(i) * n + k];
+            std::memset(&r, 0, sizeof r);
+            const int row = h.step_row[static_cast<size_t>(k) * S + i];
+            r.org = name_step_org<R>(h.row_lo[row], h.row_inv_dx[row]), r.inv_dx = static_cast<R>(h.row_inv_dx[row]);
+            r.row = row * (h.n_x - 1);
+        }
+    a.off.name_step = put(ns.data(), ns.size() * sizeof(NameStep<R>));
+    std::vector<R> root(static_cast<size_t>(n) * n);
+    for (size_t k = 0; k < root.size(); ++k) root[k] = static_cast<R>(h.root[k]);
+    a.off.root = put(root.data(), root.size() * sizeof(R));
+    std::vector<Pair2<R>> tab(static_cast<size_t>(h.n_rows) * (h.n_x - 1));
+    for (int r = 0; r < h.n_rows; ++r)
+        for (int k = 0; k + 1 < h.n_x; ++k) {
+            const double y = h.table[static_cast<size_t>(r) * h.n_x + k], y1 = h.table[static_cast<size_t>(r) * h.n_x + k + 1];
+            tab[static_cast<size_t>(r) * (h.n_x - 1) + k] = {static_cast<R>(y), static_cast<R>(y1 - y)};
+        }
+    a.off.table2 = put(tab.data(), tab.size() * sizeof(Pair2<R>));
+    std::vector<int2> sched(S + 1);
+    for (int i = 0, j = 0; i <= S; ++i) {
+        sched[i].x = j;
+        while (j < h.n_obs && h.obs_step[j] == i) ++j;
+        sched[i].y = j;
+    }
+    a.off.sched = put(sched.data(), sched.size() * sizeof(int2));
+    a.off.col = put(h.col_of, static_cast<size_t>(h.n_obs) * sizeof(int));
+    std::vector<R> fwd(static_cast<size_t>(n) * h.n_obs);
+    for (size_t k = 0; k < fwd.size(); ++k) fwd[k] = static_cast<R>(h.fwd[k]);
+    a.off.fwd = put(fwd.data(), fwd.size() * sizeof(R));
+    const size_t budget = sizeof(R) == 4 ? (110u << 10) : (200u << 10);
+    if (blob.size() > budget) return false;
+    a.smem_blob = static_cast<int>(blob.size());
+    a.blob = arena.put<unsigned char>(blob.data(), blob.size());
+    a.n_steps = S, a.n_obs = h.n_obs, a.n_cols = h.n_cols, a.n_keep = h.n_keep, a.n_win = h.n_windows;
+    for (int w = 0; w < 2; ++w) {
+        a.win_lo[w] = w < h.n_windows ? h.win_lo[w] : 0;
+        a.win_hi[w] = w < h.n_windows ? h.win_hi[w] : -1;
+    }
+    a.k0 = static_cast<uint32_t>(h.seed), a.k1 = static_cast<uint32_t>(h.seed >> 32);
+    a.top = static_cast<R>(h.n_x - 1) - static_cast<R>(1e-4);
+    return true;
+}
+
+inline int lv_block_of(int n) { return n <= 2 ? lv_block<1>() : lv_block<3>(); }
+
+template <typename R>
+const void* pick_paths_lv(int n) {
+    switch (n) {
+        case 1: return reinterpret_cast<const void*>(paths_lv_kernel<R, 1>);
+        case 2: return reinterpret_cast<const void*>(paths_lv_kernel<R, 2>);
+        case 3: return reinterpret_cast<const void*>(paths_lv_kernel<R, 3>);
+        case 4: return reinterpret_cast<const void*>(paths_lv_kernel<R, 4>);
+        default: return reinterpret_cast<const void*>(paths_lv_kernel<R, 5>);
+    }
+}
+
 template <typename R>
 void run_paths(ob_paths_request& h) {
     const auto t_start = std::chrono::steady_clock::now();
@@ -158,6 +375,18 @@ void run_paths(ob_paths_request& h) {
     s.win_lo = arena.put<int>(h.win_lo, h.n_windows);
     s.win_hi = arena.put<int>(h.win_hi, h.n_windows);
     s.fwd = arena.put<R>(h.fwd, static_cast<size_t>(n) * h.n_obs);
+    PathsLvArgs<R> lv{};
+    const bool fast = pack_paths_lv<R>(h, arena, lv);
+    const void* lv_fn = fast ? pick_paths_lv<R>(n) : nullptr;
+    int lv_grid = 0;
+    if (fast) {
+        check_cuda(cudaFuncSetAttribute(lv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lv.smem_blob),
+                   "cudaFuncSetAttribute");
+        int per_sm = 0;
+        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lv_fn, lv_block_of(n), lv.smem_blob),
+                   "occupancy");
+        lv_grid = require_device() * std::max(1, per_sm);
+    }
 
     // Chunks of pairs: the output of one chunk within a quarter of the free memory (at most 4 GB).
     const long long cols = static_cast<long long>(n) * h.n_cols;
@@ -183,7 +412,14 @@ void run_paths(ob_paths_request& h) {
             const int block = 256;
             const unsigned grid = static_cast<unsigned>((mcount + block - 1) / block);
             check_cuda(cudaEventRecord(ev0), "cudaEventRecord");
-            if (n <= 1) paths_kernel<R, 1><<<grid, block>>>(part);
+            if (fast) {
+                PathsLvArgs<R> la = lv;
+                la.n_pairs = mcount, la.first_pair = h.first_pair + c0, la.rows = 2 * mcount, la.out = dout;
+                const int lb = lv_block_of(n);
+                const unsigned g = static_cast<unsigned>(std::max<long long>(
+                    1, std::min<long long>(lv_grid, (mcount + lb - 1) / lb)));
+                reinterpret_cast<void (*)(PathsLvArgs<R>)>(const_cast<void*>(lv_fn))<<<g, lb, la.smem_blob>>>(la);
+            } else if (n <= 1) paths_kernel<R, 1><<<grid, block>>>(part);
             else if (n <= 2) paths_kernel<R, 2><<<grid, block>>>(part);
             else if (n <= 4) paths_kernel<R, 4><<<grid, block>>>(part);
             else paths_kernel<R, 8><<<grid, block>>>(part);
