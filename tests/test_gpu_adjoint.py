@@ -1,6 +1,6 @@
 """Adjoint Greeks of the worst-of autocall on the GPU: the smoothed price against the oracle, deltas and node vegas
 against central finite differences on common random numbers (the engine's FP64 revaluation and the CPU oracle), and
-FP32 against FP64 within 4 standard errors (north_star's check: every Greek within 4 SE and 1e-4 relative of FP64)."""
+FP32 against FP64 within 4 standard errors (the target's check: every Greek within 4 SE and 1e-4 relative of FP64)."""
 
 import numpy as np
 import pytest
