@@ -24,8 +24,8 @@
 //               compare-and-swap loop, a global reduction is one instruction the warp does not wait for (the
 //               backward took half the time with it). At the end the block adds its copy into the caller's
 //               per-batch gradient.
-// adj_backward_dense  the same reverse sweep when the forward stored the state after every step (when those
-//               states fit in the dense budget): nothing is recomputed. A step from x to x' read the variance v at x
+// adj_backward_dense  the same reverse sweep, one leg a thread, when the forward stored the state after every step
+//               (when those states fit in the dense budget): nothing is recomputed. A step from x to x' read the variance v at x
 //               and moved by v (-dt/2) + sqrt(v dt) z, so its noise term is d = x' - x - v (-dt/2) and
 //               dx'/dv = -dt/2 + d / (2 v): no normals are drawn again. Each segment's states are loaded while
 //               the previous segment is swept (two register buffers).
@@ -52,7 +52,6 @@ struct AdjArgs {
     uint32_t k0, k1;
     const StepRec<R>* steps;   // n_steps
     const NameStep<R>* ns;     // n_steps x n_names
-    const int* row_ix;         // n_steps x n_names: the table row read (gradient entry of pair idx: idx + row)
     const R* root;             // n x n
     const Pair2<R>* table;     // n_rows x (n_x - 1): (y_i, y_i+1 - y_i)
     const R* trig;             // n_obs, in performance (<= 0: no call)
@@ -69,7 +68,8 @@ struct AdjArgs {
     unsigned char* ki_name;    // 2 x n_pairs
     double* partial;           // per block: price sum and square, then per name delta sum and square
     double* grad;              // kAdjBatches x n_rows x n_x
-    R* priv;                   // per backward block: its n_rows x n_x gradient, zeroed before each backward
+    R* priv;                   // per backward block: (left, right) weights of each table interval, n_rows x (n_x - 1)
+                               // pairs, zeroed before each backward
     unsigned long long* batch_pairs;  // kAdjBatches
 };
 
@@ -344,21 +344,31 @@ __global__ void __launch_bounds__(ST ? 1024 : 256) adj_forward(AdjArgs<R> a) {
     }
 }
 
-// A reduction into the block's gradient copy (the result unused: no return value is waited for).
-template <typename T>
-__device__ __forceinline__ void grad_add(T* p, T v) {
-    atomicAdd(p, v);
+// A step's gradient into the block's copy: interval idx of a row receives vb (1 - w) for its left point and vb w for
+// its right one, as one 8-byte reduction in float (half the reduction operations of two scalar ones: the L2's atomic
+// rate bounds the backward), two in double. The result is unused: no return value is waited for.
+__device__ __forceinline__ void cell_add(float* cell, float left, float right) {
+    atomicAdd(reinterpret_cast<float2*>(cell), make_float2(left, right));
+}
+__device__ __forceinline__ void cell_add(double* cell, double left, double right) {
+    atomicAdd(cell, left);
+    atomicAdd(cell + 1, right);
 }
 
-// The block's gradient copy added into the caller's gradient of batch blockIdx % kAdjBatches, and its pair count.
+// The block's gradient copy added into the caller's gradient of batch blockIdx % kAdjBatches (entry k of a row: the
+// left weight of interval k plus the right weight of interval k - 1), and its pair count.
 template <typename R>
 __device__ __forceinline__ void flush_gradient(const AdjArgs<R>& a, const R* sg, unsigned long long mine) {
     __syncthreads();
-    const int tab_n = a.n_rows * a.n_x;
+    const int nx = a.n_x, tab_n = a.n_rows * nx;
     const int batch = blockIdx.x % kAdjBatches;
     double* out = a.grad + static_cast<long long>(batch) * tab_n;
     for (int t = threadIdx.x; t < tab_n; t += blockDim.x) {
-        const double v = static_cast<double>(__ldcg(sg + t));  // from L2, where the reductions were made
+        const int row = t / nx, k = t - row * nx;
+        const R* cells = sg + 2 * static_cast<long long>(row) * (nx - 1);  // from L2, where the reductions were made
+        double v = 0.0;
+        if (k < nx - 1) v += static_cast<double>(__ldcg(cells + 2 * k));
+        if (k > 0) v += static_cast<double>(__ldcg(cells + 2 * (k - 1) + 1));
         if (v != 0.0) atomicAdd(out + t, v);
     }
     __shared__ unsigned long long s_cnt;
@@ -373,7 +383,7 @@ template <typename R, int N>
 __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
     constexpr int G = Batch<N>::G;
     using GT = R;  // gradient accumulators: float in the float build, double in the double one
-    GT* sg = a.priv + static_cast<long long>(blockIdx.x) * a.n_rows * a.n_x;
+    GT* sg = a.priv + 2 * static_cast<long long>(blockIdx.x) * a.n_rows * (a.n_x - 1);
     const Pair2<R>* tab = a.table;
     const int lane = threadIdx.x & 31;
     const long long P = a.n_pairs;
@@ -455,7 +465,6 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     const NameStep<R> ns = a.ns[(i - 1) * N + n];
-                    const int rix = __ldg(a.row_ix + (i - 1) * N + n);
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
@@ -463,12 +472,7 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
                         const R sv = m_sqrt(r.var);
                         const R c = st.hdt + st.sdt * z / (R(2) * sv);  // d x_i / d var
                         const R vb = xb[leg][n] * c;
-                        if (vb != R(0)) {
-                            // pair index row (n_x - 1) + i is table entry row n_x + i
-                            GT* gr = sg + r.idx + rix;
-                            grad_add(gr, static_cast<GT>(vb * (R(1) - r.w)));
-                            grad_add(gr + 1, static_cast<GT>(vb * r.w));
-                        }
+                        if (vb != R(0)) cell_add(sg + 2 * r.idx, vb * (R(1) - r.w), vb * r.w);
                         xb[leg][n] += vb * r.dvdx;
                     }
                 }
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
 }
 
 template <typename R, int N>
-__device__ __forceinline__ void dense_segment(const AdjArgs<R>& a, long long p, int s, R (&xs)[kCk + 1][2][N]) {
+__device__ __forceinline__ void dense_segment(const AdjArgs<R>& a, long long p, int leg, int s, R (&xs)[kCk + 1][N]) {
     const long long P = a.n_pairs;
 #pragma unroll
     for (int g = 0; g <= kCk; ++g) {
@@ -487,37 +491,37 @@ __device__ __forceinline__ void dense_segment(const AdjArgs<R>& a, long long p, 
         if (i > a.n_steps) break;
 #pragma unroll
         for (int n = 0; n < N; ++n)
-#pragma unroll
-            for (int leg = 0; leg < 2; ++leg)
-                xs[g][leg][n] = i == 0 ? R(0) : a.ckpt[((static_cast<long long>(i - 1) * N + n) * 2 + leg) * P + p];
+            xs[g][n] = i == 0 ? R(0) : a.ckpt[((static_cast<long long>(i - 1) * N + n) * 2 + leg) * P + p];
     }
 }
 
+// One leg a warp: warps 2k and 2k + 1 of a block take the two legs of the same 32 pairs (so a pair's gradient stays
+// in one block's batch). Half the state of a pair a thread, so more warps fit an SM to hide the states' loads.
 template <typename R, int N>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1) adj_backward_dense(AdjArgs<R> a) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1) adj_backward_dense(AdjArgs<R> a) {
     using GT = R;
-    GT* sg = a.priv + static_cast<long long>(blockIdx.x) * a.n_rows * a.n_x;
+    GT* sg = a.priv + 2 * static_cast<long long>(blockIdx.x) * a.n_rows * (a.n_x - 1);
     const Pair2<R>* tab = a.table;  // (staging it in shared memory measured no faster: the state loads bound it)
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, leg = warp & 1;
+    const int chunks_per_block = blockDim.x >> 6;  // pairs of warps
     const long long P = a.n_pairs;
-    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    const long long n_chunks = (P + 31) / 32;
     unsigned long long mine = 0;
-    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < P;
-         base += stride) {
-        const bool active = base + lane < P;
-        if (!active) continue;  // no block-wide synchronisation below: inactive lanes may leave
-        const long long p = base + lane;
-        ++mine;
-        const int kstep[2] = {a.ki_step[p], a.ki_step[P + p]};
-        const int kname[2] = {a.ki_name[p], a.ki_name[P + p]};
-        const R kd[2] = {a.dki[p], a.dki[P + p]};
-        R xb[2][N];
+    for (long long c = static_cast<long long>(blockIdx.x) * chunks_per_block + (warp >> 1); c < n_chunks;
+         c += static_cast<long long>(gridDim.x) * chunks_per_block) {
+        const long long p = c * 32 + lane;
+        if (p >= P) continue;  // no block-wide synchronisation below: inactive lanes may leave
+        if (leg == 0) ++mine;
+        const int kstep = a.ki_step[leg * P + p];
+        const int kname = a.ki_name[leg * P + p];
+        const R kd = a.dki[leg * P + p];
+        R xb[N];
 #pragma unroll
-        for (int n = 0; n < N; ++n) xb[0][n] = xb[1][n] = R(0);
-        R cur[kCk + 1][2][N], nxt[kCk + 1][2][N];
-        dense_segment<R, N>(a, p, a.n_seg - 1, cur);
+        for (int n = 0; n < N; ++n) xb[n] = R(0);
+        R cur[kCk + 1][N], nxt[kCk + 1][N];
+        dense_segment<R, N>(a, p, leg, a.n_seg - 1, cur);
         for (int s = a.n_seg - 1; s >= 0; --s) {
-            if (s > 0) dense_segment<R, N>(a, p, s - 1, nxt);
+            if (s > 0) dense_segment<R, N>(a, p, leg, s - 1, nxt);
             const int i_first = s * kCk + 1;
             const int len = min(kCk, a.n_steps - s * kCk);
 #pragma unroll
@@ -526,48 +530,33 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1) adj_backward_dens
                 const int i = i_first + g;
                 const StepRec<R> st = a.steps[i - 1];
                 if (st.obs >= 0) {
+                    const long long o = (static_cast<long long>(st.obs) * 2 + leg) * P + p;
+                    const R d = a.dobs[o];
+                    const int w = a.who[o];
 #pragma unroll
-                    for (int leg = 0; leg < 2; ++leg) {
-                        const long long o = (static_cast<long long>(st.obs) * 2 + leg) * P + p;
-                        const R d = a.dobs[o];
-                        const int w = a.who[o];
-#pragma unroll
-                        for (int n = 0; n < N; ++n)
-                            if (w == n) xb[leg][n] += d;
-                    }
+                    for (int n = 0; n < N; ++n)
+                        if (w == n) xb[n] += d;
                 }
+                if (kstep == i) {
 #pragma unroll
-                for (int leg = 0; leg < 2; ++leg)
-                    if (kstep[leg] == i) {
-#pragma unroll
-                        for (int n = 0; n < N; ++n)
-                            if (kname[leg] == n) xb[leg][n] += kd[leg];
-                    }
+                    for (int n = 0; n < N; ++n)
+                        if (kname == n) xb[n] += kd;
+                }
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     const NameStep<R> ns = a.ns[(i - 1) * N + n];
-                    const int rix = __ldg(a.row_ix + (i - 1) * N + n);
-#pragma unroll
-                    for (int leg = 0; leg < 2; ++leg) {
-                        const LvStep<R> r = lv_read(a, tab, ns, cur[g][leg][n]);
-                        const R d = cur[g + 1][leg][n] - cur[g][leg][n] - r.var * st.hdt;  // sqrt(v dt) z
-                        const R c = st.hdt + d / (R(2) * r.var);                            // d x_i / d var
-                        const R vb = xb[leg][n] * c;
-                        if (vb != R(0)) {
-                            GT* gr = sg + r.idx + rix;  // pair index row (n_x - 1) + i is entry row n_x + i
-                            grad_add(gr, static_cast<GT>(vb * (R(1) - r.w)));
-                            grad_add(gr + 1, static_cast<GT>(vb * r.w));
-                        }
-                        xb[leg][n] += vb * r.dvdx;
-                    }
+                    const LvStep<R> r = lv_read(a, tab, ns, cur[g][n]);
+                    const R d = cur[g + 1][n] - cur[g][n] - r.var * st.hdt;  // sqrt(v dt) z
+                    const R cc = st.hdt + d / (R(2) * r.var);               // d x_i / d var
+                    const R vb = xb[n] * cc;
+                    if (vb != R(0)) cell_add(sg + 2 * r.idx, vb * (R(1) - r.w), vb * r.w);
+                    xb[n] += vb * r.dvdx;
                 }
             }
 #pragma unroll
             for (int g = 0; g <= kCk; ++g)
 #pragma unroll
-                for (int n = 0; n < N; ++n)
-#pragma unroll
-                    for (int leg = 0; leg < 2; ++leg) cur[g][leg][n] = nxt[g][leg][n];
+                for (int n = 0; n < N; ++n) cur[g][n] = nxt[g][n];
         }
     }
     flush_gradient(a, sg, mine);
@@ -689,13 +678,11 @@ void AdjPlan::build(const ob_adjoint_request& r) {
     }
     for (int j = 0; j < rq.n_obs; ++j) steps[rq.obs_step[j] - 1].obs = j;
     std::vector<NameStep<R>> ns(static_cast<size_t>(S) * n);
-    std::vector<int> row_ix(static_cast<size_t>(S) * n);
     for (int i = 1; i <= S; ++i)
         for (int k = 0; k < n; ++k) {
             NameStep<R>& e = ns[static_cast<size_t>(i - 1) * n + k];
             std::memset(&e, 0, sizeof e);
             const int row = rq.step_row[static_cast<size_t>(k) * S + (i - 1)];
-            row_ix[static_cast<size_t>(i - 1) * n + k] = row;
             e.org = name_step_org<R>(rq.row_lo[row], rq.row_inv_dx[row]);
             e.inv_dx = static_cast<R>(rq.row_inv_dx[row]);
             e.lf = static_cast<R>(rq.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
@@ -706,7 +693,6 @@ void AdjPlan::build(const ob_adjoint_request& r) {
     for (int j = 0; j < rq.n_obs; ++j) trig[j] = rq.trigger[j] > 0 ? static_cast<R>(rq.trigger[j]) : R(0);
     a.steps = arena.put<StepRec<R>>(steps.data(), steps.size());
     a.ns = arena.put<NameStep<R>>(ns.data(), ns.size());
-    a.row_ix = arena.put<int>(row_ix.data(), row_ix.size());
     a.root = arena.put<R>(root.data(), root.size());
     a.trig = arena.put<R>(trig.data(), trig.size());
     a.disc = arena.put<double>(rq.obs_discount, rq.n_obs);
@@ -750,11 +736,13 @@ void AdjPlan::build(const ob_adjoint_request& r) {
     check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_b, kb, block_b, smem_b), "occupancy");
     grid_f = static_cast<int>(std::max<long long>(
         1, std::min<long long>((P + block_f - 1) / block_f, static_cast<long long>(sms) * std::max(1, per_f))));
+    const long long pairs_b = dense ? block_b / 2 : block_b;  // the dense backward takes one leg a thread
     grid_b = static_cast<int>(std::max<long long>(
-        1, std::min<long long>((P + block_b - 1) / block_b, static_cast<long long>(sms) * std::max(1, per_b))));
+        1, std::min<long long>((P + pairs_b - 1) / pairs_b, static_cast<long long>(sms) * std::max(1, per_b))));
     a.partial = arena.alloc<double>(static_cast<size_t>(grid_f) * (2 + 2 * n));
-    priv_bytes = static_cast<size_t>(grid_b) * tab_n * sizeof(R);
-    a.priv = arena.alloc<R>(static_cast<size_t>(grid_b) * tab_n);
+    const size_t cells2 = 2 * static_cast<size_t>(rq.n_rows) * (rq.n_x - 1);
+    priv_bytes = static_cast<size_t>(grid_b) * cells2 * sizeof(R);
+    a.priv = arena.alloc<R>(static_cast<size_t>(grid_b) * cells2);
     for (int k = 0; k < n; ++k) spot[k] = rq.spot[k];
 }
 
