@@ -546,6 +546,12 @@ void Batch::build(const ob_batch_request& rq) {
         // 1 % (the oracle rebuilds its rows the same way), as (var_i, var_i+1 - var_i) pairs
         const int nx = rq.n_x;
         d.tab_stride = static_cast<long long>(max_row) * (nx - 1);
+        const double tab_bytes = static_cast<double>(1 + n_vol) * d.tab_stride * sizeof(Pair2<R>);
+        size_t free_mem = 0, total_mem = 0;
+        check_cuda(cudaMemGetInfo(&free_mem, &total_mem), "cudaMemGetInfo");
+        if (tab_bytes > 0.5 * static_cast<double>(free_mem))
+            invalid("the vol scenarios' tables (one copy of the table pool per scenario) need more than half the free "
+                    "device memory: fewer vol scenarios or a smaller pool");
         std::vector<Pair2<R>> tab(static_cast<size_t>(1 + n_vol) * d.tab_stride);
         std::vector<double> v(nx);
         for (int s = 0; s <= n_vol; ++s)
