@@ -151,6 +151,25 @@ def test_paths_depend_on_the_seed_and_the_global_pair_only():
     assert np.array_equal(W[:, :, 3000:4000], T[:, :, 1000:2000])
 
 
+@pytest.mark.parametrize("kinds", [[1], [3, 1]])
+def test_a_large_output_read_back_in_chunks_equals_the_same_pairs_in_two_calls(kinds):
+    """Outputs of 32 MB and more come back in four chunks on two streams (one chunk's kernel running while the
+    previous chunk is copied); each half of the pairs, asked for alone, is one chunk: the same columns bit for bit
+    (the local-vol kernel and the generic one)."""
+    n = 2**19
+    kw = _paths_case(kinds, n_pairs=n, first_pair=0)
+    whole = paths_request(**kw)
+    engine.paths(whole, "fp32")
+    W = out_of(whole)
+    assert W.nbytes >= 32 << 20
+    for f in (0, n // 2):
+        part = paths_request(**dict(kw, n_pairs=n // 2, first_pair=f))
+        engine.paths(part, "fp32")
+        P = out_of(part)
+        assert np.array_equal(W[:, :, f:f + n // 2], P[:, :, : n // 2])
+        assert np.array_equal(W[:, :, n + f:n + f + n // 2], P[:, :, n // 2:])
+
+
 # ------------------------------------------------------------------------------------------------------ fused
 
 
