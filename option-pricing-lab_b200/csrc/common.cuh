@@ -60,7 +60,6 @@ int require_device();
 
 // ------------------------------------------------------------------------------------------------ device memory
 
-// Owns device allocations for one call or one plan.
 // A non-blocking stream owned by one call, destroyed with it.
 struct Stream {
     cudaStream_t s = nullptr;
@@ -73,6 +72,7 @@ struct Stream {
     cudaStream_t get() const { return s; }
 };
 
+// Owns device allocations for one call or one plan.
 struct DeviceArena {
     void* ptrs[64] = {};
     int n = 0;
