@@ -168,9 +168,18 @@ def input_bytes(held) -> int:
 # ---------------------------------------------------------------------------------------------------- CPU baseline
 
 
-def phoenix_paths_request(n_paths: int, seed: int = 7):
+def reference_rows():
+    """The default surface tabulated as the reference's plan() does it: one 801-point row for each of the 756 daily
+    steps of three years (4.8 MB of float intervals, beyond the kernels' shared-memory stage)."""
+    from optlab_b200 import workloads
+
+    return workloads.LocalVarGrid.from_surface(workloads.lv_surface(horizon=3.0), 3.0 * np.arange(1, 757) / 756, 801)
+
+
+def phoenix_paths_request(n_paths: int, seed: int = 7, table: str = "builder"):
     """The local-vol Phoenix's model as a drop-in paths request (the reference's `run()`): the 12 quarterly columns
-    and one daily window (lowest, highest) of the name, for n_paths paths; returns (request, Phoenix, market)."""
+    and one daily window (lowest, highest) of the name, for n_paths paths; returns (request, Phoenix, market). table:
+    "builder" (200 points x 40 expiries) or "reference" (801 points x 756 per-step rows)."""
     from optlab_b200 import workloads
     from optlab_b200.requests import paths_request
 
@@ -185,7 +194,7 @@ def phoenix_paths_request(n_paths: int, seed: int = 7):
     m = workloads.FlatMarket(100.0, 0.02, 0.01)
     dt = np.ctypeslib.as_array(s.dt, shape=(n_steps,)).copy()
     t_end = np.concatenate([[0.0], np.cumsum(dt)])
-    g = workloads.lv_grid()
+    g = workloads.lv_grid() if table == "builder" else reference_rows()
     t0 = t_end[:-1]
     rq = paths_request(
         dt=dt, t0=t0, obs_step=all_obs, root=[[1.0]], kind=[1], cvar=[0.0], heston=[0.0, 1, 1, 0, 0], same=1,
@@ -273,6 +282,8 @@ def main():
                     choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage", "script", "paths"])
     ap.add_argument("--trades", type=int, default=512, help="batch workload: trades in the book")
     ap.add_argument("--paths", type=int, default=None)
+    ap.add_argument("--table", default="builder", choices=["builder", "reference"],
+                    help="paths workload: the builder's 200 x 40 grid or the reference plan's 801-point per-step rows")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -804,7 +815,7 @@ def run_paths(args, world, rank):
     if rank != 0:
         return
     n_paths = args.paths or 2**20
-    rq, _, _ = phoenix_paths_request(n_paths)
+    rq, _, _ = phoenix_paths_request(n_paths, table=args.table)
     s = rq.struct
     units = 2 * s.n_pairs * s.n_steps * s.n_names
     for _ in range(args.warmup):
@@ -841,14 +852,16 @@ def run_paths(args, world, rank):
         "dtype": "f32",
         "data": "synthetic (seeded SSVI surface)",
         "config": {"workload": "paths", "n_paths": 2 * s.n_pairs, "n_steps": s.n_steps, "columns": s.n_cols,
+                   "table": f"{s.n_rows} rows x {s.n_x} points ({args.table})",
                    "output_bytes": out_bytes, "l2": "each call uploads its inputs and writes 117 MB of columns"},
-        "roofline": issue_roofline(ipu * units / t_k if ipu and n_paths == 2**20 else None,
+        "roofline": issue_roofline(ipu * units / t_k if ipu and n_paths == 2**20 and args.table == "builder" else None,
                                    "the local-vol step plus the column and window stores; achieved = ncu warp "
                                    "instructions per path-step x live rate"),
         "cpu_baseline": cpu,
         "e2e": {"value": units / statistics.median(wall), "unit": "path-steps/s", "h2d_bytes_per_step": int(in_bytes),
                 "d2h_bytes_per_step": int(out_bytes)},
-        "gpu_launches": args.steps,
+        # outputs of 32 MB or more run in four chunks of pairs, one launch each
+        "gpu_launches": args.steps * (4 if out_bytes >= 32 << 20 and s.n_pairs >= 4 else 1),
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
     }
     print(json.dumps(line))

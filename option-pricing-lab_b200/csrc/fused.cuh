@@ -54,6 +54,17 @@ struct alignas(2 * sizeof(R)) Pair2 {
     R a, b;
 };
 
+// An interval of a table left in global memory (too large for the shared-memory stage): one 8- or 16-byte load
+// through the read-only data cache.
+__device__ __forceinline__ Pair2<float> ldg_pair(const Pair2<float>* p) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    return {v.x, v.y};
+}
+__device__ __forceinline__ Pair2<double> ldg_pair(const Pair2<double>* p) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    return {v.x, v.y};
+}
+
 // Per step: -dt / 2, sqrt(dt), dt, and the index of the observation taken at the step's end (-1: none).
 template <typename R>
 struct alignas(16) StepRec {

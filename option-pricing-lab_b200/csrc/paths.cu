@@ -106,6 +106,8 @@ struct PathsLvArgs {
     uint32_t k0, k1;
     R top;
     double* out;
+    const Pair2<R>* tab;  // the table in global memory when it does not fit the stage (table_global), else unused
+    int table_global;
 };
 
 // Observation j of both legs: the kept column and the windows that hold it, on S = F_j exp(x) as the reference.
@@ -149,7 +151,8 @@ constexpr int lv_block() {
     return N <= 2 ? 512 : 256;
 }
 
-template <typename R, int N>
+// GT: the table is read from global memory (a.tab) instead of the stage.
+template <typename R, int N, bool GT>
 __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 1) paths_lv_kernel(PathsLvArgs<R> a) {
     constexpr int C = N;
     constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);  // steps per batch of whole Philox blocks
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
     const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
     const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
     const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
-    const Pair2<R>* s_tab = reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
+    const Pair2<R>* tab = GT ? a.tab : reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
     const int2* s_sched = reinterpret_cast<const int2*>(sm + a.off.sched);  // observations [x, y) at each step end
     const int* s_col = reinterpret_cast<const int*>(sm + a.off.col);
     const R* s_fwd = reinterpret_cast<const R*>(sm + a.off.fwd);
@@ -205,7 +208,8 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
                     u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
                     const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
                     const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
-                    const Pair2<R> y0 = s_tab[ns.row + j0], y1 = s_tab[ns.row + j1];
+                    const Pair2<R> y0 = GT ? ldg_pair(tab + ns.row + j0) : tab[ns.row + j0];
+                    const Pair2<R> y1 = GT ? ldg_pair(tab + ns.row + j1) : tab[ns.row + j1];
                     const R v0 = y0.a + f0 * y0.b, v1 = y1.a + f1 * y1.b;
                     const R zd = st.sdt * zc;  // sqrt(dt) z, the legs' +-
                     x0[n] += m_fma(m_sqrt(v0), zd, v0 * st.hdt);
@@ -259,7 +263,10 @@ void check_request(const ob_paths_request& c) {
 }
 
 // The staged blob of paths_lv_kernel, or false when the request is not for it (a name not in local vol, a mixer,
-// more than five names, or a blob beyond the shared-memory budget: 110 KB in float, 200 KB in double).
+// more than five names, or a blob beyond the shared-memory budget: 110 KB in float, 200 KB in double, without the
+// table). The table goes into the stage when it fits beside the rest, else into global memory: a plan's per-step rows
+// (801 points for each of the 756 steps of three daily years, 4.8 MB in float) stay in L2 and are read through the
+// read-only cache.
 template <typename R>
 bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>& a) {
     const int n = h.n_names, S = h.n_steps;
@@ -293,13 +300,6 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
     std::vector<R> root(static_cast<size_t>(n) * n);
     for (size_t k = 0; k < root.size(); ++k) root[k] = static_cast<R>(h.root[k]);
     a.off.root = put(root.data(), root.size() * sizeof(R));
-    std::vector<Pair2<R>> tab(static_cast<size_t>(h.n_rows) * (h.n_x - 1));
-    for (int r = 0; r < h.n_rows; ++r)
-        for (int k = 0; k + 1 < h.n_x; ++k) {
-            const double y = h.table[static_cast<size_t>(r) * h.n_x + k], y1 = h.table[static_cast<size_t>(r) * h.n_x + k + 1];
-            tab[static_cast<size_t>(r) * (h.n_x - 1) + k] = {static_cast<R>(y), static_cast<R>(y1 - y)};
-        }
-    a.off.table2 = put(tab.data(), tab.size() * sizeof(Pair2<R>));
     std::vector<int2> sched(S + 1);
     for (int i = 0, j = 0; i <= S; ++i) {
         sched[i].x = j;
@@ -311,8 +311,18 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
     std::vector<R> fwd(static_cast<size_t>(n) * h.n_obs);
     for (size_t k = 0; k < fwd.size(); ++k) fwd[k] = static_cast<R>(h.fwd[k]);
     a.off.fwd = put(fwd.data(), fwd.size() * sizeof(R));
+    std::vector<Pair2<R>> tab(static_cast<size_t>(h.n_rows) * (h.n_x - 1));
+    for (int r = 0; r < h.n_rows; ++r)
+        for (int k = 0; k + 1 < h.n_x; ++k) {
+            const double y = h.table[static_cast<size_t>(r) * h.n_x + k], y1 = h.table[static_cast<size_t>(r) * h.n_x + k + 1];
+            tab[static_cast<size_t>(r) * (h.n_x - 1) + k] = {static_cast<R>(y), static_cast<R>(y1 - y)};
+        }
     const size_t budget = sizeof(R) == 4 ? (110u << 10) : (200u << 10);
+    const size_t tab_bytes = tab.size() * sizeof(Pair2<R>);
     if (blob.size() > budget) return false;
+    a.table_global = ((blob.size() + 15) & ~static_cast<size_t>(15)) + tab_bytes > budget;
+    if (a.table_global) a.tab = arena.put<Pair2<R>>(tab.data(), tab.size());
+    else a.off.table2 = put(tab.data(), tab_bytes);
     a.smem_blob = static_cast<int>(blob.size());
     a.blob = arena.put<unsigned char>(blob.data(), blob.size());
     a.n_steps = S, a.n_obs = h.n_obs, a.n_cols = h.n_cols, a.n_keep = h.n_keep, a.n_win = h.n_windows;
@@ -327,15 +337,20 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
 
 inline int lv_block_of(int n) { return n <= 2 ? lv_block<1>() : lv_block<3>(); }
 
-template <typename R>
-const void* pick_paths_lv(int n) {
+template <typename R, bool GT>
+const void* pick_paths_lv_gt(int n) {
     switch (n) {
-        case 1: return reinterpret_cast<const void*>(paths_lv_kernel<R, 1>);
-        case 2: return reinterpret_cast<const void*>(paths_lv_kernel<R, 2>);
-        case 3: return reinterpret_cast<const void*>(paths_lv_kernel<R, 3>);
-        case 4: return reinterpret_cast<const void*>(paths_lv_kernel<R, 4>);
-        default: return reinterpret_cast<const void*>(paths_lv_kernel<R, 5>);
+        case 1: return reinterpret_cast<const void*>(paths_lv_kernel<R, 1, GT>);
+        case 2: return reinterpret_cast<const void*>(paths_lv_kernel<R, 2, GT>);
+        case 3: return reinterpret_cast<const void*>(paths_lv_kernel<R, 3, GT>);
+        case 4: return reinterpret_cast<const void*>(paths_lv_kernel<R, 4, GT>);
+        default: return reinterpret_cast<const void*>(paths_lv_kernel<R, 5, GT>);
     }
+}
+
+template <typename R>
+const void* pick_paths_lv(int n, bool table_global) {
+    return table_global ? pick_paths_lv_gt<R, true>(n) : pick_paths_lv_gt<R, false>(n);
 }
 
 template <typename R>
@@ -377,7 +392,7 @@ void run_paths(ob_paths_request& h) {
     s.fwd = arena.put<R>(h.fwd, static_cast<size_t>(n) * h.n_obs);
     PathsLvArgs<R> lv{};
     const bool fast = pack_paths_lv<R>(h, arena, lv);
-    const void* lv_fn = fast ? pick_paths_lv<R>(n) : nullptr;
+    const void* lv_fn = fast ? pick_paths_lv<R>(n, lv.table_global != 0) : nullptr;
     int lv_grid = 0;
     if (fast) {
         check_cuda(cudaFuncSetAttribute(lv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lv.smem_blob),

@@ -81,6 +81,29 @@ def reference_size_grid():
     return workloads.LocalVarGrid.from_surface(workloads.lv_surface(horizon=3.0), 3.0 * np.arange(1, 757) / 756, 801)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_paths_on_a_reference_size_table_match_the_oracle(oracle, reference_size_grid, prec):
+    """The drop-in path kernel with the rows left in global memory: quarterly columns and a window over them."""
+    g = reference_size_grid
+    n_steps = 756
+    dt, t0 = workloads.uniform_grid(3.0, n_steps)
+    t_end = np.concatenate([[0.0], t0 + dt])
+    obs = np.arange(0, n_steps + 1, 63)
+    m = workloads.FlatMarket(100.0, 0.02, 0.01)
+    kw = dict(dt=dt, t0=t0, obs_step=obs, root=[[1.0]], kind=[1], cvar=[0.0], heston=[0.0, 1, 1, 0, 0], same=1,
+              fwd=m.F(t_end[obs])[None, :], n_pairs=2**12, seed=9, step_row=g.row_of(t0), lo=g.lo, inv_dx=g.inv_dx,
+              table=g.rows, n_x=g.n_x, win_lo=[0], win_hi=[len(obs) - 1])
+    assert len(np.unique(g.row_of(t0))) > 700  # a row for (nearly) every step
+    gh, oh = paths_request(**kw), paths_request(**kw)
+    engine.paths(gh, prec)
+    oracle.paths(oh)
+    rel = np.abs(_out(gh) / _out(oh) - 1.0)
+    if prec == "fp64":
+        assert rel.max() < 1e-12, rel.max()
+    else:
+        assert np.median(rel) < 1e-6 and rel.max() < 1e-4, (np.median(rel), rel.max())
+
+
 def test_a_table_larger_than_the_shared_memory_stage_prices_like_the_oracle(oracle, reference_size_grid):
     held = _phoenix(2**12, reference_size_grid)
     assert held.struct.n_rows == 756 and held.struct.n_x == 801  # 2.4 MB of float (value, slope) pairs: global
