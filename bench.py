@@ -137,13 +137,15 @@ class ClockSampler:
         }
 
 
-def build_workload(name: str, n_paths: int | None):
+def build_workload(name: str, n_paths: int | None, table: str = "builder"):
     from optlab_b200 import workloads
 
     if name == "lv_phoenix":
-        return workloads.lv_phoenix(n_paths=n_paths or 2**20, seed=7), "fp32", {
+        grid = reference_rows() if table == "reference" else None
+        return workloads.lv_phoenix(n_paths=n_paths or 2**20, seed=7, grid=grid), "fp32", {
             "workload": "lv_phoenix",
-            "model": "Dupire local vol, SSVI power law (rho -0.6, eta 1, gamma 0.5, theta 0.04 t), 200 x 40 table",
+            "model": "Dupire local vol, SSVI power law (rho -0.6, eta 1, gamma 0.5, theta 0.04 t), "
+            + ("200 x 40 table" if table == "builder" else "801 x 756 per-step rows (the reference plan's)"),
             "product": "3y Phoenix, quarterly autocall 100%, coupon 2% at 70% with memory, daily KI 60%",
             "n_paths": n_paths or 2**20,
             "n_steps": 756,
@@ -283,7 +285,8 @@ def main():
     ap.add_argument("--trades", type=int, default=512, help="batch workload: trades in the book")
     ap.add_argument("--paths", type=int, default=None)
     ap.add_argument("--table", default="builder", choices=["builder", "reference"],
-                    help="paths workload: the builder's 200 x 40 grid or the reference plan's 801-point per-step rows")
+                    help="lv_phoenix and paths: the builder's 200 x 40 grid or the reference plan's 801-point "
+                    "per-step rows")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -320,7 +323,7 @@ def main():
     from optlab_b200 import engine
     from optlab_b200.workloads import path_steps
 
-    held, prec, config = build_workload(args.workload, args.paths)
+    held, prec, config = build_workload(args.workload, args.paths, args.table)
     n_pairs = held.struct.n_pairs
     first = rank * n_pairs
     units = path_steps(held)
@@ -390,14 +393,14 @@ def main():
     props = torch.cuda.get_device_properties(local)
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     issue_peak = props.multi_processor_count * 4 * sm_max * 1e6 / 1e9  # G warp-instructions/s
-    ipu = INST_PER_PATH_STEP.get(args.workload)
+    ipu = INST_PER_PATH_STEP.get(args.workload) if args.table == "builder" else None  # counted on the builder grid
     roofline = {
         "bound": "issue",
         "achieved": (ipu * value / world / 1e9) if ipu else None,
         "peak": issue_peak,
         "unit": "Gwarp-inst/s",
         "frac": (ipu * value / world / 1e9 / issue_peak) if ipu else None,
-        "traffic": DRAM_PER_LAUNCH.get(args.workload),
+        "traffic": DRAM_PER_LAUNCH.get(args.workload) if args.table == "builder" else None,
         "note": ("FP32/SFU issue-bound kernel" if prec == "fp32" else "FP64 kernel bound by its dependent FP64 chain")
         + " (no HBM or tensor-core bound applies); peak = SMs x 4 schedulers x "
         f"max SM clock ({sm_max:.0f} MHz, {peak_kind}); achieved = ncu instructions per path-step x live rate",

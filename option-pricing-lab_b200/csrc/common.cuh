@@ -96,6 +96,13 @@ struct DeviceArena {
     T* alloc(size_t count) {
         return static_cast<T*>(raw(count * sizeof(T)));
     }
+    // Host array of count elements of T, already in the device's layout, to a new device buffer in one copy.
+    template <typename T>
+    T* put_raw(const T* host, size_t count) {
+        T* d = alloc<T>(count);
+        check_cuda(cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy (inputs)");
+        return d;
+    }
     // Host array of count elements (converted to T) to a new device buffer; null or empty gives null.
     template <typename T, typename S>
     T* put(const S* host, size_t count, cudaStream_t st = nullptr) {

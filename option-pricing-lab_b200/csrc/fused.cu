@@ -83,7 +83,8 @@ constexpr int min_blocks() {
 }
 
 // KIND: 1 local vol (table), 2 Heston (Euler), 3 SLV (table x Heston, residuals on the aux stream), 4 Heston QE-M.
-template <typename R, int N, int KIND, int PRODUCT>
+// GT: the table is read from global memory (a.tab) instead of the stage.
+template <typename R, int N, int KIND, int PRODUCT, bool GT = false>
 __global__ void __launch_bounds__(512, min_blocks<R>())
     fused_kernel(FusedArgs<R> a, long long n_pairs, long long first_pair, uint32_t k0, uint32_t k1,
                  double* __restrict__ partial) {
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
     const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
     const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
     const R* s_hes = reinterpret_cast<const R*>(sm + a.off.hes);
-    const Pair2<R>* s_tab = reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
+    const Pair2<R>* s_tab = GT ? a.tab : reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
     const R* s_trig = reinterpret_cast<const R*>(sm + a.off.ln_trig);
     const double* s_disc = reinterpret_cast<const double*>(sm + a.off.obs_disc);
     const int S = a.n_steps;
@@ -190,7 +191,8 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                             u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
                             const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
                             const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
-                            const Pair2<R> y0 = s_tab[ns.row + j0], y1 = s_tab[ns.row + j1];
+                            const Pair2<R> y0 = GT ? ldg_pair(s_tab + ns.row + j0) : s_tab[ns.row + j0];
+                            const Pair2<R> y1 = GT ? ldg_pair(s_tab + ns.row + j1) : s_tab[ns.row + j1];
                             const R t0 = y0.a + f0 * y0.b, t1 = y1.a + f1 * y1.b;
                             var0 = KIND == 1 ? t0 : t0 * vp0, var1 = KIND == 1 ? t1 : t1 * vp1;
                         } else {
@@ -331,24 +333,25 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
 template <typename R>
 using FusedFn = void (*)(FusedArgs<R>, long long, long long, uint32_t, uint32_t, double*);
 
-template <typename R, int KIND, int PRODUCT>
+template <typename R, int KIND, int PRODUCT, bool GT>
 FusedFn<R> pick_n(int n) {
-    if (n == 1) return fused_kernel<R, 1, KIND, PRODUCT>;
-    if (n == 2) return fused_kernel<R, 2, KIND, PRODUCT>;
-    if (n == 3) return fused_kernel<R, 3, KIND, PRODUCT>;
+    if (n == 1) return fused_kernel<R, 1, KIND, PRODUCT, GT>;
+    if (n == 2) return fused_kernel<R, 2, KIND, PRODUCT, GT>;
+    if (n == 3) return fused_kernel<R, 3, KIND, PRODUCT, GT>;
     if constexpr (KIND == 1) {
-        if (n == 4) return fused_kernel<R, 4, 1, PRODUCT>;
-        if (n == 5) return fused_kernel<R, 5, 1, PRODUCT>;
+        if (n == 4) return fused_kernel<R, 4, 1, PRODUCT, GT>;
+        if (n == 5) return fused_kernel<R, 5, 1, PRODUCT, GT>;
     }
     return nullptr;
 }
 
+// table_global: the kinds with a table (local vol, SLV) read it from global memory.
 template <typename R, int PRODUCT>
-FusedFn<R> pick_fused(int kind, int n) {
+FusedFn<R> pick_fused(int kind, int n, bool table_global) {
     switch (kind) {
-        case 1: return pick_n<R, 1, PRODUCT>(n);
-        case 2: return pick_n<R, 2, PRODUCT>(n);
-        case 3: return pick_n<R, 3, PRODUCT>(n);
+        case 1: return table_global ? pick_n<R, 1, PRODUCT, true>(n) : pick_n<R, 1, PRODUCT, false>(n);
+        case 2: return pick_n<R, 2, PRODUCT, false>(n);
+        case 3: return table_global ? pick_n<R, 3, PRODUCT, true>(n) : pick_n<R, 3, PRODUCT, false>(n);
         case 4: return n == 1 ? qe_pair_kernel<R, PRODUCT> : nullptr;
         default: return nullptr;
     }
@@ -373,7 +376,9 @@ struct Blob {
 }  // namespace
 
 // Packs the request for the specialised kernel; false when it does not apply (mixed kinds, a basket size without an
-// instantiation, or inputs that would not fit the shared-memory budget), and the generic kernel then runs.
+// instantiation, or inputs that would not fit the shared-memory budget), and the generic kernel then runs. The
+// table goes into the stage when it fits beside the rest, else into global memory (the reference plan's rows: 801
+// points for every step, megabytes), where it stays in L2 and is read through the read-only cache.
 template <typename R>
 bool fused_build(McPlan& plan, const ob_mc_request& rq) {
     const int n = rq.n_names, S = rq.n_steps;
@@ -386,9 +391,11 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
             if (rq.kind[a] != kind) return false;
         if (kind == 0) return false;
     }
-    FusedFn<R> fn = rq.product == OB_PRODUCT_LADDER ? pick_fused<R, OB_PRODUCT_LADDER>(kind, n)
-                                                    : pick_fused<R, OB_PRODUCT_AUTOCALL>(kind, n);
-    if (!fn) return false;
+    auto pick = [&](bool table_global) {
+        return rq.product == OB_PRODUCT_LADDER ? pick_fused<R, OB_PRODUCT_LADDER>(kind, n, table_global)
+                                               : pick_fused<R, OB_PRODUCT_AUTOCALL>(kind, n, table_global);
+    };
+    if (!pick(false)) return false;
     FusedArgs<R> a{};
     a.n_steps = S, a.n_x = rq.n_x, a.same = rq.same;
     a.n_obs = rq.product == OB_PRODUCT_AUTOCALL ? rq.n_obs : 0;
@@ -436,16 +443,6 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
             hes[8 * k + 5] = static_cast<R>(std::sqrt(R(1) - rho * rho));
         }
         a.off.hes = blob.put(hes);
-        if (table) {
-            std::vector<Pair2<R>> tab(static_cast<size_t>(rq.n_rows) * (rq.n_x - 1));
-            for (int r = 0; r < rq.n_rows; ++r)
-                for (int k = 0; k + 1 < rq.n_x; ++k) {
-                    const double* row = rq.table + static_cast<size_t>(r) * rq.n_x;
-                    tab[static_cast<size_t>(r) * (rq.n_x - 1) + k] = {static_cast<R>(row[k]),
-                                                                       static_cast<R>(row[k + 1] - row[k])};
-                }
-            a.off.table2 = blob.put(tab);
-        }
     }
     if (rq.product == OB_PRODUCT_LADDER) {
         std::vector<int> type(rq.n_legs), bar(rq.n_legs);
@@ -470,11 +467,26 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
         a.ln_ki = rq.ki_barrier > 0 ? static_cast<R>(std::log(rq.ki_barrier)) : R(-1e30);
         a.coupon = rq.coupon, a.put_strike = rq.put_strike, a.memory = rq.memory, a.ki_daily = rq.ki_daily;
     }
-    a.smem_blob = static_cast<int>((blob.bytes.size() + 15) & ~static_cast<size_t>(15));
     const int block = 512;
     const size_t acc_bytes = static_cast<size_t>(block / 32) * 2 * a.n_out * sizeof(double);
-    const size_t smem = a.smem_blob + acc_bytes;
     const size_t budget = sizeof(R) == 4 ? (110u << 10) : (220u << 10);  // two blocks a SM in float, one in double
+    bool table_global = false;
+    if (table) {
+        std::vector<Pair2<R>> tab(static_cast<size_t>(rq.n_rows) * (rq.n_x - 1));
+        for (int r = 0; r < rq.n_rows; ++r)
+            for (int k = 0; k + 1 < rq.n_x; ++k) {
+                const double* row = rq.table + static_cast<size_t>(r) * rq.n_x;
+                tab[static_cast<size_t>(r) * (rq.n_x - 1) + k] = {static_cast<R>(row[k]),
+                                                                   static_cast<R>(row[k + 1] - row[k])};
+            }
+        const size_t at = (blob.bytes.size() + 15) & ~static_cast<size_t>(15);
+        table_global = at + tab.size() * sizeof(Pair2<R>) + acc_bytes > budget;
+        if (table_global) a.tab = plan.arena.put_raw(tab.data(), tab.size());
+        else a.off.table2 = blob.put(tab);
+    }
+    const FusedFn<R> fn = pick(table_global);
+    a.smem_blob = static_cast<int>((blob.bytes.size() + 15) & ~static_cast<size_t>(15));
+    const size_t smem = a.smem_blob + acc_bytes;
     if (smem > budget) return false;
     unsigned char* d = plan.arena.alloc<unsigned char>(std::max<size_t>(16, blob.bytes.size()));
     check_cuda(cudaMemcpy(d, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice), "copy blob");

@@ -90,6 +90,7 @@ struct FusedArgs {
     int has_coupon, memory, ki_daily;
     R ln_cb, ln_ki;
     double coupon, put_strike;
+    const Pair2<R>* tab;  // the table in global memory when it does not fit the stage (kernels with GT), else unused
 };
 
 }  // namespace ob

@@ -321,7 +321,7 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
     const size_t tab_bytes = tab.size() * sizeof(Pair2<R>);
     if (blob.size() > budget) return false;
     a.table_global = ((blob.size() + 15) & ~static_cast<size_t>(15)) + tab_bytes > budget;
-    if (a.table_global) a.tab = arena.put<Pair2<R>>(tab.data(), tab.size());
+    if (a.table_global) a.tab = arena.put_raw(tab.data(), tab.size());
     else a.off.table2 = put(tab.data(), tab_bytes);
     a.smem_blob = static_cast<int>(blob.size());
     a.blob = arena.put<unsigned char>(blob.data(), blob.size());
