@@ -739,7 +739,8 @@ def run_script(args, world, rank):
     if rank != 0:
         return
     ph = workloads.Phoenix()
-    held = workloads.lv_phoenix(n_paths=args.paths or 2**20, phoenix=ph)
+    held = workloads.lv_phoenix(n_paths=args.paths or 2**20, phoenix=ph,
+                                grid=reference_rows() if args.table == "reference" else None)
     comp = sc.compile_script(phoenix_script(ph, 252))
     req = sc.script_request(comp, held, lambda t: float(np.exp(-0.02 * t)))
     units = workloads.path_steps(held)
@@ -778,11 +779,13 @@ def run_script(args, world, rank):
         "data": "synthetic (seeded SSVI surface; the default workload's Phoenix as a script)",
         "config": {"workload": "script_phoenix", "n_paths": 2 * held.struct.n_pairs, "n_steps": held.struct.n_steps,
                    "instructions": int(comp.code.shape[0]), "registers": int(comp.n_regs),
+                   "table": f"{held.struct.n_rows} rows x {held.struct.n_x} points ({args.table})",
                    "l2": "no flush: one call holds uploads, kernel and read-back"},
         "fused_kernel": {"ms_per_step": statistics.median(fused_ms), "price": fused.price[0],
                          "script_over_fused_time": t_ms / statistics.median(fused_ms)},
         "roofline": issue_roofline(
-            INST_PER_PATH_STEP["script"] * units / (t_ms / 1e3) if held.struct.n_pairs == 2**19 else None,
+            INST_PER_PATH_STEP["script"] * units / (t_ms / 1e3)
+            if held.struct.n_pairs == 2**19 and args.table == "builder" else None,
             "the local-vol step plus the interpreter at events; achieved = ncu warp instructions per path-step x "
             "live rate"),
         "cpu_baseline": None,

@@ -433,11 +433,14 @@ struct LvArgs {
     const unsigned char* blob;
     int smem_blob;
     R top;
+    const Pair2<R>* tab;  // the table in global memory when it does not fit the stage (kernels with GT), else unused
+    int table_global;
 };
 
 // BRANCH: the pairs continue the paths of an outer simulation after step end d.branch_step (one leg per outer path:
 // before the branch both legs take the outer path's normals, the outer antithetic leg's with the sign flipped).
-template <typename R, int N, int NW, bool BRANCH, bool CALLS>
+// GT: the table is read from global memory (a.tab) instead of the stage.
+template <typename R, int N, int NW, bool BRANCH, bool CALLS, bool GT = false>
 __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
     script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0, uint32_t k1,
                      double* __restrict__ partial) {
@@ -457,7 +460,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
     const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
     const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
     const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
-    const Pair2<R>* s_tab = reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
+    const Pair2<R>* s_tab = GT ? a.tab : reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
     const int2* s_sched = reinterpret_cast<const int2*>(sm + a.off.sched);  // (event, window mask) per step end
     const R* s_lf0 = reinterpret_cast<const R*>(sm + a.off.lf0);
     const int S = d.n_steps;
@@ -548,7 +551,8 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
                     u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
                     const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
                     const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
-                    const Pair2<R> p0 = s_tab[ns.row + j0], p1 = s_tab[ns.row + j1];
+                    const Pair2<R> p0 = GT ? ldg_pair(s_tab + ns.row + j0) : s_tab[ns.row + j0];
+                    const Pair2<R> p1 = GT ? ldg_pair(s_tab + ns.row + j1) : s_tab[ns.row + j1];
                     const R v0 = p0.a + f0 * p0.b, v1 = p1.a + f1 * p1.b;
                     // sqrt(dt) z with the legs' signs (+1, -1 but before a branch), the step's multiply-add written
                     // out: the same arithmetic in every instantiation, so a branch at step 0 is an ordinary run bit
@@ -589,14 +593,14 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
 template <typename R>
 using ScriptLvFn = void (*)(ScriptDev<R>, LvArgs<R>, long long, uint32_t, uint32_t, double*);
 
-template <typename R, int NW, bool CALLS>
+template <typename R, int NW, bool CALLS, bool GT = false>
 ScriptLvFn<R> pick_lv_calls(int n) {
     switch (n) {
-        case 1: return script_lv_kernel<R, 1, NW, false, CALLS>;
-        case 2: return script_lv_kernel<R, 2, NW, false, CALLS>;
-        case 3: return script_lv_kernel<R, 3, NW, false, CALLS>;
-        case 4: return script_lv_kernel<R, 4, NW, false, CALLS>;
-        case 5: return script_lv_kernel<R, 5, NW, false, CALLS>;
+        case 1: return script_lv_kernel<R, 1, NW, false, CALLS, GT>;
+        case 2: return script_lv_kernel<R, 2, NW, false, CALLS, GT>;
+        case 3: return script_lv_kernel<R, 3, NW, false, CALLS, GT>;
+        case 4: return script_lv_kernel<R, 4, NW, false, CALLS, GT>;
+        case 5: return script_lv_kernel<R, 5, NW, false, CALLS, GT>;
         default: return nullptr;
     }
 }
@@ -609,15 +613,19 @@ ScriptLvFn<R> pick_lv_nw(int n, bool branch, bool calls) {
 
 // Kernels for one window (a knock-in barrier: its state alone stays in registers under the 64-register cap of two
 // blocks an SM, where a second window's spills it to local memory, 3.11 -> 2.67 ms for the 3-year daily-window
-// Phoenix), up to 2 and up to 8.
+// Phoenix), up to 2 and up to 8. A table in global memory (table_global) only comes with up to 2 windows, no call and
+// no branch (pack_lv checks).
 template <typename R>
-ScriptLvFn<R> pick_lv(int n, int n_windows, bool branch, bool calls) {
+ScriptLvFn<R> pick_lv(int n, int n_windows, bool branch, bool calls, bool table_global) {
+    if (table_global) return n_windows <= 1 ? pick_lv_calls<R, 1, false, true>(n) : pick_lv_calls<R, 2, false, true>(n);
     if (n_windows <= 1 && !branch && !calls) return pick_lv_calls<R, 1, false>(n);
     return n_windows <= 2 ? pick_lv_nw<R, 2>(n, branch, calls) : pick_lv_nw<R, kMaxWindows>(n, branch, calls);
 }
 
 // The staged blob of the local-vol path, or false when it does not apply (a name not local vol, more than five
-// names, or more than the shared-memory budget: 110 KB in float, 220 KB in double).
+// names, or more than the shared-memory budget: 110 KB in float, 220 KB in double, without the table). The table
+// goes into the stage when it fits beside the rest, else into global memory (L2-resident, read through the read-only
+// cache) for scripts with up to two windows, no call and no branch.
 template <typename R>
 bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, DeviceArena& arena, LvArgs<R>& a) {
     const ob_mc_request& q = rq.model;
@@ -655,16 +663,19 @@ bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, Device
     for (int k = 0; k < n; ++k) lf0[k] = static_cast<R>(q.log_fwd[static_cast<size_t>(k) * (S + 1)]);
     a.off.root = put(root.data(), root.size() * sizeof(R));
     a.off.lf0 = put(lf0.data(), lf0.size() * sizeof(R));
+    a.off.sched = put(sched.data(), sched.size() * sizeof(int2));
     std::vector<Pair2<R>> tab(static_cast<size_t>(q.n_rows) * (q.n_x - 1));
     for (int r = 0; r < q.n_rows; ++r)
         for (int k = 0; k + 1 < q.n_x; ++k) {
             const double* row = q.table + static_cast<size_t>(r) * q.n_x;
             tab[static_cast<size_t>(r) * (q.n_x - 1) + k] = {static_cast<R>(row[k]), static_cast<R>(row[k + 1] - row[k])};
         }
-    a.off.table2 = put(tab.data(), tab.size() * sizeof(Pair2<R>));
-    a.off.sched = put(sched.data(), sched.size() * sizeof(int2));
     const size_t budget = sizeof(R) == 4 ? (110u << 10) : (220u << 10);
     if (blob.size() > budget) return false;
+    a.table_global = ((blob.size() + 15) & ~static_cast<size_t>(15)) + tab.size() * sizeof(Pair2<R>) > budget;
+    if (a.table_global && (rq.branch || rq.n_calls > 0 || rq.n_windows > 2)) return false;
+    if (a.table_global) a.tab = arena.put_raw(tab.data(), tab.size());
+    else a.off.table2 = put(tab.data(), tab.size() * sizeof(Pair2<R>));
     a.smem_blob = static_cast<int>((blob.size() + 15) & ~static_cast<size_t>(15));
     unsigned char* dblob = arena.alloc<unsigned char>(std::max<size_t>(16, blob.size()));
     check_cuda(cudaMemcpy(dblob, blob.data(), blob.size(), cudaMemcpyHostToDevice), "copy blob");
@@ -898,7 +909,8 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     LvArgs<R> lv{};
     const bool fast = pack_lv<R>(rq, sched, arena, lv);
     if (rq.branch && !fast) invalid("a branched run needs the staged local-vol kernel (its tables too large)");
-    const void* fn = fast ? reinterpret_cast<const void*>(pick_lv<R>(n, rq.n_windows, rq.branch != 0, rq.n_calls > 0))
+    const void* fn = fast ? reinterpret_cast<const void*>(
+                                pick_lv<R>(n, rq.n_windows, rq.branch != 0, rq.n_calls > 0, lv.table_global != 0))
                           : reinterpret_cast<const void*>(pick_script<R>(mq.model, n, rq.n_windows));
     const int block = fast ? 512 : 128;
     const size_t smem = fast ? static_cast<size_t>(lv.smem_blob) : 0;

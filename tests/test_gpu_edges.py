@@ -1,8 +1,8 @@
 """Edge sizes on the GPU against the oracle: pair counts that fill no warp or leave the last one ragged, a single time
 step, the first pair far into the stream, and a local-variance table as large as the reference's own rows (801
-points for each of 756 steps, RN/src/optlab/native/__init__.py:129-144): more than the fused kernel's shared-memory
-stage holds, so the request falls through to the kernel that reads the table from global memory. FP64 within the
-tolerances of the parity tests, FP32 within 4 standard errors of the FP64 oracle."""
+points for each of 756 steps, RN/src/optlab/native/__init__.py:129-144): more than the kernels' shared-memory stage
+holds, so the path, fused and script kernels read the rows from global memory. FP64 within the tolerances of the
+parity tests, FP32 within 4 standard errors of the FP64 oracle."""
 
 import numpy as np
 import pytest
@@ -106,7 +106,7 @@ def test_paths_on_a_reference_size_table_match_the_oracle(oracle, reference_size
 
 def test_a_table_larger_than_the_shared_memory_stage_prices_like_the_oracle(oracle, reference_size_grid):
     held = _phoenix(2**12, reference_size_grid)
-    assert held.struct.n_rows == 756 and held.struct.n_x == 801  # 2.4 MB of float (value, slope) pairs: global
+    assert held.struct.n_rows == 756 and held.struct.n_x == 801  # 4.8 MB of float (value, slope) pairs: global
     g64 = engine.mc_price(held, "fp64")
     o = oracle.mc_price(_phoenix(2**12, reference_size_grid))
     assert abs(g64.price[0] / o.price[0] - 1) < 1e-10, (g64.price[0], o.price[0])
@@ -125,3 +125,20 @@ def test_a_script_at_a_ragged_pair_count_matches_the_oracle(oracle):
     assert res.n_paths == 90
     assert abs(res.price - want) <= 1e-10 * max(abs(want), 1e-3), (res.price, want)
     assert abs(res.se - se) <= 1e-6 * se + 1e-15
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_a_script_on_a_reference_size_table_equals_the_fused_kernel(reference_size_grid, prec):
+    """The Phoenix as a payoff script with the rows left in global memory, against the fused kernel on the same rows
+    (itself checked against the oracle above): FP64 to rounding, FP32 within 4 standard errors."""
+    from test_gpu_script import _phoenix_script
+
+    ph = workloads.Phoenix()
+    held = _phoenix(2**12, reference_size_grid)
+    comp = sc.compile_script(_phoenix_script(ph, 252), params={"S0": float(held.struct.spot[0])})
+    fused = engine.mc_price(_phoenix(2**12, reference_size_grid), "fp64")
+    res = sc.run(sc.script_request(comp, held, lambda t: np.exp(-0.02 * t)), prec)
+    if prec == "fp64":
+        assert abs(res.price - fused.price[0]) <= 1e-10 * abs(fused.price[0]), (res.price, fused.price[0])
+    else:
+        assert abs(res.price - fused.price[0]) < 4 * fused.se[0], (res.price, fused.price[0], fused.se[0])
