@@ -3,13 +3,15 @@
 // extremes written in the reference's layout (out[(a n_cols + c) 2 n_pairs + row], pair p at row p, its antithetic
 // at n_pairs + p), in float or double. The request is checked as RC/src/requests.cpp:168-207 does.
 //
-// Baskets of one to five names all in local vol without a mixer (the common case: every local-vol quote) run a
-// specialised kernel, paths_lv_kernel: the fused kernels' step (per-step records, correlation root and the table as
-// (y, dy) pairs staged in shared memory, normals drawn in batches of whole Philox blocks; the same stream order as
-// the generic engine), and per step end the observations taken there, read from a staged schedule. Columns and
-// window extremes are the reference's S = F_j exp(x) at each observation (kept columns written, window extremes
-// compared on S), so a window's extremes equal those of the full columns bit for bit. Other requests run the generic
-// kernel, which follows RC/include/optlab_cuda/paths.hpp step for step.
+// Baskets whose names share one model kind, without a mixer (one to five names in local vol, one to three in Heston
+// or SLV: every single-model quote), run a specialised kernel, paths_staged_kernel: the fused kernels' step
+// (per-step records, correlation root, Heston parameters and the table as (y, dy) pairs staged in shared memory,
+// normals drawn in batches of whole Philox blocks in the generic engine's stream order: the spot normals, then the
+// residuals, from stream 0 for Heston and from the aux stream for SLV), and per step end the observations taken
+// there, read from a staged schedule. Columns and window extremes are the reference's S = F_j exp(x) at each
+// observation (kept columns written, window extremes compared on S), so a window's extremes equal those of the full
+// columns bit for bit. Other requests run the generic kernel, which follows RC/include/optlab_cuda/paths.hpp step for
+// step.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -90,9 +92,9 @@ __global__ void __launch_bounds__(256) paths_kernel(PathsDev<R> s) {
     }
 }
 
-// Offsets of the staged blob of paths_lv_kernel (bytes).
+// Offsets of the staged blob of paths_staged_kernel (bytes).
 struct PathsLvOffsets {
-    int step, name_step, root, table2, sched, col, fwd;
+    int step, name_step, root, hes, table2, sched, col, fwd;
 };
 
 template <typename R>
@@ -108,6 +110,7 @@ struct PathsLvArgs {
     double* out;
     const Pair2<R>* tab;  // the table in global memory when it does not fit the stage (table_global), else unused
     int table_global;
+    int kind, same;  // the names' model kind (1 local vol, 2 Heston, 3 SLV); residuals through the root
 };
 
 // Observation j of both legs: the kept column and the windows that hold it, on S = F_j exp(x) as the reference.
@@ -151,12 +154,17 @@ constexpr int lv_block() {
     return N <= 2 ? 512 : 256;
 }
 
-// GT: the table is read from global memory (a.tab) instead of the stage.
-template <typename R, int N, bool GT>
-__global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 1) paths_lv_kernel(PathsLvArgs<R> a) {
-    constexpr int C = N;
+// KIND: 1 local vol (table), 2 Heston (Euler), 3 SLV (table x Heston, residuals on the aux stream). GT: the table is
+// read from global memory (a.tab) instead of the stage.
+template <typename R, int N, int KIND, bool GT>
+__global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 1)
+    paths_staged_kernel(PathsLvArgs<R> a) {
+    constexpr bool VAR = KIND == 2 || KIND == 3;
+    constexpr bool TABLE = KIND == 1 || KIND == 3;
+    constexpr int C = KIND == 2 ? 2 * N : N;  // normals per step, stream 0
+    constexpr int CA = KIND == 3 ? N : 0;     // normals per step, aux stream
     constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);  // steps per batch of whole Philox blocks
-    constexpr int NB = C * G / 4;
+    constexpr int NB = C * G / 4, NBA = CA * G / 4;
     extern __shared__ __align__(16) unsigned char sm[];
     {
         const int4* src = reinterpret_cast<const int4*>(a.blob);
@@ -167,6 +175,7 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
     const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
     const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
     const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
+    const R* s_hes = reinterpret_cast<const R*>(sm + a.off.hes);  // per name: v0, kappa, theta, xi, rho, sqrt(1 - rho^2)
     const Pair2<R>* tab = GT ? a.tab : reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
     const int2* s_sched = reinterpret_cast<const int2*>(sm + a.off.sched);  // observations [x, y) at each step end
     const int* s_col = reinterpret_cast<const int*>(sm + a.off.col);
@@ -179,41 +188,71 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
         const bool active = base + lane < a.n_pairs;
         const long long p = active ? base + lane : a.n_pairs - 1;
         const uint64_t pair = static_cast<uint64_t>(a.first_pair + p);
-        R x0[N], x1[N], lo[2][N][2], hi[2][N][2];
+        R x0[N], x1[N], v0[N], v1[N], lo[2][N][2], hi[2][N][2];
 #pragma unroll
         for (int n = 0; n < N; ++n) {
             x0[n] = x1[n] = R(0);
+            v0[n] = v1[n] = VAR ? s_hes[8 * n] : R(0);
 #pragma unroll
             for (int w = 0; w < 2; ++w) lo[0][n][w] = lo[1][n][w] = hi[0][n][w] = hi[1][n][w] = R(0);
         }
         for (int j = s_sched[0].x; j < s_sched[0].y; ++j) lv_record<R, N>(a, s_col, s_fwd, j, p, active, x0, x1, lo, hi);
         for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) {
             R z[C * G];
+            R za[CA > 0 ? CA * G : 1];
 #pragma unroll
             for (int k = 0; k < NB; ++k)
                 normals4<R>(pair, static_cast<uint64_t>(b) * NB + k, 0u, a.k0, a.k1, z[4 * k], z[4 * k + 1],
                             z[4 * k + 2], z[4 * k + 3]);
 #pragma unroll
+            for (int k = 0; k < NBA; ++k)
+                normals4<R>(pair, static_cast<uint64_t>(b) * NBA + k, kAuxStream, a.k0, a.k1, za[4 * k],
+                            za[4 * k + 1], za[4 * k + 2], za[4 * k + 3]);
+#pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int i = i0 + g;
                 if (G > 1 && i > S) break;
                 const StepRec<R> st = s_step[i - 1];
+                R wc[N];  // the variance's residual normals (correlated through the root when `same`)
+                if (VAR) {
+                    const R* zr = KIND == 3 ? &za[g * CA] : &z[g * C + N];
+#pragma unroll
+                    for (int n = 0; n < N; ++n) {
+                        R acc = R(0);
+#pragma unroll
+                        for (int m = 0; m < N; ++m) acc += s_root[n * N + m] * zr[m];
+                        wc[n] = a.same ? acc : zr[n];
+                    }
+                }
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     R zc = R(0);
 #pragma unroll
                     for (int m = 0; m < N; ++m) zc += s_root[n * N + m] * z[g * C + m];
                     const NameStep<R> ns = s_ns[(i - 1) * N + n];
-                    R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
-                    u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
-                    const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
-                    const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
-                    const Pair2<R> y0 = GT ? ldg_pair(tab + ns.row + j0) : tab[ns.row + j0];
-                    const Pair2<R> y1 = GT ? ldg_pair(tab + ns.row + j1) : tab[ns.row + j1];
-                    const R v0 = y0.a + f0 * y0.b, v1 = y1.a + f1 * y1.b;
+                    R var0, var1, vp0 = R(0), vp1 = R(0);
+                    if (VAR) vp0 = m_max(v0[n], R(0)), vp1 = m_max(v1[n], R(0));
+                    if (TABLE) {
+                        R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
+                        u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
+                        const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
+                        const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
+                        const Pair2<R> y0 = GT ? ldg_pair(tab + ns.row + j0) : tab[ns.row + j0];
+                        const Pair2<R> y1 = GT ? ldg_pair(tab + ns.row + j1) : tab[ns.row + j1];
+                        const R t0 = y0.a + f0 * y0.b, t1 = y1.a + f1 * y1.b;
+                        var0 = KIND == 1 ? t0 : t0 * vp0, var1 = KIND == 1 ? t1 : t1 * vp1;
+                    } else {
+                        var0 = vp0, var1 = vp1;
+                    }
+                    if (VAR) {
+                        const R* h = s_hes + 8 * n;
+                        const R zv = h[4] * zc + h[5] * wc[n];
+                        v0[n] += h[1] * (h[2] - vp0) * st.dt + h[3] * (m_sqrt(vp0) * st.sdt) * zv;
+                        v1[n] += h[1] * (h[2] - vp1) * st.dt + h[3] * (m_sqrt(vp1) * st.sdt) * (-zv);
+                    }
                     const R zd = st.sdt * zc;  // sqrt(dt) z, the legs' +-
-                    x0[n] += m_fma(m_sqrt(v0), zd, v0 * st.hdt);
-                    x1[n] += m_fma(-m_sqrt(v1), zd, v1 * st.hdt);
+                    x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
+                    x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
                 }
                 const int2 ob = s_sched[i];
                 for (int j = ob.x; j < ob.y; ++j) lv_record<R, N>(a, s_col, s_fwd, j, p, active, x0, x1, lo, hi);
@@ -262,17 +301,19 @@ void check_request(const ob_paths_request& c) {
         if (c.win_lo[w] < 0 || c.win_hi[w] < c.win_lo[w] || c.win_hi[w] >= c.n_obs) invalid("bad window");
 }
 
-// The staged blob of paths_lv_kernel, or false when the request is not for it (a name not in local vol, a mixer,
-// more than five names, or a blob beyond the shared-memory budget: 110 KB in float, 200 KB in double, without the
-// table). The table goes into the stage when it fits beside the rest, else into global memory: a plan's per-step rows
+// The staged blob of paths_staged_kernel, or false when the request is not for it (names of different kinds or in
+// Black-Scholes, a mixer, more than five local-vol or three Heston / SLV names, or a blob beyond the shared-memory
+// budget: 110 KB in float, 200 KB in double, without the table). The table goes into the stage when it fits beside the rest, else into global memory: a plan's per-step rows
 // (801 points for each of the 756 steps of three daily years, 4.8 MB in float) stay in L2 and are read through the
 // read-only cache.
 template <typename R>
-bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>& a) {
-    const int n = h.n_names, S = h.n_steps;
-    if (h.mixer || n > 5 || S < 1) return false;
+bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>& a) {
+    const int n = h.n_names, S = h.n_steps, kind = h.kind[0];
+    if (h.mixer || S < 1 || kind < 1 || kind > 3 || n > (kind == 1 ? 5 : 3)) return false;
     for (int k = 0; k < n; ++k)
-        if (h.kind[k] != 1) return false;
+        if (h.kind[k] != kind) return false;
+    const bool table = kind != 2;
+    a.kind = kind, a.same = h.same;
     std::vector<unsigned char> blob;
     auto put = [&](const void* src, size_t bytes) {
         const size_t at = (blob.size() + 15) & ~static_cast<size_t>(15);
@@ -292,6 +333,7 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
         for (int k = 0; k < n; ++k) {
             NameStep<R>& r = ns[static_cast<size_t>(i) * n + k];
             std::memset(&r, 0, sizeof r);
+            if (!table) continue;
             const int row = h.step_row[static_cast<size_t>(k) * S + i];
             r.org = name_step_org<R>(h.row_lo[row], h.row_inv_dx[row]), r.inv_dx = static_cast<R>(h.row_inv_dx[row]);
             r.row = row * (h.n_x - 1);
@@ -300,6 +342,12 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
     std::vector<R> root(static_cast<size_t>(n) * n);
     for (size_t k = 0; k < root.size(); ++k) root[k] = static_cast<R>(h.root[k]);
     a.off.root = put(root.data(), root.size() * sizeof(R));
+    std::vector<R> hes(8 * static_cast<size_t>(n), R(0));
+    for (int k = 0; k < n; ++k) {
+        for (int f = 0; f < 5; ++f) hes[8 * k + f] = static_cast<R>(h.heston[5 * k + f]);
+        hes[8 * k + 5] = static_cast<R>(std::sqrt(1.0 - h.heston[5 * k + 4] * h.heston[5 * k + 4]));
+    }
+    a.off.hes = put(hes.data(), hes.size() * sizeof(R));
     std::vector<int2> sched(S + 1);
     for (int i = 0, j = 0; i <= S; ++i) {
         sched[i].x = j;
@@ -311,8 +359,8 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
     std::vector<R> fwd(static_cast<size_t>(n) * h.n_obs);
     for (size_t k = 0; k < fwd.size(); ++k) fwd[k] = static_cast<R>(h.fwd[k]);
     a.off.fwd = put(fwd.data(), fwd.size() * sizeof(R));
-    std::vector<Pair2<R>> tab(static_cast<size_t>(h.n_rows) * (h.n_x - 1));
-    for (int r = 0; r < h.n_rows; ++r)
+    std::vector<Pair2<R>> tab(table ? static_cast<size_t>(h.n_rows) * (h.n_x - 1) : 0);
+    for (int r = 0; r < (table ? h.n_rows : 0); ++r)
         for (int k = 0; k + 1 < h.n_x; ++k) {
             const double y = h.table[static_cast<size_t>(r) * h.n_x + k], y1 = h.table[static_cast<size_t>(r) * h.n_x + k + 1];
             tab[static_cast<size_t>(r) * (h.n_x - 1) + k] = {static_cast<R>(y), static_cast<R>(y1 - y)};
@@ -337,20 +385,28 @@ bool pack_paths_lv(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>
 
 inline int lv_block_of(int n) { return n <= 2 ? lv_block<1>() : lv_block<3>(); }
 
-template <typename R, bool GT>
-const void* pick_paths_lv_gt(int n) {
+template <typename R, int KIND, bool GT>
+const void* pick_paths_n(int n) {
     switch (n) {
-        case 1: return reinterpret_cast<const void*>(paths_lv_kernel<R, 1, GT>);
-        case 2: return reinterpret_cast<const void*>(paths_lv_kernel<R, 2, GT>);
-        case 3: return reinterpret_cast<const void*>(paths_lv_kernel<R, 3, GT>);
-        case 4: return reinterpret_cast<const void*>(paths_lv_kernel<R, 4, GT>);
-        default: return reinterpret_cast<const void*>(paths_lv_kernel<R, 5, GT>);
+        case 1: return reinterpret_cast<const void*>(paths_staged_kernel<R, 1, KIND, GT>);
+        case 2: return reinterpret_cast<const void*>(paths_staged_kernel<R, 2, KIND, GT>);
+        case 3: return reinterpret_cast<const void*>(paths_staged_kernel<R, 3, KIND, GT>);
     }
+    if constexpr (KIND == 1) {
+        if (n == 4) return reinterpret_cast<const void*>(paths_staged_kernel<R, 4, KIND, GT>);
+        if (n == 5) return reinterpret_cast<const void*>(paths_staged_kernel<R, 5, KIND, GT>);
+    }
+    return nullptr;
 }
 
 template <typename R>
-const void* pick_paths_lv(int n, bool table_global) {
-    return table_global ? pick_paths_lv_gt<R, true>(n) : pick_paths_lv_gt<R, false>(n);
+const void* pick_paths_staged(int n, int kind, bool table_global) {
+    switch (kind) {
+        case 1: return table_global ? pick_paths_n<R, 1, true>(n) : pick_paths_n<R, 1, false>(n);
+        case 2: return pick_paths_n<R, 2, false>(n);
+        case 3: return table_global ? pick_paths_n<R, 3, true>(n) : pick_paths_n<R, 3, false>(n);
+        default: return nullptr;
+    }
 }
 
 template <typename R>
@@ -391,8 +447,9 @@ void run_paths(ob_paths_request& h) {
     s.win_hi = arena.put<int>(h.win_hi, h.n_windows);
     s.fwd = arena.put<R>(h.fwd, static_cast<size_t>(n) * h.n_obs);
     PathsLvArgs<R> lv{};
-    const bool fast = pack_paths_lv<R>(h, arena, lv);
-    const void* lv_fn = fast ? pick_paths_lv<R>(n, lv.table_global != 0) : nullptr;
+    const void* lv_fn = pack_paths_staged<R>(h, arena, lv) ? pick_paths_staged<R>(n, lv.kind, lv.table_global != 0)
+                                                          : nullptr;
+    const bool fast = lv_fn != nullptr;
     int lv_grid = 0;
     if (fast) {
         check_cuda(cudaFuncSetAttribute(lv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lv.smem_blob),
