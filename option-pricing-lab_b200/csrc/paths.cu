@@ -3,8 +3,8 @@
 // extremes written in the reference's layout (out[(a n_cols + c) 2 n_pairs + row], pair p at row p, its antithetic
 // at n_pairs + p), in float or double. The request is checked as RC/src/requests.cpp:168-207 does.
 //
-// Baskets whose names share one model kind, without a mixer (one to five names in local vol, one to three in Heston
-// or SLV: every single-model quote), run a specialised kernel, paths_staged_kernel: the fused kernels' step
+// Baskets whose names share one model kind, without a mixer (one to five names in Black-Scholes or local vol, one to
+// three in Heston or SLV: every single-model quote), run a specialised kernel, paths_staged_kernel: the fused kernels' step
 // (per-step records, correlation root, Heston parameters and the table as (y, dy) pairs staged in shared memory,
 // normals drawn in batches of whole Philox blocks in the generic engine's stream order: the spot normals, then the
 // residuals, from stream 0 for Heston and from the aux stream for SLV), and per step end the observations taken
@@ -110,7 +110,7 @@ struct PathsLvArgs {
     double* out;
     const Pair2<R>* tab;  // the table in global memory when it does not fit the stage (table_global), else unused
     int table_global;
-    int kind, same;  // the names' model kind (1 local vol, 2 Heston, 3 SLV); residuals through the root
+    int kind, same;  // the names' model kind (0 Black-Scholes, 1 local vol, 2 Heston, 3 SLV); residuals through the root
 };
 
 // Observation j of both legs: the kept column and the windows that hold it, on S = F_j exp(x) as the reference.
@@ -154,8 +154,8 @@ constexpr int lv_block() {
     return N <= 2 ? 512 : 256;
 }
 
-// KIND: 1 local vol (table), 2 Heston (Euler), 3 SLV (table x Heston, residuals on the aux stream). GT: the table is
-// read from global memory (a.tab) instead of the stage.
+// KIND: 0 Black-Scholes (constant variance), 1 local vol (table), 2 Heston (Euler), 3 SLV (table x Heston, residuals
+// on the aux stream). GT: the table is read from global memory (a.tab) instead of the stage.
 template <typename R, int N, int KIND, bool GT>
 __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 1)
     paths_staged_kernel(PathsLvArgs<R> a) {
@@ -175,7 +175,8 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
     const StepRec<R>* s_step = reinterpret_cast<const StepRec<R>*>(sm + a.off.step);
     const NameStep<R>* s_ns = reinterpret_cast<const NameStep<R>*>(sm + a.off.name_step);
     const R* s_root = reinterpret_cast<const R*>(sm + a.off.root);
-    const R* s_hes = reinterpret_cast<const R*>(sm + a.off.hes);  // per name: v0, kappa, theta, xi, rho, sqrt(1 - rho^2)
+    // per name: v0, kappa, theta, xi, rho, sqrt(1 - rho^2), the constant variance (Black-Scholes)
+    const R* s_hes = reinterpret_cast<const R*>(sm + a.off.hes);
     const Pair2<R>* tab = GT ? a.tab : reinterpret_cast<const Pair2<R>*>(sm + a.off.table2);
     const int2* s_sched = reinterpret_cast<const int2*>(sm + a.off.sched);  // observations [x, y) at each step end
     const int* s_col = reinterpret_cast<const int*>(sm + a.off.col);
@@ -241,8 +242,10 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
                         const Pair2<R> y1 = GT ? ldg_pair(tab + ns.row + j1) : tab[ns.row + j1];
                         const R t0 = y0.a + f0 * y0.b, t1 = y1.a + f1 * y1.b;
                         var0 = KIND == 1 ? t0 : t0 * vp0, var1 = KIND == 1 ? t1 : t1 * vp1;
-                    } else {
+                    } else if (VAR) {
                         var0 = vp0, var1 = vp1;
+                    } else {
+                        var0 = var1 = s_hes[8 * n + 6];
                     }
                     if (VAR) {
                         const R* h = s_hes + 8 * n;
@@ -301,18 +304,18 @@ void check_request(const ob_paths_request& c) {
         if (c.win_lo[w] < 0 || c.win_hi[w] < c.win_lo[w] || c.win_hi[w] >= c.n_obs) invalid("bad window");
 }
 
-// The staged blob of paths_staged_kernel, or false when the request is not for it (names of different kinds or in
-// Black-Scholes, a mixer, more than five local-vol or three Heston / SLV names, or a blob beyond the shared-memory
-// budget: 110 KB in float, 200 KB in double, without the table). The table goes into the stage when it fits beside the rest, else into global memory: a plan's per-step rows
-// (801 points for each of the 756 steps of three daily years, 4.8 MB in float) stay in L2 and are read through the
-// read-only cache.
+// The staged blob of paths_staged_kernel, or false when the request is not for it (names of different kinds, a
+// mixer, more than five Black-Scholes / local-vol or three Heston / SLV names, or a blob beyond the shared-memory
+// budget: 110 KB in float, 200 KB in double, without the table). The table goes into the stage when it fits beside
+// the rest, else into global memory: a plan's per-step rows (801 points for each of the 756 steps of three daily
+// years, 4.8 MB in float) stay in L2 and are read through the read-only cache.
 template <typename R>
 bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>& a) {
     const int n = h.n_names, S = h.n_steps, kind = h.kind[0];
-    if (h.mixer || S < 1 || kind < 1 || kind > 3 || n > (kind == 1 ? 5 : 3)) return false;
+    if (h.mixer || S < 1 || kind < 0 || kind > 3 || n > (kind <= 1 ? 5 : 3)) return false;
     for (int k = 0; k < n; ++k)
         if (h.kind[k] != kind) return false;
-    const bool table = kind != 2;
+    const bool table = kind == 1 || kind == 3;
     a.kind = kind, a.same = h.same;
     std::vector<unsigned char> blob;
     auto put = [&](const void* src, size_t bytes) {
@@ -346,6 +349,7 @@ bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArg
     for (int k = 0; k < n; ++k) {
         for (int f = 0; f < 5; ++f) hes[8 * k + f] = static_cast<R>(h.heston[5 * k + f]);
         hes[8 * k + 5] = static_cast<R>(std::sqrt(1.0 - h.heston[5 * k + 4] * h.heston[5 * k + 4]));
+        hes[8 * k + 6] = static_cast<R>(h.cvar[k]);
     }
     a.off.hes = put(hes.data(), hes.size() * sizeof(R));
     std::vector<int2> sched(S + 1);
@@ -392,7 +396,7 @@ const void* pick_paths_n(int n) {
         case 2: return reinterpret_cast<const void*>(paths_staged_kernel<R, 2, KIND, GT>);
         case 3: return reinterpret_cast<const void*>(paths_staged_kernel<R, 3, KIND, GT>);
     }
-    if constexpr (KIND == 1) {
+    if constexpr (KIND <= 1) {
         if (n == 4) return reinterpret_cast<const void*>(paths_staged_kernel<R, 4, KIND, GT>);
         if (n == 5) return reinterpret_cast<const void*>(paths_staged_kernel<R, 5, KIND, GT>);
     }
@@ -402,6 +406,7 @@ const void* pick_paths_n(int n) {
 template <typename R>
 const void* pick_paths_staged(int n, int kind, bool table_global) {
     switch (kind) {
+        case 0: return pick_paths_n<R, 0, false>(n);
         case 1: return table_global ? pick_paths_n<R, 1, true>(n) : pick_paths_n<R, 1, false>(n);
         case 2: return pick_paths_n<R, 2, false>(n);
         case 3: return table_global ? pick_paths_n<R, 3, true>(n) : pick_paths_n<R, 3, false>(n);

@@ -145,12 +145,13 @@ def test_a_script_on_a_reference_size_table_equals_the_fused_kernel(reference_si
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
-@pytest.mark.parametrize("kinds,same", [([2, 2], 1), ([2, 2, 2], 0), ([3, 3], 1), ([3, 3, 3], 0)],
-                         ids=["heston x2", "heston x3 independent", "slv x2", "slv x3 independent"])
-def test_heston_and_slv_baskets_on_the_staged_path_kernel_match_the_oracle(oracle, kinds, same, prec):
-    """Names of one variance kind run the staged path kernel (residuals from stream 0 for Heston, from the aux
-    stream for SLV; correlated through the root when `same`): FP64 to the Heston criterion of the parity tests, FP32
-    to the reference's float criterion (packages/native/tests/test_native.py:95-111)."""
+@pytest.mark.parametrize("kinds,same", [([2, 2], 1), ([2, 2, 2], 0), ([3, 3], 1), ([3, 3, 3], 0), ([0] * 5, 1)],
+                         ids=["heston x2", "heston x3 independent", "slv x2", "slv x3 independent", "bs x5"])
+def test_baskets_of_one_kind_on_the_staged_path_kernel_match_the_oracle(oracle, kinds, same, prec):
+    """Names of one kind run the staged path kernel (Heston residuals from stream 0, SLV residuals from the aux
+    stream, correlated through the root when `same`; Black-Scholes at its constant variance): FP64 to the Heston
+    criterion of the parity tests, FP32 to the reference's float criterion
+    (packages/native/tests/test_native.py:95-111)."""
     kw = dict(_paths(kinds, 2048, n_steps=60), same=same)
     g, o = paths_request(**kw), paths_request(**kw)
     engine.paths(g, prec)
