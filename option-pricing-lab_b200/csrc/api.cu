@@ -124,6 +124,7 @@ int ob_philox_normals(unsigned long long seed, long long first_pair, long long n
         if (n > (1LL << 28)) ob::invalid("at most 2^28 blocks per call");
         ob::require_device();
         ob::DeviceArena arena;
+        arena.recycle = true;  // the blocking copies below end the call's device work
         unsigned* du = arena.alloc<unsigned>(4 * n);
         double* dz = arena.alloc<double>(4 * n);
         float* df = arena.alloc<float>(4 * n);

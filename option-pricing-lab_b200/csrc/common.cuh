@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -72,24 +73,88 @@ struct Stream {
     cudaStream_t get() const { return s; }
 };
 
-// Owns device allocations for one call or one plan.
+// Device buffers that finished calls handed back, for the next call of the process: a one-shot call's cudaMalloc and
+// cudaFree (a few hundred microseconds together, and cudaFree waits for the whole device) become a lookup. At most
+// kBytes are held over all devices; a buffer is reused for a request of at least half its size. The cache is never
+// destroyed: its buffers go with the process.
+class BufferCache {
+  public:
+    static constexpr size_t kBytes = size_t(512) << 20;
+    static BufferCache& get() {
+        static BufferCache* c = new BufferCache();
+        return *c;
+    }
+    // The smallest held buffer of device dev with bytes <= size <= 2 bytes (its size in got), or null.
+    void* take(int dev, size_t bytes, size_t& got) {
+        std::lock_guard<std::mutex> lock(m_);
+        int best = -1;
+        for (int i = 0; i < n_; ++i)
+            if (e_[i].dev == dev && e_[i].bytes >= bytes && e_[i].bytes <= 2 * bytes &&
+                (best < 0 || e_[i].bytes < e_[best].bytes))
+                best = i;
+        if (best < 0) return nullptr;
+        void* p = e_[best].p;
+        got = e_[best].bytes;
+        held_ -= got;
+        e_[best] = e_[--n_];
+        return p;
+    }
+    // Keeps a buffer no kernel uses any more; false when the cache is full (the caller frees it).
+    bool give(int dev, void* p, size_t bytes) {
+        std::lock_guard<std::mutex> lock(m_);
+        if (n_ == kSlots || held_ + bytes > kBytes) return false;
+        e_[n_++] = {dev, p, bytes};
+        held_ += bytes;
+        return true;
+    }
+
+  private:
+    static constexpr int kSlots = 256;
+    struct Entry {
+        int dev;
+        void* p;
+        size_t bytes;
+    };
+    std::mutex m_;
+    Entry e_[kSlots];
+    int n_ = 0;
+    size_t held_ = 0;
+};
+
+// Owns device allocations for one call or one plan. With `recycle` (set by calls that synchronise their work before
+// returning, never by plans, whose callers may destroy them with kernels in flight) the buffers come from and go back
+// to the BufferCache; on an error path they are freed as usual, since kernels may still be using them.
 struct DeviceArena {
     void* ptrs[64] = {};
+    size_t sizes[64] = {};
     int n = 0;
+    int dev = -1;
+    bool recycle = false;
     ~DeviceArena() { release(); }
     void release() {
-        for (int i = 0; i < n; ++i) cudaFree(ptrs[i]);
+        const bool keep = recycle && std::uncaught_exceptions() == 0;
+        for (int i = 0; i < n; ++i)
+            if (!keep || !BufferCache::get().give(dev, ptrs[i], sizes[i])) cudaFree(ptrs[i]);
         n = 0;
     }
     void* raw(size_t bytes) {
         if (n == 64) throw Error(OB_ENOMEM, "too many device buffers");
+        const size_t want = bytes ? bytes : 16;
+        size_t got = want;
         void* d = nullptr;
-        const cudaError_t e = cudaMalloc(&d, bytes ? bytes : 16);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            throw Error(OB_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        if (recycle) {
+            if (dev < 0) check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+            d = BufferCache::get().take(dev, want, got);
         }
-        ptrs[n++] = d;
+        if (!d) {
+            got = want;
+            const cudaError_t e = cudaMalloc(&d, want);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw Error(OB_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            }
+        }
+        ptrs[n] = d, sizes[n] = got, ++n;
         return d;
     }
     template <typename T>

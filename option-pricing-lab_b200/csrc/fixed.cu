@@ -135,6 +135,7 @@ void run_fixed(const ob_request& rq, ob_result& res) {
     const int grid = static_cast<int>(std::max<long long>(
         1, std::min<long long>((n_units + 255) / 256, static_cast<long long>(sms) * std::max(1, per_sm))));
     DeviceArena arena;
+    arena.recycle = true;  // the blocking copy of the sums below ends the call's device work
     double* partial = arena.alloc<double>(static_cast<size_t>(grid) * 8);
     double* sums = arena.alloc<double>(8);
     cudaEvent_t e0, e1;

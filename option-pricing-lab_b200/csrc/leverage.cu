@@ -461,6 +461,7 @@ void run_leverage(ob_leverage_request& rq) {
     const auto t_start = std::chrono::steady_clock::now();
     const int sms = require_device();
     DeviceArena arena;
+    arena.recycle = true;  // the stream is synchronised before the call returns
     LevDev d{};
     const long long n = 2 * rq.n_pairs;
     const int S = rq.n_steps;

@@ -574,6 +574,7 @@ int ob_mc_price(const ob_mc_request* rq, int precision, ob_mc_result* res) {
         if (precision != OB_FP32 && precision != OB_FP64) ob::invalid("precision must be OB_FP32 or OB_FP64");
         const auto t0 = std::chrono::steady_clock::now();
         ob::McPlan p;
+        p.arena.recycle = true;  // the call reads its result back (synchronises) before p goes
         p.create(*rq, precision);
         p.run(rq->n_pairs, rq->first_pair, rq->seed, nullptr);
         p.result(*res);

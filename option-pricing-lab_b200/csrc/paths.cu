@@ -426,6 +426,7 @@ void run_paths(ob_paths_request& h) {
         has_slv |= h.kind[a] == 3;
     }
     DeviceArena arena;
+    arena.recycle = true;  // both streams are synchronised before the call returns
     PathsDev<R> s{};
     ModelDev<R>& m = s.m;
     m.n_names = n, m.n_steps = h.n_steps, m.n_x = h.n_x, m.same = h.same, m.mixer = h.mixer;

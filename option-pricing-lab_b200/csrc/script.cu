@@ -817,6 +817,7 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     const auto t_start = std::chrono::steady_clock::now();
     const int sms = require_device();
     DeviceArena arena;
+    arena.recycle = true;  // the blocking copies of the sums and records end the call's device work
     const ob_mc_request& mq = rq.model;
     const int n = mq.n_names, S = mq.n_steps;
     ScriptDev<R> d{};

@@ -161,3 +161,21 @@ def test_baskets_of_one_kind_on_the_staged_path_kernel_match_the_oracle(oracle, 
         assert np.median(rel) < 1e-13 and np.quantile(rel, 0.999) < 1e-9, (np.median(rel), rel.max())
     else:
         assert np.median(rel) < 1e-5 and np.mean(rel > 1e-3) < 0.06, (np.median(rel), np.mean(rel > 1e-3))
+
+
+def test_one_shot_calls_reuse_device_buffers_without_changing_their_results():
+    """One-shot calls hand their device buffers to the next call; interleaved calls of other sizes and kinds (which
+    take and return those buffers) leave every result bit-identical to its first run."""
+    kw = _paths([1, 1], 3000, n_steps=30)
+    first = paths_request(**kw)
+    engine.paths(first, "fp64")
+    m1 = engine.mc_price(_phoenix(1500), "fp64")
+    for n_pairs in (50, 5000, 3000):
+        engine.paths(paths_request(**_paths([3], n_pairs, n_steps=20)), "fp32")
+        engine.mc_price(_phoenix(n_pairs), "fp32")
+        again = paths_request(**kw)
+        engine.paths(again, "fp64")
+        assert np.array_equal(_out(again), _out(first))
+        m2 = engine.mc_price(_phoenix(1500), "fp64")
+        assert list(m2.price[: m2.n_out]) == list(m1.price[: m1.n_out])
+        assert list(m2.se[: m2.n_out]) == list(m1.se[: m1.n_out])
