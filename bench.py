@@ -13,7 +13,8 @@ range of pairs (first_pair = rank x pairs): weak scaling, no collective in the t
 of the sums after them (optlab_b200.shard). `--workload adjoint` times the Greeks of the worst-of autocall (FP32
 adjoint against FP64 bump-and-revalue); `--workload batch` the batched revaluation of a 512-trade book;
 `--workload leverage` the SLV leverage calibration; `--workload script` the default Phoenix written as a payoff script
-and run by the device's script interpreter.
+and run by the device's script interpreter; `--workload paths` the drop-in path engine's columns; `--workload
+callable` a whole issuer-call valuation (pilot, policy fit, pricing, dual bound).
 
 `--impl reference` times the reference's CPU implementation of the same workload instead: its path engine
 (optlab::api::paths, compiled from the reference's sources into oracle/_ref) writing the 12 quarterly columns and the
@@ -281,7 +282,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="lv_phoenix",
-                    choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage", "script", "paths"])
+                    choices=["lv_phoenix", "heston_qe", "adjoint", "batch", "leverage", "script", "paths", "callable"])
     ap.add_argument("--trades", type=int, default=512, help="batch workload: trades in the book")
     ap.add_argument("--paths", type=int, default=None)
     ap.add_argument("--table", default="builder", choices=["builder", "reference"],
@@ -308,6 +309,8 @@ def main():
         return run_script(args, world, rank)
     if args.workload == "paths":
         return run_paths(args, world, rank)
+    if args.workload == "callable":
+        return run_callable(args, world, rank)
 
     import torch
 
@@ -869,6 +872,92 @@ def run_paths(args, world, rank):
         # outputs of 32 MB or more run in four chunks of pairs, one launch each
         "gpu_launches": args.steps * (4 if out_bytes >= 32 << 20 and s.n_pairs >= 4 else 1),
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+    }
+    print(json.dumps(line))
+
+
+def run_callable(args, world, rank):
+    """The issuer's call: the callable reverse convertible of the reference's issuer-call test (2y, semiannual 3 %
+    coupons, callable at par on the first three dates, redemption min(S / S0, 1)) under Black-Scholes as a flat
+    local-variance table, FP64. One step is one whole valuation: the device pilot (pilot_paths(2 pairs) paths,
+    recorded), the Longstaff-Schwartz fit on the host, the pricing run applying the policy (2^17 pairs), and the
+    Andersen-Broadie dual bound from 1000 outer paths x 200 branched continuations at each of the 3 call dates. Timed
+    by the host clock around the whole valuation (every stage reads its results back); `value` is valuations per
+    second, `e2e` the same figure (the stages take host arrays and return host results)."""
+    import torch
+
+    from optlab_b200 import exercise
+    from optlab_b200 import script as sc
+    from optlab_b200._abi import OB_MODEL_PATHS, OB_PRODUCT_LADDER
+    from optlab_b200.models import time_grid
+    from optlab_b200.requests import mc_request
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    case = json.loads((ROOT / "tests" / "golden" / "script_dual.json").read_text())
+    r, q, vol = case["r"], case["q"], case["vol"]
+    comp = sc.compile_script(case["script"])
+
+    def disc(t):
+        return float(np.exp(-r * t))
+
+    def make_sim(n_pairs, seed):
+        grid = time_grid(comp.timeline.sim_times, 1 / 12)
+        dt, t0 = np.diff(grid), grid[:-1]
+        n_x = 11
+        return mc_request(model=OB_MODEL_PATHS, dt=dt, t0=t0, spot=[100.0], n_pairs=n_pairs, seed=seed, root=[[1.0]],
+                          kind=np.ones(1, np.int32), cvar=[vol**2], log_fwd=(r - q) * grid[None, :],
+                          step_row=np.zeros((1, len(dt)), np.int32), lo=[-5.0], inv_dx=[(n_x - 1) / 10.0],
+                          table=np.full((1, n_x), vol**2), n_x=n_x, r=r, q=q, product=OB_PRODUCT_LADDER, leg_type=[1],
+                          leg_strike=[1.0])
+
+    n_pairs = (args.paths or 2**18) // 2
+    n_outer, n_inner = 1000, 200
+
+    def valuation():
+        res, policy = exercise.price(comp, make_sim, n_pairs, 11, disc, "fp64")
+        b = exercise.dual_bound(comp, make_sim, policy, res.price, res.se, 11, disc, n_outer=n_outer, n_inner=n_inner,
+                                precision="fp64")
+        return res, b
+
+    for _ in range(args.warmup):
+        valuation()
+    wall = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            res, b = valuation()
+            torch.cuda.synchronize()
+            wall.append(time.perf_counter() - t)
+    t_s = statistics.median(wall)
+    clk = clocks.summary()
+    n_calls = len(comp.calls)
+    line = {
+        "metric": "callable valuations/s",
+        "value": 1.0 / t_s,
+        "unit": "valuations/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_s * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (the reference's callable reverse convertible under Black-Scholes)",
+        "config": {"workload": "callable", "pricing_pairs": n_pairs, "pilot_paths": exercise.pilot_paths(2 * n_pairs),
+                   "dual_outer": n_outer, "dual_inner": n_inner, "call_dates": n_calls,
+                   "l2": "no flush: each stage uploads its inputs and reads its results back"},
+        "roofline": None,
+        "cpu_baseline": None,
+        "e2e": {"value": 1.0 / t_s, "unit": "valuations/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "gpu_launches": 2 * (3 + n_calls),  # pilot, pricing, outer paths, one branched run a call date
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+        "result": {"price": res.price, "se": res.se, "dual_lower": b["lower"], "gap": b["gap"], "gap_se": b["gap_se"],
+                   "pde": case["pde"]},
     }
     print(json.dumps(line))
 

@@ -70,10 +70,15 @@ class Rule:
     coef: tuple = ()
 
     def features(self, state: np.ndarray) -> np.ndarray:
+        """(paths, terms): the monomials of z, then the hinges, z the normalised state; written column by column
+        into one array (one variable: z ** e itself, the product of a single factor)."""
         z = (state - np.asarray(self.mean)) / np.asarray(self.scale)
-        cols = [np.prod(z ** np.asarray(p), axis=1) for p in self.powers]
-        cols += [np.maximum(z[:, i] - k, 0.0) for i, k in self.knots]
-        return np.stack(cols, axis=1)
+        out = np.empty((z.shape[0], len(self.powers) + len(self.knots)))
+        for j, p in enumerate(self.powers):
+            out[:, j] = z[:, 0] ** p[0] if z.shape[1] == 1 else np.prod(z ** np.asarray(p), axis=1)
+        for j, (i, k) in enumerate(self.knots):
+            np.maximum(z[:, i] - k, 0.0, out=out[:, len(self.powers) + j])
+        return out
 
     def continuation(self, state: np.ndarray) -> np.ndarray:
         return self.features(state) @ np.asarray(self.coef)
@@ -150,10 +155,11 @@ def fit(rec: PilotRecord, call_events: list, pay_discount: list) -> Policy:
             scale = np.where(scale > 0, scale, 1.0)
             pw, knots = basis((x - mean) / scale)
             shape = Rule(tuple(float(v) for v in mean), tuple(float(v) for v in scale), tuple(pw), tuple(knots))
-            coef = np.linalg.lstsq(shape.features(x), y, rcond=None)[0]
+            feats = shape.features(rec.state[c])  # every path's terms: the regression's rows, then the decisions
+            coef = np.linalg.lstsq(feats[on], y, rcond=None)[0]
             rule = Rule(shape.mean, shape.scale, shape.powers, shape.knots, tuple(float(v) for v in coef))
             rules[c] = rule
-            decide = (rule.continuation(rec.state[c]) > rec.amount[c]).astype(float)
+            decide = (feats @ np.asarray(rule.coef) > rec.amount[c]).astype(float)
         called = rec.mask[c] * decide
         paid = d * called * rec.alive[c] * rec.amount[c]
         future = rec.pre[k] + (1.0 - called) * after + paid
