@@ -179,10 +179,12 @@ def reference_rows():
     return workloads.LocalVarGrid.from_surface(workloads.lv_surface(horizon=3.0), 3.0 * np.arange(1, 757) / 756, 801)
 
 
-def phoenix_paths_request(n_paths: int, seed: int = 7, table: str = "builder"):
+def phoenix_paths_request(n_paths: int, seed: int = 7, table: str = "builder", model: str = "lv"):
     """The local-vol Phoenix's model as a drop-in paths request (the reference's `run()`): the 12 quarterly columns
     and one daily window (lowest, highest) of the name, for n_paths paths; returns (request, Phoenix, market). table:
-    "builder" (200 points x 40 expiries) or "reference" (801 points x 756 per-step rows)."""
+    "builder" (200 points x 40 expiries) or "reference" (801 points x 756 per-step rows); model: "lv", "heston"
+    (v0 .04, kappa 1.5, theta .04, xi .5, rho -.7, Euler) or "slv" (the same Heston with the local variance over 0.04
+    as its leverage-squared table)."""
     from optlab_b200 import workloads
     from optlab_b200.requests import paths_request
 
@@ -199,10 +201,13 @@ def phoenix_paths_request(n_paths: int, seed: int = 7, table: str = "builder"):
     t_end = np.concatenate([[0.0], np.cumsum(dt)])
     g = workloads.lv_grid() if table == "builder" else reference_rows()
     t0 = t_end[:-1]
+    kind = {"lv": 1, "heston": 2, "slv": 3}[model]
     rq = paths_request(
-        dt=dt, t0=t0, obs_step=all_obs, root=[[1.0]], kind=[1], cvar=[0.0], heston=[0.0, 1, 1, 0, 0], same=1,
-        fwd=m.F(t_end)[None, :], n_pairs=n_paths // 2, seed=seed, step_row=g.row_of(t0), lo=g.lo, inv_dx=g.inv_dx,
-        table=g.rows, n_x=g.n_x, col_of=col_of, n_keep=len(obs_step), win_lo=[0], win_hi=[n_steps],
+        dt=dt, t0=t0, obs_step=all_obs, root=[[1.0]], kind=[kind], cvar=[0.04],
+        heston=[0.0, 1, 1, 0, 0] if kind == 1 else [0.04, 1.5, 0.04, 0.5, -0.7], same=1, fwd=m.F(t_end)[None, :],
+        n_pairs=n_paths // 2, seed=seed, step_row=g.row_of(t0), lo=g.lo, inv_dx=g.inv_dx,
+        table=g.rows / 0.04 if kind == 3 else g.rows, n_x=g.n_x, col_of=col_of, n_keep=len(obs_step), win_lo=[0],
+        win_hi=[n_steps],
     )
     return rq, ph, m
 
@@ -288,6 +293,8 @@ def main():
     ap.add_argument("--table", default="builder", choices=["builder", "reference"],
                     help="lv_phoenix and paths: the builder's 200 x 40 grid or the reference plan's 801-point "
                     "per-step rows")
+    ap.add_argument("--model", default="lv", choices=["lv", "heston", "slv"],
+                    help="paths workload: the name's model (Heston and SLV with the Heston parameters of heston_qe)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -824,7 +831,7 @@ def run_paths(args, world, rank):
     if rank != 0:
         return
     n_paths = args.paths or 2**20
-    rq, _, _ = phoenix_paths_request(n_paths, table=args.table)
+    rq, _, _ = phoenix_paths_request(n_paths, table=args.table, model=args.model)
     s = rq.struct
     units = 2 * s.n_pairs * s.n_steps * s.n_names
     for _ in range(args.warmup):
@@ -840,7 +847,7 @@ def run_paths(args, world, rank):
     out_bytes = 2 * s.n_pairs * s.n_names * s.n_cols * 8
     in_bytes = input_bytes(rq) - out_bytes
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and args.model == "lv":
         n_s = 2**18
         secs, kind, cores, detail = cpu_reference_sample("paths", n_s, os.cpu_count() or 1)
         cpu = {"value": n_s * s.n_steps / secs, "unit": "path-steps/s", "cores": cores, "kind": kind,
@@ -861,9 +868,11 @@ def run_paths(args, world, rank):
         "dtype": "f32",
         "data": "synthetic (seeded SSVI surface)",
         "config": {"workload": "paths", "n_paths": 2 * s.n_pairs, "n_steps": s.n_steps, "columns": s.n_cols,
-                   "table": f"{s.n_rows} rows x {s.n_x} points ({args.table})",
+                   "table": f"{s.n_rows} rows x {s.n_x} points ({args.table})", "model": args.model,
                    "output_bytes": out_bytes, "l2": "each call uploads its inputs and writes 117 MB of columns"},
-        "roofline": issue_roofline(ipu * units / t_k if ipu and n_paths == 2**20 and args.table == "builder" else None,
+        "roofline": issue_roofline(ipu * units / t_k
+                                   if ipu and n_paths == 2**20 and args.table == "builder" and args.model == "lv"
+                                   else None,
                                    "the local-vol step plus the column and window stores; achieved = ncu warp "
                                    "instructions per path-step x live rate"),
         "cpu_baseline": cpu,
