@@ -93,9 +93,10 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
     constexpr bool TABLE = KIND == 1 || KIND == 3;
     constexpr int C = QE ? 2 : (KIND == 2 ? 2 * N : N);  // normals per step, stream 0
     constexpr int CA = KIND == 3 ? N : 0;                // normals per step, aux stream
-    // steps per batch of whole Philox blocks; one name draws two blocks a batch (8 steps), whose two independent
-    // multiply chains interleave (1.317 -> 1.300 ms for the 2^20-path Phoenix)
-    constexpr int G = C == 1 ? 8 : 4 / gcd4(C);
+    // steps per batch of whole Philox blocks; one local-vol name draws two blocks a batch (8 steps), whose two
+    // independent multiply chains interleave (1.317 -> 1.300 ms for the 2^20-path Phoenix; one SLV name would draw four
+    // and spill in FP64)
+    constexpr int G = C == 1 && KIND == 1 ? 8 : 4 / gcd4(C);
     constexpr int NB = C * G / 4, NBA = CA * G / 4;
 
     extern __shared__ __align__(16) unsigned char sm[];
