@@ -187,6 +187,9 @@ typedef struct {
     double price[OB_MAX_OUT], se[OB_MAX_OUT];
     long long n_paths;
     double kernel_ms, total_ms;
+    /* the FP64 sums the estimate comes from, over the n_paths / 2 pair values y of output k: sum y and sum y^2
+       (price = sum_y / n, se = sqrt((sum_y2 / n - price^2) / (n - 1))); what ranks pool to combine shards */
+    double sum_y[OB_MAX_OUT], sum_y2[OB_MAX_OUT];
 } ob_mc_result;
 
 typedef struct ob_mc_plan ob_mc_plan;
@@ -363,6 +366,11 @@ int ob_has_cuda(void);
 int ob_cpu_threads(void);
 /* requests.hpp:101: properties of a device; OB_ENODEV without it. */
 int ob_device_info(int device, ob_device* out);
+/* No counterpart in the reference (it allocates and frees per call). The one-shot calls (ob_price, ob_mc_price,
+   ob_paths, ob_script_price, ob_leverage, ob_philox_normals) keep their device buffers for the next call, at most
+   512 MB over all devices; this frees them. Call it before cudaDeviceReset or before destroying a context the
+   library has used: cached buffers belong to the context that allocated them. */
+int ob_release_buffers(void);
 
 /* The engine's random numbers for RNG parity: for pairs first_pair .. first_pair + n_pairs - 1 of key seed, blocks
    first_block .. first_block + n_blocks - 1 of the stream tagged `tag` (0 or 0x80000000, paths.hpp:207-233),
@@ -385,9 +393,11 @@ int ob_price(const ob_request* rq, ob_result* res, int precision);
 /* ob_price without any device allocation, for callers that own all device memory through another allocator or
    must not call cudaMalloc/cudaFree while pricing. No counterpart in the reference: it has no allocation-free path.
    Its scratch (the per-block and final sums) is a fixed array in the library, about 256 KiB on every device that
-   loads it, kept until exit; launches needing more than 4096 blocks are refused (OB_EINVAL). The first call on a
-   device looks up that array's address and should come before any stream capture. Calls share the array: calls
-   that overlap on the GPU race and must not be made. */
+   loads it, kept until exit; launches needing more than 4096 blocks are refused (OB_EINVAL; a B200 launch takes at
+   most 148 x 8). Every call looks up the array's address in the current device's context; the first call on a
+   device also loads the library's device code there and should come before any stream capture. Calls share the
+   array: calls that overlap on the GPU race and must not be made (within one process the library's lock and the
+   blocking read-back of the sums keep its own calls apart). */
 int ob_price_noalloc(const ob_request* rq, ob_result* res, int precision);
 
 /* Fused pricing, end to end: host request in, result out (copies and allocations included). */

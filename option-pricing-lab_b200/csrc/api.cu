@@ -78,6 +78,10 @@ int ob_gpu_count(void) {
 
 int ob_has_cuda(void) { return 1; }
 
+int ob_release_buffers(void) {
+    return ob::guarded([&] { ob::BufferCache::get().drain(); });
+}
+
 int ob_cpu_threads(void) {
     const unsigned n = std::thread::hardware_concurrency();
     return n ? static_cast<int>(n) : 1;

@@ -99,6 +99,23 @@ class BufferCache {
         e_[best] = e_[--n_];
         return p;
     }
+    // Frees every held buffer (each on its own device) and returns how many there were. Buffers belong to the
+    // context that allocated them: a caller that resets a device (cudaDeviceReset) or destroys its context must
+    // empty the cache first, or the next call could be handed memory of a context that is gone.
+    int drain() {
+        std::lock_guard<std::mutex> lock(m_);
+        int prev = 0;
+        cudaGetDevice(&prev);
+        const int n = n_;
+        for (int i = 0; i < n_; ++i) {
+            cudaSetDevice(e_[i].dev);
+            cudaFree(e_[i].p);
+        }
+        cudaSetDevice(prev);
+        cudaGetLastError();
+        n_ = 0, held_ = 0;
+        return n;
+    }
     // Keeps a buffer no kernel uses any more; false when the cache is full (the caller frees it).
     bool give(int dev, void* p, size_t bytes) {
         std::lock_guard<std::mutex> lock(m_);

@@ -98,6 +98,15 @@ __global__ void fixed_finalize(const double* __restrict__ partial, int n_blocks,
     sums[t] = s;
 }
 
+// Blocks of one launch over n_units pairs: enough for every pair, at most the resident blocks of the device.
+template <typename R>
+long long fixed_grid(long long n_units, int sms) {
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fixed_kernel<R>, 256, 0), "occupancy");
+    return std::max<long long>(1, std::min<long long>((n_units + 255) / 256,
+                                                      static_cast<long long>(sms) * std::max(1, per_sm)));
+}
+
 // RC/src/requests.cpp:140-165 (convert): the same checks and messages.
 void check_request(const ob_request& c) {
     if (c.model < 0 || c.model > 1) invalid("model must be 0 (Black-Scholes) or 1 (Heston)");
@@ -113,10 +122,13 @@ void check_request(const ob_request& c) {
         if (c.legs[k] < 0 || c.legs[k] > 3) invalid("legs must be 0 to 3");
 }
 
+// One priced request on the current device: the kernel over the pairs, its block partial sums in `partial` (room for
+// `max_blocks` blocks), the totals in `sums`; kernel_ms from events around the two launches, total_ms from the host
+// clock since t_start. Both entry points below call it: ob_price with buffers from the call's arena, ob_price_noalloc
+// with the library's fixed array.
 template <typename R>
-void run_fixed(const ob_request& rq, ob_result& res) {
-    const auto t_start = std::chrono::steady_clock::now();
-    const int sms = require_device();
+void price_fixed(const ob_request& rq, ob_result& res, std::chrono::steady_clock::time_point t_start, int sms,
+                 double* partial, long long max_blocks, double* sums) {
     FixedDev f{};
     f.model = rq.model, f.product = rq.product, f.n_steps = rq.n_steps;
     for (int k = 0; k < 3; ++k) f.leg[k] = rq.legs[k], f.K[k] = rq.strikes[k];
@@ -130,22 +142,19 @@ void run_fixed(const ob_request& rq, ob_result& res) {
     QeConsts<R> qe{};
     if (rq.model == 1) qe = make_qe_consts<R>(h, rq.r, rq.q, dt);
     const long long n_units = rq.n_paths / 2;
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fixed_kernel<R>, 256, 0), "occupancy");
-    const int grid = static_cast<int>(std::max<long long>(
-        1, std::min<long long>((n_units + 255) / 256, static_cast<long long>(sms) * std::max(1, per_sm))));
-    DeviceArena arena;
-    arena.recycle = true;  // the blocking copy of the sums below ends the call's device work
-    double* partial = arena.alloc<double>(static_cast<size_t>(grid) * 8);
-    double* sums = arena.alloc<double>(8);
-    cudaEvent_t e0, e1;
+    const long long grid = fixed_grid<R>(n_units, sms);
+    if (grid > max_blocks) invalid("the launch needs more blocks than the no-allocation scratch holds (4096)");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
     check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
-    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    const cudaError_t ee = cudaEventCreate(&e1);
+    if (ee != cudaSuccess) cudaEventDestroy(e0);
+    check_cuda(ee, "cudaEventCreate");
     cudaEventRecord(e0);
-    fixed_kernel<R><<<grid, 256>>>(f, qe, n_units, static_cast<uint32_t>(rq.seed), static_cast<uint32_t>(rq.seed >> 32),
-                                   partial);
+    fixed_kernel<R><<<static_cast<unsigned>(grid), 256>>>(f, qe, n_units, static_cast<uint32_t>(rq.seed),
+                                                          static_cast<uint32_t>(rq.seed >> 32), partial);
     const cudaError_t le = cudaGetLastError();
-    fixed_finalize<<<1, 32>>>(partial, grid, sums);
+    if (le == cudaSuccess) fixed_finalize<<<1, 32>>>(partial, static_cast<int>(grid), sums);
+    const cudaError_t le2 = cudaGetLastError();
     cudaEventRecord(e1);
     double hs[8];
     const cudaError_t ce = cudaMemcpy(hs, sums, sizeof hs, cudaMemcpyDeviceToHost);
@@ -153,6 +162,7 @@ void run_fixed(const ob_request& rq, ob_result& res) {
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0), cudaEventDestroy(e1);
     check_cuda(le, "fixed_kernel launch");
+    check_cuda(le2, "fixed_finalize launch");
     check_cuda(ce, "fixed_kernel");
     std::memset(&res, 0, sizeof res);
     const double n = static_cast<double>(n_units);
@@ -163,6 +173,18 @@ void run_fixed(const ob_request& rq, ob_result& res) {
     res.n_paths = rq.n_paths;
     res.kernel_ms = ms;
     res.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+}
+
+template <typename R>
+void run_fixed(const ob_request& rq, ob_result& res) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const int sms = require_device();
+    const long long grid = fixed_grid<R>(rq.n_paths / 2, sms);
+    DeviceArena arena;
+    arena.recycle = true;  // the blocking copy of the sums ends the call's device work
+    double* partial = arena.alloc<double>(static_cast<size_t>(grid) * 8);
+    double* sums = arena.alloc<double>(8);
+    price_fixed<R>(rq, res, t_start, sms, partial, grid, sums);
 }
 
 }  // namespace
@@ -188,70 +210,36 @@ extern "C" int ob_price(const ob_request* rq, ob_result* res, int precision) {
 // the library image: g_noalloc_scratch, 4096 blocks x 8 sums + 8 totals (about 256 KiB), held on every device that
 // loads the library until the process exits. A launch needing more blocks than that is refused.
 //
-// Set-up: the first call on a device, with that device current, asks the driver for the array's device address
-// (cudaGetSymbolAddress); make that first call before any stream capture. Every call uses the same array, and each
-// call overwrites in full the slots it reads (every block writes its partial sums, the last kernel writes the
-// totals), so nothing carries over from one call to the next; calls that overlap on the GPU (two host threads, or
-// work queued on other streams) would race for the array and must not be made.
+// Set-up: every call, with the caller's device current, asks the driver for the array's device address in that
+// device's context (cudaGetSymbolAddress; it allocates nothing). On a device's first call this also loads the
+// library's device code into the context, so make the first call on each device before any stream capture. Every
+// call uses the same array, and each call overwrites in full the slots it reads (every block writes its partial sums,
+// the last kernel writes the totals), so nothing carries over from one call to the next. Calls that overlap on the
+// GPU would race for the array: within one process the library's lock and the call's blocking read-back keep calls
+// apart; two processes share no array (each has its own context), but work that the caller queues on other streams
+// must not touch it. The timing events are driver objects, not device memory.
 namespace ob {
 namespace {
 
 constexpr int kNoAllocMaxBlocks = 4096;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks * 8 + 8];
-double* g_noalloc_address[64] = {};  // per device: the array's device address, as the driver gives it
 
+// The array's device address in the current device's context, asked of the driver on every call: the lookup is
+// cheap and allocates nothing, and a context created again (after cudaDeviceReset, say) may hold the array at
+// another address, so an address kept from an earlier call could point at memory that is no longer the array.
 double* noalloc_scratch() {
-    int dev = 0;
-    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev < 0 || dev >= 64) invalid("device index beyond 63");
-    if (!g_noalloc_address[dev]) {
-        void* p = nullptr;
-        check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
-        g_noalloc_address[dev] = static_cast<double*>(p);
-    }
-    return g_noalloc_address[dev];
+    void* p = nullptr;
+    check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    return static_cast<double*>(p);
 }
 
 template <typename R>
 void run_fixed_noalloc(const ob_request& rq, ob_result& res) {
     const auto t_start = std::chrono::steady_clock::now();
     const int sms = require_device();
-    FixedDev f{};
-    f.model = rq.model, f.product = rq.product, f.n_steps = rq.n_steps;
-    for (int k = 0; k < 3; ++k) f.leg[k] = rq.legs[k], f.K[k] = rq.strikes[k];
-    const double dt = rq.T / rq.n_steps;
-    f.S0 = rq.S0, f.D = std::exp(-rq.r * rq.T);
-    f.bs_drift = (rq.r - rq.q - 0.5 * rq.sigma * rq.sigma) * dt;
-    f.bs_vol = rq.sigma * std::sqrt(dt);
-    f.ln_h = rq.product == 2 ? std::log(rq.H / rq.S0) : 0.0;
-    f.inv_n = 1.0 / rq.n_steps;
-    const double h[5] = {rq.v0, rq.kappa, rq.theta, rq.xi, rq.rho};
-    QeConsts<R> qe{};
-    if (rq.model == 1) qe = make_qe_consts<R>(h, rq.r, rq.q, dt);
-    const long long n_units = rq.n_paths / 2;
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fixed_kernel<R>, 256, 0), "occupancy");
-    const long long grid = std::max<long long>(
-        1, std::min<long long>((n_units + 255) / 256, static_cast<long long>(sms) * std::max(1, per_sm)));
-    if (grid > kNoAllocMaxBlocks) invalid("the launch needs more blocks than the no-allocation scratch holds (4096)");
     double* partial = noalloc_scratch();
     double* sums = partial + static_cast<size_t>(kNoAllocMaxBlocks) * 8;
-    fixed_kernel<R><<<static_cast<unsigned>(grid), 256>>>(f, qe, n_units, static_cast<uint32_t>(rq.seed),
-                                                          static_cast<uint32_t>(rq.seed >> 32), partial);
-    check_cuda(cudaGetLastError(), "fixed_kernel launch");
-    fixed_finalize<<<1, 32>>>(partial, static_cast<int>(grid), sums);
-    check_cuda(cudaGetLastError(), "fixed_finalize launch");
-    double hs[8];
-    check_cuda(cudaMemcpy(hs, sums, sizeof hs, cudaMemcpyDeviceToHost), "fixed_kernel");
-    std::memset(&res, 0, sizeof res);
-    const double n = static_cast<double>(n_units);
-    for (int k = 0; k < 4; ++k) {
-        const double mean = hs[k] / n, var = hs[4 + k] / n - mean * mean;
-        res.price[k] = mean, res.se[k] = n_units > 1 ? std::sqrt(std::fmax(var, 0.0) / (n - 1.0)) : 0.0;
-    }
-    res.n_paths = rq.n_paths;
-    res.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
-    res.kernel_ms = res.total_ms;  // no events: creating them is an allocation this entry point avoids
+    price_fixed<R>(rq, res, t_start, sms, partial, kNoAllocMaxBlocks, sums);
 }
 
 }  // namespace

@@ -519,6 +519,7 @@ void McPlan::result(ob_mc_result& res) {
         const double mean = h[k] / nn, var = h[n_out + k] / nn - mean * mean;
         res.price[k] = mean;
         res.se[k] = pairs_run > 1 ? std::sqrt(std::fmax(var, 0.0) / (nn - 1.0)) : 0.0;
+        res.sum_y[k] = h[k], res.sum_y2[k] = h[n_out + k];
     }
     res.kernel_ms = ms;
     check_cuda(cudaMemset(d_sums, 0, 2 * OB_MAX_OUT * sizeof(double)), "cudaMemset");

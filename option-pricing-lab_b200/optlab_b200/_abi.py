@@ -208,6 +208,8 @@ class ObMcResult(C.Structure):
         ("n_paths", C.c_longlong),
         ("kernel_ms", C.c_double),
         ("total_ms", C.c_double),
+        ("sum_y", C.c_double * OB_MAX_OUT),
+        ("sum_y2", C.c_double * OB_MAX_OUT),
     ]
 
 
@@ -347,6 +349,7 @@ SIGNATURES = {
     "ob_gpu_count": (C.c_int, []),
     "ob_has_cuda": (C.c_int, []),
     "ob_cpu_threads": (C.c_int, []),
+    "ob_release_buffers": (C.c_int, []),
     "ob_device_info": (C.c_int, [C.c_int, C.POINTER(ObDevice)]),
     "ob_philox_normals": (
         C.c_int,

@@ -3,9 +3,11 @@
 The draws of a pair depend only on (seed, global pair index) (the reference's contract, packages/native/src/optlab/
 native/__init__.py:317-323: batches and chunks are invisible), so rank r simulates its own range of global pairs and
 the only exchange is the FP64 sums of the pair values: n, sum y and sum y^2 per output, combined once at the end.
-`pair_range` splits a fixed job (strong scaling) or gives every rank the same count (weak scaling); `sums_of` turns a
-rank's result back into its sums; `combine` and `allreduce_result` pool them into the job's price and SE, with the
-same estimator as a single run (mean of pair values, SE = sqrt((E[y^2] - mean^2) / (n - 1))).
+`pair_range` splits a fixed job (strong scaling) or gives every rank the same count (weak scaling); `result_sums`
+reads a rank's sums from its result (the engine returns them beside the estimate); `combine` and `allreduce_result`
+pool them into the job's price and SE, with the same estimator as a single run (mean of pair values,
+SE = sqrt((E[y^2] - mean^2) / (n - 1))). The sums are pooled as the kernels wrote them: rebuilding them from
+(price, se) would subtract nearly equal numbers and lose the FP64 sums' digits.
 """
 
 from __future__ import annotations
@@ -25,12 +27,11 @@ def pair_range(n_pairs: int, rank: int, world: int, weak: bool = False) -> tuple
     return first, base + (1 if rank < extra else 0)
 
 
-def sums_of(price, se, n: int) -> np.ndarray:
-    """[n, sum y_k..., sum y_k^2...] of a result over n pairs (price, se per output): the inverse of the estimator."""
-    price, se = np.asarray(price, float), np.asarray(se, float)
-    s1 = price * n
-    s2 = n * (se**2 * (n - 1) + price**2) if n > 1 else price**2 * n
-    return np.concatenate([[float(n)], s1, s2])
+def result_sums(res) -> np.ndarray:
+    """[n, sum y_k..., sum y_k^2...] of an ob_mc_result over its n_paths / 2 pairs: the FP64 sums the engine (or the
+    oracle) accumulated, as they are."""
+    k = int(res.n_out)
+    return np.concatenate([[res.n_paths / 2.0], np.asarray(res.sum_y[:k], float), np.asarray(res.sum_y2[:k], float)])
 
 
 def estimate(sums: np.ndarray):
@@ -44,20 +45,16 @@ def estimate(sums: np.ndarray):
 
 
 def combine(parts) -> tuple[np.ndarray, np.ndarray]:
-    """Pool [(price, se, n), ...] of disjoint pair ranges into the job's (price, se)."""
-    tot = None
-    for price, se, n in parts:
-        s = sums_of(price, se, n)
-        tot = s if tot is None else tot + s
-    return estimate(tot)
+    """Pool the results of disjoint pair ranges (ob_mc_result each) into the job's (price, se)."""
+    return estimate(sum(result_sums(r) for r in parts))
 
 
-def allreduce_result(price, se, n: int, group=None, device=None):
-    """The job's (price, se) from every rank's (price, se, n), by one FP64 all-reduce of the sums (gloo on CPU
-    tensors, NCCL on CUDA tensors)."""
+def allreduce_result(res, group=None, device=None):
+    """The job's (price, se) from every rank's result (ob_mc_result), by one FP64 all-reduce of the sums (gloo on
+    CPU tensors, NCCL on CUDA tensors)."""
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor(sums_of(price, se, n), dtype=torch.float64, device=device)
+    t = torch.tensor(result_sums(res), dtype=torch.float64, device=device)
     dist.all_reduce(t, group=group)
     return estimate(t.cpu().numpy())

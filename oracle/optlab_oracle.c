@@ -660,6 +660,7 @@ static int mc_price_shifted(const ob_mc_request* rq, double ln_shift, int sum_le
         const double mean = tot[k] / n, var = tot[OB_MAX_OUT + k] / n - mean * mean;
         res->price[k] = mean;
         res->se[k] = rq->n_pairs > 1 ? sqrt(fmax(var, 0.0) / (n - 1.0)) : 0.0;
+        res->sum_y[k] = tot[k], res->sum_y2[k] = tot[OB_MAX_OUT + k];
     }
     return OB_OK;
 }
@@ -1117,5 +1118,6 @@ int or_autocall_smooth(const ob_mc_request* rq, double eps, int n_threads, ob_mc
     const double n = (double)rq->n_pairs, mean = s / n;
     res->n_out = 1, res->n_paths = 2 * rq->n_pairs;
     res->price[0] = mean, res->se[0] = sqrt(fmax(s2 / n - mean * mean, 0.0) / (n - 1.0));
+    res->sum_y[0] = s, res->sum_y2[0] = s2;
     return OB_OK;
 }

@@ -7,12 +7,13 @@ reference's own Python (optlab.core from the reference tree): the Black-Scholes 
 one year (structured/context.py:154-164), the Heston model is the recorded fit, the market is Market.flat(100, 0.04,
 0.012), and the time grid is models.time_grid([0.25, 0.5, 1], 1/252, 1/2000) (Black-Scholes: one step per date).
 
-Run where the reference tree is present:  python tests/golden/make_fixtures.py [/root/reference]
+Run where the reference tree is present:  python tests/golden/make_fixtures.py [reference root; default $OPTLAB_REFERENCE, else /root/reference]
 """
 
 from __future__ import annotations
 
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -21,7 +22,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str = os.environ.get("OPTLAB_REFERENCE", "/root/reference")) -> None:
     ref = Path(ref_root)
     sys.path[:0] = [str(ref / "packages/core/src")]
     from optlab.core.market import Market

@@ -11,12 +11,13 @@ The fixings are lognormal paths of every underlying on the script's simulation t
 spot); the fake scenario answers `spot(name, t)` and `fixings(name, times)` from them. A case whose evaluation the
 reference refuses (an undefined payment or condition) records the refusal instead of values.
 
-Run where the reference tree is present:  python tests/golden/make_script_fixtures.py [/root/reference]
+Run where the reference tree is present:  python tests/golden/make_script_fixtures.py [reference root; default $OPTLAB_REFERENCE, else /root/reference]
 """
 
 from __future__ import annotations
 
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -255,7 +256,7 @@ class Scenario:
         return np.stack([self.col(name, t) for t in times], axis=1)
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str = os.environ.get("OPTLAB_REFERENCE", "/root/reference")) -> None:
     ref = Path(ref_root)
     sys.path[:0] = [str(ref / "packages/structured/src"), str(ref / "packages/core/src")]
     from optlab.structured.script.evaluator import Evaluator

@@ -2,6 +2,7 @@
 structs have the reference's layouts, and bad requests fail with the reference's messages before any device work."""
 
 import ctypes as C
+import os
 import re
 import subprocess
 from pathlib import Path
@@ -14,7 +15,7 @@ from optlab_b200.requests import paths_request
 
 ROOT = Path(__file__).resolve().parent.parent
 HEADER = ROOT / "include" / "optlab_b200.h"
-REF_HEADER = Path("/root/reference/packages/native/cuda/include/optlab_cuda/requests.hpp")
+REF_HEADER = Path(os.environ.get("OPTLAB_REFERENCE", "/root/reference")) / "packages/native/cuda/include/optlab_cuda/requests.hpp"
 
 
 def declared_symbols():

@@ -2,6 +2,7 @@
 objects, the same SSVI local variance, time grid and local-correlation factors, and registration in the reference's
 registry. The reference's packages are imported from the reference tree, where present."""
 
+import os
 import sys
 from pathlib import Path
 
@@ -12,7 +13,7 @@ import optlab_b200 as eng
 from optlab_b200 import models as M
 from optlab_b200.surfaces import SSVI
 
-REF = Path("/root/reference/packages")
+REF = Path(os.environ.get("OPTLAB_REFERENCE", "/root/reference")) / "packages"
 HAVE_REF = (REF / "core/src/optlab/core/models.py").exists()
 
 

@@ -179,3 +179,16 @@ def test_one_shot_calls_reuse_device_buffers_without_changing_their_results():
         m2 = engine.mc_price(_phoenix(1500), "fp64")
         assert list(m2.price[: m2.n_out]) == list(m1.price[: m1.n_out])
         assert list(m2.se[: m2.n_out]) == list(m1.se[: m1.n_out])
+
+
+def test_calls_after_the_buffer_cache_is_released_price_as_before():
+    """ob_release_buffers empties the one-shot calls' buffer cache (what a caller does before resetting a device);
+    the next call allocates again and gives the same prices."""
+    from optlab_b200 import _abi
+
+    lib = _abi.load()
+    first = engine.mc_price(workloads.lv_phoenix(n_paths=2**14, seed=5), "fp64")
+    _abi.check(lib.ob_release_buffers())
+    _abi.check(lib.ob_release_buffers())  # an empty cache is fine too
+    again = engine.mc_price(workloads.lv_phoenix(n_paths=2**14, seed=5), "fp64")
+    assert list(first.price[: first.n_out]) == list(again.price[: again.n_out])

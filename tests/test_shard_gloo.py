@@ -40,8 +40,7 @@ def _rank(rank, world, port, n_pairs, weak, out):
         held = wl.heston_qe_ladder(n_paths=2 * n_pairs, n_steps=24)
         held.struct.first_pair, held.struct.n_pairs = first, count
         res = Oracle().mc_price(held, threads=2)
-        k = res.n_out
-        price, se = sh.allreduce_result(res.price[:k], res.se[:k], count)
+        price, se = sh.allreduce_result(res)
         out[rank] = (list(price), list(se))
     finally:
         dist.destroy_process_group()
@@ -75,12 +74,20 @@ def test_weak_ranges_are_disjoint_and_strong_ranges_cover_the_job():
         shard.pair_range(10, 3, 3)
 
 
-def test_combine_inverts_the_estimator():
+def test_combine_pools_the_raw_sums():
+    """Shards pool the FP64 sums as accumulated: the pooled estimate equals the estimate of the summed sums exactly,
+    also where price and se could not give the sums back (a large mean with a small spread)."""
+    from types import SimpleNamespace
+
     rng = np.random.default_rng(0)
-    y = rng.normal(size=(1000, 3))
-    def est(a):
-        m = a.mean(0)
-        return m, np.sqrt(np.maximum((a**2).mean(0) - m**2, 0) / (len(a) - 1)), len(a)
-    p, s = shard.combine([est(y[:300]), est(y[300:])])
-    m, se, _ = est(y)
-    assert np.allclose(p, m, rtol=1e-13) and np.allclose(s, se, rtol=1e-10)
+    y = 1e4 + 1e-3 * rng.normal(size=(1000, 3))
+
+    def res(a):
+        return SimpleNamespace(n_out=3, n_paths=2 * len(a), sum_y=list(a.sum(0)), sum_y2=list((a**2).sum(0)))
+
+    parts = [res(y[:300]), res(y[300:])]
+    p, s = shard.combine(parts)
+    tot = np.concatenate([[1000.0], y[:300].sum(0) + y[300:].sum(0), (y[:300]**2).sum(0) + (y[300:]**2).sum(0)])
+    m, se = shard.estimate(tot)
+    assert np.array_equal(p, m) and np.array_equal(s, se)
+    assert np.allclose(p, y.mean(0), rtol=1e-14)

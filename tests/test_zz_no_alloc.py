@@ -35,6 +35,7 @@ def test_the_allocation_free_entry_point_prices_like_ob_price_call_after_call():
         _abi.check(lib.ob_price_noalloc(C.byref(rq), C.byref(got), prec))
         _abi.check(lib.ob_price(C.byref(rq), C.byref(want), prec))
         assert got.n_paths == want.n_paths == rq.n_paths
+        assert 0.0 < got.kernel_ms <= got.total_ms  # the kernels' event time, as ob_price reports it
         for k in range(4):
             tol = 1e-12 * abs(want.price[k]) + 1e-300
             assert abs(got.price[k] - want.price[k]) <= tol, (k, got.price[k], want.price[k])
@@ -48,3 +49,24 @@ def test_the_allocation_free_entry_point_refuses_a_bad_request_like_ob_price():
     res = _abi.ObResult()
     assert lib.ob_price_noalloc(C.byref(rq), C.byref(res), _abi.OB_FP64) == _abi.OB_EINVAL
     assert b"barrier" in lib.ob_last_error()
+
+
+def _free_bytes(lib):
+    dev = _abi.ObDevice()
+    _abi.check(lib.ob_device_info(0, C.byref(dev)))
+    return dev.free_mem
+
+
+def test_the_allocation_free_entry_point_leaves_device_memory_as_it_was():
+    """After one call has loaded the library's device code, further calls take no device memory: the device's free
+    memory is the same before and after a series of them."""
+    lib = _abi.load()
+    rq = _request(1, 2, (1, 0, 0), (100.0, 0.0, 0.0), 2**17, 21)
+    res = _abi.ObResult()
+    for prec in (_abi.OB_FP64, _abi.OB_FP32):
+        _abi.check(lib.ob_price_noalloc(C.byref(rq), C.byref(res), prec))
+    before = _free_bytes(lib)
+    for i in range(6):
+        rq.seed = 22 + i
+        _abi.check(lib.ob_price_noalloc(C.byref(rq), C.byref(res), (_abi.OB_FP64, _abi.OB_FP32)[i % 2]))
+    assert _free_bytes(lib) == before
