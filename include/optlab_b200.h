@@ -244,9 +244,11 @@ typedef struct {
 /* The batch: trades, pools and scenarios. Every trade steps by dt; a local-vol table row j of a trade is the
    expiry horizon (j + 1) / n_exp, read by steps starting before it (the first expiry after a step's start). The
    scenarios of each trade: the base, then n_spot relative spot moves (evaluated on the base simulation: the local vol
-   is in log-moneyness, so a spot move scales the paths), then n_vol moves of local volatility sigma(k) + shift +
-   tilt k (floored at 1 %), each a simulation on the same random numbers (Heston trades do not move under them, as
-   the reference's Heston model ignores the surface). After those, n_carry (at most 4) moves of the carry on the base
+   is in log-moneyness, so a spot move scales the paths), then n_vol moves of the implied volatilities, each a
+   simulation on the same random numbers with the pool's local variance under that move (vol_table: the host moves
+   each surface's implied vols as the reference's risk scenarios do, packages/risk/src/optlab/risk/shocks.py:63-108,
+   and re-tabulates Dupire on the same points; vol_shift and vol_tilt record each move's parallel shift and skew);
+   Heston trades do not move under them, as the reference's Heston model ignores the surface. After those, n_carry (at most 4) moves of the carry on the base
    simulation: carry_rate moves the rate in the forward and the discounting, carry_div the dividend yield (with repo)
    in the forward only, so that a path moves by exp((carry_rate - carry_div) t) at time t and a payment at t
    (the ladder's last step, an autocall's observation step) is discounted by exp(-carry_rate t) more
@@ -259,6 +261,7 @@ typedef struct {
     const ob_batch_trade* trades;
     double dt, horizon;
     int n_exp, n_x;
+    int n_rows;                /* rows of the pool (table, row_lo, row_inv_dx and each vol scenario's table) */
     const double* table;       /* pool rows x n_x: local variance */
     const double* row_lo;      /* pool rows */
     const double* row_inv_dx;  /* pool rows */
@@ -273,8 +276,9 @@ typedef struct {
     int n_spot;
     const double* spot_shift;
     int n_vol;
-    const double* vol_shift;
-    const double* vol_tilt;
+    const double* vol_shift;   /* n_vol: the parallel implied-vol move of each scenario (a record) */
+    const double* vol_tilt;    /* n_vol: the skew move (90 % - 110 % vol gap at one year) of each scenario (a record) */
+    const double* vol_table;   /* n_vol x pool rows x n_x: the pool's local variance under each vol scenario */
     int n_carry;
     const double* carry_rate;
     const double* carry_div;
@@ -383,8 +387,15 @@ int ob_philox_normals(unsigned long long seed, long long first_pair, long long n
 int ob_paths(ob_paths_request* rq, int precision);
 
 /* Drop-in for optlab::api::leverage(rq, 1, 0) (requests.hpp:107-108): fills x_grids, values and total_ms.
-   The whole calibration runs on the device; the host reads the two output tables once. */
+   The whole calibration runs on the device as one persistent kernel (grid barriers between its phases); the host
+   reads the two output tables once. OB_ETIMEOUT: a grid barrier gave up waiting (see ob_set_wait_limit). */
 int ob_leverage(ob_leverage_request* rq, int precision);
+
+/* No counterpart in the reference (its calibration synchronises through the host). The polls a persistent kernel's
+   grid barrier makes before it gives up and the call returns OB_ETIMEOUT; a barrier completes within microseconds,
+   and the default (about a second) is far above that. A negative value restores the default; returns the previous
+   limit. Process-wide; read at each call. */
+long long ob_set_wait_limit(long long polls);
 
 /* Drop-in for optlab::api::price(rq, 1, 0) (requests.hpp:103-104): the fixed products of the reference's study,
    with the engine's Philox normals (pair p reads stream 0 of pair p) instead of cuRAND. */

@@ -466,7 +466,7 @@ void check_batch(const ob_batch_request& rq) {
     if (rq.n_trades < 1 || !rq.trades) invalid("a batch needs trades");
     if (!(rq.dt > 0) || rq.n_exp < 1 || rq.n_x < 2 || !(rq.horizon > 0)) invalid("bad step or table grid");
     if (rq.n_spot < 0 || rq.n_spot + 1 > kBatchMaxOut || (rq.n_spot && !rq.spot_shift)) invalid("n_spot must be 0 to 31");
-    if (rq.n_vol < 0 || (rq.n_vol && (!rq.vol_shift || !rq.vol_tilt))) invalid("bad vol scenarios");
+    if (rq.n_vol < 0 || (rq.n_vol && (!rq.vol_shift || !rq.vol_tilt || !rq.vol_table))) invalid("bad vol scenarios");
     if (rq.n_carry < 0 || rq.n_carry > kBatchMaxCarry || (rq.n_carry && (!rq.carry_rate || !rq.carry_div)))
         invalid("n_carry must be 0 to 4, with its moves");
     if (1 + rq.n_spot + rq.n_carry > kBatchMaxOut) invalid("1 + n_spot + n_carry must be at most 32");
@@ -541,9 +541,10 @@ void Batch::build(const ob_batch_request& rq) {
         row_of[i] = j;
     }
     d.row_of = arena.put<int>(row_of.data(), row_of.size());
+    if (max_row > rq.n_rows) invalid("a trade reads table rows beyond the pool's n_rows");
     if (max_row > 0) {
-        // the base tables, then each vol move's: every node's variance (sigma + shift + tilt k)^2, sigma floored at
-        // 1 % (the oracle rebuilds its rows the same way), as (var_i, var_i+1 - var_i) pairs
+        // the base tables, then each vol move's (the host re-tabulated the pool under each move of the implied vols),
+        // as (var_i, var_i+1 - var_i) pairs
         const int nx = rq.n_x;
         d.tab_stride = static_cast<long long>(max_row) * (nx - 1);
         const double tab_bytes = static_cast<double>(1 + n_vol) * d.tab_stride * sizeof(Pair2<R>);
@@ -554,16 +555,12 @@ void Batch::build(const ob_batch_request& rq) {
                     "device memory: fewer vol scenarios or a smaller pool");
         std::vector<Pair2<R>> tab(static_cast<size_t>(1 + n_vol) * d.tab_stride);
         std::vector<double> v(nx);
+        const long long pool = static_cast<long long>(rq.n_rows) * nx;
         for (int s = 0; s <= n_vol; ++s)
             for (int r = 0; r < max_row; ++r) {
-                const double dx = 1.0 / rq.row_inv_dx[r];
-                for (int k = 0; k < nx; ++k) {
-                    v[k] = rq.table[static_cast<size_t>(r) * nx + k];
-                    if (s > 0) {
-                        const double sg = std::sqrt(v[k]) + rq.vol_shift[s - 1] + rq.vol_tilt[s - 1] * (rq.row_lo[r] + k * dx);
-                        v[k] = sg > 0.01 ? sg * sg : 0.01 * 0.01;
-                    }
-                }
+                const double* src = s == 0 ? rq.table + static_cast<size_t>(r) * nx
+                                           : rq.vol_table + (s - 1) * pool + static_cast<long long>(r) * nx;
+                for (int k = 0; k < nx; ++k) v[k] = src[k];
                 Pair2<R>* out = tab.data() + s * d.tab_stride + static_cast<long long>(r) * (nx - 1);
                 for (int k = 0; k + 1 < nx; ++k) out[k] = {static_cast<R>(v[k]), static_cast<R>(v[k + 1] - v[k])};
             }

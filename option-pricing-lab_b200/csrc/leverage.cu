@@ -27,6 +27,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -51,6 +53,7 @@ constexpr int kMaxX = 1024;
 
 struct LevDev {
     long long n_pairs;
+    int n_steps;
     int n_x, n_bins, n_fine, n_lv, local_linear, positive_part;
     uint32_t k0, k1;
     double v0, kappa, theta, xi, rho, atm_vol, bw_scale, l_min, l_max, q_lo, q_hi;
@@ -73,6 +76,11 @@ struct LevDev {
     double* x_grids;           // n_steps x n_x
     double* values;            // n_steps x n_x
     int* step;                 // the current step: 0 from lev_init, advanced by lev_bin before the step's regression
+    // the persistent kernel's grid barrier: arrivals, generation, and the status a barrier that gave up sets
+    unsigned* bar_count;
+    unsigned* bar_gen;
+    int* status;
+    long long wait_limit;      // polls of a barrier's generation before it gives up (OB_ETIMEOUT)
 };
 
 // The v sums are 64-bit fixed point with 2^36 units per unit of v: integer additions, so the sums are the same
@@ -94,7 +102,7 @@ __device__ void range_of(const LevDev& d, double& lo, double& hi, double* s_mn, 
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int b = b0 + j * blockDim.x;
-            r[j] = b < d.n_step_blocks ? pr[b] : make_double2(1.0e300, -1.0e300);
+            r[j] = b < d.n_step_blocks ? __ldcg(pr + b) : make_double2(1.0e300, -1.0e300);
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) mn = fmin(mn, r[j].x), mx = fmax(mx, r[j].y);
@@ -128,23 +136,45 @@ __device__ __forceinline__ int current_step(const LevDev& d) { return __ldcg(d.s
 
 // Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU. A block bins its
 // particles in shared memory, then adds its non-zero entries into the step's global histogram and bins.
+// The binning block's shared memory: v sums (nb + 1, fixed point), local-linear moments (3 nb), fine histogram (nf)
+// and bin counts (nb).
+struct BinShared {
+    unsigned long long* sv;
+    double* ll;
+    unsigned* fine;
+    unsigned* cnt;
+};
+
+__device__ __forceinline__ BinShared bin_shared(const LevDev& d, unsigned char* sm) {
+    BinShared b;
+    b.sv = reinterpret_cast<unsigned long long*>(sm);
+    b.ll = reinterpret_cast<double*>(b.sv + d.n_bins + 1);
+    b.fine = reinterpret_cast<unsigned*>(b.ll + (d.local_linear ? 3 * d.n_bins : 0));
+    b.cnt = b.fine + d.n_fine;
+    return b;
+}
+
+__device__ __forceinline__ void bin_clear_shared(const LevDev& d, const BinShared& b) {
+    const int nb = d.n_bins, nf = d.n_fine;
+    for (int k = threadIdx.x; k < nb + 1; k += blockDim.x) b.sv[k] = 0ull;
+    if (d.local_linear)
+        for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) b.ll[k] = 0.0;
+    for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) b.fine[k] = 0u;
+}
+
+// One block's share of a step's binning (the block's shared memory cleared by bin_clear_shared before): its particles
+// into the shared histogram and bins, then the non-zero entries added into the step's global ones. Particles and the
+// last step's ranges are read through L2: in the persistent kernel other blocks wrote them in the same launch.
 template <typename R>
-__global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x, const R* __restrict__ v) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ double s_mn[16], s_mx[16];
+__device__ void bin_phase(const LevDev& d, const R* __restrict__ x, const R* __restrict__ v, const BinShared& b,
+                          double* s_mn, double* s_mx) {
     const int nb = d.n_bins, nf = d.n_fine, ll = d.local_linear;
-    unsigned long long* s_sv = reinterpret_cast<unsigned long long*>(sm);  // nb, then the total
-    double* s_ll = reinterpret_cast<double*>(s_sv + nb + 1);               // 3 nb when local linear
-    unsigned* s_fine = reinterpret_cast<unsigned*>(s_ll + (ll ? 3 * nb : 0));
-    unsigned* s_cnt = s_fine + nf;
-    for (int k = threadIdx.x; k < nb + 1; k += blockDim.x) s_sv[k] = 0ull;
-    if (ll)
-        for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) s_ll[k] = 0.0;
-    for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) s_fine[k] = 0u;
-    wait_previous();
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(d.step, 1);  // the previous step is done: this is the next
+    unsigned long long* s_sv = b.sv;
+    double* s_ll = b.ll;
+    unsigned* s_fine = b.fine;
+    unsigned* s_cnt = b.cnt;
     double lo_d, hi_d;
-    range_of(d, lo_d, hi_d, s_mn, s_mx);  // (its barrier also orders the clearing above)
+    range_of(d, lo_d, hi_d, s_mn, s_mx);  // (its barrier also orders the clearing before)
     const R lo = static_cast<R>(lo_d), hi = static_cast<R>(hi_d);
     const R wf = (hi - lo) / static_cast<R>(nf), we = (hi + static_cast<R>(1e-12) - lo) / static_cast<R>(nb);
     const long long n = 2 * d.n_pairs;
@@ -156,7 +186,7 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const long long j = j0 + u * stride;
-            xr[u] = j < n ? x[j] : R(0), vr[u] = j < n ? v[j] : R(0);
+            xr[u] = j < n ? __ldcg(x + j) : R(0), vr[u] = j < n ? __ldcg(v + j) : R(0);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -201,6 +231,17 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
             if (s_ll[k] != 0.0) atomicAdd(&d.acc_ll[k], s_ll[k]);
 }
 
+template <typename R>
+__global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x, const R* __restrict__ v) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ double s_mn[32], s_mx[32];
+    const BinShared b = bin_shared(d, sm);
+    bin_clear_shared(d, b);
+    wait_previous();
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(d.step, 1);  // the previous step is done: this is the next
+    bin_phase<R>(d, x, v, b, s_mn, s_mx);
+}
+
 // Exclusive prefix of x over the block and the block's total (any block size that is a multiple of 32, up to 1024).
 __device__ unsigned long long block_scan(unsigned long long x, unsigned long long* s_warp, unsigned long long& total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -236,17 +277,25 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 // and E[v | x] = v0. The grid's bounds are the quantiles of the fine histogram (RC/src/leverage.cpp:26-38: the first
 // fine bin k with a count and (counts before k) + count >= q total, at lo + (k + (q total - before) / count) width),
 // computed in every block from the chunk totals and, for the chunk that holds each quantile, its 32 bins.
-__global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles) {
-    __shared__ unsigned long long s_warp[32];
-    __shared__ double s_cum[2][256];
-    __shared__ int s_best[2];
-    __shared__ double s_q[2];
-    __shared__ double s_red[5][32];
-    __shared__ double s_mn[8], s_mx[8];
-    const int g = blockIdx.x, nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
+// Shared memory of the regression (blocks of at most 512 threads).
+struct RegressShared {
+    unsigned long long warp[32];
+    double cum[2][512];
+    int best[2];
+    double q[2];
+    double red[5][32];
+    double mn[32], mx[32];
+};
+
+__device__ void regress_phase(const LevDev& d, double n_particles, int g, int i, RegressShared& sh) {
+    unsigned long long* s_warp = sh.warp;
+    double(*s_cum)[512] = sh.cum;
+    int* s_best = sh.best;
+    double* s_q = sh.q;
+    double(*s_red)[32] = sh.red;
+    double *s_mn = sh.mn, *s_mx = sh.mx;
+    const int nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-    wait_previous();
-    const int i = current_step(d);
     const double h = d.dt[i];
     double x0, cond;
     if (i == 0) {
@@ -260,7 +309,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
         const int ca = min(t * cpt, n_ch), cb = min(ca + cpt, n_ch);
         unsigned mine_c[2] = {0u, 0u};  // cpt <= 2 (n_fine <= 16384)
         unsigned long long mine = 0;
-        for (int c = ca; c < cb; ++c) mine_c[c - ca] = d.chunk[c], mine += mine_c[c - ca];
+        for (int c = ca; c < cb; ++c) mine_c[c - ca] = __ldcg(d.chunk + c), mine += mine_c[c - ca];
         if (t < 2) s_best[t] = n_ch;
         double lo, hi;
         range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also publish s_best)
@@ -292,7 +341,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
                 const double target = q2[qi] * total;
                 unsigned cc[32];  // the 32 loads issued together, then the search
 #pragma unroll
-                for (int j = 0; j < 32; ++j) cc[j] = 32 * cw + j < nf ? d.fine[32 * cw + j] : 0u;
+                for (int j = 0; j < 32; ++j) cc[j] = 32 * cw + j < nf ? __ldcg(d.fine + 32 * cw + j) : 0u;
                 double cum = s_cum[qi][t];
                 int kb = nf;
                 unsigned cb_count = 0u;
@@ -325,7 +374,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
             const int k = t + u * static_cast<int>(blockDim.x);
-            cn[u] = k < nb ? d.cnt[k] : 0u, sq[u] = k < nb ? d.sv[k] : 0ull;
+            cn[u] = k < nb ? __ldcg(d.cnt + k) : 0u, sq[u] = k < nb ? __ldcg(d.sv + k) : 0ull;
         }
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
@@ -335,7 +384,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
             const double dd = (x0 - c) / bw, w = exp(-0.5 * dd * dd);
             const double sv = static_cast<double>(static_cast<long long>(sq[u])) / kFix;
             r[0] += w * static_cast<double>(cn[u]), r[1] += w * sv;
-            if (d.local_linear) r[2] += w * sx[k], r[3] += w * sxx[k], r[4] += w * sxv[k];
+            if (d.local_linear) r[2] += w * __ldcg(sx + k), r[3] += w * __ldcg(sxx + k), r[4] += w * __ldcg(sxv + k);
         }
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
@@ -349,7 +398,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
             for (int w = 0; w < nw; ++w) r[q] += s_red[q][w];
         }
         const double S0 = r[0], T0 = r[1], Ax = r[2], Axx = r[3], Axv = r[4];
-        const double fallback = static_cast<double>(static_cast<long long>(d.sv[nb])) / kFix / n_particles;
+        const double fallback = static_cast<double>(static_cast<long long>(__ldcg(d.sv + nb))) / kFix / n_particles;
         const double nw_e = S0 > 1e-8 ? T0 / (S0 > 1e-300 ? S0 : 1e-300) : fallback;
         cond = nw_e;
         if (d.local_linear) {
@@ -371,16 +420,20 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
         d.x_grids[static_cast<long long>(i) * nx + g] = x0;
         d.values[static_cast<long long>(i) * nx + g] = L;
     }
+    __syncthreads();  // the block's shared memory is free for its next grid point
+}
+
+__global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles) {
+    __shared__ RegressShared sh;
+    wait_previous();
+    regress_phase(d, n_particles, blockIdx.x, current_step(d), sh);
 }
 
 // The SLV Euler step of every pair (grid-stride), and the block's min and max of the new x into part_range. The step's
 // histogram and bins are read (lev_regress is done): the blocks clear them for the next step's binning.
 template <typename R>
-__global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v) {
-    __shared__ R s_lev[kMaxX];
-    __shared__ R s_min[8], s_max[8];
-    wait_previous();
-    const int i = current_step(d);
+__device__ void step_phase(const LevDev& d, R* __restrict__ x, R* __restrict__ v, int i, R* s_lev, R* s_min,
+                           R* s_max) {
     {
         const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0, n_ch = (nf + 31) / 32;
         const int stride = gridDim.x * blockDim.x;
@@ -392,11 +445,11 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
             else d.chunk[k - nf - 2 * nb - 1 - n_ll] = 0u;
         }
     }
-    for (int g = threadIdx.x; g < d.n_x; g += blockDim.x) s_lev[g] = static_cast<R>(d.lev[g]);
+    for (int g = threadIdx.x; g < d.n_x; g += blockDim.x) s_lev[g] = static_cast<R>(__ldcg(d.lev + g));
     __syncthreads();
     const int nx = d.n_x;
     const R h = static_cast<R>(d.dt[i]);
-    const R a = static_cast<R>(d.x_eval[0]), b = static_cast<R>(d.x_eval[nx - 1]);
+    const R a = static_cast<R>(__ldcg(d.x_eval)), b = static_cast<R>(__ldcg(d.x_eval + nx - 1));
     const R rho = static_cast<R>(d.rho), kappa = static_cast<R>(d.kappa), theta = static_cast<R>(d.theta);
     const R xi = static_cast<R>(d.xi);
     const R rc = m_sqrt(R(1) - rho * rho);
@@ -409,7 +462,7 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
         for (int leg = 0; leg < 2; ++leg) {
             const long long j = leg ? d.n_pairs + p : p;
             const R sg = leg ? R(-1) : R(1), zz1 = sg * z0, zz2 = sg * z1;
-            const R xj = x[j];
+            const R xj = __ldcg(x + j);
             R L;
             // interpolation on the uniform grid [a, b]: the CPU's form in double, the reference GPU's in float
             const R u = sizeof(R) == 8 ? (xj - a) / (b - a) * static_cast<R>(nx - 1)
@@ -421,7 +474,7 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
                 const R w = u - static_cast<R>(k);
                 L = s_lev[k] * (R(1) - w) + s_lev[k + 1] * w;
             }
-            const R vp = m_max(v[j], R(0)), var = L * L * vp;
+            const R vp = m_max(__ldcg(v + j), R(0)), var = L * L * vp;
             const R zx = rho * zz2 + rc * zz1;
             v[j] += kappa * (theta - vp) * h + xi * m_sqrt(vp * h) * zz2;
             const R xn = xj + R(-0.5) * var * h + m_sqrt(var * h) * zx;
@@ -442,6 +495,129 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
         d.part_range[2 * blockIdx.x] = static_cast<double>(mn);
         d.part_range[2 * blockIdx.x + 1] = static_cast<double>(mx);
     }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* __restrict__ v) {
+    __shared__ R s_lev[kMaxX];
+    __shared__ R s_min[32], s_max[32];
+    wait_previous();
+    step_phase<R>(d, x, v, current_step(d), s_lev, s_min, s_max);
+}
+
+// ------------------------------------------------------------------------------------------------ persistent
+//
+// The whole calibration as one cooperative launch (every block resident at once): per step the three phases above,
+// separated by grid barriers, with the step index a loop variable. One block of 512 threads per SM. The barrier is a
+// counter and a generation word in global memory; a block that waits polls the generation at most d.wait_limit times,
+// then records OB_ETIMEOUT in d.status and returns, and every other block leaves at its next barrier on seeing the
+// status, so a calibration whose barrier cannot complete ends with an error instead of holding the GPU.
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ int status_of(const LevDev& d) { return *reinterpret_cast<volatile int*>(d.status); }
+
+// Every block's writes before the barrier are visible to every block after it. False: the calibration has failed (a
+// barrier gave up), and the caller returns.
+__device__ bool grid_barrier(const LevDev& d) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned gen = ld_acquire_gpu(d.bar_gen);
+        __threadfence();
+        if (atomicAdd(d.bar_count, 1u) == gridDim.x - 1) {
+            atomicExch(d.bar_count, 0u);
+            __threadfence();
+            st_release_gpu(d.bar_gen, gen + 1);
+        } else {
+            // at most wait_limit polls: with a limit of zero a block that has to wait gives up at once
+            for (long long polls = 0;; ++polls) {
+                if (polls >= d.wait_limit) {
+                    atomicCAS(d.status, 0, OB_ETIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                if (ld_acquire_gpu(d.bar_gen) != gen) break;
+                if (status_of(d) != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (polls > 64) __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (status_of(d) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+constexpr int kPersistentThreads = 512;
+
+template <typename R>
+__global__ void __launch_bounds__(kPersistentThreads, 1)
+    lev_persistent(LevDev d, R* __restrict__ x, R* __restrict__ v, double n_particles) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ RegressShared rs;
+    __shared__ R s_lev[kMaxX];
+    __shared__ R s_min[32], s_max[32];
+    __shared__ double s_mn[32], s_mx[32];
+    const BinShared b = bin_shared(d, sm);
+    const long long n = 2 * d.n_pairs;
+    for (long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+         j += static_cast<long long>(gridDim.x) * blockDim.x)
+        x[j] = R(0), v[j] = static_cast<R>(d.v0);
+    // (step 0's regression reads no particle; the barrier after it orders these stores before the first step)
+    for (int i = 0; i < d.n_steps; ++i) {
+        if (i > 0) {
+            bin_clear_shared(d, b);
+            bin_phase<R>(d, x, v, b, s_mn, s_mx);
+            if (!grid_barrier(d)) return;
+        }
+        for (int g = blockIdx.x; g < d.n_x; g += gridDim.x) regress_phase(d, n_particles, g, i, rs);
+        if (!grid_barrier(d)) return;
+        step_phase<R>(d, x, v, i, s_lev, s_min, s_max);
+        if (i + 1 < d.n_steps && !grid_barrier(d)) return;
+    }
+}
+
+// Polls of a grid barrier before it gives up (ob_set_wait_limit): a barrier completes within one phase, microseconds;
+// the default, 2^22 polls with a short sleep between them, is about a second.
+constexpr long long kDefaultWaitLimit = 1LL << 22;
+long long g_wait_limit = kDefaultWaitLimit;
+
+// The persistent calibration on stream st; false (nothing launched) when the device cannot hold every block at once.
+template <typename R>
+bool run_persistent(LevDev& d, R* x, R* v, double n_particles, size_t bin_smem, int sms, cudaStream_t st) {
+    check_cuda(cudaFuncSetAttribute(lev_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(bin_smem)),
+               "cudaFuncSetAttribute");
+    int occ = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, lev_persistent<R>, kPersistentThreads, bin_smem),
+               "occupancy");
+    int coop = 0, dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cudaDeviceGetAttribute");
+    if (occ < 1 || !coop || d.n_step_blocks != sms) return false;
+    void* args[] = {&d, &x, &v, &n_particles};
+    const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(lev_persistent<R>), dim3(sms),
+                                                      dim3(kPersistentThreads), args, bin_smem, st);
+    if (e == cudaErrorCooperativeLaunchTooLarge) {
+        cudaGetLastError();
+        return false;
+    }
+    check_cuda(e, "lev_persistent launch");
+    return true;
 }
 
 void check_request(const ob_leverage_request& rq) {
@@ -502,8 +678,15 @@ void run_leverage(ob_leverage_request& rq) {
                "cudaFuncSetAttribute");
     // one binning block an SM (fewer for small particle counts): each block bins many particles before it adds
     const int n_bin_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(sms, (n + 511) / 512)));
-    d.n_step_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(4LL * sms, (rq.n_pairs + 255) / 256)));
-    d.part_range = arena.alloc<double>(2 * static_cast<size_t>(d.n_step_blocks));
+    // the persistent kernel's blocks (one an SM) each write their range; the graph path's lev_step uses up to 4 an SM
+    d.n_step_blocks = sms;
+    d.part_range = arena.alloc<double>(2 * static_cast<size_t>(4 * sms));
+    d.n_steps = S;
+    d.bar_count = arena.alloc<unsigned>(4);
+    d.bar_gen = d.bar_count + 1;
+    d.status = reinterpret_cast<int*>(d.bar_count + 2);
+    check_cuda(cudaMemset(d.bar_count, 0, 4 * sizeof(unsigned)), "cudaMemset");
+    d.wait_limit = g_wait_limit;
     const double n_particles = 2.0 * static_cast<double>(rq.n_pairs);
     // the kernel bandwidth of each step, as RC/src/leverage.cpp:63 computes it
     std::vector<double> bw(S);
@@ -521,6 +704,27 @@ void run_leverage(ob_leverage_request& rq) {
         c.attrs = pdl, c.numAttrs = 1;
         return c;
     };
+    // OPTLAB_B200_LEVERAGE=graphs runs the three-kernel schedule below instead (to compare the two; same results)
+    const char* mode = std::getenv("OPTLAB_B200_LEVERAGE");
+    const bool graphs_only = mode && std::strcmp(mode, "graphs") == 0;
+    if (!graphs_only && run_persistent<R>(d, x, v, n_particles, bin_smem, sms, st)) {
+        int status = 0;
+        check_cuda(cudaMemcpyAsync(&status, d.status, sizeof status, cudaMemcpyDeviceToHost, st), "copy status");
+        check_cuda(cudaMemcpyAsync(rq.x_grids, d.x_grids, static_cast<size_t>(S) * rq.n_x * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st),
+                   "copy x_grids");
+        check_cuda(cudaMemcpyAsync(rq.values, d.values, static_cast<size_t>(S) * rq.n_x * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st),
+                   "copy values");
+        check_cuda(cudaStreamSynchronize(st), "leverage");
+        if (status == OB_ETIMEOUT)
+            throw Error(OB_ETIMEOUT, "leverage: a grid barrier of the calibration gave up waiting for the other blocks");
+        if (status != 0) throw Error(OB_ECUDA, "leverage: the calibration kernel reported a failure");
+        rq.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+        return;
+    }
+    // the device cannot hold the persistent kernel: three kernels a step, replayed as graphs
+    d.n_step_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(4LL * sms, (rq.n_pairs + 255) / 256)));
     lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(x, v, n, static_cast<R>(rq.v0), d.step);
     check_cuda(cudaGetLastError(), "lev_init launch");
     const R* cx = x;
@@ -588,4 +792,11 @@ extern "C" int ob_leverage(ob_leverage_request* rq, int precision) {
         if (precision == OB_FP32) ob::run_leverage<float>(*rq);
         else ob::run_leverage<double>(*rq);
     });
+}
+
+extern "C" long long ob_set_wait_limit(long long polls) {
+    std::lock_guard<std::mutex> lock(ob::api_mutex());
+    const long long prev = ob::g_wait_limit;
+    ob::g_wait_limit = polls < 0 ? ob::kDefaultWaitLimit : polls;
+    return prev;
 }

@@ -191,36 +191,39 @@ inline QeConsts<R> make_qe_consts(const double* h, double r, double q, double dt
     return c;
 }
 
-// One QE-M step of (y, v) with independent normals zv (variance) and zx (log-spot), schemes.hpp:154-186. The
-// arithmetic is the reference's, rearranged to fewer divisions and square roots (exact algebra, not approximations):
-// sqrt(inv) sqrt(inv - 1) as one root of their product (inv = 2 / psi >= 4/3 there), the finiteness test A < 1 / (2 a)
-// as 1 - 2 A a > 0 (a > 0), and 1 / beta = m (psi + 1) / 2 in the exponential branch.
+// One QE-M step of (y, v) with independent normals zv (variance) and zx (log-spot), schemes.hpp:154-186. Andersen's
+// scheme picks, per path and step, the quadratic branch (psi <= 3/2: v' = a (b + zv)^2) or the exponential one (mass
+// p at zero, an exponential tail above it); lanes of a warp take both, so the warp executes both. Here the branches
+// share their FP64 divisions: each division's numerator and denominator are selected per lane, so a warp whose lanes
+// split runs three divisions (plus the exponential tail's inverse) where the two branches written apart ran seven,
+// and psi is never divided out. With s2 = v c1 + c2 (the conditional variance of v') and D = s2 + m^2:
+//   branch test    psi <= 3/2            as  s2 <= 3/2 m^2
+//   division 1     quadratic: 2 / psi    exponential: 1 - p = 2 / (psi + 1)      (2 m^2 over s2 or D)
+//   division 2     quadratic: a = m / (1 + b^2)    exponential: 1 / beta = m / (1 - p)
+//   division 3     quadratic: the K0 term -A b^2 a / (1 - 2 A a)    exponential: (1 - p) / (1 - A / beta)
+// with the exponential branch's K0 argument p + beta (1 - p) / (beta - A) written as p + (1 - p) / (1 - A / beta) and
+// its finiteness A < beta as A / beta < 1 (beta > 0). The algebra is the reference's; only roundings differ.
 template <typename R>
 __device__ __forceinline__ void qe_step(const QeConsts<R>& c, R& y, R& v, R zv, R zx) {
     const R m = c.theta + (v - c.theta) * c.E;
-    const R psi = (v * c.c1 + c.c2) / (m * m);
-    R vn, lin, w, arg;
-    bool finite;
-    if (psi <= R(1.5)) {
-        const R inv = R(2) / psi;
-        const R b2 = inv - R(1) + m_sqrt(inv * m_max(inv - R(1), R(0)));
-        const R a = m / (R(1) + b2), b = m_sqrt(b2);
-        vn = a * (b + zv) * (b + zv);
-        arg = R(1) - R(2) * c.A * a;
-        finite = arg > R(0);
-        lin = -c.A * b2 * a / arg;
-        w = R(0.5);
-    } else {
-        const R h = R(1) / (psi + R(1));
-        const R p = (psi - R(1)) * h, q = R(2) * h;  // q = 1 - p
-        const R beta = q / m;
-        const R one_minus_u = m_ncdf(-zv);
-        vn = one_minus_u >= q ? R(0) : m_log(q / one_minus_u) * (R(0.5) * m * (psi + R(1)));
-        arg = p + beta * q / (beta - c.A);
-        finite = c.A < beta;
-        lin = R(0);
-        w = R(-1);
+    const R m2 = m * m, s2 = v * c.c1 + c.c2;
+    const bool quad = s2 <= R(1.5) * m2;
+    const R r1 = (R(2) * m2) / (quad ? s2 : s2 + m2);  // quadratic: 2 / psi; exponential: q = 1 - p
+    const R b2 = r1 - R(1) + m_sqrt(quad ? r1 * m_max(r1 - R(1), R(0)) : R(0));
+    const R r2 = m / (quad ? R(1) + b2 : r1);  // quadratic: a; exponential: 1 / beta
+    const R b = m_sqrt(quad ? b2 : R(0));
+    R vn = r2 * (b + zv) * (b + zv);
+    if (!quad) {
+        const R one_minus_u = m_ncdf(-zv);  // 1 - U, exact in both tails
+        vn = one_minus_u >= r1 ? R(0) : m_log(r1 / one_minus_u) * r2;
     }
+    const R arg_q = R(1) - R(2) * c.A * r2;
+    const R den_e = R(1) - c.A * r2;
+    const R r3 = (quad ? -c.A * b2 * r2 : r1) / (quad ? arg_q : den_e);
+    const R arg = quad ? arg_q : (R(1) - r1) + r3;
+    const bool finite = quad ? arg_q > R(0) : den_e > R(0);
+    const R lin = quad ? r3 : R(0);
+    const R w = quad ? R(0.5) : R(-1);
     const R K0 = finite ? lin + w * m_log(arg) - (c.K1 + R(0.5) * c.K3) * v : c.K0p;
     y += c.mu_dt + K0 + c.K1 * v + c.K2 * vn + m_sqrt(m_max(c.K3 * v + c.K4 * vn, R(0))) * zx;
     v = vn;

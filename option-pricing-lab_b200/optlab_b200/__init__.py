@@ -14,8 +14,8 @@ and this package's restatements (optlab_b200.models) both work.
 
 from __future__ import annotations
 
+import functools
 import os
-from collections import OrderedDict
 from dataclasses import asdict, dataclass
 from typing import Any
 
@@ -47,7 +47,6 @@ __all__ = [
     "unsupported",
 ]
 
-_KIND = {"const": 0, "table": 1, "heston": 2, "slv": 3}
 N_X = 801
 MAX_NAMES = 8
 MAX_WINDOWS = 2
@@ -106,46 +105,76 @@ def seed64(seed) -> int:
 
 
 # ------------------------------------------------------------------------------------------------ models to tables
+#
+# Each name of a model or basket becomes a `_NameSpec`: the kind code the kernels switch on, the constant variance
+# (Black-Scholes), the Heston tuple (Heston and SLV) and, for the tabled kinds, a block of uniform rows (local
+# variance, or the squared leverage) with the row each time step reads. `plan()` stacks the names' blocks into one
+# table and offsets each name's step rows by the rows stacked before it. Tables are built once per (model object,
+# grid) and kept for the next plan of the same object: a small LRU keyed by the object's identity.
 
-_TABLES: OrderedDict = OrderedDict()
-
-
-def _cached(key, obj, build):
-    hit = _TABLES.get(key)
-    if hit is not None and hit[0] is obj:
-        _TABLES.move_to_end(key)
-        return hit[1]
-    rows = build()
-    _TABLES[key] = (obj, rows)
-    while len(_TABLES) > 16:
-        _TABLES.popitem(last=False)
-    return rows
+_KIND = {"const": 0, "table": 1, "heston": 2, "slv": 3}
+_NO_HESTON = (0.0, 1.0, 1.0, 0.0, 0.0)
+_DEFAULT_SD_RANGE = (-8.0, 6.0)
 
 
-def _local_var_rows(surface, t0: np.ndarray, n_x: int, sd_range=(-8.0, 6.0)):
-    return _cached((id(surface), "lv", n_x, t0.tobytes(), tuple(sd_range)), surface,
-                   lambda: local_var_rows(surface, t0, n_x, sd_range))
+class _ByIdentity:
+    """A model object as a cache key: equal only to itself (surfaces and leverages need not be hashable)."""
+
+    __slots__ = ("obj",)
+
+    def __init__(self, obj):
+        self.obj = obj
+
+    def __hash__(self):
+        return id(self.obj)
+
+    def __eq__(self, other):
+        return isinstance(other, _ByIdentity) and other.obj is self.obj
 
 
-def _leverage_rows(leverage, t0: np.ndarray, n_x: int):
-    """(lo, inv_dx, squared leverage rows, row of each step): packages/native/src/optlab/native/__init__.py:147-167."""
+@functools.lru_cache(maxsize=16)
+def _local_var_block(surface: _ByIdentity, t0_bytes: bytes, n_x: int, sd_range: tuple):
+    return local_var_rows(surface.obj, np.frombuffer(t0_bytes), n_x, sd_range)
 
-    def build():
-        times = np.asarray(leverage.times, dtype=float)
-        if hasattr(leverage, "rows"):
-            src = [(x0, x0 + (len(y) - 1) / inv, np.linspace(x0, x0 + (len(y) - 1) / inv, len(y)), y)
-                   for x0, inv, y in leverage.rows]
-        else:
-            src = [(xs[0], xs[-1], xs, vs) for xs, vs in zip(leverage.x_grids, leverage.values)]
-        lo, inv, rows = np.empty(len(src)), np.empty(len(src)), np.empty((len(src), n_x))
-        for r, (a, b, xs, vs) in enumerate(src):
-            grid = np.linspace(a, b, n_x)
-            lo[r], inv[r] = a, (n_x - 1) / (b - a)
-            rows[r] = np.interp(grid, xs, vs) ** 2
-        step = np.clip(np.searchsorted(times, t0 + 1e-12, side="right") - 1, 0, len(times) - 1).astype(np.int32)
-        return lo, inv, rows, step
 
-    return _cached((id(leverage), "lev", n_x, t0.tobytes()), leverage, build)
+def _uniform_resample(xs, vs, n_x: int):
+    """(lo, inv_dx, values) of (xs, vs) linearly interpolated on n_x uniform points over [xs[0], xs[-1]]."""
+    lo, hi = float(xs[0]), float(xs[-1])
+    return lo, (n_x - 1) / (hi - lo), np.interp(np.linspace(lo, hi, n_x), xs, vs)
+
+
+def _leverage_sources(leverage):
+    """(xs, values) of each time row of a leverage: its own grids, or the uniform rows (x0, inv_dx, y) of a
+    leverage tabulated that way (the reference's UniformLeverage)."""
+    if hasattr(leverage, "rows"):
+        for x0, inv, y in leverage.rows:
+            yield np.linspace(x0, x0 + (len(y) - 1) / inv, len(y)), np.asarray(y, dtype=float)
+    else:
+        yield from zip(leverage.x_grids, leverage.values)
+
+
+@functools.lru_cache(maxsize=16)
+def _leverage_block(leverage: _ByIdentity, t0_bytes: bytes, n_x: int):
+    """(lo, inv_dx, squared leverage rows, the row of each step): every time row resampled to n_x uniform points and
+    squared (the SLV kernel multiplies the variance by it); step i reads the last time row at or before its start
+    (packages/native/src/optlab/native/__init__.py:147-167)."""
+    t0 = np.frombuffer(t0_bytes)
+    times = np.asarray(leverage.obj.times, dtype=float)
+    rows = [_uniform_resample(xs, vs, n_x) for xs, vs in _leverage_sources(leverage.obj)]
+    lo = np.array([r[0] for r in rows])
+    inv = np.array([r[1] for r in rows])
+    squared = np.stack([r[2] for r in rows]) ** 2
+    step = np.clip(np.searchsorted(times, t0 + 1e-12, side="right") - 1, 0, len(times) - 1).astype(np.int32)
+    return lo, inv, squared, step
+
+
+@dataclass
+class _NameSpec:
+    kind: int
+    cvar: float = 0.0
+    heston: tuple = _NO_HESTON
+    block: tuple | None = None  # (lo, inv_dx, rows) of the name's table
+    step_rows: np.ndarray | None = None  # per step, the row of the block it reads
 
 
 def _name(model) -> str:
@@ -157,25 +186,41 @@ def _heston_tuple(model):
     return (h.v0, h.kappa, h.theta, h.xi, h.rho)
 
 
-def _describe(model, t0: np.ndarray, n_x: int):
-    """(kind, constant variance, Heston parameters, table rows or None, step rows or None) of one name
-    (packages/native/src/optlab/native/__init__.py:170-187)."""
-    name = _name(model)
-    if name == "BlackScholesModel":
-        return _KIND["const"], model.vol**2, (0.0, 1.0, 1.0, 0.0, 0.0), None, None
-    if name in ("LocalVolModel", "TabulatedLocalVol"):
-        sd = getattr(model, "sd_range", (-8.0, 6.0))
-        lo, inv, rows = _local_var_rows(model.surface, t0, n_x, sd)
-        return _KIND["table"], 0.0, (0.0, 1.0, 1.0, 0.0, 0.0), (lo, inv, rows), np.arange(len(t0), dtype=np.int32)
-    if name == "SLVModel":
-        lo, inv, rows, step = _leverage_rows(model.leverage, t0, n_x)
-        return _KIND["slv"], 0.0, _heston_tuple(model), (lo, inv, rows), step
-    if name == "HestonModel":
-        return _KIND["heston"], 0.0, _heston_tuple(model), None, None
-    raise NotImplementedError(f"{name} is not in the path engine")
+def _spec_black_scholes(model, t0, n_x):
+    return _NameSpec(_KIND["const"], cvar=model.vol**2)
 
 
-_KNOWN = ("BlackScholesModel", "LocalVolModel", "TabulatedLocalVol", "SLVModel", "HestonModel")
+def _spec_heston(model, t0, n_x):
+    return _NameSpec(_KIND["heston"], heston=_heston_tuple(model))
+
+
+def _spec_local_vol(model, t0, n_x):
+    sd_range = tuple(getattr(model, "sd_range", _DEFAULT_SD_RANGE))
+    block = _local_var_block(_ByIdentity(model.surface), t0.tobytes(), n_x, sd_range)
+    return _NameSpec(_KIND["table"], block=block, step_rows=np.arange(len(t0), dtype=np.int32))
+
+
+def _spec_slv(model, t0, n_x):
+    lo, inv, rows, step = _leverage_block(_ByIdentity(model.leverage), t0.tobytes(), n_x)
+    return _NameSpec(_KIND["slv"], heston=_heston_tuple(model), block=(lo, inv, rows), step_rows=step)
+
+
+# the model classes the path engine takes, by class name (the reference's classes and this package's restatements)
+_SPEC_OF = {
+    "BlackScholesModel": _spec_black_scholes,
+    "LocalVolModel": _spec_local_vol,
+    "TabulatedLocalVol": _spec_local_vol,
+    "SLVModel": _spec_slv,
+    "HestonModel": _spec_heston,
+}
+_KNOWN = tuple(_SPEC_OF)
+
+
+def _spec(model, t0: np.ndarray, n_x: int) -> _NameSpec:
+    build = _SPEC_OF.get(_name(model))
+    if build is None:
+        raise NotImplementedError(f"{_name(model)} is not in the path engine")
+    return build(model, t0, n_x)
 
 
 def _is_basket(model) -> bool:
@@ -194,28 +239,32 @@ def unsupported(model) -> str | None:
     return _model_unsupported(model)
 
 
+def _leverage_usable(leverage) -> bool:
+    return hasattr(leverage, "rows") or (hasattr(leverage, "x_grids") and hasattr(leverage, "values"))
+
+
 def _model_unsupported(model) -> str | None:
-    if _is_basket(model):
-        if len(model.names) > MAX_NAMES:
-            return f"more than {MAX_NAMES} names"
-        bad = [n for n, m in model.models.items() if _name(m) not in _KNOWN]
-        if bad:
-            return f"{', '.join(_name(model.models[n]) for n in bad)} not in the path engine"
-        if model.mixer is not None and _name(model.mixer) != "LocalCorrelation":
-            return f"{_name(model.mixer)} is not in the path engine (local correlation only)"
-        return None
-    if _name(model) not in _KNOWN:
-        return f"{_name(model)} is not in the path engine"
-    if _name(model) == "SLVModel":
-        lev = model.leverage
-        if not hasattr(lev, "rows") and not (hasattr(lev, "x_grids") and hasattr(lev, "values")):
+    """The first reason the path engine refuses a model or basket, in the reference's words, or None."""
+    if not _is_basket(model):
+        if _name(model) not in _SPEC_OF:
+            return f"{_name(model)} is not in the path engine"
+        if _name(model) == "SLVModel" and not _leverage_usable(model.leverage):
             return "this leverage is not in the path engine"
+        return None
+    if len(model.names) > MAX_NAMES:
+        return f"more than {MAX_NAMES} names"
+    foreign = [_name(model.models[n]) for n in model.names if _name(model.models[n]) not in _SPEC_OF]
+    if foreign:
+        return f"{', '.join(foreign)} not in the path engine"
+    if model.mixer is not None and _name(model.mixer) != "LocalCorrelation":
+        return f"{_name(model.mixer)} is not in the path engine (local correlation only)"
     return None
 
 
 @dataclass
 class Plan:
-    """Everything of a simulation but the pairs (native/__init__.py:215-240)."""
+    """Everything of a simulation but the pairs: the field list and shapes of the reference's Plan
+    (native/__init__.py:215-240), so either engine's `run` reads it."""
 
     names: tuple
     kind: np.ndarray
@@ -241,45 +290,60 @@ class Plan:
         return len(self.obs_step)
 
 
+def _names_of(model, market):
+    """(names, models, markets, root, same) of a basket, or of one model as a one-name basket."""
+    if _is_basket(model):
+        names = tuple(model.names)
+        return (names, [model.models[n] for n in names], [model.markets[n] for n in names],
+                np.asarray(model.root, dtype=float), int(model.vol_corr == "same"))
+    return ("_",), [model], [market], np.eye(1), 1
+
+
+def _mixer_fields(model):
+    """(mixer flag, the 8 mixer constants, the aligned low-correlation root) of a basket's local-correlation mixer."""
+    mx = getattr(model, "mixer", None) if _is_basket(model) else None
+    if mx is None:
+        return 0, (0.0,) * 8, None
+    low, sign, turn = aligned_factors(model.corr, model.root, mx.w0)
+    consts = (mx.w0, mx.level, mx.down, mx.up, mx.sigma, sign, np.cos(turn), np.sin(turn))
+    return 1, tuple(float(c) for c in consts), np.ascontiguousarray(low, dtype=float)
+
+
 def plan(model, market, times, dt_max=1 / 252, dt_min=1 / 2000, n_x: int = N_X) -> Plan:
-    """A model or basket as the engine's arrays (native/__init__.py:243-302)."""
+    """A model or basket as the engine's arrays, for observations at `times` (native/__init__.py:243-302): the time
+    grid (one step when every name is Black-Scholes), each name's kind, parameters and table rows, the forwards at the
+    observations, the correlation root and the mixer."""
     why = _model_unsupported(model)
     if why:
         raise NotImplementedError(why)
     times = np.asarray(times, dtype=float)
-    if _is_basket(model):
-        names, models = tuple(model.names), [model.models[n] for n in model.names]
-        markets = [model.markets[n] for n in model.names]
-        root, same = np.asarray(model.root, dtype=float), int(model.vol_corr == "same")
-    else:
-        names, models, markets, root, same = ("_",), [model], [market], np.eye(1), 1
+    names, models, markets, root, same = _names_of(model, market)
     if all(_name(m) == "BlackScholesModel" for m in models):
         dt_max, dt_min = np.inf, None
     grid = time_grid(times, dt_max, dt_min)
-    obs = np.searchsorted(grid, times).astype(np.int32)
     dt, t0 = np.diff(grid), grid[:-1].copy()
-    k = len(models)
-    kind, cvar, hes = np.empty(k, np.int32), np.empty(k), np.empty((k, 5))
-    lo, inv, tab, rows_of = [], [], [], np.zeros((k, len(dt)), np.int32)
-    offset = 0
-    for a, m in enumerate(models):
-        kind[a], cvar[a], hes[a], rows, step = _describe(m, t0, n_x)
-        if rows is not None:
-            lo.append(rows[0]), inv.append(rows[1]), tab.append(rows[2])
-            rows_of[a] = step + offset
-            offset += len(rows[0])
-    fwd = np.stack([np.asarray(mk.F(times), dtype=float) for mk in markets]) if len(times) else np.zeros((k, 0))
-    mixer, mix, low = 0, (0.0,) * 8, None
-    if _is_basket(model) and model.mixer is not None:
-        mx = model.mixer
-        low, sign, turn = aligned_factors(model.corr, model.root, mx.w0)
-        mixer, mix = 1, (mx.w0, mx.level, mx.down, mx.up, mx.sigma, sign, np.cos(turn), np.sin(turn))
-        low = np.ascontiguousarray(low, dtype=float)
+    specs = [_spec(m, t0, n_x) for m in models]
+    tabled = [sp for sp in specs if sp.block is not None]
+    step_row = lo = inv = table = None
+    if tabled:
+        # stack the blocks; each name's step rows move by the rows of the blocks before it
+        offsets = np.cumsum([0] + [len(sp.block[0]) for sp in tabled])
+        step_row = np.zeros((len(specs), len(dt)), np.int32)
+        for off, sp in zip(offsets, tabled):
+            step_row[specs.index(sp)] = sp.step_rows + off
+        lo = np.concatenate([sp.block[0] for sp in tabled])
+        inv = np.concatenate([sp.block[1] for sp in tabled])
+        table = np.ascontiguousarray(np.concatenate([sp.block[2] for sp in tabled]))
+    fwd = np.zeros((len(specs), 0))
+    if len(times):
+        fwd = np.stack([np.asarray(mk.F(times), dtype=float) for mk in markets])
+    mixer, mix, low = _mixer_fields(model)
     return Plan(
-        names, kind, cvar, np.ascontiguousarray(hes), np.ascontiguousarray(root), same, dt, t0, obs,
-        np.ascontiguousarray(fwd), rows_of if tab else None, np.concatenate(lo) if lo else None,
-        np.concatenate(inv) if inv else None, np.ascontiguousarray(np.concatenate(tab)) if tab else None, mixer,
-        tuple(float(x) for x in mix), low, n_x,
+        names=names, kind=np.array([sp.kind for sp in specs], np.int32), cvar=np.array([sp.cvar for sp in specs]),
+        heston=np.ascontiguousarray([sp.heston for sp in specs], dtype=float), root=np.ascontiguousarray(root),
+        same=same, dt=dt, t0=t0, obs_step=np.searchsorted(grid, times).astype(np.int32),
+        fwd=np.ascontiguousarray(fwd), step_row=step_row, lo=lo, inv_dx=inv, table=table, mixer=mixer, mix=mix,
+        low_root=low, n_x=n_x,
     )
 
 
@@ -346,7 +410,7 @@ def calibrate_leverage(params, surface, market, T_max: float, mix: float = 1.0, 
         raise ValueError(f"unknown regression {regression!r}, expected nadaraya_watson or local_linear")
     grid = time_grid([T_max], dt_max, dt_min)
     dt, t0 = np.diff(grid), grid[:-1].copy()
-    lv_lo, lv_inv, lv_rows = _local_var_rows(surface, t0, N_X)
+    lv_lo, lv_inv, lv_rows = _local_var_block(_ByIdentity(surface), t0.tobytes(), N_X, _DEFAULT_SD_RANGE)
     T1 = min(1.0, float(surface.maturities[-1]))
     atm_vol = float(np.sqrt(surface.theta(T1) / T1))
     h = (params.v0, params.kappa, params.theta, mix * params.xi, params.rho)

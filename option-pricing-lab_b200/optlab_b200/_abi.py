@@ -269,6 +269,7 @@ class ObBatchRequest(C.Structure):
         ("horizon", C.c_double),
         ("n_exp", C.c_int),
         ("n_x", C.c_int),
+        ("n_rows", C.c_int),
         ("table", _dp),
         ("row_lo", _dp),
         ("row_inv_dx", _dp),
@@ -285,6 +286,7 @@ class ObBatchRequest(C.Structure):
         ("n_vol", C.c_int),
         ("vol_shift", _dp),
         ("vol_tilt", _dp),
+        ("vol_table", _dp),
         ("n_carry", C.c_int),
         ("carry_rate", _dp),
         ("carry_div", _dp),
@@ -350,6 +352,7 @@ SIGNATURES = {
     "ob_has_cuda": (C.c_int, []),
     "ob_cpu_threads": (C.c_int, []),
     "ob_release_buffers": (C.c_int, []),
+    "ob_set_wait_limit": (C.c_longlong, [C.c_longlong]),
     "ob_device_info": (C.c_int, [C.c_int, C.POINTER(ObDevice)]),
     "ob_philox_normals": (
         C.c_int,

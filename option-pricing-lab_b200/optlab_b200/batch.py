@@ -10,9 +10,12 @@ same launch.
 
 `sample_book` draws the benchmark's book: 512 trades of 1 to 5 names, 1 to 5 years of daily steps, 2^14 to 2^18 paths,
 European, barrier or autocall payoffs (worst-of with several names), under Heston QE or local vol of per-name SSVI
-surfaces, with 60 scenarios: 20 spot moves of +-1..20 %, 20 parallel moves of local vol of +-1..10 points, 20 skew
-tilts of +-1..10 points per unit of log-moneyness. Carry moves (CARRY_MOVES: rates +-1 %, dividend yield +-1 %) and
-correlation moves (CORR_MOVES: every pair +-0.10) are added on request.
+surfaces, with 60 scenarios: 20 spot moves of +-1..20 %, 20 parallel moves of the implied vols of +-1..10 points and 20
+skew moves of +-1..10 points (the rise of the 90 % vol against the 110 % one at one year). A vol scenario moves each
+surface's implied vols as the reference's risk scenarios do (packages/risk/src/optlab/risk/shocks.py:63-108,
+VolMove.apply -> bumped_surface, risk/surfaces.py:204) and re-tabulates Dupire's local variance on the base table's
+points (optlab_b200.ivnodes.moved_local_var); the device reads those tables. Carry moves (CARRY_MOVES: rates +-1 %,
+dividend yield +-1 %) and correlation moves (CORR_MOVES: every pair +-0.10) are added on request.
 """
 
 from __future__ import annotations
@@ -36,12 +39,13 @@ from ._abi import (
 )
 from .engine import precision_code
 from .models import correlation_root, nearest_correlation
+from .ivnodes import grid_points, moved_local_var
 from .surfaces import SSVI, LocalVarGrid
 
 _STEPS = np.array([0.01, 0.02, 0.03, 0.04, 0.05, 0.075, 0.10, 0.125, 0.15, 0.20])
 SPOT_MOVES = np.concatenate([-_STEPS[::-1], _STEPS])
-VOL_SHIFTS = np.concatenate([-np.arange(10, 0, -1), np.arange(1, 11)]) / 100.0
-SKEW_TILTS = VOL_SHIFTS.copy()
+VOL_SHIFTS = np.concatenate([-np.arange(10, 0, -1), np.arange(1, 11)]) / 100.0  # parallel implied-vol moves
+SKEW_TILTS = VOL_SHIFTS.copy()  # skew moves: the 90 % - 110 % implied-vol gap at one year
 CARRY_MOVES = ((0.01, 0.0), (-0.01, 0.0), (0.0, 0.01), (0.0, -0.01))  # (rate, dividend yield)
 CORR_MOVES = (-0.10, 0.10)
 MAX_OBS = 64
@@ -79,13 +83,14 @@ class Book:
     spot_shift: np.ndarray
     vol_shift: np.ndarray
     vol_tilt: np.ndarray
+    vol_table: np.ndarray = field(default_factory=lambda: np.zeros(0))  # n_vol x pool rows x n_x
     carry_rate: np.ndarray = field(default_factory=lambda: np.zeros(0))
     carry_div: np.ndarray = field(default_factory=lambda: np.zeros(0))
     corr_move: np.ndarray = field(default_factory=lambda: np.zeros(0))  # each trade's moved roots at corr_root0
     struct: ObBatchRequest = field(init=False)
 
     _DOUBLES = ("table", "row_lo", "row_inv_dx", "root", "leg_strike", "leg_level", "obs_trigger", "obs_discount",
-                "spot_shift", "vol_shift", "vol_tilt", "carry_rate", "carry_div", "corr_move")
+                "spot_shift", "vol_shift", "vol_tilt", "vol_table", "carry_rate", "carry_div", "corr_move")
 
     def __post_init__(self):
         for k in self._DOUBLES:
@@ -97,6 +102,9 @@ class Book:
         s.n_trades = len(self.trades)
         s.trades = self._trades
         s.dt, s.horizon, s.n_exp, s.n_x = self.dt, self.horizon, self.n_exp, self.n_x
+        s.n_rows = len(self.row_lo)
+        if len(self.vol_shift) and self.vol_table.size != len(self.vol_shift) * len(self.row_lo) * self.n_x:
+            raise ValueError("vol_table must hold every pool row under every vol scenario")
         for k in self._DOUBLES[:-1]:
             a = getattr(self, k)
             setattr(s, k, a.ctypes.data_as(_dp) if a.size else None)
@@ -152,14 +160,29 @@ class Book:
 
 
 def _surfaces(rng, n_names, horizon, n_exp, n_x):
-    """Per-name SSVI power-law surfaces (theta_t = c t, c in 0.03..0.06, rho in -0.7..-0.4, eta 1, gamma 0.5)
-    tabulated as local variance on n_exp expiries x n_x log-strikes over the horizon."""
+    """Per-name SSVI power-law surfaces (theta_t = c t, c in 0.03..0.06, rho in -0.7..-0.4, eta 1, gamma 0.5) and
+    their local variance tabulated on n_exp expiries x n_x log-strikes over the horizon."""
     T = horizon * np.arange(1, n_exp + 1) / n_exp
-    grids = []
+    surfaces, grids = [], []
     for _ in range(n_names):
         c, rho = rng.uniform(0.03, 0.06), rng.uniform(-0.7, -0.4)
-        grids.append(LocalVarGrid.from_surface(SSVI.power_law(rho, 1.0, 0.5, T, c * T), T, n_x))
-    return grids
+        surfaces.append(SSVI.power_law(rho, 1.0, 0.5, T, c * T))
+        grids.append(LocalVarGrid.from_surface(surfaces[-1], T, n_x))
+    return surfaces, grids
+
+
+def scenario_tables(surfaces, grids, vol_shifts, skew_moves) -> np.ndarray:
+    """(n_vol, pool rows, n_x): each grid's local variance on its own points with the surface's implied vols moved by
+    each scenario's (parallel shift, skew move)."""
+    out = []
+    for p, k in zip(vol_shifts, skew_moves):
+        rows = []
+        for surf, g in zip(surfaces, grids):
+            kk = grid_points(g.lo, g.inv_dx, g.n_x)
+            TT = np.broadcast_to(g.expiries[:, None], kk.shape)
+            rows.append(moved_local_var(surf, kk, TT, parallel=float(p), skew=float(k)))
+        out.append(np.vstack(rows))
+    return np.asarray(out).reshape(len(out), -1, grids[0].n_x if grids else 0)
 
 
 def moved_corr(corr, move: float) -> np.ndarray:
@@ -186,12 +209,13 @@ def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), year
     step a day; 2^k paths with k uniform in paths_log2; a European ladder (1 to 3 calls or puts), a barrier option
     (up-and-out or up-and-in call, down-and-in or down-and-out put), or a Phoenix autocall (quarterly or monthly),
     each on the worst performance of its names. Scenarios: the spot moves, the carry moves ((rate, dividend yield)
-    pairs), the parallel vol shifts, then the skew tilts (a vol scenario is a (shift, tilt) pair: (s, 0) or (0, t)),
+    pairs), the parallel implied-vol shifts, then the skew moves (a vol scenario is a (shift, skew) pair: (s, 0) or
+    (0, k), its tables re-tabulated from the moved implied vols),
     then the correlation moves (every pair of a multi-name trade; its moved roots follow its root in the pool)."""
     rng = np.random.default_rng(seed)
     horizon = float(years[1])
     dt = 1.0 / steps_per_year
-    grids = _surfaces(rng, n_surfaces, horizon, n_exp, n_x)
+    surfaces, grids = _surfaces(rng, n_surfaces, horizon, n_exp, n_x)
     table = np.vstack([g.rows for g in grids])
     row_lo = np.concatenate([g.lo for g in grids])
     row_inv = np.concatenate([g.inv_dx for g in grids])
@@ -264,6 +288,7 @@ def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), year
     carry = np.asarray(carry_moves, float).reshape(-1, 2)
     vs = np.concatenate([np.asarray(vol_shifts, float), np.zeros(len(skew_tilts))])
     vt = np.concatenate([np.zeros(len(vol_shifts)), np.asarray(skew_tilts, float)])
+    vol_table = scenario_tables(surfaces, grids, vs, vt) if len(vs) else np.zeros(0)
     return Book(
         trades=trades,
         labels=labels,
@@ -285,6 +310,7 @@ def sample_book(n_trades: int = 512, seed: int = 2024, paths_log2=(14, 18), year
         spot_shift=np.asarray(spot_moves, float),
         vol_shift=vs,
         vol_tilt=vt,
+        vol_table=vol_table,
         carry_rate=carry[:, 0],
         carry_div=carry[:, 1],
         corr_move=np.asarray(corr_moves, float),

@@ -755,16 +755,8 @@ int or_batch_trade(const ob_batch_request* b, int trade, int n_threads, double* 
         if (lv)
             for (int r = 0; r < N * E; ++r) {
                 const double* src = b->table + (size_t)(t->table_row0 + r) * X;
-                const double dx = 1.0 / inv[r];
-                for (int k = 0; k < X; ++k) {
-                    double v = src[k];
-                    if (vol >= 0) {
-                        double sg = sqrt(v) + b->vol_shift[vol] + b->vol_tilt[vol] * (lo[r] + k * dx);
-                        sg = sg > 0.01 ? sg : 0.01;
-                        v = sg * sg;
-                    }
-                    table[(size_t)r * X + k] = v;
-                }
+                const double* moved = vol >= 0 ? b->vol_table + ((size_t)vol * b->n_rows + t->table_row0 + r) * X : src;
+                for (int k = 0; k < X; ++k) table[(size_t)r * X + k] = moved[k];
             }
         const double shift = sc >= 1 && sc <= b->n_spot ? log1p(b->spot_shift[sc - 1]) : 0.0;
         ob_mc_result res;

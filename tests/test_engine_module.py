@@ -145,3 +145,27 @@ def test_the_cpu_backend_is_refused_there_is_no_fallback():
 def test_the_entry_point_is_declared():
     text = (Path(__file__).resolve().parent.parent / "option-pricing-lab_b200" / "pyproject.toml").read_text()
     assert '[project.entry-points."optlab.engines"]' in text and 'native = "optlab_b200"' in text
+
+
+def test_the_monotone_cubic_is_the_pchip_the_reference_fits_with():
+    """MonotoneCubic against scipy's PchipInterpolator (the reference's interpolant of theta(T) and the wings):
+    values and slopes on monotone, flat-stretched and sign-changing data, ends included."""
+    from scipy.interpolate import PchipInterpolator
+
+    from optlab_b200.surfaces import MonotoneCubic
+
+    rng = np.random.default_rng(3)
+    cases = [
+        (np.append(0.0, np.cumsum(rng.uniform(0.1, 1.0, 12))), np.append(0.0, np.cumsum(rng.uniform(0, 1, 12)))),
+        (np.arange(8.0), np.array([0.0, 1.0, 1.0, 1.0, 2.0, 5.0, 5.5, 9.0])),
+        (np.cumsum(rng.uniform(0.2, 1.0, 10)), rng.normal(size=10)),
+        (np.array([0.0, 1.0]), np.array([2.0, -1.0])),
+        (np.array([0.0, 0.5, 2.0]), np.array([0.0, 3.0, 2.5])),
+    ]
+    for x, y in cases:
+        ref = PchipInterpolator(x, y, extrapolate=False)
+        t = np.concatenate([x, np.linspace(x[0], x[-1], 257)])
+        v, s = MonotoneCubic(x, y).at(t)
+        scale = np.abs(y).max() + 1.0
+        assert np.max(np.abs(v - ref(t))) <= 1e-13 * scale
+        assert np.max(np.abs(s - ref.derivative()(t))) <= 1e-12 * scale / np.diff(x).min()

@@ -134,3 +134,34 @@ def test_fp64_paths_reproduce_the_references_golden_vectors(name):
     exp = case["expected"]
     assert np.max(np.abs(S[idx] / np.asarray(exp["samples"]) - 1)) < 1e-12
     assert abs(S.sum() / exp["sum"] - 1) < 1e-12
+
+
+def test_the_persistent_calibration_equals_the_three_kernel_schedule(monkeypatch):
+    """The calibration runs as one persistent kernel with grid barriers; OPTLAB_B200_LEVERAGE=graphs runs the same
+    phases as three kernels a step replayed as graphs. The counts and v sums are integers and the regression the same
+    arithmetic, so the two give the same tables (FP64 to the last bits of the regression's block sums)."""
+    a, b = leverage_request(**_lev_kw()), leverage_request(**_lev_kw())
+    engine.leverage(a, "fp64")
+    monkeypatch.setenv("OPTLAB_B200_LEVERAGE", "graphs")
+    engine.leverage(b, "fp64")
+    assert np.abs(a.x_grids - b.x_grids).max() <= 1e-12 * np.abs(b.x_grids).max()
+    assert np.abs(a.values / b.values - 1).max() < 1e-12
+
+
+def test_a_grid_barrier_that_gives_up_returns_a_timeout_and_the_device_stays_usable():
+    """With a wait limit of zero polls every block but the last to arrive at the first grid barrier gives up at once
+    (a flag nobody has set yet, as far as each of them may wait); the call returns OB_ETIMEOUT, every block leaves the
+    kernel at its next barrier, and the next calibration, with the default limit, runs as before."""
+    lib = _abi.load()
+    h = leverage_request(**_lev_kw(n_pairs=2**12, n_steps=8))
+    prev = lib.ob_set_wait_limit(0)
+    try:
+        with pytest.raises(_abi.EngineError, match="gave up waiting"):
+            engine.leverage(h, "fp32")
+    finally:
+        lib.ob_set_wait_limit(-1)
+    assert lib.ob_set_wait_limit(-1) == prev  # the default was restored
+    g, o = leverage_request(**_lev_kw()), leverage_request(**_lev_kw())
+    engine.leverage(g, "fp64")
+    engine.leverage(o, "fp64")
+    assert np.array_equal(g.values, o.values)
