@@ -49,6 +49,19 @@ INST_PER_PATH_STEP = {"lv_phoenix": 1.461, "heston_qe": 20.3, "script": 2.507,
                       "batch": 1.623,
                       # the drop-in path engine's local-vol kernel on the Phoenix model (12 columns + a daily window)
                       "paths": 2.639}
+# The ALGORITHM's lane instructions per path-step of the local-vol Phoenix (one name, both legs of a pair share each
+# normal), counted from the algorithm, not from the compiled code, so that extra instructions lower the fraction:
+#   Philox4x32-10, one call per 4 normals = 4 pair-steps = 8 path-steps: 10 rounds x (2 wide multiplies, 2 three-way
+#     xors, 2 key additions) + 4 to set the counter = 64, so 8 per path-step;
+#   Box-Muller, per 2 normals = 4 path-steps: 2 conversions and 2 multiply-adds to (0, 1), a logarithm (10 with its
+#     range reduction), a square root (2), sin and cos of 2 pi v (10), 2 products = 28, so 7 per path-step;
+#   the local-vol step, per path-step: the table coordinate (1 multiply-add), its integer part and back (2), the
+#     weight (1), the index clamp (2), the address (1), one 8-byte shared load of the interval (1), the interpolation
+#     (1 multiply-add); variance x dt (1), its square root (2), the drift and the diffusion (2 multiply-adds); the
+#     knock-in's running minimum (1): 14.
+# 29 lane instructions = 0.906 warp instructions per path-step. The observations (12 over 756 steps) add < 1 %.
+ALG_INST_PER_PATH_STEP = {"lv_phoenix": (8 + 7 + 14) / 32.0}
+
 # Warp instructions of one leverage calibration at 2^18 particles x 504 steps: lev_bin 4.24 M x 503 + lev_regress
 # 1.44 M x 504 + lev_step 1.70 M x 504 (ncu, one launch of each).
 LEV_INST_PER_CALIBRATION = 4.24e6 * 503 + 1.44e6 * 504 + 1.70e6 * 504
@@ -414,16 +427,26 @@ def main():
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     issue_peak = props.multi_processor_count * 4 * sm_max * 1e6 / 1e9  # G warp-instructions/s
     ipu = INST_PER_PATH_STEP.get(args.workload) if args.table == "builder" else None  # counted on the builder grid
+    alg = ALG_INST_PER_PATH_STEP.get(args.workload)
+    per_gpu = value / world
+    executed = {"achieved": ipu * per_gpu / 1e9 if ipu else None,
+                "frac": ipu * per_gpu / 1e9 / issue_peak if ipu else None, "inst_per_path_step": ipu,
+                "note": "warp instructions the compiled kernel executes per path-step (ncu) x live rate"}
     roofline = {
         "bound": "issue",
-        "achieved": (ipu * value / world / 1e9) if ipu else None,
+        "achieved": (alg * per_gpu / 1e9) if alg else executed["achieved"],
         "peak": issue_peak,
         "unit": "Gwarp-inst/s",
-        "frac": (ipu * value / world / 1e9 / issue_peak) if ipu else None,
+        "frac": (alg * per_gpu / 1e9 / issue_peak) if alg else executed["frac"],
         "traffic": DRAM_PER_LAUNCH.get(args.workload) if args.table == "builder" else None,
+        "algorithmic_inst_per_path_step": alg,
+        "executed": executed,
+        "executed_over_algorithmic": (ipu / alg) if (alg and ipu) else None,
         "note": ("FP32/SFU issue-bound kernel" if prec == "fp32" else "FP64 kernel bound by its dependent FP64 chain")
         + " (no HBM or tensor-core bound applies); peak = SMs x 4 schedulers x "
-        f"max SM clock ({sm_max:.0f} MHz, {peak_kind}); achieved = ncu instructions per path-step x live rate",
+        f"max SM clock ({sm_max:.0f} MHz, {peak_kind}); achieved = the algorithm's warp instructions per path-step "
+        "(frozen in bench.py from the algorithm's operation count) x live rate"
+        + ("" if alg else " (no algorithmic count for this workload: the executed count stands in)"),
     }
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -730,7 +753,9 @@ def run_batch(args, world, rank):
         "revaluations_per_s": book.revaluations() / t_step,
         "per_trade_launches": {"ms_per_step": t_pt * 1e3, "path_steps_per_s": units / t_pt,
                                "speedup_of_graph": t_pt / t_step, "launches": n_sims},
-        "autotune": {"seconds": t_tune, "create_seconds": t_create, "classes": shapes},
+        "autotune": {"seconds": t_tune, "create_seconds": t_create, "classes": shapes,
+                     "sample_speedup_over_untuned_shapes": (sum(c["untuned_us"] for c in shapes) /
+                                                            max(1, sum(c["tuned_us"] for c in shapes)))},
         "roofline": issue_roofline(INST_PER_PATH_STEP["batch"] * units / t_step,
                                    "FP32/SFU issue-bound stepping as the fused kernels; achieved = ncu warp "
                                    "instructions per path-step of the class kernels (32-trade book) x live rate"),

@@ -180,6 +180,13 @@ typedef struct {
     double coupon_barrier, coupon, ki_barrier, put_strike;
     int memory;                /* coupons missed are paid at the next coupon */
     int ki_daily;              /* 1: knock-in on the lowest close of every step end; 0: at maturity only */
+    /* local correlation (OB_MODEL_PATHS, 2 names or more; paths.hpp:219-237): with mixer 1 every step draws one more
+       normal after the names' and mixes a common factor into the names' normals, with a weight that moves with the
+       level of the basket at the step's start. mix = (w0, level, down, up, sigma, sign, cos, sin), low_root the root
+       of the low correlation aligned to the factor: the reference plan's mix and low_root (localcorr.py:47-83). */
+    int mixer;
+    double mix[8];
+    const double* low_root;    /* n_names x n_names */
 } ob_mc_request;
 
 typedef struct {
@@ -449,7 +456,9 @@ int ob_batch_launch(ob_batch* batch, void* stream);
 int ob_batch_run_per_trade(ob_batch* batch, void* stream);
 int ob_batch_result(ob_batch* batch, double* price, double* se, double* device_ms);
 /* The trade classes (one persistent kernel each) and their current shapes: *n_classes, and for the first
-   max_classes of them 6 ints each in info: model, names, product, trades, tile (pairs per work item), block. */
+   max_classes of them 8 ints each in info: model, names, product, trades, tile (pairs per work item), block, and
+   after ob_batch_tune the time in microseconds of the tuner's sample of the class at its shape before tuning and at
+   the kept one (0 before tuning). */
 int ob_batch_classes(const ob_batch* batch, int max_classes, int* n_classes, int* info);
 int ob_batch_destroy(ob_batch* batch);
 

@@ -641,6 +641,7 @@ void check_adjoint(const ob_adjoint_request& r) {
     if (rq.model != OB_MODEL_PATHS || rq.product != OB_PRODUCT_AUTOCALL)
         invalid("the adjoint prices an autocall under the path engine's local vol");
     if (rq.n_names > 4) invalid("the adjoint takes 1 to 4 names");
+    if (rq.mixer) invalid("the adjoint takes no local correlation");
     for (int a = 0; a < rq.n_names; ++a)
         if (rq.kind[a] != 1) invalid("the adjoint needs every name in local vol (kind 1)");
     if (rq.n_obs > kMaxObs) invalid("the adjoint takes at most 64 observations");

@@ -368,6 +368,7 @@ struct BClass {
     bool qe = false;
     int n = 1, product = 0;
     int tile = 8192, block = 256;
+    double untuned_ms = 0.0, tuned_ms = 0.0;  // the autotuner's sample at the shape before tuning and at the kept one
     std::vector<int> trades;
     const void* kernel = nullptr;
     cudaStream_t stream = nullptr;
@@ -820,31 +821,42 @@ int ob_batch_create(const ob_batch_request* rq, int precision, ob_batch** batch)
     });
 }
 
-// The autotuner: for each class, every (tile, block) candidate is timed on the same sample of the class's work (up to
-// kTuneSims of its simulations, spread over its sizes: enough pairs to fill the GPU several times over) after one
-// untimed launch, and the fastest kept; past budget_ms the untried candidates are skipped.
+// The autotuner, by successive halving per class: every (tile, block) candidate is timed on a small sample of the
+// class's work (kProbeSims simulations spread over its sizes), the kFinalists fastest again on a larger one
+// (kTuneSims: enough pairs to fill the GPU several times over), each after one untimed launch, and the fastest kept;
+// the shape the class had before is timed on the larger sample too, so that the class records what tuning gained.
+// Past budget_ms the untried candidates are skipped.
 int ob_batch_tune(ob_batch* batch, int budget_ms) {
     return ob::guarded([&] {
         if (!batch) ob::invalid("null batch");
         ob::Batch& b = batch->impl;
         if (b.exec) ob::invalid("tune before capture");
-        constexpr int kTuneSims = 32;
+        constexpr int kProbeSims = 4, kTuneSims = 32, kFinalists = 3;
         const auto t0 = std::chrono::steady_clock::now();
+        auto over = [&] {
+            const double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return budget_ms > 0 && el > budget_ms;
+        };
         const int tiles[] = {512, 1024, 2048, 4096, 8192, 16384};
         const int blocks[] = {128, 256};
         for (size_t ci = 0; ci < b.classes.size(); ++ci) {
-            double best = 1e300;
-            int bt = b.classes[ci].tile, bb = b.classes[ci].block;
-            b.time_class(static_cast<int>(ci), bt, bb, kTuneSims);  // warm: module load, caches
+            ob::BClass& c = b.classes[ci];
+            const int k = static_cast<int>(ci);
+            b.time_class(k, c.tile, c.block, kProbeSims);  // warm: module load, caches
+            std::vector<std::pair<double, std::pair<int, int>>> probe;
             for (int tile : tiles)
-                for (int block : blocks) {
-                    const double el =
-                        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-                    if (budget_ms > 0 && el > budget_ms) continue;
-                    const double ms = b.time_class(static_cast<int>(ci), tile, block, kTuneSims);
-                    if (ms < best) best = ms, bt = tile, bb = block;
-                }
-            b.classes[ci].tile = bt, b.classes[ci].block = bb;
+                for (int block : blocks)
+                    if (!over()) probe.push_back({b.time_class(k, tile, block, kProbeSims), {tile, block}});
+            std::sort(probe.begin(), probe.end());
+            const double before = b.time_class(k, c.tile, c.block, kTuneSims);
+            double best = before;
+            int bt = c.tile, bb = c.block;
+            for (int f = 0; f < std::min<int>(kFinalists, static_cast<int>(probe.size())); ++f) {
+                const auto [tile, block] = probe[f].second;
+                const double ms = b.time_class(k, tile, block, kTuneSims);
+                if (ms < best) best = ms, bt = tile, bb = block;
+            }
+            c.tile = bt, c.block = bb, c.untuned_ms = before, c.tuned_ms = best;
         }
         b.layout(b.main, b.tiles());
     });
@@ -977,9 +989,10 @@ int ob_batch_classes(const ob_batch* batch, int max_classes, int* n_classes, int
         *n_classes = static_cast<int>(b.classes.size());
         for (int k = 0; k < std::min(max_classes, *n_classes) && info; ++k) {
             const ob::BClass& c = b.classes[k];
-            int* o = info + 6 * k;
+            int* o = info + 8 * k;
             o[0] = c.qe ? OB_MODEL_HESTON_QE : OB_MODEL_PATHS, o[1] = c.n, o[2] = c.product;
             o[3] = static_cast<int>(c.trades.size()), o[4] = c.tile, o[5] = c.block;
+            o[6] = static_cast<int>(c.untuned_ms * 1e3 + 0.5), o[7] = static_cast<int>(c.tuned_ms * 1e3 + 0.5);
         }
     });
 }

@@ -84,14 +84,23 @@ constexpr int min_blocks() {
 
 // KIND: 1 local vol (table), 2 Heston (Euler), 3 SLV (table x Heston, residuals on the aux stream), 4 Heston QE-M.
 // GT: the table is read from global memory (a.tab) instead of the stage.
-template <typename R, int N, int KIND, int PRODUCT, bool GT = false>
-__global__ void __launch_bounds__(512, min_blocks<R>())
+// Blocks of 512 an SM the register budget allows: two in float (64 registers), one in double; one for the mixer's
+// 4- and 5-name baskets in float too, whose two legs' normals would spill at 64.
+template <typename R, int N, bool MIX>
+constexpr int fused_min_blocks() {
+    return MIX && N >= 4 ? 1 : min_blocks<R>();
+}
+
+// MIX (local vol, 2 to 5 names): the local-correlation mixer, one more normal a step after the names'.
+template <typename R, int N, int KIND, int PRODUCT, bool GT = false, bool MIX = false>
+__global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
     fused_kernel(FusedArgs<R> a, long long n_pairs, long long first_pair, uint32_t k0, uint32_t k1,
                  double* __restrict__ partial) {
     constexpr bool QE = KIND == 4;
     constexpr bool VAR = KIND == 2 || KIND == 3;
     constexpr bool TABLE = KIND == 1 || KIND == 3;
-    constexpr int C = QE ? 2 : (KIND == 2 ? 2 * N : N);  // normals per step, stream 0
+    static_assert(!MIX || (KIND == 1 && N >= 2), "the mixer runs local-vol baskets");
+    constexpr int C = QE ? 2 : (KIND == 2 ? 2 * N : N + (MIX ? 1 : 0));  // normals per step, stream 0
     constexpr int CA = KIND == 3 ? N : 0;                // normals per step, aux stream
     // steps per batch of whole Philox blocks; one local-vol name draws two blocks a batch (8 steps), whose two
     // independent multiply chains interleave (1.317 -> 1.300 ms for the 2^20-path Phoenix; one SLV name would draw four
@@ -162,11 +171,45 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                     const StepRec<R> st = s_step[i - 1];
                     const R* zs = &z[g * C];
                     R zc[N], wc[N];
+                    R zm0[MIX ? N : 1], zm1[MIX ? N : 1];  // with the mixer each leg's own normals (signs in)
+                    if (MIX) {
+                        // paths.hpp:219-237: a common factor whose weight moves with the level of the basket (the
+                        // log of the mean of S / F at the step's start), per leg
+                        const R* s_low = reinterpret_cast<const R*>(sm + a.off.low_root);
+                        const R den = reinterpret_cast<const R*>(sm + a.off.mix_den)[i - 1];
+#pragma unroll
+                        for (int leg = 0; leg < 2; ++leg) {
+                            const R sg = leg ? R(-1) : R(1);
+                            R mm = R(0);
+#pragma unroll
+                            for (int n = 0; n < N; ++n) mm += m_exp(leg ? x1[n] : x0[n]);
+                            const R u = m_log(mm / static_cast<R>(N)) / den;
+                            R wt = a.mix_base + a.mix_down * m_max(-u, R(0)) - a.mix_up * m_max(u, R(0));
+                            wt = m_min(m_max(wt, R(0)), R(1));
+                            const R market = a.mix_sign * sg * zs[N - 1], fr = sg * zs[N];
+                            const R common = a.mix_cos * market + a.mix_sin * fr;
+                            R other[N];
+#pragma unroll
+                            for (int n = 0; n < N - 1; ++n) other[n] = sg * zs[n];
+                            other[N - 1] = a.mix_sin * market - a.mix_cos * fr;
+                            const R sw = m_sqrt(wt), sl = m_sqrt(R(1) - wt);
+#pragma unroll
+                            for (int n = 0; n < N; ++n) {
+                                R acc = R(0);
+#pragma unroll
+                                for (int b = 0; b < N; ++b) acc += s_low[n * N + b] * other[b];
+                                (leg ? zm1 : zm0)[n] = sw * common + sl * acc;
+                            }
+                        }
+                    }
 #pragma unroll
                     for (int n = 0; n < N; ++n) {
                         R acc = R(0);
+                        if (!MIX) {
 #pragma unroll
-                        for (int b = 0; b < N; ++b) acc += (kRootRegs ? rt[n * N + b] : s_root[n * N + b]) * zs[b];
+                            for (int b = 0; b < N; ++b)
+                                acc += (kRootRegs ? rt[n * N + b] : s_root[n * N + b]) * zs[b];
+                        }
                         zc[n] = acc;
                     }
                     if (VAR) {
@@ -207,9 +250,14 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
                             v0[n] += h[1] * (h[2] - vp0) * st.dt + h[3] * (m_sqrt(vp0) * st.sdt) * zv;
                             v1[n] += h[1] * (h[2] - vp1) * st.dt + h[3] * (m_sqrt(vp1) * st.sdt) * (-zv);
                         }
-                        const R zd = st.sdt * zc[n];  // sqrt(dt) z, the legs' +-
-                        x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
-                        x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
+                        if (MIX) {
+                            x0[n] += m_fma(m_sqrt(var0), st.sdt * zm0[n], var0 * st.hdt);
+                            x1[n] += m_fma(m_sqrt(var1), st.sdt * zm1[n], var1 * st.hdt);
+                        } else {
+                            const R zd = st.sdt * zc[n];  // sqrt(dt) z, the legs' +-
+                            x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
+                            x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
+                        }
                         if (n == 0) w0 = x0[n] + ns.lf, w1 = x1[n] + ns.lf;
                         else w0 = m_min(w0, x0[n] + ns.lf), w1 = m_min(w1, x1[n] + ns.lf);
                     }
@@ -348,6 +396,18 @@ FusedFn<R> pick_n(int n) {
     return nullptr;
 }
 
+// Local-vol baskets of 2 to 5 names with the local-correlation mixer.
+template <typename R, int PRODUCT, bool GT>
+FusedFn<R> pick_mix(int n) {
+    switch (n) {
+        case 2: return fused_kernel<R, 2, 1, PRODUCT, GT, true>;
+        case 3: return fused_kernel<R, 3, 1, PRODUCT, GT, true>;
+        case 4: return fused_kernel<R, 4, 1, PRODUCT, GT, true>;
+        case 5: return fused_kernel<R, 5, 1, PRODUCT, GT, true>;
+        default: return nullptr;
+    }
+}
+
 // table_global: the kinds with a table (local vol, SLV) read it from global memory.
 template <typename R, int PRODUCT>
 FusedFn<R> pick_fused(int kind, int n, bool table_global) {
@@ -394,9 +454,15 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
             if (rq.kind[a] != kind) return false;
         if (kind == 0) return false;
     }
-    auto pick = [&](bool table_global) {
-        return rq.product == OB_PRODUCT_LADDER ? pick_fused<R, OB_PRODUCT_LADDER>(kind, n, table_global)
-                                               : pick_fused<R, OB_PRODUCT_AUTOCALL>(kind, n, table_global);
+    if (rq.mixer && kind != 1) return false;  // the mixer beside other kinds: the generic kernel
+    auto pick = [&](bool table_global) -> FusedFn<R> {
+        const bool ladder = rq.product == OB_PRODUCT_LADDER;
+        if (rq.mixer)
+            return ladder ? (table_global ? pick_mix<R, OB_PRODUCT_LADDER, true>(n) : pick_mix<R, OB_PRODUCT_LADDER, false>(n))
+                          : (table_global ? pick_mix<R, OB_PRODUCT_AUTOCALL, true>(n)
+                                          : pick_mix<R, OB_PRODUCT_AUTOCALL, false>(n));
+        return ladder ? pick_fused<R, OB_PRODUCT_LADDER>(kind, n, table_global)
+                      : pick_fused<R, OB_PRODUCT_AUTOCALL>(kind, n, table_global);
     };
     if (!pick(false)) return false;
     FusedArgs<R> a{};
@@ -446,6 +512,17 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
             hes[8 * k + 5] = static_cast<R>(std::sqrt(R(1) - rho * rho));
         }
         a.off.hes = blob.put(hes);
+        if (rq.mixer) {
+            std::vector<R> den(S), low(static_cast<size_t>(n) * n);
+            for (int i = 0; i < S; ++i)  // R arithmetic as the generic step: sigma sqrt(max(t0, 1/12))
+                den[i] = static_cast<R>(rq.mix[4]) * std::sqrt(std::max(static_cast<R>(rq.t0[i]), R(1.0 / 12)));
+            for (size_t k = 0; k < low.size(); ++k) low[k] = static_cast<R>(rq.low_root[k]);
+            a.off.mix_den = blob.put(den), a.off.low_root = blob.put(low);
+            a.mix_base = static_cast<R>(rq.mix[0]) + static_cast<R>(rq.mix[1]);
+            a.mix_down = static_cast<R>(rq.mix[2]), a.mix_up = static_cast<R>(rq.mix[3]);
+            a.mix_sign = static_cast<R>(rq.mix[5]), a.mix_cos = static_cast<R>(rq.mix[6]);
+            a.mix_sin = static_cast<R>(rq.mix[7]);
+        }
     }
     if (rq.product == OB_PRODUCT_LADDER) {
         std::vector<int> type(rq.n_legs), bar(rq.n_legs);

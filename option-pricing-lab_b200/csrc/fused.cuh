@@ -75,6 +75,7 @@ struct alignas(16) StepRec {
 // Byte offsets inside the staged blob.
 struct FusedOffsets {
     int step, name_step, root, hes, table2, ln_trig, obs_disc, leg_type, leg_strike, leg_barrier, ln_level;
+    int mix_den, low_root;  // local correlation: per step sigma sqrt(max(t0, 1/12)); the aligned low root
 };
 
 template <typename R>
@@ -91,6 +92,8 @@ struct FusedArgs {
     R ln_cb, ln_ki;
     double coupon, put_strike;
     const Pair2<R>* tab;  // the table in global memory when it does not fit the stage (kernels with GT), else unused
+    // local correlation (kernels with MIX): w0 + level, down, up, sign, cos, sin of the mixer (paths.hpp:219-237)
+    R mix_base, mix_down, mix_up, mix_sign, mix_cos, mix_sin;
 };
 
 }  // namespace ob

@@ -157,10 +157,14 @@ __global__ void __launch_bounds__(256) mc_kernel(McArgs<R> a, long long n_pairs,
     const McView<R> v = view_of(a, sm, table);
 
     ModelDev<R> m;
-    m.n_names = a.n_names, m.n_steps = a.n_steps, m.n_x = a.n_x, m.same = a.same, m.mixer = 0;
+    m.n_names = a.n_names, m.n_steps = a.n_steps, m.n_x = a.n_x, m.same = a.same, m.mixer = a.mixer;
     m.has_var = a.has_var, m.has_slv = a.has_slv, m.k0 = k0, m.k1 = k1;
-    m.dt = v.dt, m.t0 = nullptr, m.root = v.root, m.kind = v.kind, m.cvar = v.cvar, m.hes = v.hes;
-    m.step_row = v.step_row, m.lo = v.lo, m.inv_dx = v.inv_dx, m.table = v.table, m.low_root = nullptr;
+    m.dt = v.dt, m.root = v.root, m.kind = v.kind, m.cvar = v.cvar, m.hes = v.hes;
+    m.step_row = v.step_row, m.lo = v.lo, m.inv_dx = v.inv_dx, m.table = v.table;
+    m.t0 = a.mixer ? reinterpret_cast<const R*>(sm + a.off.t0) : nullptr;
+    m.low_root = a.mixer ? reinterpret_cast<const R*>(sm + a.off.low_root) : nullptr;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) m.mix[k] = a.mix[k];
 
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     const int S = a.n_steps;
@@ -293,7 +297,10 @@ void check_mc_model(const ob_mc_request& rq) {
                         invalid("step_row out of range");
             }
         }
+        // requests.cpp:89 (the paths request's check, the same message)
+        if (rq.mixer && (rq.mixer != 1 || !rq.low_root || !(rq.mix[4] > 0))) invalid("bad local correlation");
     } else {
+        if (rq.mixer) invalid("bad local correlation");
         if (!rq.heston) invalid("null heston");
         const double* h = rq.heston;
         if (!(h[0] >= 0 && h[1] > 0 && h[2] > 0 && h[3] > 0 && std::fabs(h[4]) <= 1))
@@ -354,6 +361,12 @@ void McPlan::build(const ob_mc_request& rq) {
             a.off.step_row = pk.put<int>(rq.step_row, static_cast<size_t>(n) * S);
             a.off.lo = pk.put<R>(rq.row_lo, rq.n_rows);
             a.off.inv_dx = pk.put<R>(rq.row_inv_dx, rq.n_rows);
+        }
+        if (rq.mixer) {
+            a.mixer = 1;
+            a.off.t0 = pk.put<R>(rq.t0, S);
+            a.off.low_root = pk.put<R>(rq.low_root, static_cast<size_t>(n) * n);
+            for (int k = 0; k < 8; ++k) a.mix[k] = static_cast<R>(rq.mix[k]);
         }
     } else {
         a.qe = make_qe_consts<R>(rq.heston, rq.r, rq.q, rq.dt[0]);

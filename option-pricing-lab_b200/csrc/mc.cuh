@@ -8,7 +8,7 @@ namespace ob {
 // Byte offsets of each array inside the packed blob (16-byte aligned).
 struct McOffsets {
     int dt, root, kind, cvar, hes, step_row, lo, inv_dx, lf, obs_of_step, ln_trig, obs_disc, leg_type, leg_strike,
-        leg_barrier, ln_level, table;
+        leg_barrier, ln_level, table, t0, low_root;
 };
 
 template <typename R>
@@ -19,6 +19,8 @@ struct McArgs {
     int table_in_smem;
     const R* table_global;      // the table, when it stays in global memory
     int n_names, n_steps, n_x, same, has_var, has_slv;
+    int mixer;   // local correlation: t0 and low_root staged, mix the constants
+    R mix[8];
     int n_out, n_legs, n_obs;
     QeConsts<R> qe;
     R spot0;

@@ -630,7 +630,7 @@ template <typename R>
 bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, DeviceArena& arena, LvArgs<R>& a) {
     const ob_mc_request& q = rq.model;
     const int n = q.n_names, S = q.n_steps;
-    if (q.model != OB_MODEL_PATHS || n > 5) return false;
+    if (q.model != OB_MODEL_PATHS || n > 5 || q.mixer) return false;
     for (int k = 0; k < n; ++k)
         if (q.kind[k] != 1) return false;
     std::vector<unsigned char> blob;
@@ -824,9 +824,13 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     d.model = mq.model, d.n_names = n, d.n_steps = S;
     for (int a = 0; a < n; ++a) d.spot0[a] = static_cast<R>(mq.spot[a]);
     ModelDev<R>& m = d.m;
-    m.n_names = n, m.n_steps = S, m.n_x = mq.n_x, m.same = mq.same, m.mixer = 0;
+    m.n_names = n, m.n_steps = S, m.n_x = mq.n_x, m.same = mq.same, m.mixer = mq.mixer;
     m.dt = arena.put<R>(mq.dt, S);
     m.t0 = arena.put<R>(mq.t0, S);
+    if (mq.mixer) {  // local correlation: the generic interpreter kernel runs it (pack_lv declines)
+        m.low_root = arena.put<R>(mq.low_root, static_cast<size_t>(n) * n);
+        for (int k = 0; k < 8; ++k) m.mix[k] = static_cast<R>(mq.mix[k]);
+    }
     if (mq.model == OB_MODEL_PATHS) {
         bool table = false;
         for (int a = 0; a < n; ++a) {

@@ -197,6 +197,9 @@ class ObMcRequest(C.Structure):
         ("put_strike", C.c_double),
         ("memory", C.c_int),
         ("ki_daily", C.c_int),
+        ("mixer", C.c_int),
+        ("mix", C.c_double * 8),
+        ("low_root", _dp),
     ]
 
 

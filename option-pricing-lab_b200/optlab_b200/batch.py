@@ -350,13 +350,14 @@ class Batch:
         return price, se, ms.value
 
     def classes(self) -> list[dict]:
-        """The trade classes (one persistent kernel each) with their trades and current tile and block."""
+        """The trade classes (one persistent kernel each) with their trades, current tile and block, and after tune()
+        the tuner's sample time at the shape before tuning and at the kept one (microseconds)."""
         n = C.c_int()
         check(load().ob_batch_classes(self._p, 0, C.byref(n), None))
-        info = np.zeros(6 * max(n.value, 1), np.int32)
+        info = np.zeros(8 * max(n.value, 1), np.int32)
         check(load().ob_batch_classes(self._p, n.value, C.byref(n), info.ctypes.data_as(_ip)))
-        keys = ("model", "names", "product", "trades", "tile", "block")
-        return [dict(zip(keys, map(int, info[6 * k:6 * k + 6]))) for k in range(n.value)]
+        keys = ("model", "names", "product", "trades", "tile", "block", "untuned_us", "tuned_us")
+        return [dict(zip(keys, map(int, info[8 * k:8 * k + 8]))) for k in range(n.value)]
 
     def close(self) -> None:
         if self._p:

@@ -147,8 +147,12 @@ def mc_request(
     put_strike=1.0,
     memory=0,
     ki_daily=0,
+    mixer=0,
+    mix=(0.0,) * 8,
+    low_root=None,
 ) -> Held:
-    """An ObMcRequest: a model (OB_MODEL_PATHS or OB_MODEL_HESTON_QE) plus a product (ladder or autocall)."""
+    """An ObMcRequest: a model (OB_MODEL_PATHS or OB_MODEL_HESTON_QE) plus a product (ladder or autocall); mixer,
+    mix and low_root: a local-correlation basket (the reference plan's fields of the same names)."""
     spot = f64(np.atleast_1d(spot))
     n = len(spot)
     a = {
@@ -171,6 +175,7 @@ def mc_request(
         "obs_step": i32(obs_step),
         "obs_discount": f64(obs_discount),
         "trigger": f64(trigger),
+        "low_root": f64(low_root) if low_root is not None else np.empty(0),
     }
     s = ObMcRequest()
     s.model, s.n_names, s.n_steps = int(model), n, len(a["dt"])
@@ -193,6 +198,9 @@ def mc_request(
         float(put_strike),
     )
     s.memory, s.ki_daily = int(memory), int(ki_daily)
+    s.mixer, s.low_root = int(mixer), ptr(a["low_root"])
+    for k in range(8):
+        s.mix[k] = float(mix[k])
     return Held(s, list(a.values()))
 
 

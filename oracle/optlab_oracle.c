@@ -606,6 +606,8 @@ static int check_mc(const ob_mc_request* rq) {
     } else {
         return fail("product must be 0 or 1");
     }
+    if (rq->mixer && (rq->model != OB_MODEL_PATHS || rq->mixer != 1 || !rq->low_root || !(rq->mix[4] > 0)))
+        return fail("bad local correlation");
     if (rq->model == OB_MODEL_PATHS) {
         if (!rq->root || !rq->kind || !rq->cvar || !rq->heston || !rq->log_fwd) return fail("null array");
         for (int a = 0; a < rq->n_names; ++a) {
@@ -643,6 +645,8 @@ static int mc_price_shifted(const ob_mc_request* rq, double ln_shift, int sum_le
         c.m.dt = rq->dt, c.m.t0 = rq->t0, c.m.root = rq->root, c.m.cvar = rq->cvar, c.m.hes = rq->heston;
         c.m.lo = rq->row_lo, c.m.inv_dx = rq->row_inv_dx, c.m.table = rq->table, c.m.kind = rq->kind;
         c.m.step_row = rq->step_row, c.m.same = rq->same;
+        c.m.mixer = rq->mixer, c.m.low_root = rq->low_root;
+        for (int k = 0; k < 8; ++k) c.m.mix[k] = rq->mix[k];
     }
     const long long n_blocks = (rq->n_pairs + OR_BLOCK - 1) / OR_BLOCK;
     McPartial* parts = (McPartial*)calloc((size_t)n_blocks, sizeof(McPartial));
@@ -1099,6 +1103,8 @@ int or_autocall_smooth(const ob_mc_request* rq, double eps, int n_threads, ob_mc
     c.m.dt = rq->dt, c.m.t0 = rq->t0, c.m.root = rq->root, c.m.cvar = rq->cvar, c.m.hes = rq->heston;
     c.m.lo = rq->row_lo, c.m.inv_dx = rq->row_inv_dx, c.m.table = rq->table, c.m.kind = rq->kind;
     c.m.step_row = rq->step_row, c.m.same = rq->same;
+    c.m.mixer = rq->mixer, c.m.low_root = rq->low_root;
+    for (int k = 0; k < 8; ++k) c.m.mix[k] = rq->mix[k];
     const long long n_blocks = (rq->n_pairs + OR_BLOCK - 1) / OR_BLOCK;
     double* parts = (double*)calloc((size_t)n_blocks * 2, sizeof(double));
     if (!parts) return fail("out of memory");
