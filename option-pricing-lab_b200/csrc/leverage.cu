@@ -76,9 +76,8 @@ struct LevDev {
     double* x_grids;           // n_steps x n_x
     double* values;            // n_steps x n_x
     int* step;                 // the current step: 0 from lev_init, advanced by lev_bin before the step's regression
-    // the persistent kernel's grid barrier: arrivals, generation, and the status a barrier that gave up sets
+    // the persistent kernel's grid barrier: its arrival counter, and the status a barrier that gave up sets
     unsigned* bar_count;
-    unsigned* bar_gen;
     int* status;
     long long wait_limit;      // polls of a barrier's generation before it gives up (OB_ETIMEOUT)
 };
@@ -165,9 +164,27 @@ __device__ __forceinline__ void bin_clear_shared(const LevDev& d, const BinShare
 // One block's share of a step's binning (the block's shared memory cleared by bin_clear_shared before): its particles
 // into the shared histogram and bins, then the non-zero entries added into the step's global ones. Particles and the
 // last step's ranges are read through L2: in the persistent kernel other blocks wrote them in the same launch.
+// Particles a phase works on: arrays x, v of 2 n particles (leg 0 of pair c at c, leg 1 at n + c) whose pair c is
+// global pair first + c, this thread taking pairs (or particles) start, start + stride, ... In global memory (SH false:
+// every pair, the grid striding over them, read through L2) or in the block's shared memory (SH true: the block's own
+// pairs, kept there from step to step by the persistent kernel).
 template <typename R>
-__device__ void bin_phase(const LevDev& d, const R* __restrict__ x, const R* __restrict__ v, const BinShared& b,
-                          double* s_mn, double* s_mx) {
+struct Particles {
+    R* x;
+    R* v;
+    long long n, first, start, stride;
+};
+
+template <bool SH, typename R>
+__device__ __forceinline__ R ld_part(const R* p) {
+    if constexpr (SH) return *p;
+    else return __ldcg(p);
+}
+
+template <typename R, bool SH = false>
+__device__ void bin_phase(const LevDev& d, const Particles<R>& pt, const BinShared& b, double* s_mn, double* s_mx) {
+    const R* __restrict__ x = pt.x;
+    const R* __restrict__ v = pt.v;
     const int nb = d.n_bins, nf = d.n_fine, ll = d.local_linear;
     unsigned long long* s_sv = b.sv;
     double* s_ll = b.ll;
@@ -177,16 +194,16 @@ __device__ void bin_phase(const LevDev& d, const R* __restrict__ x, const R* __r
     range_of(d, lo_d, hi_d, s_mn, s_mx);  // (its barrier also orders the clearing before)
     const R lo = static_cast<R>(lo_d), hi = static_cast<R>(hi_d);
     const R wf = (hi - lo) / static_cast<R>(nf), we = (hi + static_cast<R>(1e-12) - lo) / static_cast<R>(nb);
-    const long long n = 2 * d.n_pairs;
+    const long long n = 2 * pt.n;
     long long tot = 0;
-    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-    for (long long j0 = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; j0 < n; j0 += 4 * stride) {
+    const long long stride = pt.stride;
+    for (long long j0 = pt.start; j0 < n; j0 += 4 * stride) {
         // four particles' loads in flight before their atomics
         R xr[4], vr[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const long long j = j0 + u * stride;
-            xr[u] = j < n ? __ldcg(x + j) : R(0), vr[u] = j < n ? __ldcg(v + j) : R(0);
+            xr[u] = j < n ? ld_part<SH>(x + j) : R(0), vr[u] = j < n ? ld_part<SH>(v + j) : R(0);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -239,7 +256,10 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     bin_clear_shared(d, b);
     wait_previous();
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(d.step, 1);  // the previous step is done: this is the next
-    bin_phase<R>(d, x, v, b, s_mn, s_mx);
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    const Particles<R> pt{const_cast<R*>(x), const_cast<R*>(v), d.n_pairs, 0, blockIdx.x * (long long)blockDim.x + threadIdx.x,
+                          stride};
+    bin_phase<R>(d, pt, b, s_mn, s_mx);
 }
 
 // Exclusive prefix of x over the block and the block's total (any block size that is a multiple of 32, up to 1024).
@@ -431,9 +451,10 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
 
 // The SLV Euler step of every pair (grid-stride), and the block's min and max of the new x into part_range. The step's
 // histogram and bins are read (lev_regress is done): the blocks clear them for the next step's binning.
-template <typename R>
-__device__ void step_phase(const LevDev& d, R* __restrict__ x, R* __restrict__ v, int i, R* s_lev, R* s_min,
-                           R* s_max) {
+template <typename R, bool SH = false>
+__device__ void step_phase(const LevDev& d, const Particles<R>& pt, int i, R* s_lev, R* s_min, R* s_max) {
+    R* __restrict__ x = pt.x;
+    R* __restrict__ v = pt.v;
     {
         const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0, n_ch = (nf + 31) / 32;
         const int stride = gridDim.x * blockDim.x;
@@ -454,15 +475,14 @@ __device__ void step_phase(const LevDev& d, R* __restrict__ x, R* __restrict__ v
     const R xi = static_cast<R>(d.xi);
     const R rc = m_sqrt(R(1) - rho * rho);
     R mn = sizeof(R) == 4 ? R(3.0e38f) : R(1.0e300), mx = -mn;
-    for (long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; p < d.n_pairs;
-         p += static_cast<long long>(gridDim.x) * blockDim.x) {
+    for (long long p = pt.start; p < pt.n; p += pt.stride) {
         R z0, z1, z2, z3;
-        normals4<R>(static_cast<uint64_t>(p), static_cast<uint64_t>(i + 1), 0u, d.k0, d.k1, z0, z1, z2, z3);
+        normals4<R>(static_cast<uint64_t>(pt.first + p), static_cast<uint64_t>(i + 1), 0u, d.k0, d.k1, z0, z1, z2, z3);
 #pragma unroll
         for (int leg = 0; leg < 2; ++leg) {
-            const long long j = leg ? d.n_pairs + p : p;
+            const long long j = leg ? pt.n + p : p;
             const R sg = leg ? R(-1) : R(1), zz1 = sg * z0, zz2 = sg * z1;
-            const R xj = __ldcg(x + j);
+            const R xj = ld_part<SH>(x + j);
             R L;
             // interpolation on the uniform grid [a, b]: the CPU's form in double, the reference GPU's in float
             const R u = sizeof(R) == 8 ? (xj - a) / (b - a) * static_cast<R>(nx - 1)
@@ -474,7 +494,7 @@ __device__ void step_phase(const LevDev& d, R* __restrict__ x, R* __restrict__ v
                 const R w = u - static_cast<R>(k);
                 L = s_lev[k] * (R(1) - w) + s_lev[k + 1] * w;
             }
-            const R vp = m_max(__ldcg(v + j), R(0)), var = L * L * vp;
+            const R vp = m_max(ld_part<SH>(v + j), R(0)), var = L * L * vp;
             const R zx = rho * zz2 + rc * zz1;
             v[j] += kappa * (theta - vp) * h + xi * m_sqrt(vp * h) * zz2;
             const R xn = xj + R(-0.5) * var * h + m_sqrt(var * h) * zx;
@@ -502,7 +522,9 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[32], s_max[32];
     wait_previous();
-    step_phase<R>(d, x, v, current_step(d), s_lev, s_min, s_max);
+    const Particles<R> pt{x, v, d.n_pairs, 0, blockIdx.x * (long long)blockDim.x + threadIdx.x,
+                          static_cast<long long>(gridDim.x) * blockDim.x};
+    step_phase<R>(d, pt, current_step(d), s_lev, s_min, s_max);
 }
 
 // ------------------------------------------------------------------------------------------------ persistent
@@ -519,40 +541,37 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     return v;
 }
 
-__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
 __device__ __forceinline__ int status_of(const LevDev& d) { return *reinterpret_cast<volatile int*>(d.status); }
 
-// Every block's writes before the barrier are visible to every block after it. False: the calibration has failed (a
-// barrier gave up), and the caller returns.
-__device__ bool grid_barrier(const LevDev& d) {
+__device__ __forceinline__ void red_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Every block's writes before the barrier are visible to every block after it. The barrier is one arrival counter
+// that only grows: a block adds one (a release) and waits until the count reaches every block's arrivals so far
+// (`arrived`, advanced by gridDim.x at each barrier, the same in every thread). A block polls at most d.wait_limit
+// times (with a limit of zero it gives up at once), then records OB_ETIMEOUT; a block that sees the status leaves.
+// False: the calibration has failed and the caller returns.
+__device__ bool grid_barrier(const LevDev& d, unsigned& arrived) {
     __shared__ int s_ok;
+    arrived += gridDim.x;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned gen = ld_acquire_gpu(d.bar_gen);
         __threadfence();
-        if (atomicAdd(d.bar_count, 1u) == gridDim.x - 1) {
-            atomicExch(d.bar_count, 0u);
-            __threadfence();
-            st_release_gpu(d.bar_gen, gen + 1);
-        } else {
-            // at most wait_limit polls: with a limit of zero a block that has to wait gives up at once
-            for (long long polls = 0;; ++polls) {
-                if (polls >= d.wait_limit) {
-                    atomicCAS(d.status, 0, OB_ETIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                if (ld_acquire_gpu(d.bar_gen) != gen) break;
-                if (status_of(d) != 0) {
-                    ok = 0;
-                    break;
-                }
-                if (polls > 64) __nanosleep(64);
+        red_release_gpu(d.bar_count, 1u);
+        for (long long polls = 0;; ++polls) {
+            if (polls >= d.wait_limit) {
+                atomicCAS(d.status, 0, OB_ETIMEOUT);
+                ok = 0;
+                break;
             }
+            if (ld_acquire_gpu(d.bar_count) >= arrived) break;
+            if (status_of(d) != 0) {
+                ok = 0;
+                break;
+            }
+            if (polls > 256) __nanosleep(32);
         }
         __threadfence();
         if (status_of(d) != 0) ok = 0;
@@ -564,30 +583,35 @@ __device__ bool grid_barrier(const LevDev& d) {
 
 constexpr int kPersistentThreads = 512;
 
+// Block b owns pairs [b chunk, (b + 1) chunk) and keeps their particles in its shared memory (after the binning
+// arrays, at part_off) for the whole calibration: the binning and the step read them there, not through L2.
 template <typename R>
 __global__ void __launch_bounds__(kPersistentThreads, 1)
-    lev_persistent(LevDev d, R* __restrict__ x, R* __restrict__ v, double n_particles) {
+    lev_persistent(LevDev d, long long chunk, int part_off, double n_particles) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ RegressShared rs;
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[32], s_max[32];
     __shared__ double s_mn[32], s_mx[32];
     const BinShared b = bin_shared(d, sm);
-    const long long n = 2 * d.n_pairs;
-    for (long long j = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
-         j += static_cast<long long>(gridDim.x) * blockDim.x)
-        x[j] = R(0), v[j] = static_cast<R>(d.v0);
-    // (step 0's regression reads no particle; the barrier after it orders these stores before the first step)
+    const long long first = static_cast<long long>(blockIdx.x) * chunk;
+    const long long count = first < d.n_pairs ? (d.n_pairs - first < chunk ? d.n_pairs - first : chunk) : 0;
+    R* sx = reinterpret_cast<R*>(sm + part_off);
+    R* sv = sx + 2 * chunk;
+    const Particles<R> pt{sx, sv, count, first, threadIdx.x, blockDim.x};
+    for (long long j = threadIdx.x; j < 2 * count; j += blockDim.x) sx[j] = R(0), sv[j] = static_cast<R>(d.v0);
+    unsigned arrived = 0;
+    // (step 0's regression reads no particle; its barrier orders these stores before the first step)
     for (int i = 0; i < d.n_steps; ++i) {
         if (i > 0) {
             bin_clear_shared(d, b);
-            bin_phase<R>(d, x, v, b, s_mn, s_mx);
-            if (!grid_barrier(d)) return;
+            bin_phase<R, true>(d, pt, b, s_mn, s_mx);
+            if (!grid_barrier(d, arrived)) return;
         }
         for (int g = blockIdx.x; g < d.n_x; g += gridDim.x) regress_phase(d, n_particles, g, i, rs);
-        if (!grid_barrier(d)) return;
-        step_phase<R>(d, x, v, i, s_lev, s_min, s_max);
-        if (i + 1 < d.n_steps && !grid_barrier(d)) return;
+        if (!grid_barrier(d, arrived)) return;
+        step_phase<R, true>(d, pt, i, s_lev, s_min, s_max);
+        if (i + 1 < d.n_steps && !grid_barrier(d, arrived)) return;
     }
 }
 
@@ -596,22 +620,32 @@ __global__ void __launch_bounds__(kPersistentThreads, 1)
 constexpr long long kDefaultWaitLimit = 1LL << 22;
 long long g_wait_limit = kDefaultWaitLimit;
 
-// The persistent calibration on stream st; false (nothing launched) when the device cannot hold every block at once.
+// Dynamic shared memory of a persistent block at most: the binning arrays and the block's particles.
+constexpr size_t kPersistentSmemMax = size_t(200) << 10;
+
+// The persistent calibration on stream st; false (nothing launched) when a block's particles do not fit its shared
+// memory or the device cannot hold every block at once.
 template <typename R>
-bool run_persistent(LevDev& d, R* x, R* v, double n_particles, size_t bin_smem, int sms, cudaStream_t st) {
+bool run_persistent(LevDev& d, double n_particles, size_t bin_smem, int sms, cudaStream_t st) {
+    const long long chunk = (d.n_pairs + sms - 1) / sms;
+    const size_t part_off = (bin_smem + 15) & ~static_cast<size_t>(15);
+    const size_t smem = part_off + 4 * static_cast<size_t>(chunk) * sizeof(R);
+    if (smem > kPersistentSmemMax) return false;
     check_cuda(cudaFuncSetAttribute(lev_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(bin_smem)),
+                                    static_cast<int>(smem)),
                "cudaFuncSetAttribute");
     int occ = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, lev_persistent<R>, kPersistentThreads, bin_smem),
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, lev_persistent<R>, kPersistentThreads, smem),
                "occupancy");
     int coop = 0, dev = 0;
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     check_cuda(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cudaDeviceGetAttribute");
     if (occ < 1 || !coop || d.n_step_blocks != sms) return false;
-    void* args[] = {&d, &x, &v, &n_particles};
+    int off = static_cast<int>(part_off);
+    long long ch = chunk;
+    void* args[] = {&d, &ch, &off, &n_particles};
     const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(lev_persistent<R>), dim3(sms),
-                                                      dim3(kPersistentThreads), args, bin_smem, st);
+                                                      dim3(kPersistentThreads), args, smem, st);
     if (e == cudaErrorCooperativeLaunchTooLarge) {
         cudaGetLastError();
         return false;
@@ -683,7 +717,6 @@ void run_leverage(ob_leverage_request& rq) {
     d.part_range = arena.alloc<double>(2 * static_cast<size_t>(4 * sms));
     d.n_steps = S;
     d.bar_count = arena.alloc<unsigned>(4);
-    d.bar_gen = d.bar_count + 1;
     d.status = reinterpret_cast<int*>(d.bar_count + 2);
     check_cuda(cudaMemset(d.bar_count, 0, 4 * sizeof(unsigned)), "cudaMemset");
     d.wait_limit = g_wait_limit;
@@ -707,7 +740,7 @@ void run_leverage(ob_leverage_request& rq) {
     // OPTLAB_B200_LEVERAGE=graphs runs the three-kernel schedule below instead (to compare the two; same results)
     const char* mode = std::getenv("OPTLAB_B200_LEVERAGE");
     const bool graphs_only = mode && std::strcmp(mode, "graphs") == 0;
-    if (!graphs_only && run_persistent<R>(d, x, v, n_particles, bin_smem, sms, st)) {
+    if (!graphs_only && run_persistent<R>(d, n_particles, bin_smem, sms, st)) {
         int status = 0;
         check_cuda(cudaMemcpyAsync(&status, d.status, sizeof status, cudaMemcpyDeviceToHost, st), "copy status");
         check_cuda(cudaMemcpyAsync(rq.x_grids, d.x_grids, static_cast<size_t>(S) * rq.n_x * sizeof(double),

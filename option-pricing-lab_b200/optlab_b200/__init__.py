@@ -323,17 +323,17 @@ def plan(model, market, times, dt_max=1 / 252, dt_min=1 / 2000, n_x: int = N_X) 
     grid = time_grid(times, dt_max, dt_min)
     dt, t0 = np.diff(grid), grid[:-1].copy()
     specs = [_spec(m, t0, n_x) for m in models]
-    tabled = [sp for sp in specs if sp.block is not None]
+    tabled = [a for a, sp in enumerate(specs) if sp.block is not None]
     step_row = lo = inv = table = None
     if tabled:
         # stack the blocks; each name's step rows move by the rows of the blocks before it
-        offsets = np.cumsum([0] + [len(sp.block[0]) for sp in tabled])
+        offsets = np.cumsum([0] + [len(specs[a].block[0]) for a in tabled])
         step_row = np.zeros((len(specs), len(dt)), np.int32)
-        for off, sp in zip(offsets, tabled):
-            step_row[specs.index(sp)] = sp.step_rows + off
-        lo = np.concatenate([sp.block[0] for sp in tabled])
-        inv = np.concatenate([sp.block[1] for sp in tabled])
-        table = np.ascontiguousarray(np.concatenate([sp.block[2] for sp in tabled]))
+        for off, a in zip(offsets, tabled):
+            step_row[a] = specs[a].step_rows + off
+        lo = np.concatenate([specs[a].block[0] for a in tabled])
+        inv = np.concatenate([specs[a].block[1] for a in tabled])
+        table = np.ascontiguousarray(np.concatenate([specs[a].block[2] for a in tabled]))
     fwd = np.zeros((len(specs), 0))
     if len(times):
         fwd = np.stack([np.asarray(mk.F(times), dtype=float) for mk in markets])

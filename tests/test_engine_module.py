@@ -169,3 +169,26 @@ def test_the_monotone_cubic_is_the_pchip_the_reference_fits_with():
         scale = np.abs(y).max() + 1.0
         assert np.max(np.abs(v - ref(t))) <= 1e-13 * scale
         assert np.max(np.abs(s - ref.derivative()(t))) <= 1e-12 * scale / np.diff(x).min()
+
+
+def test_a_basket_of_several_tabled_names_plans_like_the_reference(ref):
+    """Two local-vol names and an SLV name: their tables stack in the names' order, each name's step rows offset by
+    the rows before it, as the reference's plan stacks them."""
+    rm, ma, Hp, Market = ref["models"], ref["ma"], ref["Hp"], ref["Market"]
+    T = 3.0 * np.arange(1, 41) / 40
+    s1r, s2r = ref["ssvi"].SSVI.power_law(-0.6, 1.0, 0.5, T, 0.04 * T), ref["ssvi"].SSVI.power_law(-0.4, 1.0, 0.5, T, 0.05 * T)
+    s1m, s2m = SSVI.power_law(-0.6, 1.0, 0.5, T, 0.04 * T), SSVI.power_law(-0.4, 1.0, 0.5, T, 0.05 * T)
+    t = np.linspace(0, 1, 11)
+    lev_vals = np.array([1.0 + 0.1 * np.sin(np.linspace(0, 3, 21) + s) for s in range(11)])
+    lev_x = np.tile(np.linspace(-1, 1, 21), (11, 1))
+    hp = (0.04, 1.5, 0.04, 0.5, -0.7)
+    names = ("A", "B", "C")
+    corr = np.array([[1.0, 0.5, 0.4], [0.5, 1.0, 0.3], [0.4, 0.3, 1.0]])
+    mk_r, mk_m = Market.flat(100.0, 0.02, 0.01), M.Market.flat(100.0, 0.02, 0.01)
+    theirs = ma.Basket(names, {"A": rm.LocalVolModel(s1r), "B": rm.SLVModel(Hp(*hp), rm.Leverage(t, lev_x, lev_vals), 0.5),
+                               "C": rm.LocalVolModel(s2r)}, {n: mk_r for n in names}, corr)
+    mine = M.Basket(names, {"A": M.LocalVolModel(s1m),
+                            "B": M.SLVModel(M.HestonParams(*hp), M.Leverage(t, lev_x, lev_vals), 0.5),
+                            "C": M.LocalVolModel(s2m)}, {n: mk_m for n in names}, corr)
+    times = [0.25, 0.5, 1.0]
+    _same_plan(eng.plan(mine, None, times), ref["native"].plan(theirs, None, times))

@@ -149,9 +149,9 @@ def test_the_persistent_calibration_equals_the_three_kernel_schedule(monkeypatch
 
 
 def test_a_grid_barrier_that_gives_up_returns_a_timeout_and_the_device_stays_usable():
-    """With a wait limit of zero polls every block but the last to arrive at the first grid barrier gives up at once
-    (a flag nobody has set yet, as far as each of them may wait); the call returns OB_ETIMEOUT, every block leaves the
-    kernel at its next barrier, and the next calibration, with the default limit, runs as before."""
+    """With a wait limit of zero polls every block gives up at its first wait on a grid barrier (a count that, as far
+    as it may wait, nobody completes); the call returns OB_ETIMEOUT, every block leaves the kernel, and the next
+    calibration, with the default limit, runs as before."""
     lib = _abi.load()
     h = leverage_request(**_lev_kw(n_pairs=2**12, n_steps=8))
     prev = lib.ob_set_wait_limit(0)

@@ -31,7 +31,7 @@ def _request(n, product, n_pairs=2**12, seed=29, n_steps=126, years=0.5, mixer=L
         mixer=1, mix=mix, low_root=low,
     )
     if product == "autocall":
-        ph = workloads.Phoenix(years=years, obs_per_year=8)
+        ph = workloads.Phoenix(years=years, obs_per_year=4)
         kw.update(workloads.autocall_fields(ph, m, int(round(n_steps / years))))
     else:
         kw.update(product=0, leg_type=[1, 2, 1], leg_strike=[100.0, 95.0, 105.0], leg_barrier=[0, 4, 1],
@@ -81,7 +81,7 @@ def test_a_worst_of_phoenix_script_on_a_local_correlation_basket_equals_the_fuse
     kernel on the same basket and the same normals (FP64, to rounding)."""
     n, years = 3, 0.5
     kw = _request(n, "autocall", n_pairs=2**13, years=years)
-    ph = workloads.Phoenix(years=years, obs_per_year=8)
+    ph = workloads.Phoenix(years=years, obs_per_year=4)
     held = mc_request(**kw)
     worst = "X0 / S0"
     for a in range(1, n):
