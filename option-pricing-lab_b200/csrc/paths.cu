@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(256) paths_kernel(PathsDev<R> s) {
 // Offsets of the staged blob of paths_staged_kernel (bytes).
 struct PathsLvOffsets {
     int step, name_step, root, hes, table2, sched, col, fwd;
+    int mix_den, low_root;  // local correlation: per step sigma sqrt(max(t0, 1/12)); the aligned low root
 };
 
 template <typename R>
@@ -111,6 +112,8 @@ struct PathsLvArgs {
     const Pair2<R>* tab;  // the table in global memory when it does not fit the stage (table_global), else unused
     int table_global;
     int kind, same;  // the names' model kind (0 Black-Scholes, 1 local vol, 2 Heston, 3 SLV); residuals through the root
+    int mixer;       // local correlation (kernels with MIX): w0 + level, down, up, sign, cos, sin of the mixer
+    R mix_base, mix_down, mix_up, mix_sign, mix_cos, mix_sin;
 };
 
 // Observation j of both legs: the kept column and the windows that hold it, on S = F_j exp(x) as the reference.
@@ -155,13 +158,15 @@ constexpr int lv_block() {
 }
 
 // KIND: 0 Black-Scholes (constant variance), 1 local vol (table), 2 Heston (Euler), 3 SLV (table x Heston, residuals
-// on the aux stream). GT: the table is read from global memory (a.tab) instead of the stage.
-template <typename R, int N, int KIND, bool GT>
+// on the aux stream). GT: the table is read from global memory (a.tab) instead of the stage. MIX (Black-Scholes or
+// local vol, 2 to 5 names): the local-correlation mixer, one more normal a step after the names'.
+template <typename R, int N, int KIND, bool GT, bool MIX = false>
 __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 1)
     paths_staged_kernel(PathsLvArgs<R> a) {
     constexpr bool VAR = KIND == 2 || KIND == 3;
     constexpr bool TABLE = KIND == 1 || KIND == 3;
-    constexpr int C = KIND == 2 ? 2 * N : N;  // normals per step, stream 0
+    static_assert(!MIX || (KIND <= 1 && N >= 2), "the staged mixer runs Black-Scholes and local-vol baskets");
+    constexpr int C = KIND == 2 ? 2 * N : N + (MIX ? 1 : 0);  // normals per step, stream 0
     constexpr int CA = KIND == 3 ? N : 0;     // normals per step, aux stream
     constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);  // steps per batch of whole Philox blocks
     constexpr int NB = C * G / 4, NBA = CA * G / 4;
@@ -214,6 +219,38 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
                 const int i = i0 + g;
                 if (G > 1 && i > S) break;
                 const StepRec<R> st = s_step[i - 1];
+                R zm0[MIX ? N : 1], zm1[MIX ? N : 1];  // with the mixer each leg's own normals (signs in)
+                if (MIX) {
+                    // paths.hpp:219-237: a common factor whose weight moves with the level of the basket (the log of
+                    // the mean of S / F at the step's start), per leg
+                    const R* zs = &z[g * C];
+                    const R* s_low = reinterpret_cast<const R*>(sm + a.off.low_root);
+                    const R den = reinterpret_cast<const R*>(sm + a.off.mix_den)[i - 1];
+#pragma unroll
+                    for (int leg = 0; leg < 2; ++leg) {
+                        const R sg = leg ? R(-1) : R(1);
+                        R mm = R(0);
+#pragma unroll
+                        for (int n = 0; n < N; ++n) mm += m_exp(leg ? x1[n] : x0[n]);
+                        const R u = m_log(mm / static_cast<R>(N)) / den;
+                        R wt = a.mix_base + a.mix_down * m_max(-u, R(0)) - a.mix_up * m_max(u, R(0));
+                        wt = m_min(m_max(wt, R(0)), R(1));
+                        const R market = a.mix_sign * sg * zs[N - 1], fr = sg * zs[N];
+                        const R common = a.mix_cos * market + a.mix_sin * fr;
+                        R other[N];
+#pragma unroll
+                        for (int n = 0; n < N - 1; ++n) other[n] = sg * zs[n];
+                        other[N - 1] = a.mix_sin * market - a.mix_cos * fr;
+                        const R sw = m_sqrt(wt), sl = m_sqrt(R(1) - wt);
+#pragma unroll
+                        for (int n = 0; n < N; ++n) {
+                            R acc = R(0);
+#pragma unroll
+                            for (int b = 0; b < N; ++b) acc += s_low[n * N + b] * other[b];
+                            (leg ? zm1 : zm0)[n] = sw * common + sl * acc;
+                        }
+                    }
+                }
                 R wc[N];  // the variance's residual normals (correlated through the root when `same`)
                 if (VAR) {
                     const R* zr = KIND == 3 ? &za[g * CA] : &z[g * C + N];
@@ -228,8 +265,10 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     R zc = R(0);
+                    if (!MIX) {
 #pragma unroll
-                    for (int m = 0; m < N; ++m) zc += s_root[n * N + m] * z[g * C + m];
+                        for (int m = 0; m < N; ++m) zc += s_root[n * N + m] * z[g * C + m];
+                    }
                     const NameStep<R> ns = s_ns[(i - 1) * N + n];
                     R var0, var1, vp0 = R(0), vp1 = R(0);
                     if (VAR) vp0 = m_max(v0[n], R(0)), vp1 = m_max(v1[n], R(0));
@@ -253,9 +292,14 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
                         v0[n] += h[1] * (h[2] - vp0) * st.dt + h[3] * (m_sqrt(vp0) * st.sdt) * zv;
                         v1[n] += h[1] * (h[2] - vp1) * st.dt + h[3] * (m_sqrt(vp1) * st.sdt) * (-zv);
                     }
-                    const R zd = st.sdt * zc;  // sqrt(dt) z, the legs' +-
-                    x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
-                    x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
+                    if (MIX) {
+                        x0[n] += m_fma(m_sqrt(var0), st.sdt * zm0[n], var0 * st.hdt);
+                        x1[n] += m_fma(m_sqrt(var1), st.sdt * zm1[n], var1 * st.hdt);
+                    } else {
+                        const R zd = st.sdt * zc;  // sqrt(dt) z, the legs' +-
+                        x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
+                        x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
+                    }
                 }
                 const int2 ob = s_sched[i];
                 for (int j = ob.x; j < ob.y; ++j) lv_record<R, N>(a, s_col, s_fwd, j, p, active, x0, x1, lo, hi);
@@ -312,7 +356,8 @@ void check_request(const ob_paths_request& c) {
 template <typename R>
 bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArgs<R>& a) {
     const int n = h.n_names, S = h.n_steps, kind = h.kind[0];
-    if (h.mixer || S < 1 || kind < 0 || kind > 3 || n > (kind <= 1 ? 5 : 3)) return false;
+    if (S < 1 || kind < 0 || kind > 3 || n > (kind <= 1 ? 5 : 3)) return false;
+    if (h.mixer && (kind > 1 || n < 2)) return false;  // the mixer beside Heston or SLV names: the generic kernel
     for (int k = 0; k < n; ++k)
         if (h.kind[k] != kind) return false;
     const bool table = kind == 1 || kind == 3;
@@ -352,6 +397,18 @@ bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArg
         hes[8 * k + 6] = static_cast<R>(h.cvar[k]);
     }
     a.off.hes = put(hes.data(), hes.size() * sizeof(R));
+    a.mixer = h.mixer;
+    if (h.mixer) {
+        std::vector<R> den(S), low(static_cast<size_t>(n) * n);
+        for (int i = 0; i < S; ++i)  // R arithmetic as the generic step: sigma sqrt(max(t0, 1/12))
+            den[i] = static_cast<R>(h.mix[4]) * std::sqrt(std::max(static_cast<R>(h.t0[i]), R(1.0 / 12)));
+        for (size_t k = 0; k < low.size(); ++k) low[k] = static_cast<R>(h.low_root[k]);
+        a.off.mix_den = put(den.data(), den.size() * sizeof(R));
+        a.off.low_root = put(low.data(), low.size() * sizeof(R));
+        a.mix_base = static_cast<R>(h.mix[0]) + static_cast<R>(h.mix[1]);
+        a.mix_down = static_cast<R>(h.mix[2]), a.mix_up = static_cast<R>(h.mix[3]);
+        a.mix_sign = static_cast<R>(h.mix[5]), a.mix_cos = static_cast<R>(h.mix[6]), a.mix_sin = static_cast<R>(h.mix[7]);
+    }
     std::vector<int2> sched(S + 1);
     for (int i = 0, j = 0; i <= S; ++i) {
         sched[i].x = j;
@@ -403,8 +460,24 @@ const void* pick_paths_n(int n) {
     return nullptr;
 }
 
+template <typename R, int KIND, bool GT>
+const void* pick_paths_mix(int n) {
+    switch (n) {
+        case 2: return reinterpret_cast<const void*>(paths_staged_kernel<R, 2, KIND, GT, true>);
+        case 3: return reinterpret_cast<const void*>(paths_staged_kernel<R, 3, KIND, GT, true>);
+        case 4: return reinterpret_cast<const void*>(paths_staged_kernel<R, 4, KIND, GT, true>);
+        case 5: return reinterpret_cast<const void*>(paths_staged_kernel<R, 5, KIND, GT, true>);
+        default: return nullptr;
+    }
+}
+
 template <typename R>
-const void* pick_paths_staged(int n, int kind, bool table_global) {
+const void* pick_paths_staged(int n, int kind, bool table_global, bool mixer) {
+    if (mixer) {
+        if (kind == 0) return pick_paths_mix<R, 0, false>(n);
+        if (kind == 1) return table_global ? pick_paths_mix<R, 1, true>(n) : pick_paths_mix<R, 1, false>(n);
+        return nullptr;
+    }
     switch (kind) {
         case 0: return pick_paths_n<R, 0, false>(n);
         case 1: return table_global ? pick_paths_n<R, 1, true>(n) : pick_paths_n<R, 1, false>(n);
@@ -453,8 +526,9 @@ void run_paths(ob_paths_request& h) {
     s.win_hi = arena.put<int>(h.win_hi, h.n_windows);
     s.fwd = arena.put<R>(h.fwd, static_cast<size_t>(n) * h.n_obs);
     PathsLvArgs<R> lv{};
-    const void* lv_fn = pack_paths_staged<R>(h, arena, lv) ? pick_paths_staged<R>(n, lv.kind, lv.table_global != 0)
-                                                          : nullptr;
+    const void* lv_fn = pack_paths_staged<R>(h, arena, lv)
+                            ? pick_paths_staged<R>(n, lv.kind, lv.table_global != 0, h.mixer != 0)
+                            : nullptr;
     const bool fast = lv_fn != nullptr;
     int lv_grid = 0;
     if (fast) {

@@ -76,6 +76,8 @@ CASES = {
     "slv,slv,lv": dict(kinds=[3, 3, 1]),
     "five lv": dict(kinds=[1, 1, 1, 1, 1]),
     "local correlation": dict(kinds=[1, 1, 1], mixer=1),
+    "black-scholes basket, local correlation": dict(kinds=[0, 0, 0, 0], mixer=1),
+    "five lv, local correlation": dict(kinds=[1, 1, 1, 1, 1], mixer=1),
     "independent residuals": dict(kinds=[3, 2, 1, 0], same=0),
     "eight names, local correlation": dict(kinds=[1, 1, 3, 1, 0, 1, 3, 1], mixer=1),
     "eight names, independent residuals": dict(kinds=[3, 2, 1, 0, 3, 2, 1, 1], same=0),
