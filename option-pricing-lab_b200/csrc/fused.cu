@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "mc.cuh"
@@ -147,7 +148,10 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
         Leg<R> l0, l1;
         leg_init<R, PRODUCT>(l0), leg_init<R, PRODUCT>(l1);
         R lp0 = R(0), lp1 = R(0);
-        for (int i0 = 1, batch = 0; i0 <= S; i0 += G, ++batch) {
+        // One batch of G steps from step i0, its normals drawn first. For one local-vol name the full batches run
+        // without testing for the last step and only the tail batch (CHECK) may stop inside.
+        auto run_batch = [&](int i0, int batch, auto check) {
+            constexpr bool CHECK = decltype(check)::value;
             R z[C * G];
             R za[CA > 0 ? CA * G : 1];
 #pragma unroll
@@ -161,7 +165,9 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int i = i0 + g;
-                if (G > 1 && i > S) break;
+                if constexpr (CHECK && G > 1) {
+                    if (i > S) break;
+                }
                 if (QE) {
                     const R zv = z[2 * g], zx = z[2 * g + 1];
                     qe_step(a.qe, x0[0], v0[0], zv, zx);
@@ -275,6 +281,14 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
                     }
                 }
             }
+        };
+        if constexpr (N == 1 && KIND == 1) {  // (a second copy of the loop costs the wider kernels registers)
+            const int n_full = S / G;
+            int i0 = 1, batch = 0;
+            for (; batch < n_full; i0 += G, ++batch) run_batch(i0, batch, std::false_type{});
+            if (i0 <= S) run_batch(i0, batch, std::true_type{});
+        } else {
+            for (int i0 = 1, batch = 0; i0 <= S; i0 += G, ++batch) run_batch(i0, batch, std::true_type{});
         }
         const int* leg_type = reinterpret_cast<const int*>(sm + a.off.leg_type);
         const R* leg_strike = reinterpret_cast<const R*>(sm + a.off.leg_strike);

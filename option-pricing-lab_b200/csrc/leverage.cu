@@ -50,11 +50,24 @@ struct GraphExecs {
 constexpr int kMaxBins = 512;
 constexpr int kMaxFine = 16384;
 constexpr int kMaxX = 1024;
+// The fine histogram's arrays (global and shared) are padded with zero bins to a multiple of 8 x 512, so that a block
+// of 256 or 512 threads splits them, packed or not, into equal runs of whole 16-byte words.
+constexpr int kFinePad = 4096;
+// The persistent kernel packs the fine histogram two bins to a 32-bit word (16-bit counts, the even bin in the low
+// half): a block's own counts fit (it bins fewer than 2^16 particles), and a step whose global count of one bin passes
+// 2^16 - 1 shows as a total other than the number of particles (a carry moves 2^16 - 1, a lost one 2^16): the kernel
+// then records kPackOverflow and the calibration is run again unpacked.
+constexpr int kPackOverflow = -2;
+// Local-variance rows of up to this many points are staged in the regression block's shared memory.
+constexpr int kMaxRowSmem = 4096;
 
 struct LevDev {
     long long n_pairs;
     int n_steps;
     int n_x, n_bins, n_fine, n_lv, local_linear, positive_part;
+    int nfp;                   // n_fine padded to a multiple of kFinePad
+    int nbq;                   // n_bins + 1 padded to a multiple of 4: the length of cnt and sv
+    int packed;                // the fine histogram two bins to a word (persistent kernel)
     uint32_t k0, k1;
     double v0, kappa, theta, xi, rho, atm_vol, bw_scale, l_min, l_max, q_lo, q_hi;
     const double* dt;
@@ -63,14 +76,14 @@ struct LevDev {
     const double* lv_inv_dx;
     const double* lv_rows;
     const double* bw;          // n_steps: the kernel bandwidth of each step, computed on the host
-    // the step's histogram and bins, added into by every binning block, cleared by the step kernel after use
-    unsigned* fine;            // n_fine
-    unsigned* chunk;           // (n_fine + 31) / 32: totals of 32-bin chunks of fine
-    unsigned* cnt;             // n_bins
-    unsigned long long* sv;    // n_bins + 1: v sums in fixed point, then the sum of all v
+    // the step's histogram and bins, added into by every binning block, cleared by the step phase after use
+    unsigned* fine;            // nfp words, nfp / 2 of them when packed (bins from n_fine on stay zero)
+    unsigned* cnt;             // nbq: bin counts
+    unsigned long long* sv;    // nbq: v sums in fixed point, then (at n_bins) the sum of all v
     double* acc_ll;            // 3 n_bins: x, x^2, x v sums (local linear only)
-    int n_step_blocks;         // blocks of lev_step, each with its min and max of the new x
+    int n_step_blocks;         // blocks of lev_step, each with its min and max of the new x (three-kernel schedule)
     double* part_range;        // n_step_blocks x 2
+    long long* rng;            // 2 x 2: min and max of the new x as order keys, by step parity (persistent kernel)
     double* x_eval;            // n_x, the current grid
     double* lev;               // n_x, the current leverage row
     double* x_grids;           // n_steps x n_x
@@ -92,7 +105,50 @@ __device__ __forceinline__ long long warp_sum_i64(long long v) {
     return v;
 }
 
-// Min and max of x over the last step's blocks, in every thread of the calling block (any multiple of 32 threads).
+// A 64-bit integer added into a pair of 32-bit words of shared memory (low, high) with two native 32-bit atomics:
+// the carry out of the low word goes into the high one, so the pair holds the exact sum modulo 2^64.
+__device__ __forceinline__ void add_u64_pair(unsigned* lo, unsigned* hi, unsigned long long q) {
+    const unsigned l = static_cast<unsigned>(q), h = static_cast<unsigned>(q >> 32);
+    const unsigned old = atomicAdd(lo, l);
+    const unsigned up = h + (old + l < old ? 1u : 0u);
+    if (up) atomicAdd(hi, up);
+}
+
+// Bulk reductions of shared memory into global memory by the TMA unit (cp.reduce.async.bulk, no multicast): one
+// thread hands over a whole array and the unit adds it element by element at L2. Both addresses must be 16-byte
+// aligned and the size a multiple of 16 bytes (bulk_aligned); the writes of the shared source must be fenced for the
+// async proxy before (fence_proxy_async_shared, by the threads that wrote it, then a barrier), and the issuing thread
+// waits for completion (bulk_wait_all) before its release of the results.
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+__device__ __forceinline__ bool bulk_aligned(const void* dst, const void* src, unsigned bytes) {
+    return ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src) | bytes) & 15u) == 0;
+}
+__device__ __forceinline__ void bulk_add_u32(unsigned* dst, const unsigned* src, unsigned bytes) {
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.u32 [%0], [%1], %2;" ::"l"(dst),
+                 "r"(static_cast<unsigned>(__cvta_generic_to_shared(src))), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_add_u64(unsigned long long* dst, const unsigned long long* src, unsigned bytes) {
+    asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.u64 [%0], [%1], %2;" ::"l"(dst),
+                 "r"(static_cast<unsigned>(__cvta_generic_to_shared(src))), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Doubles as signed 64-bit keys in the same order (negative values with their magnitude bits flipped), for
+// atomicMin / atomicMax: the min and max of the particles are exact whatever the order of the blocks.
+__device__ __forceinline__ long long order_key(double x) {
+    const long long b = __double_as_longlong(x);
+    return b >= 0 ? b : b ^ 0x7fffffffffffffffLL;
+}
+
+__device__ __forceinline__ double from_order_key(long long k) {
+    return __longlong_as_double(k >= 0 ? k : k ^ 0x7fffffffffffffffLL);
+}
+
+// Min and max of x over the last step's blocks (three-kernel schedule), in every thread of the calling block.
 __device__ void range_of(const LevDev& d, double& lo, double& hi, double* s_mn, double* s_mx) {
     double mn = 1.0e300, mx = -1.0e300;
     const double2* pr = reinterpret_cast<const double2*>(d.part_range);
@@ -135,35 +191,42 @@ __device__ __forceinline__ int current_step(const LevDev& d) { return __ldcg(d.s
 
 // Bin edges and indices as the reference computes them: in double on the CPU, in float on its GPU. A block bins its
 // particles in shared memory, then adds its non-zero entries into the step's global histogram and bins.
-// The binning block's shared memory: v sums (nb + 1, fixed point), local-linear moments (3 nb), fine histogram (nf)
-// and bin counts (nb).
+// The binning block's shared memory, every array at a multiple of 16 bytes: the fine histogram (nfp), the bin counts
+// (nbq), the v sums as 64-bit words for the bulk reduction (nbq), the v sums while binning (nbq low and nbq high
+// 32-bit words, fixed point; at n_bins the sum of all v) and the local-linear moments (3 nb).
 struct BinShared {
-    unsigned long long* sv;
-    double* ll;
     unsigned* fine;
     unsigned* cnt;
+    unsigned long long* sv;
+    unsigned* sv_lo;
+    unsigned* sv_hi;
+    double* ll;
 };
+
+__host__ __device__ __forceinline__ size_t bin_smem_bytes(int nfp, int nbq, int nb, int ll) {
+    return static_cast<size_t>(nfp) * sizeof(unsigned) + static_cast<size_t>(nbq) * (3 * sizeof(unsigned) + 8) +
+           (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0);
+}
 
 __device__ __forceinline__ BinShared bin_shared(const LevDev& d, unsigned char* sm) {
     BinShared b;
-    b.sv = reinterpret_cast<unsigned long long*>(sm);
-    b.ll = reinterpret_cast<double*>(b.sv + d.n_bins + 1);
-    b.fine = reinterpret_cast<unsigned*>(b.ll + (d.local_linear ? 3 * d.n_bins : 0));
-    b.cnt = b.fine + d.n_fine;
+    b.fine = reinterpret_cast<unsigned*>(sm);
+    b.cnt = b.fine + d.nfp;
+    b.sv = reinterpret_cast<unsigned long long*>(b.cnt + d.nbq);
+    b.sv_lo = reinterpret_cast<unsigned*>(b.sv + d.nbq);
+    b.sv_hi = b.sv_lo + d.nbq;
+    b.ll = reinterpret_cast<double*>(b.sv_hi + d.nbq);
     return b;
 }
 
 __device__ __forceinline__ void bin_clear_shared(const LevDev& d, const BinShared& b) {
-    const int nb = d.n_bins, nf = d.n_fine;
-    for (int k = threadIdx.x; k < nb + 1; k += blockDim.x) b.sv[k] = 0ull;
+    uint4* f4 = reinterpret_cast<uint4*>(b.fine);
+    const int n4 = (d.nfp + 5 * d.nbq) / 4;  // fine, cnt, sv (two words each), sv_lo, sv_hi: contiguous
+    for (int k = threadIdx.x; k < n4; k += blockDim.x) f4[k] = make_uint4(0u, 0u, 0u, 0u);
     if (d.local_linear)
-        for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x) b.ll[k] = 0.0;
-    for (int k = threadIdx.x; k < nf + nb; k += blockDim.x) b.fine[k] = 0u;
+        for (int k = threadIdx.x; k < 3 * d.n_bins; k += blockDim.x) b.ll[k] = 0.0;
 }
 
-// One block's share of a step's binning (the block's shared memory cleared by bin_clear_shared before): its particles
-// into the shared histogram and bins, then the non-zero entries added into the step's global ones. Particles and the
-// last step's ranges are read through L2: in the persistent kernel other blocks wrote them in the same launch.
 // Particles a phase works on: arrays x, v of 2 n particles (leg 0 of pair c at c, leg 1 at n + c) whose pair c is
 // global pair first + c, this thread taking pairs (or particles) start, start + stride, ... In global memory (SH false:
 // every pair, the grid striding over them, read through L2) or in the block's shared memory (SH true: the block's own
@@ -181,17 +244,14 @@ __device__ __forceinline__ R ld_part(const R* p) {
     else return __ldcg(p);
 }
 
+// One block's share of a step's binning on the range [lo, hi] of the particles (the block's shared memory cleared by
+// bin_clear_shared before, and a barrier since): its particles into the shared histogram and bins, then these added
+// into the step's global histogram and bins.
 template <typename R, bool SH = false>
-__device__ void bin_phase(const LevDev& d, const Particles<R>& pt, const BinShared& b, double* s_mn, double* s_mx) {
+__device__ void bin_phase(const LevDev& d, const Particles<R>& pt, const BinShared& b, double lo_d, double hi_d) {
     const R* __restrict__ x = pt.x;
     const R* __restrict__ v = pt.v;
     const int nb = d.n_bins, nf = d.n_fine, ll = d.local_linear;
-    unsigned long long* s_sv = b.sv;
-    double* s_ll = b.ll;
-    unsigned* s_fine = b.fine;
-    unsigned* s_cnt = b.cnt;
-    double lo_d, hi_d;
-    range_of(d, lo_d, hi_d, s_mn, s_mx);  // (its barrier also orders the clearing before)
     const R lo = static_cast<R>(lo_d), hi = static_cast<R>(hi_d);
     const R wf = (hi - lo) / static_cast<R>(nf), we = (hi + static_cast<R>(1e-12) - lo) / static_cast<R>(nb);
     const long long n = 2 * pt.n;
@@ -209,43 +269,56 @@ __device__ void bin_phase(const LevDev& d, const Particles<R>& pt, const BinShar
         for (int u = 0; u < 4; ++u) {
             if (j0 + u * stride >= n) break;
             const R xj = xr[u], vj = d.positive_part ? m_max(vr[u], R(0)) : vr[u];
-            const int f = wf > R(0) ? static_cast<int>((xj - lo) / wf) : 0;
-            atomicAdd(&s_fine[min(max(f, 0), nf - 1)], 1u);
+            const int f = min(max(wf > R(0) ? static_cast<int>((xj - lo) / wf) : 0, 0), nf - 1);
+            if (d.packed) atomicAdd(&b.fine[f >> 1], (f & 1) ? 0x10000u : 1u);
+            else atomicAdd(&b.fine[f], 1u);
             const int k = min(max(static_cast<int>((xj - lo) / we), 0), nb - 1);
             const double xd = static_cast<double>(xj), vd = static_cast<double>(vj);
             const long long q = __double2ll_rn(vd * kFix);
-            atomicAdd(&s_cnt[k], 1u);
-            atomicAdd(&s_sv[k], static_cast<unsigned long long>(q));
+            atomicAdd(&b.cnt[k], 1u);
+            add_u64_pair(&b.sv_lo[k], &b.sv_hi[k], static_cast<unsigned long long>(q));
             if (ll) {
-                atomicAdd(&s_ll[k], xd);
-                atomicAdd(&s_ll[nb + k], xd * xd);
-                atomicAdd(&s_ll[2 * nb + k], xd * vd);
+                atomicAdd(&b.ll[k], xd);
+                atomicAdd(&b.ll[nb + k], xd * xd);
+                atomicAdd(&b.ll[2 * nb + k], xd * vd);
             }
             tot += q;
         }
     }
     tot = warp_sum_i64(tot);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&s_sv[nb], static_cast<unsigned long long>(tot));
+    if ((threadIdx.x & 31) == 0) add_u64_pair(&b.sv_lo[nb], &b.sv_hi[nb], static_cast<unsigned long long>(tot));
     __syncthreads();
-    for (int k = threadIdx.x; k < nf; k += blockDim.x)
-        if (s_fine[k]) atomicAdd(&d.fine[k], s_fine[k]);
-    {
-        // the block's 32-bin chunk totals: a warp a chunk, a lane a bin
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_ch = (nf + 31) / 32;
-        for (int c = warp; c < n_ch; c += blockDim.x >> 5) {
-            const int k = 32 * c + lane;
-            unsigned u = k < nf ? s_fine[k] : 0u;
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) u += __shfl_xor_sync(0xffffffffu, u, off);
-            if (lane == 0 && u) atomicAdd(&d.chunk[c], u);
+    // the block's histogram and bins into the step's: bulk reductions by the TMA unit (issued by thread 0, waited for
+    // at the next grid_arrive or at the end of the kernel), lane atomics for any array the unit cannot take
+    const int nq = d.nbq;
+    for (int k = threadIdx.x; k < nq; k += blockDim.x) b.sv[k] = (static_cast<unsigned long long>(b.sv_hi[k]) << 32) | b.sv_lo[k];
+    fence_proxy_async_shared();
+    __syncthreads();
+    unsigned* gc = d.cnt;
+    unsigned long long* gs = d.sv;
+    const int fine_words = d.packed ? d.nfp / 2 : d.nfp;
+    const unsigned fine_bytes = static_cast<unsigned>(fine_words) * 4u, cnt_bytes = static_cast<unsigned>(nq) * 4u;
+    const bool bulk = bulk_aligned(d.fine, b.fine, fine_bytes) && bulk_aligned(gc, b.cnt, cnt_bytes) &&
+                      bulk_aligned(gs, b.sv, 2u * cnt_bytes);
+    if (bulk) {
+        if (threadIdx.x == 0) {
+            fence_proxy_async_global();  // (the clearing of the step's arrays, before the last barrier)
+            bulk_add_u32(d.fine, b.fine, fine_bytes);
+            bulk_add_u32(gc, b.cnt, cnt_bytes);
+            bulk_add_u64(gs, b.sv, 2u * cnt_bytes);
+            bulk_commit();
+        }
+    } else {
+        for (int k = threadIdx.x; k < fine_words; k += blockDim.x)
+            if (b.fine[k]) atomicAdd(&d.fine[k], b.fine[k]);
+        for (int k = threadIdx.x; k <= nb; k += blockDim.x) {
+            if (k == nb) atomicAdd(&gs[nb], b.sv[k]);
+            else if (b.cnt[k]) atomicAdd(&gc[k], b.cnt[k]), atomicAdd(&gs[k], b.sv[k]);
         }
     }
-    for (int k = threadIdx.x; k < nb; k += blockDim.x)
-        if (s_cnt[k]) atomicAdd(&d.cnt[k], s_cnt[k]), atomicAdd(&d.sv[k], s_sv[k]);
-    if (threadIdx.x == 0) atomicAdd(&d.sv[nb], s_sv[nb]);
     if (ll)
         for (int k = threadIdx.x; k < 3 * nb; k += blockDim.x)
-            if (s_ll[k] != 0.0) atomicAdd(&d.acc_ll[k], s_ll[k]);
+            if (b.ll[k] != 0.0) atomicAdd(&d.acc_ll[k], b.ll[k]);
 }
 
 template <typename R>
@@ -259,7 +332,10 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     const Particles<R> pt{const_cast<R*>(x), const_cast<R*>(v), d.n_pairs, 0, blockIdx.x * (long long)blockDim.x + threadIdx.x,
                           stride};
-    bin_phase<R>(d, pt, b, s_mn, s_mx);
+    double lo, hi;
+    range_of(d, lo, hi, s_mn, s_mx);  // (its barrier also orders the clearing before)
+    bin_phase<R>(d, pt, b, lo, hi);
+    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // Exclusive prefix of x over the block and the block's total (any block size that is a multiple of 32, up to 1024).
@@ -295,110 +371,141 @@ __device__ __forceinline__ double interp_uniform(double x, double a, double b, c
 
 // Grid, regression and leverage of step i; block g computes grid point g. Step 0 uses the reference's initial grid
 // and E[v | x] = v0. The grid's bounds are the quantiles of the fine histogram (RC/src/leverage.cpp:26-38: the first
-// fine bin k with a count and (counts before k) + count >= q total, at lo + (k + (q total - before) / count) width),
-// computed in every block from the chunk totals and, for the chunk that holds each quantile, its 32 bins.
-// Shared memory of the regression (blocks of at most 512 threads).
+// fine bin k with a count and (counts before k) + count >= q total, at lo + (k + (q total - before) / count) width).
+// The step's row and scalars are staged before (regress_stage); the particles' histogram and bins are loaded in one
+// wave: each thread a run of the fine histogram's words (into s_fine) and its bins' counts and v sums. A block scan of
+// the runs' totals finds, for each quantile, the first run that reaches it, and that run's thread finds its bin.
 struct RegressShared {
     unsigned long long warp[32];
-    double cum[2][512];
     int best[2];
     double q[2];
     double red[5][32];
-    double mn[32], mx[32];
+    double bw, lv_lo, lv_hi;  // the step's kernel bandwidth and local-variance row bounds (regress_stage)
 };
 
-__device__ void regress_phase(const LevDev& d, double n_particles, int g, int i, RegressShared& sh) {
-    unsigned long long* s_warp = sh.warp;
-    double(*s_cum)[512] = sh.cum;
-    int* s_best = sh.best;
-    double* s_q = sh.q;
-    double(*s_red)[32] = sh.red;
-    double *s_mn = sh.mn, *s_mx = sh.mx;
-    const int nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x;
-    const int lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
-    const double h = d.dt[i];
-    double x0, cond;
-    if (i == 0) {
-        x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
-        cond = d.v0;
-    } else {
-        // Two levels: each thread owns a run of 32-bin chunks and their totals (kept by lev_bin); a block scan of the
-        // runs gives the counts before every chunk; the first chunk with a count that reaches the target holds the
-        // quantile's bin, and the thread owning it scans that chunk's 32 bins.
-        const int n_ch = (nf + 31) / 32, cpt = (n_ch + blockDim.x - 1) / blockDim.x;
-        const int ca = min(t * cpt, n_ch), cb = min(ca + cpt, n_ch);
-        unsigned mine_c[2] = {0u, 0u};  // cpt <= 2 (n_fine <= 16384)
-        unsigned long long mine = 0;
-        for (int c = ca; c < cb; ++c) mine_c[c - ca] = __ldcg(d.chunk + c), mine += mine_c[c - ca];
-        if (t < 2) s_best[t] = n_ch;
-        double lo, hi;
-        range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also publish s_best)
-        unsigned long long total_u;
-        const unsigned long long before = block_scan(mine, s_warp, total_u);
-        const double total = static_cast<double>(total_u);
-        const double q2[2] = {d.q_lo, d.q_hi};
+// The step's inputs that do not depend on the particles, staged ahead of the regression (while the block waits at a
+// barrier, or after the three-kernel schedule's wait for the previous kernel): the local-variance row into s_row
+// (when it is given) and the step's scalars into sh, by threads 1 on (thread 0 is then releasing the block's arrival
+// at the barrier) when the block has more than one warp. A barrier separates this from regress_phase.
+__device__ void regress_stage(const LevDev& d, int i, RegressShared& sh, double* s_row) {
+    const double* row = d.lv_rows + static_cast<long long>(i) * d.n_lv;
+    const int skip = blockDim.x > 32 ? 1 : 0, t = static_cast<int>(threadIdx.x) - skip, nt = blockDim.x - skip;
+    if (s_row && t >= 0)
+        for (int k0 = t; k0 < d.n_lv; k0 += 4 * nt) {
+            double r[4];  // the loads issued together, then the stores
 #pragma unroll
-        for (int qi = 0; qi < 2; ++qi) {
-            const double target = q2[qi] * total;
-            double cum = static_cast<double>(before);
-            for (int c = ca; c < cb; ++c) {
-                const unsigned tc = mine_c[c - ca];
-                if (tc > 0 && cum + static_cast<double>(tc) >= target) {
-                    atomicMin(&s_best[qi], c);
-                    s_cum[qi][t] = cum;
-                    break;
-                }
-                cum += static_cast<double>(tc);
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u * nt;
+                r[u] = k < d.n_lv ? __ldg(row + k) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u * nt;
+                if (k < d.n_lv) s_row[k] = r[u];
             }
         }
+    if (static_cast<int>(threadIdx.x) == (blockDim.x > 32 ? 32 : 0)) {
+        const double lv_lo = __ldg(d.lv_lo + i), inv = __ldg(d.lv_inv_dx + i);
+        sh.bw = __ldg(d.bw + i), sh.lv_lo = lv_lo, sh.lv_hi = lv_lo + (d.n_lv - 1) / inv;
+    }
+}
+
+__device__ void regress_phase(const LevDev& d, double n_particles, int g, int i, double lo, double hi,
+                              RegressShared& sh, unsigned* s_fine, double* s_row) {
+    const int nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x, nt = blockDim.x;
+    const int lane = t & 31, warp = t >> 5, nw = nt >> 5;
+    const double* row = d.lv_rows + static_cast<long long>(i) * d.n_lv;
+    double x0, cond = d.v0;
+    unsigned long long all_v = 0;
+    if (i == 0) {
+        const double h = d.dt[i];
+        x0 = (-6.0 + 12.0 * g / (nx - 1)) * d.atm_vol * sqrt(h > 1e-4 ? h : 1e-4);
+    } else {
+        // this thread's bins (n_bins <= 512, blocks of 256 or 512 threads: at most two)
+        unsigned cn[2] = {0u, 0u};
+        unsigned long long sq[2] = {0ull, 0ull};
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int k = t + u * nt;
+            if (k < nb) cn[u] = __ldcg(d.cnt + k), sq[u] = __ldcg(d.sv + k);
+        }
+        if (t == 0) all_v = __ldcg(d.sv + nb);
+        // this thread's run of the fine histogram: seg words (a multiple of 4) from word t seg, holding bins from
+        // t seg_b on (two to a word when packed)
+        const bool pk = d.packed;
+        const int seg = (pk ? d.nfp / 2 : d.nfp) / nt, n4 = seg / 4, seg_b = pk ? 2 * seg : seg;
+        const uint4* __restrict__ src = reinterpret_cast<const uint4*>(d.fine + static_cast<long long>(t) * seg);
+        uint4* dst = reinterpret_cast<uint4*>(s_fine + t * seg);
+        unsigned long long mine = 0;
+        for (int m0 = 0; m0 < n4; m0 += 4) {
+            uint4 f[4];  // the loads issued together, then the stores
+#pragma unroll
+            for (int u = 0; u < 4; ++u) f[u] = m0 + u < n4 ? __ldcg(src + m0 + u) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (m0 + u < n4) dst[m0 + u] = f[u];
+                const unsigned w4[4] = {f[u].x, f[u].y, f[u].z, f[u].w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    mine += pk ? (w4[j] & 0xffffu) + (w4[j] >> 16) : static_cast<unsigned long long>(w4[j]);
+            }
+        }
+        if (t < 2) sh.best[t] = nt;
+        unsigned long long total_u;
+        const unsigned long long before = block_scan(mine, sh.warp, total_u);  // (its barriers publish sh.best)
+        // every particle is in one fine bin: a packed count that passed 2^16 - 1 shows here
+        if (pk && t == 0 && total_u != static_cast<unsigned long long>(n_particles)) atomicCAS(d.status, 0, kPackOverflow);
+        const double total = static_cast<double>(total_u);
+        const double q2[2] = {d.q_lo, d.q_hi};
+        // counts are integers: (count) >= q total exactly when (count) >= ceil(q total)
+        const unsigned long long need[2] = {static_cast<unsigned long long>(ceil(q2[0] * total)),
+                                            static_cast<unsigned long long>(ceil(q2[1] * total))};
+        // the first run with a count whose end reaches the target holds the quantile's bin
+#pragma unroll
+        for (int qi = 0; qi < 2; ++qi)
+            if (mine > 0 && before + mine >= need[qi]) atomicMin(&sh.best[qi], t);
         __syncthreads();
         const double width = (hi - lo) / static_cast<double>(nf);
 #pragma unroll
         for (int qi = 0; qi < 2; ++qi) {
-            const int cw = s_best[qi];
-            if (cw < n_ch && t == cw / cpt) {
-                // the bins of chunk cw: the first with a count and (counts before it) + count >= target
-                const double target = q2[qi] * total;
-                unsigned cc[32];  // the 32 loads issued together, then the search
+            const int w = sh.best[qi];
+            if (t == w) {
+                const uint4* run = reinterpret_cast<const uint4*>(s_fine + t * seg);
+                unsigned long long cum = before, before_kb = 0;
+                int kb = -1;
+                unsigned c_kb = 0u;
+                for (int m = 0; m < n4 && kb < 0; ++m) {
+                    const uint4 f = run[m];
+                    const unsigned w4[4] = {f.x, f.y, f.z, f.w};
+                    // the run's bins in order: one a word, or (packed) a word's low half before its high half
 #pragma unroll
-                for (int j = 0; j < 32; ++j) cc[j] = 32 * cw + j < nf ? __ldcg(d.fine + 32 * cw + j) : 0u;
-                double cum = s_cum[qi][t];
-                int kb = nf;
-                unsigned cb_count = 0u;
-                double before_kb = 0.0;
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const unsigned c = cc[j];
-                    if (kb == nf && c > 0 && cum + static_cast<double>(c) >= target)
-                        kb = 32 * cw + j, cb_count = c, before_kb = cum;
-                    cum += static_cast<double>(c);
+                    for (int u = 0; u < 8; ++u) {
+                        if (!pk && (u & 1)) continue;
+                        const unsigned c = pk ? ((u & 1) ? w4[u >> 1] >> 16 : w4[u >> 1] & 0xffffu) : w4[u >> 1];
+                        const int bin = t * seg_b + (pk ? 8 * m + u : 4 * m + (u >> 1));
+                        if (kb < 0 && c > 0 && cum + c >= need[qi]) kb = bin, c_kb = c, before_kb = cum;
+                        cum += c;
+                    }
                 }
-                s_q[qi] = kb >= nf ? hi
-                                   : lo + (static_cast<double>(kb) + (target - before_kb) /
-                                                                         static_cast<double>(cb_count)) *
-                                              width;
-            } else if (cw >= n_ch && t == 0) {
-                s_q[qi] = hi;
+                const double target = q2[qi] * total;
+                sh.q[qi] = kb < 0 ? hi
+                                  : lo + (static_cast<double>(kb) +
+                                          (target - static_cast<double>(before_kb)) / static_cast<double>(c_kb)) *
+                                             width;
+            } else if (w >= nt && t == 0) {
+                sh.q[qi] = hi;
             }
         }
         __syncthreads();
-        const double qv[2] = {s_q[0], s_q[1]};
+        const double qv[2] = {sh.q[0], sh.q[1]};
         x0 = qv[0] + (qv[1] - qv[0]) * g / (nx - 1);
-        const double bw = d.bw[i];
+        const double bw = sh.bw;
         const double wc = (hi + 1e-12 - lo) / nb;
         const double *sx = d.acc_ll, *sxx = sx + nb, *sxv = sxx + nb;
         double r[5] = {0, 0, 0, 0, 0};
-        // n_bins <= 512: at most two bins a thread, their loads issued together
-        unsigned cn[2];
-        unsigned long long sq[2];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
-            const int k = t + u * static_cast<int>(blockDim.x);
-            cn[u] = k < nb ? __ldcg(d.cnt + k) : 0u, sq[u] = k < nb ? __ldcg(d.sv + k) : 0ull;
-        }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            const int k = t + u * static_cast<int>(blockDim.x);
+            const int k = t + u * nt;
             if (k >= nb) break;
             const double c = lo + (k + 0.5) * wc;
             const double dd = (x0 - c) / bw, w = exp(-0.5 * dd * dd);
@@ -406,20 +513,21 @@ __device__ void regress_phase(const LevDev& d, double n_particles, int g, int i,
             r[0] += w * static_cast<double>(cn[u]), r[1] += w * sv;
             if (d.local_linear) r[2] += w * __ldcg(sx + k), r[3] += w * __ldcg(sxx + k), r[4] += w * __ldcg(sxv + k);
         }
+        const int nq = d.local_linear ? 5 : 2;
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
+            if (q >= nq) break;
             r[q] = warp_sum(r[q]);
-            if (lane == 0) s_red[q][warp] = r[q];
+            if (lane == 0) sh.red[q][warp] = r[q];
         }
         __syncthreads();
+        // the warps' sums added by warp 0 (thread 0 uses them)
+        if (warp == 0)
 #pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            r[q] = 0.0;
-            for (int w = 0; w < nw; ++w) r[q] += s_red[q][w];
-        }
+            for (int q = 0; q < 5; ++q) r[q] = q < nq ? warp_sum(lane < nw ? sh.red[q][lane] : 0.0) : 0.0;
         const double S0 = r[0], T0 = r[1], Ax = r[2], Axx = r[3], Axv = r[4];
-        const double fallback = static_cast<double>(static_cast<long long>(__ldcg(d.sv + nb))) / kFix / n_particles;
-        const double nw_e = S0 > 1e-8 ? T0 / (S0 > 1e-300 ? S0 : 1e-300) : fallback;
+        const double nw_e = S0 > 1e-8 ? T0 / (S0 > 1e-300 ? S0 : 1e-300)
+                                      : static_cast<double>(static_cast<long long>(all_v)) / kFix / n_particles;
         cond = nw_e;
         if (d.local_linear) {
             const double S1 = Ax - x0 * S0, S2 = Axx - 2 * x0 * Ax + x0 * x0 * S0, T1 = Axv - x0 * T0;
@@ -430,9 +538,7 @@ __device__ void regress_phase(const LevDev& d, double n_particles, int g, int i,
         }
     }
     if (t == 0) {
-        const double* row = d.lv_rows + static_cast<long long>(i) * d.n_lv;
-        const double lv_lo = d.lv_lo[i], lv_hi = lv_lo + (d.n_lv - 1) / d.lv_inv_dx[i];
-        const double loc = interp_uniform(x0, lv_lo, lv_hi, row, d.n_lv);
+        const double loc = interp_uniform(x0, sh.lv_lo, sh.lv_hi, s_row ? s_row : row, d.n_lv);
         double L = sqrt(loc / (cond > 1e-8 ? cond : 1e-8));
         L = L > d.l_min ? L : d.l_min;
         L = L < d.l_max ? L : d.l_max;
@@ -443,41 +549,79 @@ __device__ void regress_phase(const LevDev& d, double n_particles, int g, int i,
     __syncthreads();  // the block's shared memory is free for its next grid point
 }
 
+// Dynamic shared memory of lev_regress: the fine histogram, then the local-variance row when it is staged.
+__host__ __device__ __forceinline__ bool row_staged(int n_lv) { return n_lv <= kMaxRowSmem; }
+
 __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles) {
+    extern __shared__ __align__(16) unsigned char sm[];
     __shared__ RegressShared sh;
+    __shared__ double s_mn[32], s_mx[32];
+    unsigned* s_fine = reinterpret_cast<unsigned*>(sm);
+    double* s_row = row_staged(d.n_lv) ? reinterpret_cast<double*>(s_fine + d.nfp) : nullptr;
     wait_previous();
-    regress_phase(d, n_particles, blockIdx.x, current_step(d), sh);
+    const int i = current_step(d);
+    regress_stage(d, i, sh, s_row);
+    double lo = 0.0, hi = 0.0;
+    if (i > 0) range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also order the staging)
+    else __syncthreads();
+    regress_phase(d, n_particles, blockIdx.x, i, lo, hi, sh, s_fine, s_row);
 }
 
-// The SLV Euler step of every pair (grid-stride), and the block's min and max of the new x into part_range. The step's
-// histogram and bins are read (lev_regress is done): the blocks clear them for the next step's binning.
+// The normals of this thread's pairs at step i (Philox counter (pair, i + 1, 0, 0)): z0 at p, z1 at n + p.
+template <typename R>
+__device__ void step_normals(const LevDev& d, const Particles<R>& pt, int i, R* s_z) {
+    for (long long p = pt.start; p < pt.n; p += pt.stride) {
+        R z0, z1, z2, z3;
+        normals4<R>(static_cast<uint64_t>(pt.first + p), static_cast<uint64_t>(i + 1), 0u, d.k0, d.k1, z0, z1, z2, z3);
+        s_z[p] = z0, s_z[pt.n + p] = z1;
+    }
+}
+
+// The SLV Euler step of every pair, and the block's min and max of the new x: into part_range (SH false) or into the
+// step parity's order keys (SH true; block 0 also resets the other parity's keys for the next step). The step's
+// histogram and bins are read (the regression is done): the blocks clear them for the next step's binning. The
+// normals come from s_z when the caller computed them ahead, else from Philox here.
 template <typename R, bool SH = false>
-__device__ void step_phase(const LevDev& d, const Particles<R>& pt, int i, R* s_lev, R* s_min, R* s_max) {
+__device__ void step_phase(const LevDev& d, const Particles<R>& pt, int i, R* s_lev, R* s_min, R* s_max,
+                           const R* s_z) {
     R* __restrict__ x = pt.x;
     R* __restrict__ v = pt.v;
     {
-        const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0, n_ch = (nf + 31) / 32;
+        const int nb = d.n_bins, nf = d.n_fine, n_ll = d.local_linear ? 3 * nb : 0, n_c = d.nbq;
         const int stride = gridDim.x * blockDim.x;
-        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nf + nb + nb + 1 + n_ll + n_ch; k += stride) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nf + 2 * n_c + n_ll; k += stride) {
             if (k < nf) d.fine[k] = 0u;
-            else if (k < nf + nb) d.cnt[k - nf] = 0u;
-            else if (k < nf + 2 * nb + 1) d.sv[k - nf - nb] = 0ull;
-            else if (k < nf + 2 * nb + 1 + n_ll) d.acc_ll[k - nf - 2 * nb - 1] = 0.0;
-            else d.chunk[k - nf - 2 * nb - 1 - n_ll] = 0u;
+            else if (k < nf + n_c) d.cnt[k - nf] = 0u;
+            else if (k < nf + 2 * n_c) d.sv[k - nf - n_c] = 0ull;
+            else d.acc_ll[k - nf - 2 * n_c] = 0.0;
         }
     }
-    for (int g = threadIdx.x; g < d.n_x; g += blockDim.x) s_lev[g] = static_cast<R>(__ldcg(d.lev + g));
-    __syncthreads();
+    if constexpr (SH) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            long long* r = d.rng + 2 * ((i + 1) & 1);
+            r[0] = 0x7fffffffffffffffLL, r[1] = -0x7fffffffffffffffLL - 1;
+        }
+    }
     const int nx = d.n_x;
-    const R h = static_cast<R>(d.dt[i]);
-    const R a = static_cast<R>(__ldcg(d.x_eval)), b = static_cast<R>(__ldcg(d.x_eval + nx - 1));
+    // the grid's ends and the step's length, loaded with the leverage row
+    const double xa = __ldcg(d.x_eval), xb = __ldcg(d.x_eval + nx - 1), hd = __ldg(d.dt + i);
+    for (int g = threadIdx.x; g < nx; g += blockDim.x) s_lev[g] = static_cast<R>(__ldcg(d.lev + g));
+    __syncthreads();
+    const R h = static_cast<R>(hd);
+    const R a = static_cast<R>(xa), b = static_cast<R>(xb);
     const R rho = static_cast<R>(d.rho), kappa = static_cast<R>(d.kappa), theta = static_cast<R>(d.theta);
     const R xi = static_cast<R>(d.xi);
     const R rc = m_sqrt(R(1) - rho * rho);
     R mn = sizeof(R) == 4 ? R(3.0e38f) : R(1.0e300), mx = -mn;
     for (long long p = pt.start; p < pt.n; p += pt.stride) {
-        R z0, z1, z2, z3;
-        normals4<R>(static_cast<uint64_t>(pt.first + p), static_cast<uint64_t>(i + 1), 0u, d.k0, d.k1, z0, z1, z2, z3);
+        R z0, z1;
+        if (s_z) {
+            z0 = s_z[p], z1 = s_z[pt.n + p];
+        } else {
+            R z2, z3;
+            normals4<R>(static_cast<uint64_t>(pt.first + p), static_cast<uint64_t>(i + 1), 0u, d.k0, d.k1, z0, z1, z2,
+                        z3);
+        }
 #pragma unroll
         for (int leg = 0; leg < 2; ++leg) {
             const long long j = leg ? pt.n + p : p;
@@ -507,13 +651,27 @@ __device__ void step_phase(const LevDev& d, const Particles<R>& pt, int i, R* s_
         mn = m_min(mn, __shfl_down_sync(0xffffffffu, mn, off));
         mx = m_max(mx, __shfl_down_sync(0xffffffffu, mx, off));
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if (lane == 0) s_min[warp] = mn, s_max[warp] = mx;
     __syncthreads();
+    if (warp == 0) {
+        // the warps' extremes, by warp 0
+        mn = lane < nw ? s_min[lane] : s_min[0], mx = lane < nw ? s_max[lane] : s_max[0];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            mn = m_min(mn, __shfl_down_sync(0xffffffffu, mn, off));
+            mx = m_max(mx, __shfl_down_sync(0xffffffffu, mx, off));
+        }
+    }
     if (threadIdx.x == 0) {
-        for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) mn = m_min(mn, s_min[w]), mx = m_max(mx, s_max[w]);
-        d.part_range[2 * blockIdx.x] = static_cast<double>(mn);
-        d.part_range[2 * blockIdx.x + 1] = static_cast<double>(mx);
+        if constexpr (SH) {
+            long long* r = d.rng + 2 * (i & 1);
+            atomicMin(r, order_key(static_cast<double>(mn)));
+            atomicMax(r + 1, order_key(static_cast<double>(mx)));
+        } else {
+            d.part_range[2 * blockIdx.x] = static_cast<double>(mn);
+            d.part_range[2 * blockIdx.x + 1] = static_cast<double>(mx);
+        }
     }
 }
 
@@ -524,16 +682,18 @@ __global__ void __launch_bounds__(256) lev_step(LevDev d, R* __restrict__ x, R* 
     wait_previous();
     const Particles<R> pt{x, v, d.n_pairs, 0, blockIdx.x * (long long)blockDim.x + threadIdx.x,
                           static_cast<long long>(gridDim.x) * blockDim.x};
-    step_phase<R>(d, pt, current_step(d), s_lev, s_min, s_max);
+    step_phase<R>(d, pt, current_step(d), s_lev, s_min, s_max, nullptr);
 }
 
 // ------------------------------------------------------------------------------------------------ persistent
 //
 // The whole calibration as one cooperative launch (every block resident at once): per step the three phases above,
-// separated by grid barriers, with the step index a loop variable. One block of 512 threads per SM. The barrier is a
-// counter and a generation word in global memory; a block that waits polls the generation at most d.wait_limit times,
-// then records OB_ETIMEOUT in d.status and returns, and every other block leaves at its next barrier on seeing the
-// status, so a calibration whose barrier cannot complete ends with an error instead of holding the GPU.
+// separated by grid barriers, with the step index a loop variable. One block of 512 threads per SM. The barrier is an
+// arrival counter in global memory, split in two: grid_arrive after the block's writes, then work that needs nothing
+// from the other blocks (clearing the block's bins, the next step's normals), then grid_wait. A block that waits polls
+// the counter at most d.wait_limit times, then records OB_ETIMEOUT in d.status and returns, and every other block
+// leaves at its next barrier on seeing the status, so a calibration whose barrier cannot complete ends with an error
+// instead of holding the GPU.
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     unsigned v;
@@ -547,19 +707,28 @@ __device__ __forceinline__ void red_release_gpu(unsigned* p, unsigned v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Every block's writes before the barrier are visible to every block after it. The barrier is one arrival counter
-// that only grows: a block adds one (a release) and waits until the count reaches every block's arrivals so far
-// (`arrived`, advanced by gridDim.x at each barrier, the same in every thread). A block polls at most d.wait_limit
-// times (with a limit of zero it gives up at once), then records OB_ETIMEOUT; a block that sees the status leaves.
-// False: the calibration has failed and the caller returns.
-__device__ bool grid_barrier(const LevDev& d, unsigned& arrived) {
-    __shared__ int s_ok;
+// The counter only grows: a block adds one (a release) once all its threads' writes are done, and its next wait lasts
+// until the count reaches every block's arrivals so far (`arrived`, advanced by gridDim.x at each arrival, the same in
+// every thread).
+__device__ __forceinline__ void grid_arrive(const LevDev& d, unsigned& arrived) {
     arrived += gridDim.x;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int ok = 1;
+        bulk_wait_all();             // this block's bulk reductions are done
+        fence_proxy_async_global();  // and ordered before the release below
         __threadfence();
         red_release_gpu(d.bar_count, 1u);
+    }
+}
+
+// Every block's writes before its grid_arrive are visible to every thread after this (the acquiring load, then the
+// block's barrier). A block polls at most d.wait_limit times (with a limit of zero it gives up at once), then records
+// OB_ETIMEOUT; a block that sees the status (read every 32 polls) leaves. Once the count is reached every block has
+// arrived, so none has given up at this barrier. False: the calibration has failed and the caller returns.
+__device__ bool grid_wait(const LevDev& d, unsigned arrived) {
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = 1;
         for (long long polls = 0;; ++polls) {
             if (polls >= d.wait_limit) {
                 atomicCAS(d.status, 0, OB_ETIMEOUT);
@@ -567,14 +736,12 @@ __device__ bool grid_barrier(const LevDev& d, unsigned& arrived) {
                 break;
             }
             if (ld_acquire_gpu(d.bar_count) >= arrived) break;
-            if (status_of(d) != 0) {
+            if ((polls & 31) == 31 && status_of(d) != 0) {
                 ok = 0;
                 break;
             }
             if (polls > 256) __nanosleep(32);
         }
-        __threadfence();
-        if (status_of(d) != 0) ok = 0;
         s_ok = ok;
     }
     __syncthreads();
@@ -584,34 +751,56 @@ __device__ bool grid_barrier(const LevDev& d, unsigned& arrived) {
 constexpr int kPersistentThreads = 512;
 
 // Block b owns pairs [b chunk, (b + 1) chunk) and keeps their particles in its shared memory (after the binning
-// arrays, at part_off) for the whole calibration: the binning and the step read them there, not through L2.
+// arrays, at part_off) for the whole calibration: the binning and the step read them there, not through L2. With
+// z_off, the block computes each step's normals ahead (while the range of the particles arrives) into shared memory
+// at z_off; with row_off, a regression block stages the step's local-variance row there while it waits at the barrier
+// before the regression.
 template <typename R>
 __global__ void __launch_bounds__(kPersistentThreads, 1)
-    lev_persistent(LevDev d, long long chunk, int part_off, double n_particles) {
+    lev_persistent(LevDev d, long long chunk, int part_off, int z_off, int row_off, double n_particles) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ RegressShared rs;
     __shared__ R s_lev[kMaxX];
     __shared__ R s_min[32], s_max[32];
-    __shared__ double s_mn[32], s_mx[32];
     const BinShared b = bin_shared(d, sm);
     const long long first = static_cast<long long>(blockIdx.x) * chunk;
     const long long count = first < d.n_pairs ? (d.n_pairs - first < chunk ? d.n_pairs - first : chunk) : 0;
     R* sx = reinterpret_cast<R*>(sm + part_off);
     R* sv = sx + 2 * chunk;
+    R* s_z = z_off ? reinterpret_cast<R*>(sm + z_off) : nullptr;
+    double* s_row = row_off ? reinterpret_cast<double*>(sm + row_off) : nullptr;
     const Particles<R> pt{sx, sv, count, first, threadIdx.x, blockDim.x};
     for (long long j = threadIdx.x; j < 2 * count; j += blockDim.x) sx[j] = R(0), sv[j] = static_cast<R>(d.v0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.rng[0] = 0x7fffffffffffffffLL, d.rng[1] = -0x7fffffffffffffffLL - 1;
+    bin_clear_shared(d, b);
     unsigned arrived = 0;
-    // (step 0's regression reads no particle; its barrier orders these stores before the first step)
+    // (step 0's regression reads no particle; the barrier after it orders these stores before the first step)
+    const bool regresses = static_cast<int>(blockIdx.x) < d.n_x;
+    if (regresses) regress_stage(d, 0, rs, s_row);  // (ordered before step 0's regression by the barrier below)
+    __syncthreads();
     for (int i = 0; i < d.n_steps; ++i) {
+        double lo = 0.0, hi = 0.0;
         if (i > 0) {
-            bin_clear_shared(d, b);
-            bin_phase<R, true>(d, pt, b, s_mn, s_mx);
-            if (!grid_barrier(d, arrived)) return;
+            // the range's keys are loaded first; the step's normals are computed while they arrive
+            const long long* r = d.rng + 2 * ((i - 1) & 1);
+            const long long k_lo = __ldcg(r), k_hi = __ldcg(r + 1);
+            if (s_z) step_normals(d, pt, i, s_z);
+            lo = from_order_key(k_lo), hi = from_order_key(k_hi);
+            bin_phase<R, true>(d, pt, b, lo, hi);
+            grid_arrive(d, arrived);
+            if (regresses) regress_stage(d, i, rs, s_row);  // (while thread 0 waits for the bulk reductions)
+            if (!grid_wait(d, arrived)) return;
         }
-        for (int g = blockIdx.x; g < d.n_x; g += gridDim.x) regress_phase(d, n_particles, g, i, rs);
-        if (!grid_barrier(d, arrived)) return;
-        step_phase<R, true>(d, pt, i, s_lev, s_min, s_max);
-        if (i + 1 < d.n_steps && !grid_barrier(d, arrived)) return;
+        for (int g = blockIdx.x; g < d.n_x; g += gridDim.x) regress_phase(d, n_particles, g, i, lo, hi, rs, b.fine, s_row);
+        grid_arrive(d, arrived);
+        bin_clear_shared(d, b);
+        if (i == 0 && s_z) step_normals(d, pt, 0, s_z);
+        if (!grid_wait(d, arrived)) return;
+        step_phase<R, true>(d, pt, i, s_lev, s_min, s_max, s_z);
+        if (i + 1 < d.n_steps) {
+            grid_arrive(d, arrived);
+            if (!grid_wait(d, arrived)) return;
+        }
     }
 }
 
@@ -620,17 +809,25 @@ __global__ void __launch_bounds__(kPersistentThreads, 1)
 constexpr long long kDefaultWaitLimit = 1LL << 22;
 long long g_wait_limit = kDefaultWaitLimit;
 
-// Dynamic shared memory of a persistent block at most: the binning arrays and the block's particles.
+// Dynamic shared memory of a persistent block at most: the binning arrays and the block's particles, then (when they
+// fit) the step's normals and the local-variance row.
 constexpr size_t kPersistentSmemMax = size_t(200) << 10;
+
+__host__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
 
 // The persistent calibration on stream st; false (nothing launched) when a block's particles do not fit its shared
 // memory or the device cannot hold every block at once.
 template <typename R>
 bool run_persistent(LevDev& d, double n_particles, size_t bin_smem, int sms, cudaStream_t st) {
     const long long chunk = (d.n_pairs + sms - 1) / sms;
-    const size_t part_off = (bin_smem + 15) & ~static_cast<size_t>(15);
-    const size_t smem = part_off + 4 * static_cast<size_t>(chunk) * sizeof(R);
+    const size_t part_off = align16(bin_smem);
+    size_t smem = part_off + 4 * static_cast<size_t>(chunk) * sizeof(R);
     if (smem > kPersistentSmemMax) return false;
+    size_t z_off = 0, row_off = 0;
+    if (align16(smem) + 2 * static_cast<size_t>(chunk) * sizeof(R) <= kPersistentSmemMax)
+        z_off = align16(smem), smem = z_off + 2 * static_cast<size_t>(chunk) * sizeof(R);
+    if (row_staged(d.n_lv) && align16(smem) + static_cast<size_t>(d.n_lv) * sizeof(double) <= kPersistentSmemMax)
+        row_off = align16(smem), smem = row_off + static_cast<size_t>(d.n_lv) * sizeof(double);
     check_cuda(cudaFuncSetAttribute(lev_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)),
                "cudaFuncSetAttribute");
@@ -640,10 +837,10 @@ bool run_persistent(LevDev& d, double n_particles, size_t bin_smem, int sms, cud
     int coop = 0, dev = 0;
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     check_cuda(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cudaDeviceGetAttribute");
-    if (occ < 1 || !coop || d.n_step_blocks != sms) return false;
-    int off = static_cast<int>(part_off);
+    if (occ < 1 || !coop) return false;
+    int p_off = static_cast<int>(part_off), zo = static_cast<int>(z_off), ro = static_cast<int>(row_off);
     long long ch = chunk;
-    void* args[] = {&d, &ch, &off, &n_particles};
+    void* args[] = {&d, &ch, &p_off, &zo, &ro, &n_particles};
     const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(lev_persistent<R>), dim3(sms),
                                                       dim3(kPersistentThreads), args, smem, st);
     if (e == cudaErrorCooperativeLaunchTooLarge) {
@@ -687,15 +884,17 @@ void run_leverage(ob_leverage_request& rq) {
     d.lv_inv_dx = arena.put<double>(rq.lv_inv_dx, S);
     d.lv_rows = arena.put<double>(rq.lv_rows, static_cast<size_t>(S) * rq.n_lv);
     const int nb = rq.n_bins, nf = rq.n_fine, ll = rq.local_linear;
-    d.fine = arena.alloc<unsigned>(nf);
-    d.chunk = arena.alloc<unsigned>((nf + 31) / 32);
-    check_cuda(cudaMemset(d.chunk, 0, (nf + 31) / 32 * sizeof(unsigned)), "cudaMemset");
-    d.cnt = arena.alloc<unsigned>(nb);
-    d.sv = arena.alloc<unsigned long long>(nb + 1);
+    d.nfp = (nf + kFinePad - 1) / kFinePad * kFinePad;
+    d.nbq = (nb + 1 + 3) / 4 * 4;
+    const size_t n_c = static_cast<size_t>(d.nbq);
+    d.fine = arena.alloc<unsigned>(d.nfp);
+    d.cnt = arena.alloc<unsigned>(n_c);
+    d.sv = arena.alloc<unsigned long long>(n_c);
     d.acc_ll = arena.alloc<double>(3 * static_cast<size_t>(nb));
-    check_cuda(cudaMemset(d.fine, 0, nf * sizeof(unsigned)), "cudaMemset");
-    check_cuda(cudaMemset(d.cnt, 0, nb * sizeof(unsigned)), "cudaMemset");
-    check_cuda(cudaMemset(d.sv, 0, (nb + 1) * sizeof(unsigned long long)), "cudaMemset");
+    d.rng = arena.alloc<long long>(4);
+    check_cuda(cudaMemset(d.fine, 0, d.nfp * sizeof(unsigned)), "cudaMemset");
+    check_cuda(cudaMemset(d.cnt, 0, n_c * sizeof(unsigned)), "cudaMemset");
+    check_cuda(cudaMemset(d.sv, 0, n_c * sizeof(unsigned long long)), "cudaMemset");
     check_cuda(cudaMemset(d.acc_ll, 0, 3 * nb * sizeof(double)), "cudaMemset");
     d.x_eval = arena.alloc<double>(rq.n_x);
     d.lev = arena.alloc<double>(rq.n_x);
@@ -704,16 +903,13 @@ void run_leverage(ob_leverage_request& rq) {
     R* x = arena.alloc<R>(n);
     R* v = arena.alloc<R>(n);
     d.step = arena.alloc<int>(1);
-    const size_t bin_smem = (static_cast<size_t>(nb) + 1) * sizeof(unsigned long long) +
-                            (ll ? 3 * static_cast<size_t>(nb) * sizeof(double) : 0) +
-                            (static_cast<size_t>(nf) + nb) * sizeof(unsigned);
+    const size_t bin_smem = bin_smem_bytes(d.nfp, d.nbq, nb, ll);
     check_cuda(cudaFuncSetAttribute(lev_bin<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(bin_smem)),
                "cudaFuncSetAttribute");
     // one binning block an SM (fewer for small particle counts): each block bins many particles before it adds
     const int n_bin_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(sms, (n + 511) / 512)));
-    // the persistent kernel's blocks (one an SM) each write their range; the graph path's lev_step uses up to 4 an SM
-    d.n_step_blocks = sms;
+    // the three-kernel schedule's lev_step blocks (up to 4 an SM) each write their range
     d.part_range = arena.alloc<double>(2 * static_cast<size_t>(4 * sms));
     d.n_steps = S;
     d.bar_count = arena.alloc<unsigned>(4);
@@ -737,12 +933,31 @@ void run_leverage(ob_leverage_request& rq) {
         c.attrs = pdl, c.numAttrs = 1;
         return c;
     };
-    // OPTLAB_B200_LEVERAGE=graphs runs the three-kernel schedule below instead (to compare the two; same results)
+    // OPTLAB_B200_LEVERAGE=graphs runs the three-kernel schedule below instead, =unpacked the persistent kernel with a
+    // 32-bit fine histogram (to compare them; same results)
     const char* mode = std::getenv("OPTLAB_B200_LEVERAGE");
     const bool graphs_only = mode && std::strcmp(mode, "graphs") == 0;
-    if (!graphs_only && run_persistent<R>(d, n_particles, bin_smem, sms, st)) {
+    const bool unpacked = mode && std::strcmp(mode, "unpacked") == 0;
+    // a persistent block bins 2 chunk particles: packed 16-bit counts hold them
+    d.packed = !unpacked && 2 * ((rq.n_pairs + sms - 1) / sms) < 65536;
+    for (int attempt = 0; !graphs_only && attempt < 2; ++attempt) {
+        if (!run_persistent<R>(d, n_particles, bin_smem, sms, st)) break;
         int status = 0;
         check_cuda(cudaMemcpyAsync(&status, d.status, sizeof status, cudaMemcpyDeviceToHost, st), "copy status");
+        check_cuda(cudaStreamSynchronize(st), "leverage");
+        if (status == kPackOverflow && d.packed) {
+            // a fine bin held 2^16 particles or more: the same calibration again, unpacked, from clean buffers
+            d.packed = 0;
+            check_cuda(cudaMemset(d.fine, 0, d.nfp * sizeof(unsigned)), "cudaMemset");
+            check_cuda(cudaMemset(d.cnt, 0, n_c * sizeof(unsigned)), "cudaMemset");
+            check_cuda(cudaMemset(d.sv, 0, n_c * sizeof(unsigned long long)), "cudaMemset");
+            check_cuda(cudaMemset(d.acc_ll, 0, 3 * nb * sizeof(double)), "cudaMemset");
+            check_cuda(cudaMemset(d.bar_count, 0, 4 * sizeof(unsigned)), "cudaMemset");
+            continue;
+        }
+        if (status == OB_ETIMEOUT)
+            throw Error(OB_ETIMEOUT, "leverage: a grid barrier of the calibration gave up waiting for the other blocks");
+        if (status != 0) throw Error(OB_ECUDA, "leverage: the calibration kernel reported a failure");
         check_cuda(cudaMemcpyAsync(rq.x_grids, d.x_grids, static_cast<size_t>(S) * rq.n_x * sizeof(double),
                                    cudaMemcpyDeviceToHost, st),
                    "copy x_grids");
@@ -750,20 +965,22 @@ void run_leverage(ob_leverage_request& rq) {
                                    cudaMemcpyDeviceToHost, st),
                    "copy values");
         check_cuda(cudaStreamSynchronize(st), "leverage");
-        if (status == OB_ETIMEOUT)
-            throw Error(OB_ETIMEOUT, "leverage: a grid barrier of the calibration gave up waiting for the other blocks");
-        if (status != 0) throw Error(OB_ECUDA, "leverage: the calibration kernel reported a failure");
         rq.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
         return;
     }
     // the device cannot hold the persistent kernel: three kernels a step, replayed as graphs
+    d.packed = 0;
     d.n_step_blocks = static_cast<int>(std::max<long long>(1, std::min<long long>(4LL * sms, (rq.n_pairs + 255) / 256)));
     lev_init<R><<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(x, v, n, static_cast<R>(rq.v0), d.step);
     check_cuda(cudaGetLastError(), "lev_init launch");
     const R* cx = x;
     const R* cv = v;
     // step 0 (no binning: the particles all start at x = 0), launched directly
-    const cudaLaunchConfig_t c_reg0 = config(rq.n_x, 256, 0), c_step0 = config(d.n_step_blocks, 256, 0);
+    const size_t reg_smem = static_cast<size_t>(d.nfp) * sizeof(unsigned) +
+                            (row_staged(rq.n_lv) ? static_cast<size_t>(rq.n_lv) * sizeof(double) : 0);
+    check_cuda(cudaFuncSetAttribute(lev_regress, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(reg_smem)),
+               "cudaFuncSetAttribute");
+    const cudaLaunchConfig_t c_reg0 = config(rq.n_x, 256, reg_smem), c_step0 = config(d.n_step_blocks, 256, 0);
     check_cuda(cudaLaunchKernelEx(&c_reg0, lev_regress, d, n_particles), "lev_regress launch");
     check_cuda(cudaLaunchKernelEx(&c_step0, lev_step<R>, d, x, v), "lev_step launch");
     // the other steps: graphs of kGraphSteps steps, replayed, and one of the remainder
@@ -775,7 +992,7 @@ void run_leverage(ob_leverage_request& rq) {
     };
     const cudaLaunchConfig_t c_bin = on(config(n_bin_blocks, 512, bin_smem));
     const cudaLaunchConfig_t c_step = on(config(d.n_step_blocks, 256, 0));
-    const cudaLaunchConfig_t c_reg = on(config(rq.n_x, 256, 0));
+    const cudaLaunchConfig_t c_reg = on(config(rq.n_x, 256, reg_smem));
     GraphExecs execs;
     auto make_graph = [&](int steps) {
         check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");

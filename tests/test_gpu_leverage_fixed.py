@@ -148,6 +148,33 @@ def test_the_persistent_calibration_equals_the_three_kernel_schedule(monkeypatch
     assert np.abs(a.values / b.values - 1).max() < 1e-12
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_the_packed_fine_histogram_equals_the_unpacked_one(monkeypatch, precision):
+    """The persistent kernel packs the fine histogram two 16-bit counts to a word; OPTLAB_B200_LEVERAGE=unpacked keeps
+    32-bit counts. Counts are integers and the regression the same arithmetic: the tables are identical."""
+    a, b = leverage_request(**_lev_kw()), leverage_request(**_lev_kw())
+    engine.leverage(a, precision)
+    monkeypatch.setenv("OPTLAB_B200_LEVERAGE", "unpacked")
+    engine.leverage(b, precision)
+    assert np.array_equal(a.x_grids, b.x_grids)
+    assert np.array_equal(a.values, b.values)
+
+
+def test_a_fine_bin_past_the_packed_counts_reruns_unpacked(monkeypatch):
+    """With 16 fine bins and 2^19 particles the middle bins hold over 2^16 particles each, more than a packed count
+    holds: the kernel sees the histogram's total fall short, and the call runs the calibration again unpacked, so the
+    tables equal the unpacked run's and the three-kernel schedule's."""
+    kw = dict(_lev_kw(n_pairs=2**18, n_steps=12), n_fine=16)
+    a, b, c = (leverage_request(**kw) for _ in range(3))
+    engine.leverage(a, "fp64")
+    monkeypatch.setenv("OPTLAB_B200_LEVERAGE", "unpacked")
+    engine.leverage(b, "fp64")
+    monkeypatch.setenv("OPTLAB_B200_LEVERAGE", "graphs")
+    engine.leverage(c, "fp64")
+    assert np.array_equal(a.values, b.values) and np.array_equal(a.x_grids, b.x_grids)
+    assert np.abs(a.values / c.values - 1).max() < 1e-12
+
+
 def test_a_grid_barrier_that_gives_up_returns_a_timeout_and_the_device_stays_usable():
     """With a wait limit of zero polls every block gives up at its first wait on a grid barrier (a count that, as far
     as it may wait, nobody completes); the call returns OB_ETIMEOUT, every block leaves the kernel, and the next
