@@ -44,7 +44,7 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0
 # Executed warp instructions per path-step of the dominant kernel, measured by ncu (smsp__inst_executed.sum of one
 # launch divided by its path-steps) and recorded under profiles/. The issue roofline below multiplies it by the live
 # path-step rate. A launch's instruction count does not depend on timing, so a profiled launch gives it exactly.
-INST_PER_PATH_STEP = {"lv_phoenix": 1.459, "heston_qe": 20.40, "script": 2.507,
+INST_PER_PATH_STEP = {"lv_phoenix": 1.391, "heston_qe": 20.40, "script": 2.507,
                       # the 12 class kernels of one revaluation of the 32-trade book: 404.1 G over 2.49e11 path-steps
                       "batch": 1.623,
                       # the drop-in path engine's local-vol kernel on the Phoenix model (12 columns + a daily window)
@@ -62,9 +62,13 @@ INST_PER_PATH_STEP = {"lv_phoenix": 1.459, "heston_qe": 20.40, "script": 2.507,
 # 29 lane instructions = 0.906 warp instructions per path-step. The observations (12 over 756 steps) add < 1 %.
 ALG_INST_PER_PATH_STEP = {"lv_phoenix": (8 + 7 + 14) / 32.0}
 
-# Warp instructions of one leverage calibration at 2^18 particles x 504 steps: lev_bin 4.24 M x 503 + lev_regress
-# 1.44 M x 504 + lev_step 1.70 M x 504 (ncu, one launch of each).
-LEV_INST_PER_CALIBRATION = 4.24e6 * 503 + 1.44e6 * 504 + 1.70e6 * 504
+# Warp instructions of one leverage calibration at 2^18 particles x 504 steps: one lev_persistent launch
+# (ncu smsp__inst_executed.sum).
+LEV_INST_PER_CALIBRATION = 2.2436e9
+# One grid barrier of 148 blocks (arrival counter with a release, acquiring polls), measured alone on a B200: 1.27 us.
+# A leverage step needs three (the particles' range, the step's bins, the leverage row): 3.81 us a step is the floor
+# of any calibration that keeps this dependency structure.
+LEV_BARRIER_US = 1.27
 
 
 def issue_roofline(warp_inst_per_s: float | None, note: str) -> dict:
@@ -80,6 +84,8 @@ def issue_roofline(warp_inst_per_s: float | None, note: str) -> dict:
     return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "Gwarp-inst/s",
             "frac": achieved / peak if achieved is not None else None, "traffic": None,
             "note": f"{note}; peak = SMs x 4 schedulers x max SM clock ({sm_max:.0f} MHz, {peak_kind})"}
+
+
 # DRAM bytes (read + written) of one profiled launch of the dominant kernel: the packed inputs, read once from HBM
 # and then from L2; the loop keeps its state in registers, so the figure does not grow with the path count.
 DRAM_PER_LAUNCH = {"lv_phoenix": 119296, "heston_qe": 44288}
@@ -772,9 +778,10 @@ def run_batch(args, world, rank):
 def run_leverage(args, world, rank):
     """cfg2: the SLV leverage calibration by particles (2^18 particles x 504 steps, 128-point regression grid, 400
     bins), FP32 particles with FP64 bins and regression, through ob_leverage (upload of the 504 x 801 local-variance
-    rows, 504 dependent steps of bin / regress / step kernels, read-back of the two 504 x 128 tables). Units:
+    rows, one persistent kernel over the 504 dependent steps, read-back of the two 504 x 128 tables). Units:
     particle-steps. `value` is timed by CUDA events around the call on its stream (the upload of 3.2 MB is inside
-    it); `e2e` by the host clock around the same call."""
+    it); `e2e` by the host clock around the same call. The roofline is the latency floor of three grid barriers a
+    step, with the issue rate beside it."""
     import torch
 
     from optlab_b200 import engine, workloads
@@ -833,15 +840,27 @@ def run_leverage(args, world, rank):
         "data": "synthetic (SSVI surface, Heston parameters)",
         "config": {"workload": "slv_leverage", "particles": 2 * s.n_pairs, "n_steps": s.n_steps, "n_x": s.n_x,
                    "n_bins": s.n_bins, "n_fine": s.n_fine, "lv_row_points": s.n_lv,
-                   "l2": "particles (2 MB) stay in L2 by design: the calibration is latency-bound"},
-        "roofline": dict(issue_roofline(
-            LEV_INST_PER_CALIBRATION / (ms / 1e3) if 2 * s.n_pairs == 2**18 and s.n_steps == 504 else None,
-            "504 dependent steps of 3 small launches (bin, regress, step): latency-bound, so the issue rate is low; "
-            "achieved = ncu warp instructions of a calibration / its measured time"), bound="latency"),
+                   "l2": "particles stay in the persistent blocks' shared memory; the calibration is latency-bound"},
+        "roofline": {
+            "bound": "latency",
+            "achieved": s.n_steps / (ms / 1e3),
+            "peak": 1e6 / (3 * LEV_BARRIER_US),
+            "unit": "time-steps/s",
+            "frac": (s.n_steps / (ms / 1e3)) / (1e6 / (3 * LEV_BARRIER_US)),
+            "traffic": None,
+            "note": f"peak = three grid barriers a step at the measured {LEV_BARRIER_US} us each; achieved includes "
+                    "the call's upload and read-back",
+            "issue": issue_roofline(
+                LEV_INST_PER_CALIBRATION / (ms / 1e3)
+                if LEV_INST_PER_CALIBRATION and 2 * s.n_pairs == 2**18 and s.n_steps == 504 else None,
+                "achieved = ncu warp instructions of a calibration / its measured time"),
+        },
         "cpu_baseline": cpu,
         "e2e": {"value": units / statistics.median(wall), "unit": "path-steps/s",
-                "h2d_bytes_per_step": s.n_steps * (s.n_lv + 4) * 8, "d2h_bytes_per_step": 2 * s.n_steps * s.n_x * 8},
-        "gpu_launches": args.steps * 3 * s.n_steps,  # lev_init, then per step bin (not at step 0), regress, step
+                "h2d_bytes_per_step": s.n_steps * (s.n_lv + 5) * 8, "d2h_bytes_per_step": 2 * s.n_steps * s.n_x * 8},
+        # one persistent kernel a calibration; the three-kernel schedule: lev_init, then per step bin (not at step 0),
+        # regress and step
+        "gpu_launches": args.steps * (3 * s.n_steps if os.environ.get("OPTLAB_B200_LEVERAGE") == "graphs" else 1),
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "result": {"leverage_at_atm_last_step": float(held.values[-1, s.n_x // 2])},
     }

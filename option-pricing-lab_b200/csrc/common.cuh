@@ -17,6 +17,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #include "../../include/optlab_b200.h"
 
@@ -185,11 +186,17 @@ struct DeviceArena {
         check_cuda(cudaMemcpy(d, host, count * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy (inputs)");
         return d;
     }
-    // Host array of count elements (converted to T) to a new device buffer; null or empty gives null.
+    // Host array of count elements (converted to T) to a new device buffer; null or empty gives null. An array already
+    // of T is copied as it is (no host copy to convert into).
     template <typename T, typename S>
     T* put(const S* host, size_t count, cudaStream_t st = nullptr) {
         if (!host || !count) return nullptr;
         T* d = alloc<T>(count);
+        if constexpr (std::is_same_v<T, S>) {
+            check_cuda(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync (inputs)");
+            check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize (inputs)");
+            return d;
+        }
         T* tmp = static_cast<T*>(std::malloc(count * sizeof(T)));
         if (!tmp) throw std::bad_alloc();
         for (size_t i = 0; i < count; ++i) tmp[i] = static_cast<T>(host[i]);

@@ -2,28 +2,27 @@
 // leverage by the particle method of Guyon and Henry-Labordere, as RC/src/leverage.cpp:97-152 (host algorithm) with
 // the particle device of RC/src/leverage.cpp:156-214 / RC/src/leverage_gpu.cu:40-106.
 //
-// Per step i, everything stays on the device (the reference crosses PCIe three times a step):
-//   lev_bin        one block an SM: its particles into a private fine histogram and regression bins in shared
-//                  memory (u32 counts, the v sums in 64-bit fixed point, the local-linear moments in FP64), then its
-//                  non-zero entries added into the step's global histogram and bins (integer atomics: the counts and v
-//                  sums do not depend on the order)
-//   lev_regress    one block per grid point g: the quantiles of the fine histogram bound the grid (the reference's
-//                  first-match search, by a block scan), then the Gaussian-kernel regression E[v | x_g]
-//                  (Nadaraya-Watson or local linear) over the bins in FP64, and L_g = clip(sqrt(sigma_loc^2 / E),
-//                  lmin, lmax) with the local variance interpolated on its uniform row; the row and the grid go
-//                  straight into the output tables
-//   lev_step       one thread per antithetic pair (grid-stride): the SLV Euler step with the leverage row staged in
-//                  shared memory, normals from Philox counter (pair, step + 1, 0, 0), each block's min and max of the
-//                  new x stored for the next step (no atomics); it also clears the histogram and bins just read
+// Per step i, everything stays on the device (the reference crosses PCIe three times a step), in three phases:
+//   bin       each block's particles into a fine histogram and regression bins in its shared memory (u32 counts, the
+//             v sums in 64-bit fixed point, the local-linear moments in FP64), then added into the step's global
+//             histogram and bins (integer additions: the sums do not depend on their order)
+//   regress   one block per grid point g: the quantiles of the fine histogram bound the grid (the reference's
+//             first-match search, by a block scan), then the Gaussian-kernel regression E[v | x_g] (Nadaraya-Watson
+//             or local linear) over the bins in FP64, and L_g = clip(sqrt(sigma_loc^2 / E), lmin, lmax) with the local
+//             variance interpolated on its uniform row; the row and the grid go straight into the output tables
+//   step      the SLV Euler step of every pair with the leverage row staged in shared memory, normals from Philox
+//             counter (pair, step + 1, 0, 0), the new range of x kept for the next step's bins; the step's histogram
+//             and bins are cleared for the next step
 // Particles are float (OB_FP32) or double (OB_FP64); bins, regression and the leverage ratio are FP64 in both (each v
-// enters the sums rounded to 2^-37).
+// enters the sums rounded to 2^-36).
 //
-// The 3 x 504 launches are a few microseconds of GPU work each, so launching them one by one makes the host the
-// bound on a slow CPU (measured: 54.8 us a step against 28.6 us of kernels). The kernels therefore take the step
-// index from a device counter (set by lev_init, advanced by lev_bin once the previous step is done) rather than as
-// an argument, so every step after the first is the same three launches: they are captured once as a CUDA graph of
-// kGraphSteps steps (programmatic dependent launches inside it) and the graph is replayed, with one more graph for
-// the remaining steps. The host then issues a few dozen graph launches instead of 1,500 kernel launches.
+// The calibration runs as one persistent cooperative kernel, lev_persistent: one block of 512 threads per SM holds its
+// particles in shared memory for the whole calibration, the phases are separated by grid barriers with bounded waits
+// (OB_ETIMEOUT), the range of x travels as two order-key atomics, and the histogram and bins are added into global
+// memory by TMA bulk reductions (the fine histogram packed two 16-bit counts to a word). When the device cannot hold
+// it (particles beyond a block's shared memory, no cooperative launch), the phases run as three kernels a step
+// (lev_bin, lev_regress, lev_step) that take the step index from a device counter, captured as CUDA graphs of
+// kGraphSteps steps with programmatic dependent launches, and replayed.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
