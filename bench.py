@@ -1043,7 +1043,8 @@ def run_callable(args, world, rank):
     """The issuer's call: the callable reverse convertible of the reference's issuer-call test (2y, semiannual 3 %
     coupons, callable at par on the first three dates, redemption min(S / S0, 1)) under Black-Scholes as a flat
     local-variance table, FP64. One step is one whole valuation: the device pilot (pilot_paths(2 pairs) paths,
-    recorded), the Longstaff-Schwartz fit on the host, the pricing run applying the policy (2^17 pairs), and the
+    recorded in device memory), the Longstaff-Schwartz fit on the device (ob_script_pilot_fit), the pricing run
+    applying the policy (2^17 pairs), and the
     Andersen-Broadie dual bound from 1000 outer paths x 200 branched continuations at each of the 3 call dates. Timed
     by the host clock around the whole valuation (every stage reads its results back); `value` is valuations per
     second, `e2e` the same figure (the stages take host arrays and return host results)."""
@@ -1117,7 +1118,10 @@ def run_callable(args, world, rank):
         "roofline": None,
         "cpu_baseline": None,
         "e2e": {"value": 1.0 / t_s, "unit": "valuations/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
-        "gpu_launches": 2 * (3 + n_calls),  # pilot, pricing, outer paths, one branched run a call date
+        # script runs (kernel and sums, 2 each): pilot, pricing, outer paths, one branched run a call date; the fit:
+        # per call date its preparation, moments, order statistics, three normal-equation passes (2 each) and the
+        # decisions, then the flows before the first call date (when it is not the first event) and the total
+        "gpu_launches": 2 * (3 + n_calls) + 10 * n_calls + (comp.calls[0][0] != 0) + 1,
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
         "result": {"price": res.price, "se": res.se, "dual_lower": b["lower"], "gap": b["gap"], "gap_se": b["gap_se"],
                    "pde": case["pde"]},

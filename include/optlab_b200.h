@@ -3,7 +3,8 @@
  * Every entry point returns an int status (OB_OK = 0) and never exits, aborts or traps: the engine runs inside the
  * caller's process. On an error, ob_last_error() gives a message for the calling thread. The status splits the
  * reference's exceptions: OB_EINVAL where it throws std::invalid_argument (a bad request), OB_ENODEV and OB_ECUDA
- * where it throws std::runtime_error (no device, a CUDA failure), OB_ETIMEOUT where a bounded device wait gave up.
+ * where it throws std::runtime_error (no device, a CUDA failure), OB_ETIMEOUT where a bounded device wait gave up,
+ * OB_ESINGULAR where the device's pilot fit meets a regression it leaves to the host (ob_script_pilot_fit).
  *
  * Reference interfaces replaced (paths relative to the reference project, RC = packages/native/cuda):
  *   optlab::api::paths     RC/include/optlab_cuda/requests.hpp:105-106, request layout :36-63   -> ob_paths
@@ -33,6 +34,7 @@ extern "C" {
 #define OB_ECUDA 3
 #define OB_ETIMEOUT 4
 #define OB_ENOMEM 5
+#define OB_ESINGULAR 6
 
 #define OB_FP32 0
 #define OB_FP64 1
@@ -466,6 +468,18 @@ int ob_batch_destroy(ob_batch* batch);
    the host (packages/structured/src/optlab/structured/engine.py:143-153 with script/evaluator.py:123-231): the
    paths are simulated and the script evaluated on the device, and only the price and its SE come back. */
 int ob_script_price(const ob_script_request* rq, int precision, ob_script_result* res);
+
+/* The issuer's Longstaff-Schwartz policy fitted on the device: replaces the reference's pilot and fit
+   (packages/structured/src/optlab/structured/exercise.py:212-252 with the basis of :125-140, run from
+   structured/engine.py:342-370). Runs the pilot `rq` (call_mode 1; rq->record may be NULL, and the record then stays
+   on the device) and fits the rules backward over its calls on the device: call_event[c] is the event of call c,
+   pay_discount[k] the discount factor of event k's payment (0: none counted). rules receives n_calls rows of
+   OB_RULE_STRIDE doubles in the layout call_mode 2 reads (a call no path reaches: a row of zeros), in_sample the
+   pilot's value under its own policy, res the pilot's own result (never called). OB_ESINGULAR: a regression's terms
+   were nearly collinear (a pivot of its normal equations below 1e-13 of its diagonal), where the reference's SVD solve
+   and the device's refined normal equations may part; the caller fits that pilot on the host. */
+int ob_script_pilot_fit(const ob_script_request* rq, int precision, const int* call_event, const double* pay_discount,
+                        double* rules, double* in_sample, ob_script_result* res);
 
 #ifdef __cplusplus
 }

@@ -18,8 +18,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 
+#include "exercise.cuh"
 #include "mc.cuh"
 
 namespace ob {
@@ -712,7 +714,7 @@ ScriptFn<R> pick_script(int model, int n, int n_windows) {
 }
 
 // Every index the device will follow is checked here: registers, names, windows, tags, code ranges and steps.
-void check_script(const ob_script_request& rq) {
+void check_script(const ob_script_request& rq, bool record_needed = true) {
     check_mc_model(rq.model);
     const int S = rq.model.n_steps, n = rq.model.n_names;
     if (rq.n_regs < 1 || rq.n_regs > kMaxRegs) invalid("n_regs must be 1 to 128");
@@ -753,7 +755,7 @@ void check_script(const ob_script_request& rq) {
     if (rq.n_calls < 0 || rq.n_state < 0 || rq.n_state > kMaxState) invalid("n_calls >= 0 and n_state 0 to 4");
     if (rq.call_mode < 0 || rq.call_mode > 2) invalid("call_mode must be 0, 1 or 2");
     if (rq.n_calls && !rq.call_state) invalid("null call_state");
-    if (rq.call_mode == 1 && rq.n_calls && !rq.record) invalid("call_mode 1 needs a record array");
+    if (record_needed && rq.call_mode == 1 && rq.n_calls && !rq.record) invalid("call_mode 1 needs a record array");
     if (rq.call_mode == 2 && rq.n_calls && !rq.rules) invalid("call_mode 2 needs rules");
     for (int c = 0; c < rq.n_calls; ++c)
         for (int j = 0; j < rq.n_state; ++j)
@@ -812,8 +814,12 @@ void check_script(const ob_script_request& rq) {
     }
 }
 
+// Called with the pilot's record while it is in device memory (call_mode 1): rows of stride doubles, one a path, and
+// the call's device arena.
+using RecordHook = std::function<void(const double* record, long long n_paths, int stride, DeviceArena& arena)>;
+
 template <typename R>
-void run_script(const ob_script_request& rq, ob_script_result& res) {
+void run_script(const ob_script_request& rq, ob_script_result& res, const RecordHook* hook = nullptr) {
     const auto t_start = std::chrono::steady_clock::now();
     const int sms = require_device();
     DeviceArena arena;
@@ -945,8 +951,9 @@ void run_script(const ob_script_request& rq, ob_script_result& res) {
     unsigned long long bad[3];
     check_cuda(cudaMemcpy(h, sums, sizeof h, cudaMemcpyDeviceToHost), "copy sums");
     check_cuda(cudaMemcpy(bad, d.bad, sizeof bad, cudaMemcpyDeviceToHost), "copy counts");
-    if (rec_count) check_cuda(cudaMemcpy(rq.record, d.record, rec_count * sizeof(double), cudaMemcpyDeviceToHost),
-                              "copy record");
+    if (rec_count && rq.record)
+        check_cuda(cudaMemcpy(rq.record, d.record, rec_count * sizeof(double), cudaMemcpyDeviceToHost), "copy record");
+    if (rec_count && hook) (*hook)(d.record, 2 * mq.n_pairs, d.rec_stride, arena);
     if (rq.pair_value)
         check_cuda(cudaMemcpy(rq.pair_value, d.pair_value, static_cast<size_t>(mq.n_pairs) * sizeof(double),
                               cudaMemcpyDeviceToHost),
@@ -975,5 +982,31 @@ extern "C" int ob_script_price(const ob_script_request* rq, int precision, ob_sc
         *res = ob_script_result{};
         if (precision == OB_FP32) ob::run_script<float>(*rq, *res);
         else ob::run_script<double>(*rq, *res);
+    });
+}
+
+extern "C" int ob_script_pilot_fit(const ob_script_request* rq, int precision, const int* call_event,
+                                   const double* pay_discount, double* rules, double* in_sample, ob_script_result* res) {
+    return ob::guarded([&] {
+        if (!rq || !res || !call_event || !pay_discount || !rules || !in_sample) ob::invalid("null argument");
+        if (precision != OB_FP32 && precision != OB_FP64) ob::invalid("precision must be OB_FP32 or OB_FP64");
+        if (rq->call_mode != 1 || rq->n_calls < 1) ob::invalid("the pilot fit runs a pilot (call_mode 1) of a script with calls");
+        ob::check_script(*rq, false);
+        std::vector<char> seen(rq->n_events, 0);
+        for (int c = 0; c < rq->n_calls; ++c) {
+            if (call_event[c] < 0 || call_event[c] >= rq->n_events || seen[call_event[c]])
+                ob::invalid("call_event must name distinct events");
+            seen[call_event[c]] = 1;
+        }
+        *res = ob_script_result{};
+        bool fitted = false;
+        const ob::RecordHook hook = [&](const double* record, long long n_paths, int stride, ob::DeviceArena& arena) {
+            fitted = ob::fit_policy_on_device(record, n_paths, stride, rq->n_events, rq->n_calls, rq->n_state, call_event,
+                                              pay_discount, rules, in_sample, arena);
+        };
+        if (precision == OB_FP32) ob::run_script<float>(*rq, *res, &hook);
+        else ob::run_script<double>(*rq, *res, &hook);
+        if (!fitted)
+            throw ob::Error(OB_ESINGULAR, "pilot fit: a regression's terms are nearly collinear; fit it on the host");
     });
 }

@@ -11,7 +11,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-OB_OK, OB_EINVAL, OB_ENODEV, OB_ECUDA, OB_ETIMEOUT, OB_ENOMEM = 0, 1, 2, 3, 4, 5
+OB_OK, OB_EINVAL, OB_ENODEV, OB_ECUDA, OB_ETIMEOUT, OB_ENOMEM, OB_ESINGULAR = 0, 1, 2, 3, 4, 5, 6
 OB_FP32, OB_FP64 = 0, 1
 OB_MAX_NAMES, OB_MAX_WINDOWS, OB_MAX_OUT = 8, 2, 32
 OB_BATCH_MAX_CARRY = 4
@@ -393,6 +393,8 @@ SIGNATURES = {
     "ob_batch_classes": (C.c_int, [C.c_void_p, C.c_int, _ip, _ip]),
     "ob_batch_destroy": (C.c_int, [C.c_void_p]),
     "ob_script_price": (C.c_int, [C.POINTER(ObScriptRequest), C.c_int, C.POINTER(ObScriptResult)]),
+    "ob_script_pilot_fit": (C.c_int, [C.POINTER(ObScriptRequest), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(ObScriptResult)]),
 }
 
 _lib: list = []

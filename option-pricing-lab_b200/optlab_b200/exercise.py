@@ -6,20 +6,23 @@ at :125-140): the script runs on the pilot as if the issuer never called, record
 flows before and after its call statement and, at each call, its mask, the alive mass, the amount and the state;
 backward from the last call date, the note's continuation per unit reached, in money of the call date, is regressed on
 polynomials and hinges of the normalised state over the paths the call reaches, and the issuer calls where the fitted
-continuation is above the amount. Here the pilot's record comes from the device (call mode 1 of ob_script_price), the
-regressions (a few tens of thousands of paths, at most 25 terms) run on the host, and the pricing run applies the rules
-on the device (call mode 2): a call there pays the amount as redemption and terminates, which is what the reference's
-`survival_and_flows` rebuilds from the uncalled record.
+continuation is above the amount. Here the pilot runs on the device and the fit too (ob_script_pilot_fit: the record
+stays in device memory, every pass over the paths is a kernel, the at most 25 x 25 normal equations are solved and
+refined on the host), and the pricing run applies the rules on the device (call mode 2): a call there pays the amount
+as redemption and terminates, which is what the reference's `survival_and_flows` rebuilds from the uncalled record.
+`fit` is the same regression on a record brought to the host, with the reference's own least-squares solve: the
+device hands a pilot to it when a regression's terms are nearly collinear.
 """
 
 from __future__ import annotations
 
+import ctypes as C
 import itertools
 from dataclasses import dataclass
 
 import numpy as np
 
-from ._abi import OB_RULE_STRIDE
+from ._abi import OB_ESINGULAR, OB_RULE_STRIDE, ObScriptResult, check, load, ptr
 from . import script as sc
 
 MAX_TERMS = 25  # regression terms, the constant included
@@ -110,6 +113,22 @@ class Policy:
             row[161:161 + len(r.coef)] = r.coef
         return out
 
+    @classmethod
+    def unpack(cls, rows: np.ndarray, n_state: int, pilot_paths: int, in_sample: float = float("nan")) -> Policy:
+        """The policy of packed rules (the layout of pack; a row whose first value is 0: no rule)."""
+        rules = []
+        for row in np.asarray(rows, dtype=np.float64):
+            if row[0] == 0.0:
+                rules.append(None)
+                continue
+            n_poly, n_knots = int(row[1]), int(row[2])
+            rules.append(Rule(
+                tuple(float(v) for v in row[3:3 + n_state]), tuple(float(v) for v in row[7:7 + n_state]),
+                tuple(tuple(int(v) for v in row[11 + 4 * t:11 + 4 * t + n_state]) for t in range(n_poly)),
+                tuple((int(row[111 + q]), float(row[136 + q])) for q in range(n_knots)),
+                tuple(float(v) for v in row[161:161 + n_poly + n_knots])))
+        return cls(tuple(rules), pilot_paths, in_sample)
+
 
 @dataclass
 class PilotRecord:
@@ -166,6 +185,31 @@ def fit(rec: PilotRecord, call_events: list, pay_discount: list) -> Policy:
     return Policy(tuple(rules), n, float(np.mean(future)))
 
 
+def pilot_fit(pilot: sc.ScriptHeld, call_events: list, pay_discount: list, precision="fp32"):
+    """Run the pilot (a call_mode 1 request) and fit the policy on the device (ob_script_pilot_fit): the record stays
+    in device memory. Returns (policy, the pilot's result), or None where a regression's terms are nearly collinear
+    (the device then leaves the fit to `fit` and the reference's own least squares)."""
+    from .engine import precision_code
+
+    s = pilot.struct
+    rules = np.zeros((s.n_calls, OB_RULE_STRIDE))
+    events = np.ascontiguousarray(call_events, dtype=np.int32)
+    disc = np.ascontiguousarray(pay_discount, dtype=np.float64)
+    res, ins = ObScriptResult(), C.c_double()
+    kept = C.cast(s.record, C.c_void_p).value  # (a pointer field read from a Structure shares its memory)
+    s.record = None  # the record stays on the device
+    try:
+        status = load().ob_script_pilot_fit(C.byref(s), precision_code(precision), ptr(events, C.c_int), ptr(disc),
+                                            ptr(rules), C.byref(ins), C.byref(res))
+    finally:
+        s.record = C.cast(kept, C.POINTER(C.c_double))
+    if status == OB_ESINGULAR:
+        return None
+    check(status)
+    sc.check_result(pilot, res)
+    return Policy.unpack(rules, s.n_state, 2 * s.model.n_pairs, ins.value), res
+
+
 def pilot_paths(n_paths: int) -> int:
     """The pilot's size: half the pricing paths, between 20,000 and 100,000, even (exercise.py:256-259)."""
     n = max(20_000, min(n_paths // 2, 100_000))
@@ -177,17 +221,23 @@ PILOT_KEY = 0x5EEDCA11  # the pilot's Philox key is the pricing seed xor this: n
 
 def price(compiled, make_sim, n_pairs: int, seed: int, discount, precision="fp32"):
     """The price of a callable script: a pilot of pilot_paths(2 n_pairs) paths on seed ^ PILOT_KEY, the policy fitted
-    on its record, then the pricing run of n_pairs pairs on `seed` applying it. make_sim(n_pairs, seed) builds the
+    on its record on the device (the host's `fit` where the device refuses a regression), then the pricing run of
+    n_pairs pairs on `seed` applying it. make_sim(n_pairs, seed) builds the
     simulation request. Returns (result, policy)."""
     if not compiled.calls:
         return sc.run(sc.script_request(compiled, make_sim(n_pairs, seed), discount), precision), None
     n_state = len(compiled.calls[0][1])
     pilot = sc.script_request(compiled, make_sim(pilot_paths(2 * n_pairs) // 2, seed ^ PILOT_KEY), discount,
                               call_mode=1)
-    sc.run(pilot, precision)
-    rec = PilotRecord.from_device(pilot.keep[1]["record"], len(compiled.event_times), len(compiled.calls), n_state)
     pay_d = [float(discount(t)) if t is not None and t > 0 else 0.0 for t in compiled.pay_times]
-    policy = fit(rec, [k for k, _ in compiled.calls], pay_d)
+    call_events = [k for k, _ in compiled.calls]
+    fitted = pilot_fit(pilot, call_events, pay_d, precision)
+    if fitted is not None:
+        policy = fitted[0]
+    else:
+        sc.run(pilot, precision)
+        rec = PilotRecord.from_device(pilot.keep[1]["record"], len(compiled.event_times), len(compiled.calls), n_state)
+        policy = fit(rec, call_events, pay_d)
     held = sc.script_request(compiled, make_sim(n_pairs, seed), discount, call_mode=2, rules=policy.pack(n_state))
     return sc.run(held, precision), policy
 

@@ -1011,6 +1011,12 @@ def run(held: ScriptHeld, precision="fp64") -> ObScriptResult:
     paths where the script was undefined (counts), raised as ScriptError like the reference's evaluator."""
     res = ObScriptResult()
     check(load().ob_script_price(C.byref(held.struct), precision_code(precision), C.byref(res)))
+    return check_result(held, res)
+
+
+def check_result(held: ScriptHeld, res: ObScriptResult) -> ObScriptResult:
+    """Raise ScriptError for the paths where a run's script was undefined (the counts of res), as the reference's
+    evaluator raises; else res."""
     if res.bad_pay:
         raise ScriptError(f"an amount paid is not finite on {res.bad_pay} paths it reaches")
     if res.bad_cond:

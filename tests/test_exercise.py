@@ -95,6 +95,19 @@ def test_the_packed_rules_hold_every_term():
     assert exercise.pilot_paths(2**15) == 20000 and exercise.pilot_paths(2**20) == 100000
 
 
+def test_packed_rules_unpack_to_the_same_policy():
+    """The device fit returns packed rules (the layout call mode 2 reads): unpacking them gives the rules back, a row
+    of zeros a call without a rule."""
+    comp = sc.compile_script(CASE["script"])
+    pay_d = [_disc(t) if t is not None and t > 0 else 0.0 for t in comp.pay_times]
+    policy = exercise.fit(_record(), [k for k, _ in comp.calls], pay_d)
+    packed = policy.pack(2)
+    back = exercise.Policy.unpack(packed, 2, policy.pilot_paths, policy.in_sample)
+    assert back == policy
+    packed[1] = 0.0
+    assert exercise.Policy.unpack(packed, 2, 0).rules[1] is None
+
+
 DUAL = json.loads((Path(__file__).resolve().parent / "golden" / "script_dual.json").read_text())
 
 
