@@ -279,9 +279,18 @@ __device__ __forceinline__ WinMeta<NW> win_meta(const ScriptDev<R>& d) {
     return m;
 }
 
-template <typename R, int NW, typename LogFn>
+// WF >= 0: the script's one window is a lowest (0) or a highest (1), known when the kernel is compiled, so a fixing
+// is one comparison; WF < 0: any windows, each fixing dispatched on its function.
+template <int WF = -1, typename R, int NW, typename LogFn>
 __device__ __forceinline__ void fix_windows(const ScriptDev<R>& d, const WinMeta<NW>& meta, WinState<R, NW>& win,
                                             unsigned mask, LogFn logp) {
+    if constexpr (WF >= 0) {
+        if (mask & 1u) {
+            const R y = logp(meta.fn[0] >> 2);
+            win.v[0] = WF == 0 ? m_min(win.v[0], y) : m_max(win.v[0], y);
+        }
+        return;
+    }
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
         if (!((mask >> w) & 1u)) continue;
@@ -442,7 +451,7 @@ struct LvArgs {
 // BRANCH: the pairs continue the paths of an outer simulation after step end d.branch_step (one leg per outer path:
 // before the branch both legs take the outer path's normals, the outer antithetic leg's with the sign flipped).
 // GT: the table is read from global memory (a.tab) instead of the stage.
-template <typename R, int N, int NW, bool BRANCH, bool CALLS, bool GT = false>
+template <typename R, int N, int NW, bool BRANCH, bool CALLS, bool GT = false, int WF = -1>
 __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
     script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0, uint32_t k1,
                      double* __restrict__ partial) {
@@ -497,13 +506,14 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
                 auto logp = [&](int nm) -> R {
+                    if constexpr (N == 1) return l ? y1[0] : y0[0];
                     R v = R(0);
 #pragma unroll
                     for (int n = 0; n < N; ++n)
                         if (n == nm) v = l ? y1[n] : y0[n];
                     return v;
                 };
-                if (sc.y) fix_windows(d, meta, win[l], static_cast<unsigned>(sc.y), logp);
+                if (sc.y) fix_windows<WF>(d, meta, win[l], static_cast<unsigned>(sc.y), logp);
                 if (sc.x >= 0) {
                     R sp[N];
 #pragma unroll
@@ -617,8 +627,17 @@ ScriptLvFn<R> pick_lv_nw(int n, bool branch, bool calls) {
 // blocks an SM, where a second window's spills it to local memory, 3.11 -> 2.67 ms for the 3-year daily-window
 // Phoenix), up to 2 and up to 8. A table in global memory (table_global) only comes with up to 2 windows, no call and
 // no branch (pack_lv checks).
+// One name whose one window is a lowest or a highest (a knock-in or knock-out barrier of a single-name note), no call
+// and no branch: the window's function is compiled in (fix_windows, WF).
+template <typename R, bool GT>
+ScriptLvFn<R> pick_lv_single_window(int win_func) {
+    return win_func == 0 ? script_lv_kernel<R, 1, 1, false, false, GT, 0> : script_lv_kernel<R, 1, 1, false, false, GT, 1>;
+}
+
 template <typename R>
-ScriptLvFn<R> pick_lv(int n, int n_windows, bool branch, bool calls, bool table_global) {
+ScriptLvFn<R> pick_lv(int n, int n_windows, int win_func0, bool branch, bool calls, bool table_global) {
+    if (n == 1 && n_windows == 1 && !branch && !calls && (win_func0 == 0 || win_func0 == 1))
+        return table_global ? pick_lv_single_window<R, true>(win_func0) : pick_lv_single_window<R, false>(win_func0);
     if (table_global) return n_windows <= 1 ? pick_lv_calls<R, 1, false, true>(n) : pick_lv_calls<R, 2, false, true>(n);
     if (n_windows <= 1 && !branch && !calls) return pick_lv_calls<R, 1, false>(n);
     return n_windows <= 2 ? pick_lv_nw<R, 2>(n, branch, calls) : pick_lv_nw<R, kMaxWindows>(n, branch, calls);
@@ -921,7 +940,8 @@ void run_script(const ob_script_request& rq, ob_script_result& res, const Record
     const bool fast = pack_lv<R>(rq, sched, arena, lv);
     if (rq.branch && !fast) invalid("a branched run needs the staged local-vol kernel (its tables too large)");
     const void* fn = fast ? reinterpret_cast<const void*>(
-                                pick_lv<R>(n, rq.n_windows, rq.branch != 0, rq.n_calls > 0, lv.table_global != 0))
+                                pick_lv<R>(n, rq.n_windows, rq.n_windows ? rq.win_func[0] : -1, rq.branch != 0, rq.n_calls > 0,
+                                          lv.table_global != 0))
                           : reinterpret_cast<const void*>(pick_script<R>(mq.model, n, rq.n_windows));
     const int block = fast ? 512 : 128;
     const size_t smem = fast ? static_cast<size_t>(lv.smem_blob) : 0;
