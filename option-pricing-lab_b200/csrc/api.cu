@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "host_copy.cuh"
 
 namespace ob {
 
@@ -79,7 +80,10 @@ int ob_gpu_count(void) {
 int ob_has_cuda(void) { return 1; }
 
 int ob_release_buffers(void) {
-    return ob::guarded([&] { ob::BufferCache::get().drain(); });
+    return ob::guarded([&] {
+        ob::BufferCache::get().drain();
+        ob::PinnedStage::get().release();
+    });
 }
 
 int ob_cpu_threads(void) {

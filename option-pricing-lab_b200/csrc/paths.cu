@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "fused.cuh"
+#include "host_copy.cuh"
 
 namespace ob {
 
@@ -542,17 +543,25 @@ void run_paths(ob_paths_request& h) {
 
     // Chunks of pairs, on two streams: the kernel of one chunk runs while the previous chunk's columns are copied to
     // the host. Large outputs go in four chunks at least; each chunk's output (two buffers) within an eighth of the
-    // free memory, at most 2 GB. The caller's array is not pinned: pinning 117 MB took 12.5 ms on a B200 host,
-    // longer than the pageable copy itself (6.7 ms; pinned, 2.2 ms).
+    // free memory, at most 2 GB. The caller's array is not pinned (pinning 117 MB took 12.5 ms on a B200 host, longer
+    // than the pageable copy itself, 6.7 ms; pinned, 2.2 ms): a chunk is copied into the library's pinned staging
+    // (PinnedStage, at most a slot a chunk), and host threads spread it into the caller's array while the next chunk
+    // runs; without the staging, straight into the caller's array.
     const long long cols = static_cast<long long>(n) * h.n_cols;
     size_t free_mem = 0, total_mem = 0;
     check_cuda(cudaMemGetInfo(&free_mem, &total_mem), "cudaMemGetInfo");
     const long long budget = std::min<long long>(static_cast<long long>(free_mem) / 8, 2LL << 30);
     const long long row_bytes = cols * 2 * 8;  // one pair's output
+    double* stage[2] = {nullptr, nullptr};
+    if (cols > 0 && row_bytes <= static_cast<long long>(PinnedStage::kSlotBytes)) {
+        stage[0] = PinnedStage::get().slot(0), stage[1] = PinnedStage::get().slot(1);
+        if (!stage[0] || !stage[1]) stage[0] = stage[1] = nullptr;
+    }
     long long chunk = h.n_pairs;
     if (cols > 0) {
         chunk = std::min(chunk, std::max<long long>(1024, budget / row_bytes));
         if (row_bytes * h.n_pairs >= (32LL << 20)) chunk = std::min(chunk, (h.n_pairs + 3) / 4);
+        if (stage[0]) chunk = std::min(chunk, static_cast<long long>(PinnedStage::kSlotBytes) / row_bytes);
     }
     double* dbuf[2] = {arena.alloc<double>(std::max<long long>(1, cols * 2 * chunk)),
                        chunk < h.n_pairs ? arena.alloc<double>(std::max<long long>(1, cols * 2 * chunk)) : nullptr};
@@ -572,9 +581,39 @@ void run_paths(ob_paths_request& h) {
         }
     } done{evs};
     const long long n_chunks = (h.n_pairs + chunk - 1) / chunk;
-    std::vector<cudaEvent_t> k0(n_chunks), k1(n_chunks);
+    std::vector<cudaEvent_t> k0(n_chunks), k1(n_chunks), staged(n_chunks);
+    // with the staging: chunk c's columns into slot c % 2 on its stream (after its kernel) ...
+    auto stage_chunk = [&](long long c) {
+        const long long mcount = std::min(chunk, h.n_pairs - c * chunk);
+        check_cuda(cudaMemcpyAsync(stage[c % 2], dbuf[c % 2], static_cast<size_t>(cols * 2 * mcount) * sizeof(double),
+                                   cudaMemcpyDeviceToHost, sts[c % 2]),
+                   "cudaMemcpyAsync (columns)");
+        staged[c] = event();
+        check_cuda(cudaEventRecord(staged[c], sts[c % 2]), "cudaEventRecord");
+    };
+    // ... then spread by the host threads into the caller's array: column a of the chunk holds its rows of leg 0, then
+    // those of leg 1; each leg's run is cut into pieces of kPiece doubles, the pool's items
+    auto spread_chunk = [&](long long c) {
+        check_cuda(cudaEventSynchronize(staged[c]), "cudaEventSynchronize");
+        const long long c0 = c * chunk, mcount = std::min(chunk, h.n_pairs - c0);
+        constexpr long long kPiece = 1 << 16;
+        const long long pieces = (mcount + kPiece - 1) / kPiece;
+        const double* src = stage[c % 2];
+        double* out = h.out;
+        const long long P = h.n_pairs;
+        HostPool::get().run(static_cast<int>(cols * 2 * pieces), [&](int item) {
+            const long long col = item / (2 * pieces), leg = (item / pieces) % 2, q = item % pieces;
+            const long long r0 = q * kPiece, r1 = std::min(mcount, r0 + kPiece);
+            std::memcpy(out + col * 2 * P + leg * P + c0 + r0, src + col * 2 * mcount + leg * mcount + r0,
+                        static_cast<size_t>(r1 - r0) * sizeof(double));
+        });
+    };
     auto copy_back = [&](long long c) {
         if (cols <= 0) return;
+        if (stage[0]) {
+            spread_chunk(c);
+            return;
+        }
         const long long c0 = c * chunk, mcount = std::min(chunk, h.n_pairs - c0);
         const double* src = dbuf[c % 2];
         const size_t width = static_cast<size_t>(mcount) * sizeof(double);
@@ -611,7 +650,8 @@ void run_paths(ob_paths_request& h) {
         else paths_kernel<R, 8><<<grid, block, 0, st>>>(part);
         check_cuda(cudaGetLastError(), "paths_kernel launch");
         check_cuda(cudaEventRecord(k1[c], st), "cudaEventRecord");
-        if (c > 0) copy_back(c - 1);  // pageable: the host waits for it while chunk c runs on the other stream
+        if (cols > 0 && stage[0]) stage_chunk(c);
+        if (c > 0) copy_back(c - 1);  // the host waits for it while chunk c runs on the other stream
     }
     copy_back(n_chunks - 1);
     check_cuda(cudaStreamSynchronize(sts[0]), "paths");
