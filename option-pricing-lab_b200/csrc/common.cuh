@@ -5,7 +5,8 @@
 //     (RC/include/optlab_cuda/philox.hpp:22-44, RC/include/optlab_cuda/paths.hpp:207-233);
 //   u = (i + 1/2) 2^-32 (philox.hpp:45-49); Box-Muller r = sqrt(-2 ln u), (cos, sin)(2 pi v) by sincospi
 //     (philox.hpp:51-66).
-// The integer stream is bit-exact with the reference; the normals differ from its CPU's only by libm rounding.
+// The integer stream is bit-exact with the reference; in double the normals differ from its CPU's only by libm
+// rounding, in float by the hardware sine and cosine of the angle (below) as well.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -237,11 +238,16 @@ __device__ __forceinline__ double to_unit<double>(uint32_t i) {
     return static_cast<double>(i) * 2.3283064365386963e-10 + 1.1641532182693481e-10;
 }
 
+// Float: the radius with the precise logarithm (near u = 1 an approximate one's absolute error would be a large part
+// of the small radius); the angle 2 pi v taken as 2 pi (v - 1/2) + pi, inside [-pi, pi), where the hardware sine and
+// cosine keep an absolute error near 1e-6 (a normal moves by a few 1e-6 at most, |z| <= 6.7: inside the reference's
+// float-against-double criteria), the shift by pi flipping both signs. v - 1/2 rounds only where v < 1/4, by at most
+// 2^-26 of a turn.
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, float& z1) {
     const float r = sqrtf(-2.0f * logf(to_unit<float>(a)));
     float s, c;
-    sincospif(2.0f * to_unit<float>(b), &s, &c);
-    z0 = r * c, z1 = r * s;
+    __sincosf(6.28318530717958647692f * (to_unit<float>(b) - 0.5f), &s, &c);
+    z0 = -r * c, z1 = -r * s;
 }
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double& z0, double& z1) {
     const double r = sqrt(-2.0 * log(to_unit<double>(a)));
