@@ -338,7 +338,9 @@ __global__ void __launch_bounds__(512) lev_bin(LevDev d, const R* __restrict__ x
 }
 
 // Exclusive prefix of x over the block and the block's total (any block size that is a multiple of 32, up to 1024).
-__device__ unsigned long long block_scan(unsigned long long x, unsigned long long* s_warp, unsigned long long& total) {
+// Without `reuse` the caller guarantees a barrier before s_warp is written again, and the last one is left out.
+__device__ unsigned long long block_scan(unsigned long long x, unsigned long long* s_warp, unsigned long long& total,
+                                         bool reuse = true) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     unsigned long long inc = x;
 #pragma unroll
@@ -354,7 +356,7 @@ __device__ unsigned long long block_scan(unsigned long long x, unsigned long lon
         before += w < warp ? c : 0ull;
         tot += c;
     }
-    __syncthreads();
+    if (reuse) __syncthreads();
     total = tot;
     return before + inc - x;
 }
@@ -409,8 +411,9 @@ __device__ void regress_stage(const LevDev& d, int i, RegressShared& sh, double*
     }
 }
 
+// `more`: the block regresses another grid point after this one (its shared memory must be free again).
 __device__ void regress_phase(const LevDev& d, double n_particles, int g, int i, double lo, double hi,
-                              RegressShared& sh, unsigned* s_fine, double* s_row) {
+                              RegressShared& sh, unsigned* s_fine, double* s_row, bool more) {
     const int nx = d.n_x, nb = d.n_bins, nf = d.n_fine, t = threadIdx.x, nt = blockDim.x;
     const int lane = t & 31, warp = t >> 5, nw = nt >> 5;
     const double* row = d.lv_rows + static_cast<long long>(i) * d.n_lv;
@@ -451,7 +454,8 @@ __device__ void regress_phase(const LevDev& d, double n_particles, int g, int i,
         }
         if (t < 2) sh.best[t] = nt;
         unsigned long long total_u;
-        const unsigned long long before = block_scan(mine, sh.warp, total_u);  // (its barriers publish sh.best)
+        // (its barrier publishes sh.best; the next write of sh.warp is in the next regression, barriers later)
+        const unsigned long long before = block_scan(mine, sh.warp, total_u, false);
         // every particle is in one fine bin: a packed count that passed 2^16 - 1 shows here
         if (pk && t == 0 && total_u != static_cast<unsigned long long>(n_particles)) atomicCAS(d.status, 0, kPackOverflow);
         const double total = static_cast<double>(total_u);
@@ -545,7 +549,7 @@ __device__ void regress_phase(const LevDev& d, double n_particles, int g, int i,
         d.x_grids[static_cast<long long>(i) * nx + g] = x0;
         d.values[static_cast<long long>(i) * nx + g] = L;
     }
-    __syncthreads();  // the block's shared memory is free for its next grid point
+    if (more) __syncthreads();  // the block's shared memory is free for its next grid point
 }
 
 // Dynamic shared memory of lev_regress: the fine histogram, then the local-variance row when it is staged.
@@ -563,7 +567,7 @@ __global__ void __launch_bounds__(256) lev_regress(LevDev d, double n_particles)
     double lo = 0.0, hi = 0.0;
     if (i > 0) range_of(d, lo, hi, s_mn, s_mx);  // (its barriers also order the staging)
     else __syncthreads();
-    regress_phase(d, n_particles, blockIdx.x, i, lo, hi, sh, s_fine, s_row);
+    regress_phase(d, n_particles, blockIdx.x, i, lo, hi, sh, s_fine, s_row, false);
 }
 
 // The normals of this thread's pairs at step i (Philox counter (pair, i + 1, 0, 0)): z0 at p, z1 at n + p.
@@ -790,7 +794,8 @@ __global__ void __launch_bounds__(kPersistentThreads, 1)
             if (regresses) regress_stage(d, i, rs, s_row);  // (while thread 0 waits for the bulk reductions)
             if (!grid_wait(d, arrived)) return;
         }
-        for (int g = blockIdx.x; g < d.n_x; g += gridDim.x) regress_phase(d, n_particles, g, i, lo, hi, rs, b.fine, s_row);
+        for (int g = blockIdx.x; g < d.n_x; g += gridDim.x)
+            regress_phase(d, n_particles, g, i, lo, hi, rs, b.fine, s_row, g + static_cast<int>(gridDim.x) < d.n_x);
         grid_arrive(d, arrived);
         bin_clear_shared(d, b);
         if (i == 0 && s_z) step_normals(d, pt, 0, s_z);
