@@ -177,7 +177,9 @@ struct LvStep {
     int idx;  // index of the (y_i, dy_i) pair: row offset + i
 };
 
-template <typename R>
+// GLOBAL: tab is the table in global memory, read through the read-only data cache (never a staged copy in shared
+// memory).
+template <bool GLOBAL, typename R>
 __device__ __forceinline__ LvStep<R> lv_read(const AdjArgs<R>& a, const Pair2<R>* tab, const NameStep<R>& ns, R x) {
     LvStep<R> s;
     R u = table_u(ns, x);
@@ -186,7 +188,7 @@ __device__ __forceinline__ LvStep<R> lv_read(const AdjArgs<R>& a, const Pair2<R>
     const int j = static_cast<int>(u);
     s.w = u - static_cast<R>(j);
     s.idx = ns.row + j;
-    const Pair2<R> y = tab[s.idx];
+    const Pair2<R> y = GLOBAL ? ldg_pair(tab + s.idx) : tab[s.idx];
     s.var = y.a + s.w * y.b;
     s.dvdx = inside ? y.b * ns.inv_dx : R(0);
     return s;
@@ -267,16 +269,16 @@ __global__ void __launch_bounds__(ST ? 1024 : 256) adj_forward(AdjArgs<R> a) {
             for (int g = 0; g < G; ++g) {
                 const int i = i0 + g;
                 if (G > 1 && i > a.n_steps) break;
-                const StepRec<R> st = a.steps[i - 1];
+                const StepRec<R> st = ldg_rec(a.steps + i - 1);
                 R wv[2] = {R(1e30), R(1e30)};
                 int wn[2] = {0, 0};
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
-                    const NameStep<R> ns = a.ns[(i - 1) * N + n];
+                    const NameStep<R> ns = ldg_rec(a.ns + (i - 1) * N + n);
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
-                        const LvStep<R> s = lv_read(a, tab, ns, x[leg][n]);
+                        const LvStep<R> s = lv_read<!ST>(a, tab, ns, x[leg][n]);
                         x[leg][n] += s.var * st.hdt + (m_sqrt(s.var) * st.sdt) * z;
                         const R lp = x[leg][n] + ns.lf;
                         if (lp < wv[leg]) wv[leg] = lp, wn[leg] = n;
@@ -396,9 +398,9 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
         const long long p = base + lane;
         ++mine;
         const uint64_t pair = static_cast<uint64_t>(p);
-        const int kstep[2] = {a.ki_step[p], a.ki_step[P + p]};
-        const int kname[2] = {a.ki_name[p], a.ki_name[P + p]};
-        const R kd[2] = {a.dki[p], a.dki[P + p]};
+        const int kstep[2] = {__ldg(a.ki_step + p), __ldg(a.ki_step + P + p)};
+        const int kname[2] = {__ldg(a.ki_name + p), __ldg(a.ki_name + P + p)};
+        const R kd[2] = {__ldg(a.dki + p), __ldg(a.dki + P + p)};
         R xb[2][N];
 #pragma unroll
         for (int n = 0; n < N; ++n) xb[0][n] = xb[1][n] = R(0);
@@ -410,7 +412,8 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
             for (int n = 0; n < N; ++n)
 #pragma unroll
                 for (int leg = 0; leg < 2; ++leg)
-                    xs[0][leg][n] = s == 0 ? R(0) : a.ckpt[((static_cast<long long>(s - 1) * N + n) * 2 + leg) * P + p];
+                    xs[0][leg][n] =
+                        s == 0 ? R(0) : __ldg(a.ckpt + ((static_cast<long long>(s - 1) * N + n) * 2 + leg) * P + p);
             R zc[kCk][N];
 #pragma unroll
             for (int bb = 0; bb < kCk / G; ++bb) {
@@ -425,14 +428,14 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
 #pragma unroll
             for (int g = 0; g < kCk; ++g) {
                 if (g >= len) break;
-                const StepRec<R> st = a.steps[i_first + g - 1];
+                const StepRec<R> st = ldg_rec(a.steps + i_first + g - 1);
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
-                    const NameStep<R> ns = a.ns[(i_first + g - 1) * N + n];
+                    const NameStep<R> ns = ldg_rec(a.ns + (i_first + g - 1) * N + n);
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
-                        const LvStep<R> r = lv_read(a, tab, ns, xs[g][leg][n]);
+                        const LvStep<R> r = lv_read<true>(a, tab, ns, xs[g][leg][n]);
                         xs[g + 1][leg][n] = xs[g][leg][n] + r.var * st.hdt + (m_sqrt(r.var) * st.sdt) * z;
                     }
                 }
@@ -442,14 +445,14 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
             for (int g = kCk - 1; g >= 0; --g) {
                 if (g >= len) continue;
                 const int i = i_first + g;
-                const StepRec<R> st = a.steps[i - 1];
+                const StepRec<R> st = ldg_rec(a.steps + i - 1);
                 // the payoff's sensitivities at grid point i
                 if (st.obs >= 0) {
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const long long o = (static_cast<long long>(st.obs) * 2 + leg) * P + p;
-                        const R d = a.dobs[o];
-                        const int w = a.who[o];
+                        const R d = __ldg(a.dobs + o);
+                        const int w = __ldg(a.who + o);
 #pragma unroll
                         for (int n = 0; n < N; ++n)
                             if (w == n) xb[leg][n] += d;
@@ -464,11 +467,11 @@ __global__ void __launch_bounds__(256) adj_backward(AdjArgs<R> a) {
                     }
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
-                    const NameStep<R> ns = a.ns[(i - 1) * N + n];
+                    const NameStep<R> ns = ldg_rec(a.ns + (i - 1) * N + n);
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
                         const R z = leg ? -zc[g][n] : zc[g][n];
-                        const LvStep<R> r = lv_read(a, tab, ns, xs[g][leg][n]);
+                        const LvStep<R> r = lv_read<true>(a, tab, ns, xs[g][leg][n]);
                         const R sv = m_sqrt(r.var);
                         const R c = st.hdt + st.sdt * z / (R(2) * sv);  // d x_i / d var
                         const R vb = xb[leg][n] * c;
@@ -491,7 +494,7 @@ __device__ __forceinline__ void dense_segment(const AdjArgs<R>& a, long long p, 
         if (i > a.n_steps) break;
 #pragma unroll
         for (int n = 0; n < N; ++n)
-            xs[g][n] = i == 0 ? R(0) : a.ckpt[((static_cast<long long>(i - 1) * N + n) * 2 + leg) * P + p];
+            xs[g][n] = i == 0 ? R(0) : __ldg(a.ckpt + ((static_cast<long long>(i - 1) * N + n) * 2 + leg) * P + p);
     }
 }
 
@@ -512,9 +515,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1) adj_backward_dens
         const long long p = c * 32 + lane;
         if (p >= P) continue;  // no block-wide synchronisation below: inactive lanes may leave
         if (leg == 0) ++mine;
-        const int kstep = a.ki_step[leg * P + p];
-        const int kname = a.ki_name[leg * P + p];
-        const R kd = a.dki[leg * P + p];
+        const int kstep = __ldg(a.ki_step + leg * P + p);
+        const int kname = __ldg(a.ki_name + leg * P + p);
+        const R kd = __ldg(a.dki + leg * P + p);
         R xb[N];
 #pragma unroll
         for (int n = 0; n < N; ++n) xb[n] = R(0);
@@ -528,11 +531,11 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1) adj_backward_dens
             for (int g = kCk - 1; g >= 0; --g) {
                 if (g >= len) continue;
                 const int i = i_first + g;
-                const StepRec<R> st = a.steps[i - 1];
+                const StepRec<R> st = ldg_rec(a.steps + i - 1);
                 if (st.obs >= 0) {
                     const long long o = (static_cast<long long>(st.obs) * 2 + leg) * P + p;
-                    const R d = a.dobs[o];
-                    const int w = a.who[o];
+                    const R d = __ldg(a.dobs + o);
+                    const int w = __ldg(a.who + o);
 #pragma unroll
                     for (int n = 0; n < N; ++n)
                         if (w == n) xb[n] += d;
@@ -544,8 +547,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 1) adj_backward_dens
                 }
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
-                    const NameStep<R> ns = a.ns[(i - 1) * N + n];
-                    const LvStep<R> r = lv_read(a, tab, ns, cur[g][n]);
+                    const NameStep<R> ns = ldg_rec(a.ns + (i - 1) * N + n);
+                    const LvStep<R> r = lv_read<true>(a, tab, ns, cur[g][n]);
                     const R d = cur[g + 1][n] - cur[g][n] - r.var * st.hdt;  // sqrt(v dt) z
                     const R cc = st.hdt + d / (R(2) * r.var);               // d x_i / d var
                     const R vb = xb[n] * cc;

@@ -55,7 +55,7 @@ struct BDev {
     const BTrade<R>* trades;
     const Pair2<R>* tab;  // (1 + n_vol) x pool rows x (n_x - 1): (var_i, var_i+1 - var_i), base then each vol move
     long long tab_stride; // pool rows x (n_x - 1)
-    const R* row_org;     // the row's origin in table_u's form (name_step_org)
+    const R* row_org;     // the row's origin and 1 / dx in the cell form (cell_row)
     const R* row_inv_dx;
     const int* row_of;    // step -> expiry row
     const R* root;
@@ -281,13 +281,12 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
 #pragma unroll
                             for (int leg = 0; leg < 2; ++leg) {
                                 R& x = leg ? x1[n] : x0[n];
-                                R u = table_u(org, inv, x);
-                                u = m_min(m_max(u, R(0)), d.top);
-                                const int j = static_cast<int>(u);
-                                const R w = u - static_cast<R>(j);
+                                int j;
+                                R w;
+                                table_cell(org, inv, d.top, x, j, w);
                                 const Pair2<R> p = trow[j];
                                 const R var = p.a + w * p.b;
-                                x += m_fma(leg ? -m_sqrt(var) : m_sqrt(var), zd, var * d.hdt);
+                                x = lv_advance(x, var, d.hdt, leg ? -zd : zd);
                                 if (leg) lp1 = m_min(lp1, x + lf);
                                 else lp0 = m_min(lp0, x + lf);
                             }
@@ -566,10 +565,10 @@ void Batch::build(const ob_batch_request& rq) {
                 for (int k = 0; k + 1 < nx; ++k) out[k] = {static_cast<R>(v[k]), static_cast<R>(v[k + 1] - v[k])};
             }
         d.tab = arena.put<Pair2<R>>(tab.data(), tab.size());
-        std::vector<R> org(max_row);
-        for (int r = 0; r < max_row; ++r) org[r] = name_step_org<R>(rq.row_lo[r], rq.row_inv_dx[r]);
+        std::vector<R> org(max_row), inv(max_row);
+        for (int r = 0; r < max_row; ++r) cell_row(rq.row_lo[r], rq.row_inv_dx[r], d.top, org[r], inv[r]);
         d.row_org = arena.put<R>(org.data(), org.size());
-        d.row_inv_dx = arena.put<R>(rq.row_inv_dx, max_row);
+        d.row_inv_dx = arena.put<R>(inv.data(), inv.size());
         d.root = arena.put<R>(rq.root, max_root);
     }
     if (max_leg > 0) {

@@ -149,9 +149,10 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
         leg_init<R, PRODUCT>(l0), leg_init<R, PRODUCT>(l1);
         R lp0 = R(0), lp1 = R(0);
         // One batch of G steps from step i0, its normals drawn first. For one local-vol name the full batches run
-        // without testing for the last step and only the tail batch (CHECK) may stop inside.
-        auto run_batch = [&](int i0, int batch, auto check) {
-            constexpr bool CHECK = decltype(check)::value;
+        // without testing for the last step and only the tail batch (CHECK) may stop inside, and an autocall's batches
+        // without an observation run without testing each step for one (OBS false).
+        auto run_batch = [&](int i0, int batch, auto check, auto observe) {
+            constexpr bool CHECK = decltype(check)::value, OBS = decltype(observe)::value;
             R z[C * G];
             R za[CA > 0 ? CA * G : 1];
 #pragma unroll
@@ -239,10 +240,9 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
                         R var0, var1, vp0 = R(0), vp1 = R(0);
                         if (VAR) vp0 = m_max(v0[n], R(0)), vp1 = m_max(v1[n], R(0));
                         if (TABLE) {
-                            R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
-                            u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
-                            const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
-                            const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
+                            int j0, j1;
+                            R f0, f1;
+                            table_cell(ns, a.top, x0[n], j0, f0), table_cell(ns, a.top, x1[n], j1, f1);
                             const Pair2<R> y0 = GT ? ldg_pair(s_tab + ns.row + j0) : s_tab[ns.row + j0];
                             const Pair2<R> y1 = GT ? ldg_pair(s_tab + ns.row + j1) : s_tab[ns.row + j1];
                             const R t0 = y0.a + f0 * y0.b, t1 = y1.a + f1 * y1.b;
@@ -257,12 +257,12 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
                             v1[n] += h[1] * (h[2] - vp1) * st.dt + h[3] * (m_sqrt(vp1) * st.sdt) * (-zv);
                         }
                         if (MIX) {
-                            x0[n] += m_fma(m_sqrt(var0), st.sdt * zm0[n], var0 * st.hdt);
-                            x1[n] += m_fma(m_sqrt(var1), st.sdt * zm1[n], var1 * st.hdt);
+                            x0[n] = lv_advance(x0[n], var0, st.hdt, st.sdt * zm0[n]);
+                            x1[n] = lv_advance(x1[n], var1, st.hdt, st.sdt * zm1[n]);
                         } else {
                             const R zd = st.sdt * zc[n];  // sqrt(dt) z, the legs' +-
-                            x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
-                            x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
+                            x0[n] = lv_advance(x0[n], var0, st.hdt, zd);
+                            x1[n] = lv_advance(x1[n], var1, st.hdt, -zd);
                         }
                         if (n == 0) w0 = x0[n] + ns.lf, w1 = x1[n] + ns.lf;
                         else w0 = m_min(w0, x0[n] + ns.lf), w1 = m_min(w1, x1[n] + ns.lf);
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
                     l1.hi = m_max(l1.hi, lp1), l1.lo = m_min(l1.lo, lp1);
                 } else {
                     l0.lo = m_min(l0.lo, lp0), l1.lo = m_min(l1.lo, lp1);
-                    const int j = s_step[i - 1].obs;
+                    const int j = OBS ? s_step[i - 1].obs : -1;
                     if (j >= 0) {
                         leg_observe(a, s_trig, s_disc, l0, lp0, j);
                         leg_observe(a, s_trig, s_disc, l1, lp1, j);
@@ -283,12 +283,21 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
             }
         };
         if constexpr (N == 1 && KIND == 1) {  // (a second copy of the loop costs the wider kernels registers)
+            // a step without an observation holds minus the steps to the next one: none in steps i0 .. i0 + G - 1
+            // when step i0's entry is at most -G
+            constexpr bool kSplitObs = PRODUCT == OB_PRODUCT_AUTOCALL;
             const int n_full = S / G;
             int i0 = 1, batch = 0;
-            for (; batch < n_full; i0 += G, ++batch) run_batch(i0, batch, std::false_type{});
-            if (i0 <= S) run_batch(i0, batch, std::true_type{});
+            for (; batch < n_full; i0 += G, ++batch) {
+                if (!kSplitObs || s_step[i0 - 1].obs <= -G)
+                    run_batch(i0, batch, std::false_type{}, std::false_type{});
+                else
+                    run_batch(i0, batch, std::false_type{}, std::true_type{});
+            }
+            if (i0 <= S) run_batch(i0, batch, std::true_type{}, std::true_type{});
         } else {
-            for (int i0 = 1, batch = 0; i0 <= S; i0 += G, ++batch) run_batch(i0, batch, std::true_type{});
+            for (int i0 = 1, batch = 0; i0 <= S; i0 += G, ++batch)
+                run_batch(i0, batch, std::true_type{}, std::true_type{});
         }
         const int* leg_type = reinterpret_cast<const int*>(sm + a.off.leg_type);
         const R* leg_strike = reinterpret_cast<const R*>(sm + a.off.leg_strike);
@@ -495,8 +504,16 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
         steps[i].sdt = static_cast<R>(std::sqrt(rq.dt[i]));
         steps[i].obs = -1;
     }
-    if (rq.product == OB_PRODUCT_AUTOCALL)
+    if (rq.product == OB_PRODUCT_AUTOCALL) {
         for (int j = 0; j < rq.n_obs; ++j) steps[rq.obs_step[j] - 1].obs = j;
+        // steps without an observation: minus the number of steps to the next one (past the last, more than any
+        // batch)
+        int next = S + (1 << 20);
+        for (int i = S; i >= 1; --i) {
+            if (steps[i - 1].obs >= 0) next = i;
+            else steps[i - 1].obs = i - next;
+        }
+    }
     a.off.step = blob.put(steps);
     const bool table = kind == 1 || kind == 3;
     if (kind == 4) {
@@ -510,8 +527,7 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
                 r.lf = static_cast<R>(rq.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
                 if (table) {
                     const int row = rq.step_row[static_cast<size_t>(k) * S + (i - 1)];
-                    r.org = name_step_org<R>(rq.row_lo[row], rq.row_inv_dx[row]);
-                    r.inv_dx = static_cast<R>(rq.row_inv_dx[row]);
+                    set_cell_row(r, rq.row_lo[row], rq.row_inv_dx[row], a.top);
                     r.row = row * (rq.n_x - 1);
                 }
             }

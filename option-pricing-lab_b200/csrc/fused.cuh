@@ -15,8 +15,9 @@
 
 namespace ob {
 
-// org is the row's origin in the form its interpolation coordinate u = table_u(step, x) uses: -lo inv_dx in float
-// (u = x inv_dx + org, one multiply-add), lo in double (u = (x - lo) inv_dx, the reference's order).
+// org and inv_dx locate x in the step's row: in the cell form (set_cell_row, the fused, script and path kernels) or in
+// the form of u = table_u(step, x) (the adjoint): -lo inv_dx in float (u = x inv_dx + org, one multiply-add), lo in
+// double (u = (x - lo) inv_dx, the reference's order).
 template <typename R>
 struct alignas(16) NameStep;
 template <>
@@ -47,6 +48,50 @@ __device__ __forceinline__ R table_u(const NameStep<R>& s, R x) {
     return table_u(s.org, s.inv_dx, x);
 }
 
+// The cell form of a row, for the kernels that need only a coordinate's interval and weight (the fused, script and
+// path kernels; the adjoint keeps table_u's form for its derivative). In float the coordinate is stored divided by
+// top, so that its clamp to [0, top] is the saturation of its multiply-add: u / top = sat(x inv_dx / top - lo inv_dx
+// / top). In double the row keeps table_u's form.
+inline void cell_row(double lo, double inv_dx, float top, float& org, float& inv) {
+    org = static_cast<float>(-lo * inv_dx / top), inv = static_cast<float>(inv_dx / top);
+}
+inline void cell_row(double lo, double inv_dx, double, double& org, double& inv) { org = lo, inv = inv_dx; }
+template <typename R>
+inline void set_cell_row(NameStep<R>& r, double lo, double inv_dx, R top) {
+    cell_row(lo, inv_dx, top, r.org, r.inv_dx);
+}
+
+// The interval j = floor(u) and the weight f = u - j of x's coordinate u, clamped to [0, top], in a row of the cell
+// form. Float: s = sat(x inv_dx' + org') = u / top; s top + 2^23 rounded toward zero is a float in [2^23, 2^24)
+// whose low mantissa bits hold floor(u) exactly (u < 2^23), and f = s top - floor(u) in one more multiply-add (the
+// subtraction 2^23 - that float is exact). Four FMA-pipe instructions where the clamp, the conversion to an integer
+// and back and the subtraction take six, two of them on the MUFU pipe. Double: the clamp and the conversions.
+__device__ __forceinline__ void table_cell(float org, float inv, float top, float x, int& j, float& f) {
+    float s;
+    asm("fma.rn.ftz.sat.f32 %0, %1, %2, %3;" : "=f"(s) : "f"(x), "f"(inv), "f"(org));
+    const float big = __fmaf_rz(s, top, 8388608.0f);
+    j = __float_as_int(big) - 0x4B000000;
+    f = fmaf(s, top, 8388608.0f - big);
+}
+__device__ __forceinline__ void table_cell(double org, double inv, double top, double x, int& j, double& f) {
+    const double u = fmin(fmax(table_u(org, inv, x), 0.0), top);
+    j = static_cast<int>(u);
+    f = u - static_cast<double>(j);
+}
+template <typename R>
+__device__ __forceinline__ void table_cell(const NameStep<R>& r, R top, R x, int& j, R& f) {
+    table_cell(r.org, r.inv_dx, top, x, j, f);
+}
+
+// One leg's log-spot step, x + var (-dt / 2) + sqrt(var) (sqrt(dt) z): in float as two multiply-adds (the drift into
+// x, then the diffusion), in double in the reference's grouping (the two terms summed, then added to x).
+__device__ __forceinline__ float lv_advance(float x, float var, float hdt, float zd) {
+    return fmaf(sqrtf(var), zd, fmaf(var, hdt, x));
+}
+__device__ __forceinline__ double lv_advance(double x, double var, double hdt, double zd) {
+    return x + fma(sqrt(var), zd, var * hdt);
+}
+
 // One table interval: the value at its left point and the increment to the right one, so that an interpolation is
 // one multiply-add (y + w dy, the reference's y_i (1 - w) + y_i+1 w up to rounding).
 template <typename R>
@@ -65,7 +110,21 @@ __device__ __forceinline__ Pair2<double> ldg_pair(const Pair2<double>* p) {
     return {v.x, v.y};
 }
 
-// Per step: -dt / 2, sqrt(dt), dt, and the index of the observation taken at the step's end (-1: none).
+// A record of whole 16-byte words (StepRec, NameStep) read from global memory through the read-only data cache: the
+// compiler may then issue the load ahead of the kernel's stores and reductions, which a plain load could alias.
+template <typename T>
+__device__ __forceinline__ T ldg_rec(const T* p) {
+    static_assert(sizeof(T) % 16 == 0 && alignof(T) >= 16, "a record of whole 16-byte words");
+    T out;
+    const int4* src = reinterpret_cast<const int4*>(p);
+    int4* dst = reinterpret_cast<int4*>(&out);
+#pragma unroll
+    for (int k = 0; k < static_cast<int>(sizeof(T) / 16); ++k) dst[k] = __ldg(src + k);
+    return out;
+}
+
+// Per step: -dt / 2, sqrt(dt), dt, and the index of the observation taken at the step's end (negative: none; in an
+// autocall minus the number of steps to the next observation).
 template <typename R>
 struct alignas(16) StepRec {
     R hdt, sdt, dt;

@@ -274,10 +274,9 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
                     R var0, var1, vp0 = R(0), vp1 = R(0);
                     if (VAR) vp0 = m_max(v0[n], R(0)), vp1 = m_max(v1[n], R(0));
                     if (TABLE) {
-                        R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
-                        u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
-                        const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
-                        const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
+                        int j0, j1;
+                        R f0, f1;
+                        table_cell(ns, a.top, x0[n], j0, f0), table_cell(ns, a.top, x1[n], j1, f1);
                         const Pair2<R> y0 = GT ? ldg_pair(tab + ns.row + j0) : tab[ns.row + j0];
                         const Pair2<R> y1 = GT ? ldg_pair(tab + ns.row + j1) : tab[ns.row + j1];
                         const R t0 = y0.a + f0 * y0.b, t1 = y1.a + f1 * y1.b;
@@ -294,12 +293,12 @@ __global__ void __launch_bounds__(lv_block<N>(), N == 1 && sizeof(R) == 4 ? 2 : 
                         v1[n] += h[1] * (h[2] - vp1) * st.dt + h[3] * (m_sqrt(vp1) * st.sdt) * (-zv);
                     }
                     if (MIX) {
-                        x0[n] += m_fma(m_sqrt(var0), st.sdt * zm0[n], var0 * st.hdt);
-                        x1[n] += m_fma(m_sqrt(var1), st.sdt * zm1[n], var1 * st.hdt);
+                        x0[n] = lv_advance(x0[n], var0, st.hdt, st.sdt * zm0[n]);
+                        x1[n] = lv_advance(x1[n], var1, st.hdt, st.sdt * zm1[n]);
                     } else {
                         const R zd = st.sdt * zc;  // sqrt(dt) z, the legs' +-
-                        x0[n] += m_fma(m_sqrt(var0), zd, var0 * st.hdt);
-                        x1[n] += m_fma(-m_sqrt(var1), zd, var1 * st.hdt);
+                        x0[n] = lv_advance(x0[n], var0, st.hdt, zd);
+                        x1[n] = lv_advance(x1[n], var1, st.hdt, -zd);
                     }
                 }
                 const int2 ob = s_sched[i];
@@ -377,6 +376,7 @@ bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArg
         steps[i].dt = static_cast<R>(h.dt[i]), steps[i].obs = -1;
     }
     a.off.step = put(steps.data(), steps.size() * sizeof(StepRec<R>));
+    a.top = static_cast<R>(h.n_x - 1) - static_cast<R>(1e-4);
     std::vector<NameStep<R>> ns(static_cast<size_t>(S) * n);
     for (int i = 0; i < S; ++i)
         for (int k = 0; k < n; ++k) {
@@ -384,7 +384,7 @@ bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArg
             std::memset(&r, 0, sizeof r);
             if (!table) continue;
             const int row = h.step_row[static_cast<size_t>(k) * S + i];
-            r.org = name_step_org<R>(h.row_lo[row], h.row_inv_dx[row]), r.inv_dx = static_cast<R>(h.row_inv_dx[row]);
+            set_cell_row(r, h.row_lo[row], h.row_inv_dx[row], a.top);
             r.row = row * (h.n_x - 1);
         }
     a.off.name_step = put(ns.data(), ns.size() * sizeof(NameStep<R>));
@@ -441,7 +441,6 @@ bool pack_paths_staged(const ob_paths_request& h, DeviceArena& arena, PathsLvArg
         a.win_hi[w] = w < h.n_windows ? h.win_hi[w] : -1;
     }
     a.k0 = static_cast<uint32_t>(h.seed), a.k1 = static_cast<uint32_t>(h.seed >> 32);
-    a.top = static_cast<R>(h.n_x - 1) - static_cast<R>(1e-4);
     return true;
 }
 

@@ -559,10 +559,9 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     const NameStep<R> ns = s_ns[(i - 1) * N + n];
-                    R u0 = table_u(ns, x0[n]), u1 = table_u(ns, x1[n]);
-                    u0 = m_min(m_max(u0, R(0)), a.top), u1 = m_min(m_max(u1, R(0)), a.top);
-                    const int j0 = static_cast<int>(u0), j1 = static_cast<int>(u1);
-                    const R f0 = u0 - static_cast<R>(j0), f1 = u1 - static_cast<R>(j1);
+                    int j0, j1;
+                    R f0, f1;
+                    table_cell(ns, a.top, x0[n], j0, f0), table_cell(ns, a.top, x1[n], j1, f1);
                     const Pair2<R> p0 = GT ? ldg_pair(s_tab + ns.row + j0) : s_tab[ns.row + j0];
                     const Pair2<R> p1 = GT ? ldg_pair(s_tab + ns.row + j1) : s_tab[ns.row + j1];
                     const R v0 = p0.a + f0 * p0.b, v1 = p1.a + f1 * p1.b;
@@ -570,8 +569,8 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
                     // out: the same arithmetic in every instantiation, so a branch at step 0 is an ordinary run bit
                     // for bit
                     const R zd = st.sdt * zc[n], z0 = sg0 * zd, z1 = sg1 * zd;
-                    x0[n] += m_fma(m_sqrt(v0), z0, v0 * st.hdt);
-                    x1[n] += m_fma(m_sqrt(v1), z1, v1 * st.hdt);
+                    x0[n] = lv_advance(x0[n], v0, st.hdt, z0);
+                    x1[n] = lv_advance(x1[n], v1, st.hdt, z1);
                     y0[n] = x0[n] + ns.lf, y1[n] = x1[n] + ns.lf;
                 }
                 observe(i);
@@ -668,6 +667,7 @@ bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, Device
         steps[i].dt = static_cast<R>(q.dt[i]), steps[i].obs = -1;
     }
     a.off.step = put(steps.data(), steps.size() * sizeof(StepRec<R>));
+    a.top = static_cast<R>(q.n_x - 1) - static_cast<R>(1e-4);
     std::vector<NameStep<R>> ns(static_cast<size_t>(S) * n);
     for (int i = 1; i <= S; ++i)
         for (int k = 0; k < n; ++k) {
@@ -675,7 +675,7 @@ bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, Device
             std::memset(&r, 0, sizeof r);
             const int row = q.step_row[static_cast<size_t>(k) * S + (i - 1)];
             r.lf = static_cast<R>(q.log_fwd[static_cast<size_t>(k) * (S + 1) + i]);
-            r.org = name_step_org<R>(q.row_lo[row], q.row_inv_dx[row]), r.inv_dx = static_cast<R>(q.row_inv_dx[row]);
+            set_cell_row(r, q.row_lo[row], q.row_inv_dx[row], a.top);
             r.row = row * (q.n_x - 1);
         }
     a.off.name_step = put(ns.data(), ns.size() * sizeof(NameStep<R>));
@@ -701,7 +701,6 @@ bool pack_lv(const ob_script_request& rq, const std::vector<int2>& sched, Device
     unsigned char* dblob = arena.alloc<unsigned char>(std::max<size_t>(16, blob.size()));
     check_cuda(cudaMemcpy(dblob, blob.data(), blob.size(), cudaMemcpyHostToDevice), "copy blob");
     a.blob = dblob;
-    a.top = static_cast<R>(q.n_x - 1) - static_cast<R>(1e-4);
     return true;
 }
 
