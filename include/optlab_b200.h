@@ -381,9 +381,10 @@ int ob_cpu_threads(void);
 int ob_device_info(int device, ob_device* out);
 /* No counterpart in the reference (it allocates and frees per call). The one-shot calls (ob_price, ob_mc_price,
    ob_paths, ob_script_price, ob_leverage, ob_philox_normals) keep their device buffers for the next call, at most
-   512 MB over all devices, and ob_paths keeps 64 MB of pinned host memory through which it copies its columns; this
-   frees both. Call it before cudaDeviceReset or before destroying a context the library has used: cached buffers
-   belong to the context that allocated them. */
+   512 MB over all devices, and ob_paths keeps 64 MB of pinned host memory through which it copies its columns (the
+   result reads 16 KB more); this frees them and forgets the kernels' occupancy answers and shared-memory limits the
+   plans cached. Call it before cudaDeviceReset or before destroying a context the library has used: cached buffers
+   and attributes belong to the context that made them. */
 int ob_release_buffers(void);
 
 /* The engine's random numbers for RNG parity: for pairs first_pair .. first_pair + n_pairs - 1 of key seed, blocks

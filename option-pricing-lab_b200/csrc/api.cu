@@ -1,8 +1,11 @@
 // Status, device queries and the random-number surface of the C ABI (include/optlab_b200.h).
 // Reference counterparts: optlab::api::{gpu_count, has_cuda, cpu_threads, device_info}
 // (RC/include/optlab_cuda/requests.hpp:97-101, RC/src/requests.cpp:225-325).
+#include <algorithm>
 #include <cstdarg>
+#include <map>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -36,6 +39,87 @@ int require_device() {
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
     return sms;
+}
+
+namespace {
+struct OccKey {
+    const void* kernel;
+    int device, block;
+    size_t smem;
+    bool operator<(const OccKey& o) const {
+        return std::tie(kernel, device, block, smem) < std::tie(o.kernel, o.device, o.block, o.smem);
+    }
+};
+// What the launch caches hold: occupancy answers, and the shared-memory limit set on each kernel of each device.
+struct LaunchCaches {
+    std::mutex m;
+    std::map<OccKey, int> occ;
+    std::map<std::pair<const void*, int>, size_t> smem_set;
+    static LaunchCaches& get() {
+        static LaunchCaches* c = new LaunchCaches();
+        return *c;
+    }
+};
+}  // namespace
+
+int occupancy(const void* kernel, int block, size_t smem) {
+    LaunchCaches& c = LaunchCaches::get();
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    const OccKey key{kernel, dev, block, smem};
+    {
+        std::lock_guard<std::mutex> lock(c.m);
+        const auto it = c.occ.find(key);
+        if (it != c.occ.end()) return it->second;
+    }
+    int per_sm = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem), "occupancy");
+    std::lock_guard<std::mutex> lock(c.m);
+    c.occ[key] = per_sm;
+    return per_sm;
+}
+
+void allow_smem(const void* kernel, size_t smem) {
+    LaunchCaches& c = LaunchCaches::get();
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(c.m);
+    size_t& have = c.smem_set[{kernel, dev}];
+    if (have >= smem && have > 0) return;
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+               "cudaFuncSetAttribute");
+    have = smem;
+}
+
+void clear_launch_caches() {
+    LaunchCaches& c = LaunchCaches::get();
+    std::lock_guard<std::mutex> lock(c.m);
+    c.occ.clear(), c.smem_set.clear();
+}
+
+namespace {
+std::mutex g_pin_m;
+void* g_pin = nullptr;
+bool g_pin_tried = false;
+}  // namespace
+
+void* small_pinned() {
+    std::lock_guard<std::mutex> lock(g_pin_m);
+    if (!g_pin_tried) {
+        g_pin_tried = true;
+        if (cudaHostAlloc(&g_pin, kSmallPinnedBytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            g_pin = nullptr;
+        }
+    }
+    return g_pin;
+}
+
+void release_small_pinned() {
+    std::lock_guard<std::mutex> lock(g_pin_m);
+    if (g_pin) cudaFreeHost(g_pin);
+    cudaGetLastError();
+    g_pin = nullptr, g_pin_tried = false;
 }
 
 namespace {
@@ -83,6 +167,8 @@ int ob_release_buffers(void) {
     return ob::guarded([&] {
         ob::BufferCache::get().drain();
         ob::PinnedStage::get().release();
+        ob::clear_launch_caches();
+        ob::release_small_pinned();
     });
 }
 

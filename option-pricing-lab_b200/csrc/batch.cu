@@ -743,8 +743,7 @@ void Batch::run_all(cudaStream_t st) {
         BClass& c = classes[ci];
         check_cuda(cudaStreamWaitEvent(c.stream, fork, 0), "cudaStreamWaitEvent");
         check_cuda(cudaMemsetAsync(L.d_counter[ci], 0, sizeof(int), c.stream), "cudaMemsetAsync");
-        int per_sm = 0;
-        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, c.kernel, c.block, 0), "occupancy");
+        const int per_sm = occupancy(c.kernel, c.block, 0);
         const int grid = std::max(1, std::min(L.n_items[ci], sms * std::max(1, per_sm)));
         if (precision == OB_FP32)
             launch_class<float>(L, static_cast<int>(ci), c.stream, L.d_items[ci], L.n_items[ci], L.d_counter[ci], grid,
@@ -772,8 +771,7 @@ double Batch::time_class(int ci, int tile, int block, int max_sims) {
     cudaEvent_t a, b;
     check_cuda(cudaEventCreate(&a), "cudaEventCreate");
     check_cuda(cudaEventCreate(&b), "cudaEventCreate");
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, c.kernel, block, 0), "occupancy");
+    const int per_sm = occupancy(c.kernel, block, 0);
     const int grid = std::max(1, std::min(L.n_items[ci], sms * std::max(1, per_sm)));
     check_cuda(cudaMemsetAsync(L.d_counter[ci], 0, sizeof(int)), "cudaMemsetAsync");
     check_cuda(cudaEventRecord(a), "cudaEventRecord");

@@ -15,10 +15,12 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <functional>
 #include <mutex>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/optlab_b200.h"
 
@@ -60,6 +62,22 @@ int guarded(F&& f) {
 
 // Device 0 must exist; returns its SM count.
 int require_device();
+
+// Resident blocks an SM of kernel at block threads and smem bytes of dynamic shared memory on the current device (0:
+// it cannot launch so). Cached for the process: a query costs microseconds and a one-shot call builds a plan that
+// asks for each candidate block size.
+int occupancy(const void* kernel, int block, size_t smem);
+// Raises kernel's dynamic shared-memory limit on the current device to at least smem bytes (once per kernel and
+// size: the attribute is a maximum, so a larger setting serves smaller launches).
+void allow_smem(const void* kernel, size_t smem);
+// Forgets both (ob_release_buffers: after a device reset the kernels' attributes are gone).
+void clear_launch_caches();
+
+// A small pinned host buffer (kSmallPinnedBytes) for the read-back of results, allocated at its first use and kept;
+// null where pinned memory cannot be had. The library's calls are serialised, so one buffer serves them all.
+constexpr size_t kSmallPinnedBytes = 16384;
+void* small_pinned();
+void release_small_pinned();  // (ob_release_buffers)
 
 // ------------------------------------------------------------------------------------------------ device memory
 
@@ -208,6 +226,51 @@ struct DeviceArena {
         check_cuda(e2, "cudaStreamSynchronize (inputs)");
         return d;
     }
+};
+
+// A call's inputs gathered into one host buffer and copied to the device in one transfer by commit(): a call with
+// many small inputs pays one copy's driver work instead of one for each (a few microseconds apiece). add() converts
+// to T as DeviceArena::put does (null or empty gives a null pointer) and names the pointer that receives the device
+// address; the pointers hold their addresses once commit() has returned.
+class Upload {
+  public:
+    template <typename T, typename S, typename P>
+    void add(P*& field, const S* host, size_t count) {
+        static_assert(std::is_same_v<std::remove_const_t<P>, T>, "the field points to T");
+        if (!host || !count) {
+            field = nullptr;
+            return;
+        }
+        const size_t off = (bytes_.size() + 15) & ~static_cast<size_t>(15);
+        bytes_.resize(off + count * sizeof(T));
+        T* out = reinterpret_cast<T*>(bytes_.data() + off);
+        if constexpr (std::is_same_v<T, S>) std::memcpy(out, host, count * sizeof(T));
+        else
+            for (size_t i = 0; i < count; ++i) out[i] = static_cast<T>(host[i]);
+        fixes_.push_back({off, [&field](unsigned char* base) { field = reinterpret_cast<P*>(base); }});
+    }
+    // count zero-filled elements of T
+    template <typename T, typename P>
+    void zeros(P*& field, size_t count) {
+        static_assert(std::is_same_v<std::remove_const_t<P>, T>, "the field points to T");
+        const size_t off = (bytes_.size() + 15) & ~static_cast<size_t>(15);
+        bytes_.resize(off + count * sizeof(T), 0);
+        fixes_.push_back({off, [&field](unsigned char* base) { field = reinterpret_cast<P*>(base); }});
+    }
+    void commit(DeviceArena& arena) {
+        if (bytes_.empty()) return;
+        unsigned char* d = arena.alloc<unsigned char>(bytes_.size());
+        check_cuda(cudaMemcpy(d, bytes_.data(), bytes_.size(), cudaMemcpyHostToDevice), "cudaMemcpy (inputs)");
+        for (const Fix& f : fixes_) f.set(d + f.off);
+    }
+
+  private:
+    struct Fix {
+        size_t off;
+        std::function<void(unsigned char*)> set;
+    };
+    std::vector<unsigned char> bytes_;
+    std::vector<Fix> fixes_;
 };
 
 // ------------------------------------------------------------------------------------------------ normals

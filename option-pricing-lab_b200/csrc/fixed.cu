@@ -101,8 +101,7 @@ __global__ void fixed_finalize(const double* __restrict__ partial, int n_blocks,
 // Blocks of one launch over n_units pairs: enough for every pair, at most the resident blocks of the device.
 template <typename R>
 long long fixed_grid(long long n_units, int sms) {
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fixed_kernel<R>, 256, 0), "occupancy");
+    const int per_sm = occupancy(reinterpret_cast<const void*>(fixed_kernel<R>), 256, 0);
     return std::max<long long>(1, std::min<long long>((n_units + 255) / 256,
                                                       static_cast<long long>(sms) * std::max(1, per_sm)));
 }

@@ -602,10 +602,8 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
     check_cuda(cudaMemcpy(d, blob.bytes.data(), blob.bytes.size(), cudaMemcpyHostToDevice), "copy blob");
     a.blob = d;
     const void* k = reinterpret_cast<const void*>(fn);
-    check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-               "cudaFuncSetAttribute");
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, smem), "occupancy");
+    allow_smem(k, smem);
+    const int per_sm = occupancy(k, block, smem);
     if (per_sm < 1) return false;
     plan.fused = true;
     plan.threads_per_pair = kind == 4 ? 2 : 1;

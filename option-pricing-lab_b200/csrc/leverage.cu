@@ -832,12 +832,8 @@ bool run_persistent(LevDev& d, double n_particles, size_t bin_smem, int sms, cud
         z_off = align16(smem), smem = z_off + 2 * static_cast<size_t>(chunk) * sizeof(R);
     if (row_staged(d.n_lv) && align16(smem) + static_cast<size_t>(d.n_lv) * sizeof(double) <= kPersistentSmemMax)
         row_off = align16(smem), smem = row_off + static_cast<size_t>(d.n_lv) * sizeof(double);
-    check_cuda(cudaFuncSetAttribute(lev_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)),
-               "cudaFuncSetAttribute");
-    int occ = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, lev_persistent<R>, kPersistentThreads, smem),
-               "occupancy");
+    allow_smem(reinterpret_cast<const void*>(lev_persistent<R>), smem);
+    const int occ = occupancy(reinterpret_cast<const void*>(lev_persistent<R>), kPersistentThreads, smem);
     int coop = 0, dev = 0;
     check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
     check_cuda(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cudaDeviceGetAttribute");

@@ -223,13 +223,15 @@ __global__ void __launch_bounds__(256) mc_kernel(McArgs<R> a, long long n_pairs,
 
 // Adds the blocks' totals to the plan's running sums: one warp per sum, lane l adding blocks l, l + 32, ... and the
 // lanes combined by a fixed shuffle tree, so the order (and the result) depends only on the grid.
-__global__ void mc_finalize(const double* __restrict__ partial, int n_blocks, int n_acc, double* sums) {
+// The blocks' partial sums of one run into the plan's sums: added to them (add), or replacing them on the first run
+// after a result was read (so the sums need no clearing between calls).
+__global__ void mc_finalize(const double* __restrict__ partial, int n_blocks, int n_acc, double* sums, int add) {
     const int lane = threadIdx.x & 31;
     for (int t = threadIdx.x >> 5; t < n_acc; t += blockDim.x >> 5) {
         double s = 0.0;
         for (int b = lane; b < n_blocks; b += 32) s += partial[static_cast<long long>(b) * n_acc + t];
         s = warp_sum(s);
-        if (lane == 0) sums[t] += s;
+        if (lane == 0) sums[t] = add ? sums[t] + s : s;
     }
 }
 
@@ -415,11 +417,8 @@ void McPlan::build(const ob_mc_request& rq) {
     if (table && !a.table_in_smem) a.table_global = arena.put<R>(rq.table, static_cast<size_t>(rq.n_rows) * rq.n_x);
     smem_bytes = static_cast<size_t>(a.smem_blob) + acc_bytes;
     kernel = reinterpret_cast<const void*>(pick<R>(rq.model, rq.product, n));
-    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes)),
-               "cudaFuncSetAttribute");
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem_bytes), "occupancy");
-    blocks_per_sm = std::max(1, per_sm);
+    allow_smem(kernel, smem_bytes);
+    blocks_per_sm = std::max(1, occupancy(kernel, block, smem_bytes));
 }
 
 template void McPlan::build<float>(const ob_mc_request&);
@@ -435,8 +434,7 @@ void McPlan::create(const ob_mc_request& rq, int prec) {
     else build<double>(rq);
     max_blocks = sms * 64;
     d_partial = arena.alloc<double>(static_cast<size_t>(max_blocks) * 2 * n_out);
-    d_sums = arena.alloc<double>(2 * OB_MAX_OUT);
-    check_cuda(cudaMemset(d_sums, 0, 2 * OB_MAX_OUT * sizeof(double)), "cudaMemset");
+    d_sums = arena.alloc<double>(2 * OB_MAX_OUT);  // written by the first run's finalize
     check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
     check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
 }
@@ -454,9 +452,7 @@ int McPlan::occupancy_at(int blk) {
     if (blk == block) return blocks_per_sm;
     for (int k = 0; k < 16; ++k)
         if (occ_block[k] == blk) return occ_blocks[k];
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, blk, smem_bytes), "occupancy");
-    per_sm = std::max(1, per_sm);
+    const int per_sm = std::max(1, occupancy(kernel, blk, smem_bytes));
     for (int k = 0; k < 16; ++k)
         if (!occ_block[k]) {
             occ_block[k] = blk, occ_blocks[k] = per_sm;
@@ -511,7 +507,7 @@ void McPlan::run(long long n_pairs, long long first_pair, unsigned long long see
         reinterpret_cast<KernelFn<double>>(fn)<<<grid, blk, smem_bytes, st>>>(args_d, n_pairs, first_pair, k0, k1,
                                                                                d_partial);
     check_cuda(cudaGetLastError(), "mc_kernel launch");
-    mc_finalize<<<1, 1024, 0, st>>>(d_partial, grid, 2 * n_out, d_sums);
+    mc_finalize<<<1, 1024, 0, st>>>(d_partial, grid, 2 * n_out, d_sums, pairs_run > 0);
     check_cuda(cudaGetLastError(), "mc_finalize launch");
     check_cuda(cudaEventRecord(e1, st), "cudaEventRecord");
     pairs_run += n_pairs;
@@ -519,9 +515,16 @@ void McPlan::run(long long n_pairs, long long first_pair, unsigned long long see
 }
 
 void McPlan::result(ob_mc_result& res) {
-    check_cuda(cudaStreamSynchronize(last_stream), "mc_kernel");
-    double h[2 * OB_MAX_OUT];
-    check_cuda(cudaMemcpy(h, d_sums, sizeof h, cudaMemcpyDeviceToHost), "copy sums");
+    double h[2 * OB_MAX_OUT] = {};
+    if (pairs_run > 0) {  // (no run since the last result: empty sums)
+        // the sums through the small pinned buffer: an asynchronous copy on the runs' stream, then one wait
+        static_assert(sizeof h <= kSmallPinnedBytes, "the sums fit the pinned buffer");
+        double* pin = static_cast<double*>(small_pinned());
+        check_cuda(cudaMemcpyAsync(pin ? pin : h, d_sums, sizeof h, cudaMemcpyDeviceToHost, last_stream),
+                   "copy sums");
+        check_cuda(cudaStreamSynchronize(last_stream), "mc_kernel");
+        if (pin) std::memcpy(h, pin, sizeof h);
+    }
     float ms = 0.0f;
     if (timing) check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
     std::memset(&res, 0, sizeof res);
@@ -535,7 +538,6 @@ void McPlan::result(ob_mc_result& res) {
         res.sum_y[k] = h[k], res.sum_y2[k] = h[n_out + k];
     }
     res.kernel_ms = ms;
-    check_cuda(cudaMemset(d_sums, 0, 2 * OB_MAX_OUT * sizeof(double)), "cudaMemset");
     pairs_run = 0;
     timing = false;
 }

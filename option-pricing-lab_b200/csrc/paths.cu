@@ -505,26 +505,28 @@ void run_paths(ob_paths_request& h) {
     m.n_names = n, m.n_steps = h.n_steps, m.n_x = h.n_x, m.same = h.same, m.mixer = h.mixer;
     m.has_var = has_var, m.has_slv = has_slv;
     m.k0 = static_cast<uint32_t>(h.seed), m.k1 = static_cast<uint32_t>(h.seed >> 32);
-    m.dt = arena.put<R>(h.dt, h.n_steps);
-    m.t0 = arena.put<R>(h.t0, h.n_steps);
-    m.root = arena.put<R>(h.root, static_cast<size_t>(n) * n);
-    m.kind = arena.put<int>(h.kind, n);
-    m.cvar = arena.put<R>(h.cvar, n);
-    m.hes = arena.put<R>(h.heston, 5 * static_cast<size_t>(n));
+    Upload up;  // the inputs in one copy
+    up.add<R>(m.dt, h.dt, h.n_steps);
+    up.add<R>(m.t0, h.t0, h.n_steps);
+    up.add<R>(m.root, h.root, static_cast<size_t>(n) * n);
+    up.add<int>(m.kind, h.kind, n);
+    up.add<R>(m.cvar, h.cvar, n);
+    up.add<R>(m.hes, h.heston, 5 * static_cast<size_t>(n));
     if (table) {
-        m.step_row = arena.put<int>(h.step_row, static_cast<size_t>(n) * h.n_steps);
-        m.lo = arena.put<R>(h.row_lo, h.n_rows);
-        m.inv_dx = arena.put<R>(h.row_inv_dx, h.n_rows);
-        m.table = arena.put<R>(h.table, static_cast<size_t>(h.n_rows) * h.n_x);
+        up.add<int>(m.step_row, h.step_row, static_cast<size_t>(n) * h.n_steps);
+        up.add<R>(m.lo, h.row_lo, h.n_rows);
+        up.add<R>(m.inv_dx, h.row_inv_dx, h.n_rows);
+        up.add<R>(m.table, h.table, static_cast<size_t>(h.n_rows) * h.n_x);
     }
-    if (h.mixer) m.low_root = arena.put<R>(h.low_root, static_cast<size_t>(n) * n);
+    if (h.mixer) up.add<R>(m.low_root, h.low_root, static_cast<size_t>(n) * n);
     for (int k = 0; k < 8; ++k) m.mix[k] = static_cast<R>(h.mix[k]);
     s.n_obs = h.n_obs, s.n_cols = h.n_cols, s.n_keep = h.n_keep, s.n_win = h.n_windows;
-    s.obs_step = arena.put<int>(h.obs_step, h.n_obs);
-    s.col_of = arena.put<int>(h.col_of, h.n_obs);
-    s.win_lo = arena.put<int>(h.win_lo, h.n_windows);
-    s.win_hi = arena.put<int>(h.win_hi, h.n_windows);
-    s.fwd = arena.put<R>(h.fwd, static_cast<size_t>(n) * h.n_obs);
+    up.add<int>(s.obs_step, h.obs_step, h.n_obs);
+    up.add<int>(s.col_of, h.col_of, h.n_obs);
+    up.add<int>(s.win_lo, h.win_lo, h.n_windows);
+    up.add<int>(s.win_hi, h.win_hi, h.n_windows);
+    up.add<R>(s.fwd, h.fwd, static_cast<size_t>(n) * h.n_obs);
+    up.commit(arena);
     PathsLvArgs<R> lv{};
     const void* lv_fn = pack_paths_staged<R>(h, arena, lv)
                             ? pick_paths_staged<R>(n, lv.kind, lv.table_global != 0, h.mixer != 0)
@@ -532,12 +534,8 @@ void run_paths(ob_paths_request& h) {
     const bool fast = lv_fn != nullptr;
     int lv_grid = 0;
     if (fast) {
-        check_cuda(cudaFuncSetAttribute(lv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, lv.smem_blob),
-                   "cudaFuncSetAttribute");
-        int per_sm = 0;
-        check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lv_fn, lv_block_of(n), lv.smem_blob),
-                   "occupancy");
-        lv_grid = require_device() * std::max(1, per_sm);
+        allow_smem(lv_fn, lv.smem_blob);
+        lv_grid = require_device() * std::max(1, occupancy(lv_fn, lv_block_of(n), lv.smem_blob));
     }
 
     // Chunks of pairs, on two streams: the kernel of one chunk runs while the previous chunk's columns are copied to

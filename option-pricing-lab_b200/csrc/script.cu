@@ -456,7 +456,12 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
     script_lv_kernel(ScriptDev<R> d, LvArgs<R> a, long long n_pairs, uint32_t k0, uint32_t k1,
                      double* __restrict__ partial) {
     constexpr int C = N;
-    constexpr int G = C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4);
+    // One name, at most one window, no branch (the Phoenix and the barrier products): two Philox blocks a batch (8
+    // steps, their independent multiply chains interleave), the full batches without the last-step test and the
+    // batches without an event without its test, as in the fused kernel. Wider scripts keep one loop (its copies
+    // would spill their window states).
+    constexpr bool kLean = N == 1 && NW <= 1 && !BRANCH;
+    constexpr int G = kLean ? 8 : (C % 4 == 0 ? 1 : (C % 2 == 0 ? 2 : 4));
     constexpr int NB = C * G / 4;
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ double wacc[16][2];
@@ -500,9 +505,11 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
         R x0[N], x1[N], y0[N], y1[N];
 #pragma unroll
         for (int n = 0; n < N; ++n) x0[n] = x1[n] = R(0), y0[n] = y1[n] = s_lf0[n];
-        auto observe = [&](int i) {
+        // the step end i: its window fixings and (EV) its event; a batch whose steps hold no event runs with EV false
+        auto observe = [&](int i, auto events) {
+            constexpr bool EV = decltype(events)::value;
             const int2 sc = s_sched[i];
-            if (!sc.y && sc.x < 0) return;
+            if (!sc.y && (!EV || sc.x < 0)) return;
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
                 auto logp = [&](int nm) -> R {
@@ -514,7 +521,7 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
                     return v;
                 };
                 if (sc.y) fix_windows<WF>(d, meta, win[l], static_cast<unsigned>(sc.y), logp);
-                if (sc.x >= 0) {
+                if (EV && sc.x >= 0) {
                     R sp[N];
 #pragma unroll
                     for (int n = 0; n < N; ++n) sp[n] = d.spot0[n] * m_exp(l ? y1[n] : y0[n]);
@@ -523,8 +530,10 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
                 }
             }
         };
-        observe(0);
-        for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) {
+        observe(0, std::true_type{});
+        // One batch of G steps from step i0; only the tail batch (CHECK) may stop inside.
+        auto run_batch = [&](int i0, int b, auto check, auto events) {
+            constexpr bool CHECK = decltype(check)::value;
             R z[C * G];
             const bool own = !BRANCH || i0 + G - 1 > d.branch_step;  // a step of the batch draws its own normals
             if (own) {
@@ -543,7 +552,9 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
 #pragma unroll
             for (int g = 0; g < G; ++g) {
                 const int i = i0 + g;
-                if (G > 1 && i > S) break;
+                if constexpr (CHECK && G > 1) {
+                    if (i > S) break;
+                }
                 const StepRec<R> st = s_step[i - 1];
                 const bool before = BRANCH && i <= d.branch_step;
                 const R* zs = before ? &zo[g * C] : &z[g * C];
@@ -573,8 +584,21 @@ __global__ void __launch_bounds__(512, sizeof(R) == 4 ? 2 : 1)
                     x1[n] = lv_advance(x1[n], v1, st.hdt, z1);
                     y0[n] = x0[n] + ns.lf, y1[n] = x1[n] + ns.lf;
                 }
-                observe(i);
+                observe(i, events);
             }
+        };
+        // a step end without an event holds minus the steps to the next one: none in i0 .. i0 + G - 1 when step
+        // i0's entry is at most -G
+        if constexpr (kLean) {
+            const int n_full = S / G;
+            int i0 = 1, b = 0;
+            for (; b < n_full; i0 += G, ++b) {
+                if (s_sched[i0].x <= -G) run_batch(i0, b, std::false_type{}, std::false_type{});
+                else run_batch(i0, b, std::false_type{}, std::true_type{});
+            }
+            if (i0 <= S) run_batch(i0, b, std::true_type{}, std::true_type{});
+        } else {
+            for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) run_batch(i0, b, std::true_type{}, std::true_type{});
         }
         double y_pair = 0.0;
         if (active) {
@@ -847,12 +871,13 @@ void run_script(const ob_script_request& rq, ob_script_result& res, const Record
     ScriptDev<R> d{};
     d.model = mq.model, d.n_names = n, d.n_steps = S;
     for (int a = 0; a < n; ++a) d.spot0[a] = static_cast<R>(mq.spot[a]);
+    Upload up;
     ModelDev<R>& m = d.m;
     m.n_names = n, m.n_steps = S, m.n_x = mq.n_x, m.same = mq.same, m.mixer = mq.mixer;
-    m.dt = arena.put<R>(mq.dt, S);
-    m.t0 = arena.put<R>(mq.t0, S);
+    up.add<R>(m.dt, mq.dt, S);
+    up.add<R>(m.t0, mq.t0, S);
     if (mq.mixer) {  // local correlation: the generic interpreter kernel runs it (pack_lv declines)
-        m.low_root = arena.put<R>(mq.low_root, static_cast<size_t>(n) * n);
+        up.add<R>(m.low_root, mq.low_root, static_cast<size_t>(n) * n);
         for (int k = 0; k < 8; ++k) m.mix[k] = static_cast<R>(mq.mix[k]);
     }
     if (mq.model == OB_MODEL_PATHS) {
@@ -862,42 +887,42 @@ void run_script(const ob_script_request& rq, ob_script_result& res, const Record
             m.has_slv |= mq.kind[a] == 3;
             table |= mq.kind[a] == 1 || mq.kind[a] == 3;
         }
-        m.root = arena.put<R>(mq.root, static_cast<size_t>(n) * n);
-        m.kind = arena.put<int>(mq.kind, n);
-        m.cvar = arena.put<R>(mq.cvar, n);
-        m.hes = arena.put<R>(mq.heston, 5 * static_cast<size_t>(n));
+        up.add<R>(m.root, mq.root, static_cast<size_t>(n) * n);
+        up.add<int>(m.kind, mq.kind, n);
+        up.add<R>(m.cvar, mq.cvar, n);
+        up.add<R>(m.hes, mq.heston, 5 * static_cast<size_t>(n));
         if (table) {
-            m.step_row = arena.put<int>(mq.step_row, static_cast<size_t>(n) * S);
-            m.lo = arena.put<R>(mq.row_lo, mq.n_rows);
-            m.inv_dx = arena.put<R>(mq.row_inv_dx, mq.n_rows);
-            m.table = arena.put<R>(mq.table, static_cast<size_t>(mq.n_rows) * mq.n_x);
+            up.add<int>(m.step_row, mq.step_row, static_cast<size_t>(n) * S);
+            up.add<R>(m.lo, mq.row_lo, mq.n_rows);
+            up.add<R>(m.inv_dx, mq.row_inv_dx, mq.n_rows);
+            up.add<R>(m.table, mq.table, static_cast<size_t>(mq.n_rows) * mq.n_x);
         }
-        d.lf = arena.put<R>(mq.log_fwd, static_cast<size_t>(n) * (S + 1));
+        up.add<R>(d.lf, mq.log_fwd, static_cast<size_t>(n) * (S + 1));
     } else {
         d.qe = make_qe_consts<R>(mq.heston, mq.r, mq.q, mq.dt[0]);
     }
-    std::vector<int4> code(static_cast<size_t>(rq.n_code));
+    std::vector<int4> code(static_cast<size_t>(rq.n_code));  // (the caller's ints need not be 16-byte aligned)
     if (rq.n_code) std::memcpy(code.data(), rq.code, code.size() * sizeof(int4));
-    d.code = arena.put<int4>(code.data(), code.size());
-    d.consts = arena.put<double>(rq.consts, rq.n_const);
+    up.add<int4>(d.code, code.data(), code.size());
+    up.add<double>(d.consts, rq.consts, rq.n_const);
     d.n_const = rq.n_const, d.n_regs = rq.n_regs;
     std::vector<int> event_at(S + 1, -1);
     for (int k = 0; k < rq.n_events; ++k) event_at[rq.event_step[k]] = k;
-    d.event_at = arena.put<int>(event_at.data(), event_at.size());
-    d.event_code = arena.put<int>(rq.event_code, rq.n_events + 1);
-    d.event_disc = arena.put<double>(rq.event_discount, rq.n_events);
+    up.add<int>(d.event_at, event_at.data(), event_at.size());
+    up.add<int>(d.event_code, rq.event_code, rq.n_events + 1);
+    up.add<double>(d.event_disc, rq.event_discount, rq.n_events);
     std::vector<unsigned> fix_mask(S + 1, 0u);
     std::vector<int> nfix(std::max(1, rq.n_windows), 0);
     for (int w = 0; w < rq.n_windows; ++w) {
         for (int k = rq.win_fix0[w]; k < rq.win_fix0[w + 1]; ++k) fix_mask[rq.fix_step[k]] |= 1u << w;
         nfix[w] = rq.win_fix0[w + 1] - rq.win_fix0[w];
     }
-    d.fix_mask = arena.put<unsigned>(fix_mask.data(), fix_mask.size());
+    up.add<unsigned>(d.fix_mask, fix_mask.data(), fix_mask.size());
     d.n_windows = rq.n_windows;
     if (rq.n_windows) {
-        d.win_name = arena.put<int>(rq.win_name, rq.n_windows);
-        d.win_func = arena.put<int>(rq.win_func, rq.n_windows);
-        d.win_nfix = arena.put<int>(nfix.data(), rq.n_windows);
+        up.add<int>(d.win_name, rq.win_name, rq.n_windows);
+        up.add<int>(d.win_func, rq.win_func, rq.n_windows);
+        up.add<int>(d.win_nfix, nfix.data(), rq.n_windows);
         // the corridor as bounds on ln(S / spot0) of the window's name (NaN: no bound)
         std::vector<double> llo(rq.n_windows), lhi(rq.n_windows);
         for (int w = 0; w < rq.n_windows; ++w) {
@@ -907,17 +932,17 @@ void run_script(const ob_script_request& rq, ob_script_result& res, const Record
             };
             llo[w] = bound(rq.win_lower[w]), lhi[w] = bound(rq.win_upper[w]);
         }
-        d.win_lo = arena.put<double>(llo.data(), llo.size());
-        d.win_hi = arena.put<double>(lhi.data(), lhi.size());
+        up.add<double>(d.win_lo, llo.data(), llo.size());
+        up.add<double>(d.win_hi, lhi.data(), lhi.size());
         std::vector<double> ws0(rq.n_windows);
         for (int w = 0; w < rq.n_windows; ++w) ws0[w] = mq.spot[rq.win_name[w]];
-        d.win_spot0 = arena.put<R>(ws0.data(), ws0.size());
+        up.add<R>(d.win_spot0, ws0.data(), ws0.size());
     }
     d.n_events = rq.n_events, d.n_calls = rq.n_calls, d.n_state = rq.n_state, d.call_mode = rq.call_mode;
     d.rec_stride = 2 * rq.n_events + rq.n_calls * (3 + rq.n_state);
     if (rq.n_calls) {
-        d.call_state = arena.put<int>(rq.call_state, 4 * static_cast<size_t>(rq.n_calls));
-        if (rq.call_mode == 2) d.rules = arena.put<double>(rq.rules, static_cast<size_t>(rq.n_calls) * OB_RULE_STRIDE);
+        up.add<int>(d.call_state, rq.call_state, 4 * static_cast<size_t>(rq.n_calls));
+        if (rq.call_mode == 2) up.add<double>(d.rules, rq.rules, static_cast<size_t>(rq.n_calls) * OB_RULE_STRIDE);
     }
     const size_t rec_count = rq.call_mode == 1 ? static_cast<size_t>(2 * mq.n_pairs) * d.rec_stride : 0;
     if (rec_count) {
@@ -930,11 +955,20 @@ void run_script(const ob_script_request& rq, ob_script_result& res, const Record
     if (rq.pair_value) d.pair_value = arena.alloc<double>(static_cast<size_t>(mq.n_pairs));
     d.eps = static_cast<R>(rq.smoothing);
     d.red_tol = rq.smoothing == 0.0 ? 1e-12 : (sizeof(R) == 8 ? 1e-9 : 1e-5);
-    d.bad = arena.alloc<unsigned long long>(3);
-    check_cuda(cudaMemset(d.bad, 0, 3 * sizeof(unsigned long long)), "cudaMemset");
+    // the run's outputs read back by one copy: the three counts (zeroed here), then the two sums (slots 4, 5)
+    unsigned long long* outs = nullptr;
+    up.zeros<unsigned long long>(outs, 8);
+    // the inputs but the staged kernel's blob (pack_lv) in one copy
+    up.commit(arena);
+    d.bad = outs;
 
+    // per step end (event, window mask); a step end without an event holds minus the number of steps to the next
+    // one (past the last, more than any batch)
     std::vector<int2> sched(S + 1);
-    for (int i = 0; i <= S; ++i) sched[i] = make_int2(event_at[i], static_cast<int>(fix_mask[i]));
+    for (int i = S, next = S + (1 << 20); i >= 0; --i) {
+        if (event_at[i] >= 0) next = i;
+        sched[i] = make_int2(event_at[i] >= 0 ? event_at[i] : i - next, static_cast<int>(fix_mask[i]));
+    }
     LvArgs<R> lv{};
     const bool fast = pack_lv<R>(rq, sched, arena, lv);
     if (rq.branch && !fast) invalid("a branched run needs the staged local-vol kernel (its tables too large)");
@@ -944,15 +978,12 @@ void run_script(const ob_script_request& rq, ob_script_result& res, const Record
                           : reinterpret_cast<const void*>(pick_script<R>(mq.model, n, rq.n_windows));
     const int block = fast ? 512 : 128;
     const size_t smem = fast ? static_cast<size_t>(lv.smem_blob) : 0;
-    if (fast)
-        check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-                   "cudaFuncSetAttribute");
-    int per_sm = 0;
-    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem), "occupancy");
+    if (fast) allow_smem(fn, smem);
+    const int per_sm = occupancy(fn, block, smem);
     const long long need = (mq.n_pairs + block - 1) / block;
     const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(need, 1LL * sms * std::max(1, per_sm))));
     double* partial = arena.alloc<double>(2 * static_cast<size_t>(grid));
-    double* sums = arena.alloc<double>(2);
+    double* sums = reinterpret_cast<double*>(outs + 4);
     cudaEvent_t e0, e1;
     check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
     check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
@@ -966,10 +997,14 @@ void run_script(const ob_script_request& rq, ob_script_result& res, const Record
     script_finalize<<<1, 64>>>(partial, grid, sums);
     check_cuda(cudaGetLastError(), "script_finalize launch");
     check_cuda(cudaEventRecord(e1), "cudaEventRecord");
+    unsigned long long out[8];
+    void* pin = small_pinned();
+    check_cuda(cudaMemcpyAsync(pin ? pin : out, outs, sizeof out, cudaMemcpyDeviceToHost), "copy sums and counts");
+    check_cuda(cudaStreamSynchronize(nullptr), "script kernel");
+    if (pin) std::memcpy(out, pin, sizeof out);
     double h[2];
-    unsigned long long bad[3];
-    check_cuda(cudaMemcpy(h, sums, sizeof h, cudaMemcpyDeviceToHost), "copy sums");
-    check_cuda(cudaMemcpy(bad, d.bad, sizeof bad, cudaMemcpyDeviceToHost), "copy counts");
+    std::memcpy(h, out + 4, sizeof h);
+    const unsigned long long* bad = out;
     if (rec_count && rq.record)
         check_cuda(cudaMemcpy(rq.record, d.record, rec_count * sizeof(double), cudaMemcpyDeviceToHost), "copy record");
     if (rec_count && hook) (*hook)(d.record, 2 * mq.n_pairs, d.rec_stride, arena);

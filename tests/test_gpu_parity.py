@@ -267,3 +267,20 @@ def test_a_plan_runs_in_pieces_like_one_call():
         two = plan.result()
     assert two.n_paths == one.n_paths
     assert _rel(two.price[:4], one.price[:4]).max() < 1e-12
+
+
+def test_a_result_starts_the_next_accumulation():
+    """A plan's result reads the runs since the previous result: the first run after it replaces the sums (no
+    clearing between calls), later runs add to them, and a result with no run since is empty."""
+    h = workloads.lv_phoenix(n_paths=2**13, seed=4)
+    one = engine.mc_price(h, "fp64")
+    with engine.McPlan(h, "fp64") as plan:
+        plan.run(2**12, 0, seed=99)
+        plan.result()
+        plan.run(2**11, 0)
+        plan.run(2**11, 2**11)
+        again = plan.result()
+        empty = plan.result()
+    assert again.n_paths == one.n_paths
+    assert _rel(again.price[:4], one.price[:4]).max() < 1e-12  # nothing of the seed-99 run is left in the sums
+    assert empty.n_paths == 0 and all(v == 0.0 for v in empty.sum_y[:4])
