@@ -249,7 +249,9 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
             for (int n = 0; n < N; ++n) x0[n] = x1[n] = R(0);
             Rec<R, PRODUCT> r0, r1;
             rec_init(r0), rec_init(r1);
+            // the next observation and its step, in registers (the schedule is read again only at an observation)
             int next_obs = 0;
+            int obs_at = PRODUCT == OB_PRODUCT_AUTOCALL && t.n_obs > 0 ? d.obs_step[t.obs0] : -1;
             for (int i0 = 1, b = 0; i0 <= S; i0 += G, ++b) {
                 R z[C * G];
 #pragma unroll
@@ -293,8 +295,10 @@ __global__ void __launch_bounds__(256) batch_kernel(BDev<R> d, const int4* __res
                         }
                     }
                     int j = -1;
-                    if (PRODUCT == OB_PRODUCT_AUTOCALL && next_obs < t.n_obs && d.obs_step[t.obs0 + next_obs] == i)
+                    if (PRODUCT == OB_PRODUCT_AUTOCALL && obs_at == i) {
                         j = next_obs++;
+                        obs_at = next_obs < t.n_obs ? d.obs_step[t.obs0 + next_obs] : -1;
+                    }
                     rec_step(r0, lp0, j);
                     rec_step(r1, lp1, j);
                     if (nc) rec_carry(r0, lp0, static_cast<R>(i), d, nc), rec_carry(r1, lp1, static_cast<R>(i), d, nc);

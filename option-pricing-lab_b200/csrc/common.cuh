@@ -304,12 +304,14 @@ __device__ __forceinline__ double to_unit<double>(uint32_t i) {
 // Float: the radius with the precise logarithm (near u = 1 an approximate one's absolute error would be a large part
 // of the small radius); the angle 2 pi v taken as 2 pi (v - 1/2) + pi, inside [-pi, pi), where the hardware sine and
 // cosine keep an absolute error near 1e-6 (a normal moves by a few 1e-6 at most, |z| <= 6.7: inside the reference's
-// float-against-double criteria), the shift by pi flipping both signs. v - 1/2 rounds only where v < 1/4, by at most
-// 2^-26 of a turn.
+// float-against-double criteria), the shift by pi flipping both signs. The angle 2 pi (b + 1/2) 2^-32 - pi is one
+// multiply-add from b in float (b's conversion rounds as v's does, the sum once: within 3.9e-7 of the exact angle,
+// as 2 pi (v - 1/2) computed in steps is).
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& z0, float& z1) {
     const float r = sqrtf(-2.0f * logf(to_unit<float>(a)));
     float s, c;
-    __sincosf(6.28318530717958647692f * (to_unit<float>(b) - 0.5f), &s, &c);
+    // 2 pi 2^-32 and pi 2^-32 - pi, rounded to float
+    __sincosf(fmaf(static_cast<float>(b), 1.46291807926715968e-09f, -3.14159265285070240f), &s, &c);
     z0 = -r * c, z1 = -r * s;
 }
 __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double& z0, double& z1) {

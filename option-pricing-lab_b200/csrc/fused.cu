@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(512, min_blocks<R>())
             for (int g = 0; g < 4; ++g) {
                 const int i = i0 + g;
                 if (i > S) break;
-                qe_step(a.qe, x, v, sgn * e[0], sgn * e[1]);
+                qe_step_warp(a.qe, x, v, sgn * e[0], sgn * e[1]);  // (all 32 lanes step together)
                 e[0] = e[2], e[1] = e[3], e[2] = e[4], e[3] = e[5], e[4] = e[6], e[5] = e[7];
                 lp = x;
                 if (PRODUCT == OB_PRODUCT_LADDER) {

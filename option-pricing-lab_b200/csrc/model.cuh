@@ -203,19 +203,26 @@ inline QeConsts<R> make_qe_consts(const double* h, double r, double q, double dt
 //   division 3     quadratic: the K0 term -A b^2 a / (1 - 2 A a)    exponential: (1 - p) / (1 - A / beta)
 // with the exponential branch's K0 argument p + beta (1 - p) / (beta - A) written as p + (1 - p) / (1 - A / beta) and
 // its finiteness A < beta as A / beta < 1 (beta > 0). The algebra is the reference's; only roundings differ.
-template <typename R>
-__device__ __forceinline__ void qe_step(const QeConsts<R>& c, R& y, R& v, R zv, R zx) {
-    const R m = c.theta + (v - c.theta) * c.E;
-    const R m2 = m * m, s2 = v * c.c1 + c.c2;
-    const bool quad = s2 <= R(1.5) * m2;
+// EXP: 0 each lane takes its own branch (a lane of the exponential branch runs the tail's CDF and logarithm after the
+// step's divisions); 1 every lane evaluates the exponential tail, which each exponential lane keeps (straight-line
+// code: the CDF, which depends on zv alone, overlaps the divisions); 2 no lane is exponential.
+template <int EXP, typename R>
+__device__ __forceinline__ void qe_step_body(const QeConsts<R>& c, R& y, R& v, R zv, R zx, R m, R m2, R s2,
+                                             bool quad) {
+    R one_minus_u = R(1);
+    if (EXP == 1) one_minus_u = m_ncdf(-zv);  // 1 - U, exact in both tails
     const R r1 = (R(2) * m2) / (quad ? s2 : s2 + m2);  // quadratic: 2 / psi; exponential: q = 1 - p
     const R b2 = r1 - R(1) + m_sqrt(quad ? r1 * m_max(r1 - R(1), R(0)) : R(0));
     const R r2 = m / (quad ? R(1) + b2 : r1);  // quadratic: a; exponential: 1 / beta
     const R b = m_sqrt(quad ? b2 : R(0));
     R vn = r2 * (b + zv) * (b + zv);
-    if (!quad) {
-        const R one_minus_u = m_ncdf(-zv);  // 1 - U, exact in both tails
+    if (EXP == 0 && !quad) {
+        one_minus_u = m_ncdf(-zv);
         vn = one_minus_u >= r1 ? R(0) : m_log(r1 / one_minus_u) * r2;
+    }
+    if (EXP == 1) {
+        const R ve = one_minus_u >= r1 ? R(0) : m_log(r1 / one_minus_u) * r2;
+        vn = quad ? vn : ve;
     }
     const R arg_q = R(1) - R(2) * c.A * r2;
     const R den_e = R(1) - c.A * r2;
@@ -227,6 +234,25 @@ __device__ __forceinline__ void qe_step(const QeConsts<R>& c, R& y, R& v, R zv, 
     const R K0 = finite ? lin + w * m_log(arg) - (c.K1 + R(0.5) * c.K3) * v : c.K0p;
     y += c.mu_dt + K0 + c.K1 * v + c.K2 * vn + m_sqrt(m_max(c.K3 * v + c.K4 * vn, R(0))) * zx;
     v = vn;
+}
+
+template <typename R>
+__device__ __forceinline__ void qe_step(const QeConsts<R>& c, R& y, R& v, R zv, R zx) {
+    const R m = c.theta + (v - c.theta) * c.E;
+    const R m2 = m * m, s2 = v * c.c1 + c.c2;
+    qe_step_body<0>(c, y, v, zv, zx, m, m2, s2, s2 <= R(1.5) * m2);
+}
+
+// The same step for a warp whose 32 lanes all execute it together (none has left the loop): the warp votes. A warp
+// with an exponential lane runs the straight-line copy in which every lane evaluates the exponential tail; a warp
+// without one runs the quadratic step alone. The values are qe_step's bit for bit.
+template <typename R>
+__device__ __forceinline__ void qe_step_warp(const QeConsts<R>& c, R& y, R& v, R zv, R zx) {
+    const R m = c.theta + (v - c.theta) * c.E;
+    const R m2 = m * m, s2 = v * c.c1 + c.c2;
+    const bool quad = s2 <= R(1.5) * m2;
+    if (__any_sync(0xffffffffu, !quad)) qe_step_body<1>(c, y, v, zv, zx, m, m2, s2, quad);
+    else qe_step_body<2>(c, y, v, zv, zx, m, m2, s2, true);
 }
 
 }  // namespace ob
