@@ -44,11 +44,11 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0
 # Executed warp instructions per path-step of the dominant kernel, measured by ncu (smsp__inst_executed.sum of one
 # launch divided by its path-steps) and recorded under profiles/. The issue roofline below multiplies it by the live
 # path-step rate. A launch's instruction count does not depend on timing, so a profiled launch gives it exactly.
-INST_PER_PATH_STEP = {"lv_phoenix": 1.0662, "heston_qe": 20.30, "script": 1.532,
-                      # the 11 class kernels of one revaluation of the 32-trade book: 332.2 G over 2.49e11 path-steps
-                      "batch": 1.334,
+INST_PER_PATH_STEP = {"lv_phoenix": 1.0527, "heston_qe": 20.30, "script": 1.518,
+                      # the 11 class kernels of one revaluation of the 32-trade book: 326.2 G over 2.49e11 path-steps
+                      "batch": 1.310,
                       # the drop-in path engine's local-vol kernel on the Phoenix model (12 columns + a daily window)
-                      "paths": 2.366}
+                      "paths": 2.354}
 # The ALGORITHM's lane instructions per path-step of the local-vol Phoenix (one name, both legs of a pair share each
 # normal), counted from the algorithm, not from the compiled code, so that extra instructions lower the fraction:
 #   Philox4x32-10, one call per 4 normals = 4 pair-steps = 8 path-steps: 10 rounds x (2 wide multiplies, 2 three-way
