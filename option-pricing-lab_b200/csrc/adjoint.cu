@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(ST ? 1024 : 256) adj_forward(AdjArgs<R> a) {
     const Pair2<R>* tab = stage_table<R, ST>(a, dyn);
     __syncthreads();
     const long long P = a.n_pairs;
+    const R rtop = R(1) / a.top;  // (float rows scaled to the cell form)
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < P;
          base += stride) {
@@ -275,11 +276,24 @@ __global__ void __launch_bounds__(ST ? 1024 : 256) adj_forward(AdjArgs<R> a) {
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
                     const NameStep<R> ns = ldg_rec(a.ns + (i - 1) * N + n);
+                    // float: the fused kernel's step (the row in the cell form, scaled here once for both legs; the
+                    // log-spot step as two multiply-adds); double: the reference's grouping, as the backward reads it
+                    R org_c = ns.org, inv_c = ns.inv_dx;
+                    if constexpr (sizeof(R) == 4) org_c *= rtop, inv_c *= rtop;
+                    const R zd = st.sdt * zc[g][n];
 #pragma unroll
                     for (int leg = 0; leg < 2; ++leg) {
-                        const R z = leg ? -zc[g][n] : zc[g][n];
-                        const LvStep<R> s = lv_read<!ST>(a, tab, ns, x[leg][n]);
-                        x[leg][n] += s.var * st.hdt + (m_sqrt(s.var) * st.sdt) * z;
+                        if constexpr (sizeof(R) == 4) {
+                            int j;
+                            R f;
+                            table_cell(org_c, inv_c, a.top, x[leg][n], j, f);
+                            const Pair2<R> y = !ST ? ldg_pair(tab + ns.row + j) : tab[ns.row + j];
+                            x[leg][n] = lv_advance(x[leg][n], y.a + f * y.b, st.hdt, leg ? -zd : zd);
+                        } else {
+                            const R z = leg ? -zc[g][n] : zc[g][n];
+                            const LvStep<R> s = lv_read<!ST>(a, tab, ns, x[leg][n]);
+                            x[leg][n] += s.var * st.hdt + (m_sqrt(s.var) * st.sdt) * z;
+                        }
                         const R lp = x[leg][n] + ns.lf;
                         if (lp < wv[leg]) wv[leg] = lp, wn[leg] = n;
                     }
