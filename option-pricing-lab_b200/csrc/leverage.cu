@@ -113,7 +113,7 @@ __device__ __forceinline__ void add_u64_pair(unsigned* lo, unsigned* hi, unsigne
     if (up) atomicAdd(hi, up);
 }
 
-// Bulk reductions of shared memory into global memory by the TMA unit (cp.reduce.async.bulk, no multicast): one
+// Bulk reductions of shared memory into global memory by the TMA unit (cp.reduce.async.bulk, each CTA its own): one
 // thread hands over a whole array and the unit adds it element by element at L2. Both addresses must be 16-byte
 // aligned and the size a multiple of 16 bytes (bulk_aligned); the writes of the shared source must be fenced for the
 // async proxy before (fence_proxy_async_shared, by the threads that wrote it, then a barrier), and the issuing thread
