@@ -247,8 +247,10 @@ __global__ void __launch_bounds__(512, (fused_min_blocks<R, N, MIX>()))
                             const Pair2<R> y1 = GT ? ldg_pair(s_tab + ns.row + j1) : s_tab[ns.row + j1];
                             const R t0 = y0.a + f0 * y0.b, t1 = y1.a + f1 * y1.b;
                             var0 = KIND == 1 ? t0 : t0 * vp0, var1 = KIND == 1 ? t1 : t1 * vp1;
-                        } else {
+                        } else if (VAR) {
                             var0 = vp0, var1 = vp1;
+                        } else {
+                            var0 = var1 = s_hes[8 * n + 6];  // Black-Scholes: the name's constant variance
                         }
                         if (VAR) {
                             const R* h = s_hes + 8 * n;  // v0, kappa, theta, xi, rho, sqrt(1 - rho^2)
@@ -412,9 +414,9 @@ FusedFn<R> pick_n(int n) {
     if (n == 1) return fused_kernel<R, 1, KIND, PRODUCT, GT>;
     if (n == 2) return fused_kernel<R, 2, KIND, PRODUCT, GT>;
     if (n == 3) return fused_kernel<R, 3, KIND, PRODUCT, GT>;
-    if constexpr (KIND == 1) {
-        if (n == 4) return fused_kernel<R, 4, 1, PRODUCT, GT>;
-        if (n == 5) return fused_kernel<R, 5, 1, PRODUCT, GT>;
+    if constexpr (KIND == 1 || KIND == 0) {
+        if (n == 4) return fused_kernel<R, 4, KIND, PRODUCT, GT>;
+        if (n == 5) return fused_kernel<R, 5, KIND, PRODUCT, GT>;
     }
     return nullptr;
 }
@@ -435,6 +437,7 @@ FusedFn<R> pick_mix(int n) {
 template <typename R, int PRODUCT>
 FusedFn<R> pick_fused(int kind, int n, bool table_global) {
     switch (kind) {
+        case 0: return table_global ? nullptr : pick_n<R, 0, PRODUCT, false>(n);
         case 1: return table_global ? pick_n<R, 1, PRODUCT, true>(n) : pick_n<R, 1, PRODUCT, false>(n);
         case 2: return pick_n<R, 2, PRODUCT, false>(n);
         case 3: return table_global ? pick_n<R, 3, PRODUCT, true>(n) : pick_n<R, 3, PRODUCT, false>(n);
@@ -475,7 +478,6 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
         kind = rq.kind[0];
         for (int a = 1; a < n; ++a)
             if (rq.kind[a] != kind) return false;
-        if (kind == 0) return false;
     }
     if (rq.mixer && kind != 1) return false;  // the mixer beside other kinds: the generic kernel
     auto pick = [&](bool table_global) -> FusedFn<R> {
@@ -540,6 +542,7 @@ bool fused_build(McPlan& plan, const ob_mc_request& rq) {
             for (int f = 0; f < 5; ++f) hes[8 * k + f] = static_cast<R>(rq.heston[5 * k + f]);
             const R rho = hes[8 * k + 4];
             hes[8 * k + 5] = static_cast<R>(std::sqrt(R(1) - rho * rho));
+            hes[8 * k + 6] = static_cast<R>(rq.cvar[k]);  // Black-Scholes
         }
         a.off.hes = blob.put(hes);
         if (rq.mixer) {

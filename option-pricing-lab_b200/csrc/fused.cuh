@@ -1,5 +1,5 @@
-// The specialised fused kernel: every name of one kind (local vol, Heston by Euler, SLV, or one Heston name by QE),
-// N names known at compile time, everything a step reads staged in shared memory.
+// The specialised fused kernel: every name of one kind (Black-Scholes, local vol, Heston by Euler, SLV, or one Heston
+// name by QE), N names known at compile time, everything a step reads staged in shared memory.
 //
 // Per step and name one 16-byte record {lo, inv_dx, log-forward at the step end, table row} (32 bytes in double)
 // is read as a warp-wide broadcast; the local-variance table is stored as (y_i, y_i+1) pairs so that an

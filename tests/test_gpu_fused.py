@@ -39,7 +39,8 @@ def _request(kinds, product, n_pairs=2**12, seed=17, n_steps=126, years=0.5):
 CASES = [
     ([1], "autocall"), ([1], "ladder"), ([2], "ladder"), ([3], "autocall"), ([3], "ladder"), ([1, 1], "autocall"),
     ([1, 1, 1], "autocall"), ([1, 1, 1], "ladder"), ([1, 1, 1, 1, 1], "autocall"), ([2, 2, 2], "autocall"),
-    ([3, 3], "ladder"), ([1, 2], "autocall"), ([1] * 7, "ladder"),
+    ([3, 3], "ladder"), ([1, 2], "autocall"), ([1] * 7, "ladder"), ([0], "autocall"), ([0, 0, 0], "ladder"),
+    ([0] * 5, "autocall"),
 ]
 
 
