@@ -69,6 +69,30 @@ def test_fp32_fused_prices_are_within_4_se_of_the_fp64_oracle(oracle, kinds, pro
     assert np.all(np.abs(pg - po) <= 4 * so + 1e-12), (pg - po, so)
 
 
+@pytest.mark.parametrize("kind", [1, 0])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_observations_on_the_edges_of_step_batches_are_all_taken(oracle, kind, prec):
+    """Observation dates at the first step, either side of an eight-step batch's edge, on consecutive steps and at the
+    last step. The single-name kernel runs a batch whose first step's record says the next date is at least eight
+    steps away without testing each step for one; every one of these dates must still be observed."""
+    n_steps, years = 126, 0.5
+    kw = _request([kind], "autocall", n_pairs=2**13, n_steps=n_steps, years=years)
+    steps = np.array([1, 8, 9, 16, 17, 40, 41, 42, 64, 100, 125, 126], dtype=np.int32)
+    m = workloads.FlatMarket(100.0, 0.02, 0.01)
+    trig = np.full(len(steps), kw["trigger"][0])
+    trig[-1] = 0.0
+    kw.update(obs_step=steps, obs_discount=m.D(steps * (years / n_steps)), trigger=trig)
+    g = engine.mc_price(mc_request(**kw), prec)
+    o = oracle.mc_price(mc_request(**kw))
+    n = o.n_out
+    pg, po, so = np.array(g.price[:n]), np.array(o.price[:n]), np.array(o.se[:n])
+    if prec == "fp64":
+        nz = po != 0
+        assert np.abs(pg[nz] / po[nz] - 1).max() < 1e-10, (pg, po)
+    else:
+        assert np.all(np.abs(pg - po) <= 4 * so + 1e-12), (pg - po, so)
+
+
 @pytest.mark.parametrize("prec", ["fp32", "fp64"])
 def test_heston_qe_autocall_matches_the_oracle(oracle, prec):
     h = workloads.heston_qe_ladder(n_paths=2**13, seed=5)
