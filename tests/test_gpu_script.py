@@ -155,6 +155,50 @@ def test_a_phoenix_script_equals_the_fused_phoenix_kernel():
     assert len(grid) == s.n_steps + 1
 
 
+def _dated_phoenix_script(times, n_fix: int) -> str:
+    """The Phoenix of the fused kernel's defaults with its observations at the given times."""
+    ph = workloads.Phoenix()
+    lines = ["underlying X", "param S0 = 1", f"param cb = {ph.coupon_barrier!r}", f"param cpn = {ph.coupon!r}",
+             f"param call = {ph.trigger!r}", f"param ki = {ph.ki_barrier!r}", f"param K = {ph.put_strike!r}"]
+    for j, t in enumerate(times):
+        lines.append(f"event t={t!r} pay t={t!r}")
+        if j == 0:
+            lines.append("  missed = 0")
+        lines += ["  perf = X / S0", "  if perf >= cb then", "    pay cpn * (1 + missed) as coupon", "    missed = 0",
+                  "  else", "    missed = missed + 1", "  end"]
+        if j < len(times) - 1:
+            lines += ["  if perf >= call then", "    pay 1 as redemption", "    terminate", "  end"]
+        else:
+            lines += [f"  knocked = lowest(X, t=0, t={t!r}, n={n_fix}) < ki * S0", "  if knocked then",
+                      "    pay 1 - max(K - perf, 0) as redemption", "  else", "    pay 1 as redemption", "  end"]
+        lines.append("end")
+    return "\n".join(lines) + "\n"
+
+
+def test_events_on_the_edges_of_step_batches_price_as_the_fused_kernel():
+    """Observation dates at the first step, either side of an eight-step batch's edge, on consecutive steps and at the
+    last step: the script kernel runs a batch without an event without testing its steps for one, and so does the
+    fused kernel for observations; on the same request and normals their FP64 prices agree to rounding."""
+    n_steps, years = 126, 0.5
+    ph = workloads.Phoenix(years=years, obs_per_year=8)
+    m = workloads.FlatMarket(100.0, 0.02, 0.01)
+    g = workloads.lv_grid(horizon=years, n_exp=8, n_x=120)
+    dt, t0 = workloads.uniform_grid(years, n_steps)
+    t_end = np.concatenate([[0.0], t0 + dt])
+    steps = np.array([1, 8, 9, 16, 17, 40, 41, 42, 64, 100, 125, 126], dtype=np.int32)
+    fields = workloads.autocall_fields(ph, m, int(round(n_steps / years)))
+    trig = np.full(len(steps), ph.trigger)
+    trig[-1] = 0.0
+    fields.update(obs_step=steps, obs_discount=m.D(t_end[steps]), trigger=trig)
+    held = mc_request(model=OB_MODEL_PATHS, dt=dt, t0=t0, spot=[100.0], n_pairs=2**13, seed=29, root=[[1.0]],
+                      kind=[1], cvar=[0.04], heston=[[0.04, 1.5, 0.04, 0.5, -0.7]], log_fwd=m.log_fwd(t_end)[None, :],
+                      step_row=g.row_of(t0)[None, :], lo=g.lo, inv_dx=g.inv_dx, table=g.rows, n_x=g.n_x, **fields)
+    comp = sc.compile_script(_dated_phoenix_script([float(t) for t in t_end[steps]], n_steps), params={"S0": 100.0})
+    fused = engine.mc_price(held, "fp64")
+    res = sc.run(sc.script_request(comp, held, lambda t: np.exp(-0.02 * t)), "fp64")
+    assert abs(res.price - fused.price[0]) <= 1e-10 * abs(fused.price[0]), (res.price, fused.price[0])
+
+
 def test_a_heston_qe_phoenix_script_equals_the_fused_qe_kernel():
     ph = workloads.Phoenix(years=1.0, obs_per_year=4)
     base = workloads.heston_qe_ladder(n_paths=2**13, n_steps=252)
